@@ -1,0 +1,374 @@
+// Oracle harness around the reference's OWN level-set objects (test
+// infrastructure, never shipped).  It is compiled together with the
+// reference sources listed in oracle/Makefile.ref and the single-rank MPI
+// stub, and exposes a tiny C API that tests and fixture scripts call through
+// ctypes.  One grid per process: the reference keeps loop indices and WENO
+// coefficient tables in static members (src/increment.h:38,
+// src/weno_nug_func.h:198-202), so a second grid in the same process would
+// silently reuse the first grid's tables.
+//
+// Set-up mirrors the reference's start-up order
+//   src/driver.cpp:33-57   (lexer, ghostcell, lexer_read, vellast, gc_ini,
+//                           gcx_ini, gridini)
+//   src/driver.cpp:116-120 (flagini, flagfield, makegrid)
+//   src/driver_makegrid.cpp:29-62
+// except that the DIVEMesh grid file is replaced by assigning the same
+// lexer members read_grid() assigns (src/read_grid.cpp:29-911) for a closed
+// box whose six faces are walls (boundary group 21), and the control file
+// is replaced by assigning the few control flags the path reads.
+
+#include "lexer.h"
+#include "fdm.h"
+#include "ghostcell.h"
+#include "grid_helper.h"
+#include "levelset_RK3.h"
+#include "weno_hj_df_nug.h"
+#include "reini_RK3.h"
+#include "reinidisc_f.h"
+#include "reinidisc_fsf.h"
+#include "ioflow_void.h"
+#include "particle_pls_void.h"
+#include "heat.h"
+#include "concentration.h"
+#include "fluid_update_fsf.h"
+#include "patchBC_void.h"
+
+#include <cstring>
+#include <vector>
+
+namespace {
+
+lexer* P = nullptr;
+ghostcell* PGC = nullptr;
+fdm* A = nullptr;
+weno_hj_df_nug* CONV = nullptr;
+reini_RK3* REINI = nullptr;
+levelset_RK3* LS = nullptr;
+ioflow* FLOW = nullptr;
+particle_corr* PART = nullptr;
+reinidisc* DISC = nullptr;
+heat* HEAT = nullptr;
+concentration* CONC = nullptr;
+field4* TMP = nullptr;
+
+long ncells_padded() { return (long)P->imax * P->jmax * P->kmax; }
+
+field* field_by_id(int id) {
+    switch (id) {
+        case 0: return &A->phi;
+        case 1: return &A->u;
+        case 2: return &A->v;
+        case 3: return &A->w;
+        case 4: return &A->L;
+        case 5: return TMP;
+        case 6: return &A->ro;
+        default: return nullptr;
+    }
+}
+
+int ijk(int i, int j, int k) {
+    return (i - P->imin) * P->jmax * P->kmax + (j - P->jmin) * P->kmax + (k - P->kmin);
+}
+
+}  // namespace
+
+extern "C" {
+
+// xn/yn/zn: node coordinates for index -5 .. n+5 (n+11 values), the same
+// arrays DIVEMesh writes (src/read_grid.cpp:417-433, marge=5).
+// f49 selects reinidisc_f (1) or reinidisc_fsf (0); f44 the reinit
+// pseudo-steps per physical step; f43 the reinit time-step factor; f45 the
+// interface-thickness factor.
+int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,
+               int f44, double f43, double f45, int f49) {
+    if (P) return -1;
+    int argc = 0;
+    char** argv = nullptr;
+    P = new lexer;
+    PGC = new ghostcell(argc, argv, P);
+    lexer* p = P;
+
+    // control flags on this path (defaults src/ini.cpp:400-416)
+    p->F30 = 3; p->F35 = 5; p->F40 = 3;
+    p->F43 = f43; p->F44 = f44; p->F45 = f45; p->F46 = 0; p->F49 = f49; p->F50 = 2;
+    p->X45 = 0; p->X48 = 0; p->M10 = 1; p->P12 = 1000000000;
+
+    // --- what read_grid() assigns (src/read_grid.cpp:78-300)
+    p->knox = nx; p->knoy = ny; p->knoz = nz;
+    p->gknox = nx; p->gknoy = ny; p->gknoz = nz;
+    p->origin_i = p->origin_j = p->origin_k = 0;
+    p->dx = xn[5 + 1] - xn[5];
+    p->DXM = xn[5 + 1] - xn[5];
+    p->DYM = yn[5 + 1] - yn[5];
+    p->DZM = zn[5 + 1] - zn[5];
+    p->originx = p->global_xmin = xn[5];
+    p->originy = p->global_ymin = yn[5];
+    p->originz = p->global_zmin = zn[5];
+    p->endx = p->global_xmax = xn[5 + nx];
+    p->endy = p->global_ymax = yn[5 + ny];
+    p->endz = p->global_zmax = zn[5 + nz];
+    p->nb1 = p->nb2 = p->nb3 = p->nb4 = p->nb5 = p->nb6 = -2;
+    p->mx = p->my = p->mz = 1;
+    p->periodic1 = p->periodic2 = p->periodic3 = 0;
+    p->periodicX1 = p->periodicX2 = p->periodicX3 = 0;
+    p->periodicX4 = p->periodicX5 = p->periodicX6 = 0;
+    p->i_dir = 1; p->j_dir = (ny > 1) ? 1 : 0; p->k_dir = 1;
+    p->P150 = 0; p->solidread = 0; p->toporead = 0;
+    p->solid_gcb_est = p->topo_gcb_est = 0;
+    p->solid_gcbextra_est = p->topo_gcbextra_est = p->tot_gcbextra_est = 0;
+    p->global_orig_x = p->global_orig_y = p->alpha_grid = 0.0;
+    p->gcpara1_count = p->gcpara2_count = p->gcpara3_count = 0;
+    p->gcpara4_count = p->gcpara5_count = p->gcpara6_count = 0;
+    p->gcparaco1_count = p->gcparaco2_count = p->gcparaco3_count = 0;
+    p->gcparaco4_count = p->gcparaco5_count = p->gcparaco6_count = 0;
+    p->gcslpara1_count = p->gcslpara2_count = p->gcslpara3_count = p->gcslpara4_count = 0;
+    p->gcslparaco1_count = p->gcslparaco2_count = p->gcslparaco3_count = p->gcslparaco4_count = 0;
+    p->gcin_count = p->gcout_count = 0;
+    // never assigned by the reference (read by lexer::vecsize,
+    // src/lexer_vectorsize.cpp:37); zero, as in a fresh process heap
+    p->gcextra4 = 0;
+
+    // wall list: every interior cell on each face, one entry per face side
+    // (side codes of src/gc_neumann.cpp:29-54: 1 -x, 4 +x, 3 -y, 2 +y, 5 -z, 6 +z)
+    std::vector<int> wall;
+    auto add = [&](int i, int j, int k, int side) {
+        wall.push_back(i); wall.push_back(j); wall.push_back(k); wall.push_back(side);
+    };
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                if (i == 0) add(i, j, k, 1);
+                if (i == nx - 1) add(i, j, k, 4);
+                if (j == 0) add(i, j, k, 3);
+                if (j == ny - 1) add(i, j, k, 2);
+                if (k == 0) add(i, j, k, 5);
+                if (k == nz - 1) add(i, j, k, 6);
+            }
+    p->gcwall_count = (int)(wall.size() / 4);
+
+    p->topo_gcb_est *= 4;
+    p->gcb1_count = p->gcb2_count = p->gcb3_count = p->gcb4_count = p->gcb4a_count = p->gcb_fix =
+        p->gcb_solid = p->gcb_topo = p->gcb_fb = p->gcwall_count;
+    p->gcpara_sum = 0;
+    p->gcparaco_sum = 0;
+    p->assign_margin();
+
+    p->Iarray(p->flag4, p->imax * p->jmax * p->kmax);
+    p->Darray(p->flag_solid, p->imax * p->jmax * p->kmax);
+    p->Darray(p->flag_topo, p->imax * p->jmax * p->kmax);
+    p->Darray(p->solidbed, p->imax * p->jmax);
+    p->Darray(p->topobed, p->imax * p->jmax);
+    p->Darray(p->bed, p->imax * p->jmax);
+    p->Iarray(p->wet, p->imax * p->jmax);
+    p->Iarray(p->wet_n, p->imax * p->jmax);
+    p->Iarray(p->deep, p->imax * p->jmax);
+    p->Darray(p->depth, p->imax * p->jmax);
+    p->Darray(p->data, p->imax * p->jmax);
+    p->Iarray(p->flagslice1, p->imax * p->jmax);
+    p->Iarray(p->flagslice2, p->imax * p->jmax);
+    p->Iarray(p->flagslice4, p->imax * p->jmax);
+    for (long n = 0; n < (long)p->imax * p->jmax * p->kmax; ++n) p->flag4[n] = -1;
+    for (long n = 0; n < (long)p->imax * p->jmax; ++n) {
+        p->flagslice1[n] = -10; p->flagslice2[n] = -10; p->flagslice4[n] = -10;
+    }
+    p->Iarray(p->gcb1, p->gcb1_count, 6);
+    p->Iarray(p->gcb2, p->gcb2_count, 6);
+    p->Iarray(p->gcb3, p->gcb3_count, 6);
+    p->Iarray(p->gcb4, p->gcb4_count, 6);
+    p->Iarray(p->gcb4a, p->gcb4a_count, 6);
+    p->Darray(p->gcd1, p->gcb1_count);
+    p->Darray(p->gcd2, p->gcb2_count);
+    p->Darray(p->gcd3, p->gcb3_count);
+    p->Darray(p->gcd4, p->gcb4_count);
+    p->Darray(p->gcd4a, p->gcb4a_count);
+    p->Iarray(p->gcpara1, 0, 16); p->Iarray(p->gcpara2, 0, 16); p->Iarray(p->gcpara3, 0, 16);
+    p->Iarray(p->gcpara4, 0, 16); p->Iarray(p->gcpara5, 0, 16); p->Iarray(p->gcpara6, 0, 16);
+    p->Iarray(p->gcparaco1, 0, 3); p->Iarray(p->gcparaco2, 0, 3); p->Iarray(p->gcparaco3, 0, 3);
+    p->Iarray(p->gcparaco4, 0, 3); p->Iarray(p->gcparaco5, 0, 3); p->Iarray(p->gcparaco6, 0, 3);
+    p->gcbsl1_count = p->gcbsl2_count = p->gcbsl3_count = p->gcbsl4_count = p->gcbsl4a_count = 1;
+    p->Iarray(p->gcbsl1, 1, 6); p->Iarray(p->gcbsl2, 1, 6); p->Iarray(p->gcbsl3, 1, 6);
+    p->Iarray(p->gcbsl4, 1, 6); p->Iarray(p->gcbsl4a, 1, 6);
+    p->Iarray(p->gcslin, 0, 6); p->Iarray(p->gcslout, 0, 6);
+    p->Iarray(p->gcslpara1, 0, 2); p->Iarray(p->gcslpara2, 0, 2);
+    p->Iarray(p->gcslpara3, 0, 2); p->Iarray(p->gcslpara4, 0, 2);
+    p->Iarray(p->gcslparaco1, 0, 4); p->Iarray(p->gcslparaco2, 0, 4);
+    p->Iarray(p->gcslparaco3, 0, 4); p->Iarray(p->gcslparaco4, 0, 4);
+    p->Darray(p->XN, nx + 1 + 4 * p->marge);
+    p->Darray(p->YN, ny + 1 + 4 * p->marge);
+    p->Darray(p->ZN, nz + 1 + 4 * p->marge);
+
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) p->flag4[ijk(i, j, k)] = WATER_FLAG;
+    for (int n = 0; n < nx + 1 + 2 * p->marge; ++n) p->XN[n] = xn[n];
+    for (int n = 0; n < ny + 1 + 2 * p->marge; ++n) p->YN[n] = yn[n];
+    for (int n = 0; n < nz + 1 + 2 * p->marge; ++n) p->ZN[n] = zn[n];
+    for (int q = 0; q < p->gcb4_count; ++q) {
+        p->gcb4[q][0] = wall[4 * q + 0];
+        p->gcb4[q][1] = wall[4 * q + 1];
+        p->gcb4[q][2] = wall[4 * q + 2];
+        p->gcb4[q][3] = wall[4 * q + 3];
+        p->gcb4[q][4] = 21;
+    }
+    p->Iarray(p->gcin, 0, 6); p->Iarray(p->gcout, 0, 6);
+    p->Iarray(p->gcin4a, 0, 6); p->Iarray(p->gcout4a, 0, 6);
+    p->gcin4a_count = 0; p->gcout4a_count = 0;
+
+    // --- driver start-up (src/driver.cpp:51-57, 116-120)
+    p->lexer_ini();
+    p->vellast();
+    PGC->gc_ini(p);
+    PGC->gcx_ini(p);
+    p->gridini(PGC);
+    p->flagini();
+    PGC->flagfield(p);
+    {   // body of driver::makegrid (src/driver_makegrid.cpp:29-62)
+        PGC->flagx(p, p->flagsf1); PGC->flagx(p, p->flagsf2);
+        PGC->flagx(p, p->flagsf3); PGC->flagx(p, p->flagsf4);
+        PGC->flagx(p, p->flag1); PGC->flagx(p, p->flag2); PGC->flagx(p, p->flag3);
+        PGC->flagx(p, p->flag4); PGC->flagx(p, p->flag);
+        PGC->gcxupdate(p);
+        p->vecsize(PGC);
+        grid_helper gridgen(p);
+        gridgen.fillgcb1(p);
+        gridgen.fillgcb2(p);
+        gridgen.fillgcb3(p);
+        gridgen.fillgcb4a(p);
+        gridgen.fillgcb4_wall(p);
+        gridgen.make_dgc(p);
+        gridgen.fill_dgc1(p);
+        gridgen.fill_dgc2(p);
+        gridgen.fill_dgc3(p);
+        gridgen.fill_dgc4(p);
+    }
+
+    A = new fdm(p);
+    PGC->fdm_update(A);
+    // porosity is 1 everywhere without VRANS structures
+    for (long n = 0; n < ncells_padded(); ++n) A->porosity.V[n] = 1.0;
+
+    // psi (src/ini_psi.cpp:33-37)
+    if (p->j_dir == 0) p->psi = p->F45 * (1.0 / 2.0) * (p->DXM + p->DZM);
+    if (p->j_dir == 1) p->psi = p->F45 * (1.0 / 3.0) * (p->DXM + p->DYM + p->DZM);
+
+    CONV = new weno_hj_df_nug(p);
+    // no patch boundaries: driver::patchBC_logic picks patchBC_void
+    // (src/driver_logic_cfd.cpp:661-672)
+    FLOW = new ioflow_v(p, PGC, new patchBC_void(p));
+    PART = new particle_pls_void();
+    REINI = new reini_RK3(p, 0);
+    LS = new levelset_RK3(p, A, PGC, HEAT, CONC);
+    if (f49 == 1) DISC = new reinidisc_f(p);
+    else DISC = new reinidisc_fsf(p);
+    TMP = new field4(p);
+    p->count = 1;
+    p->dt = 0.0;
+    return 0;
+}
+
+long refls_padded_size() { return P ? ncells_padded() : -1; }
+int refls_dims(int* out) {
+    if (!P) return -1;
+    out[0] = P->imax; out[1] = P->jmax; out[2] = P->kmax; out[3] = P->j_dir;
+    return 0;
+}
+
+int refls_set_field(int id, const double* src) {
+    field* f = field_by_id(id);
+    if (!f) return -1;
+    std::memcpy(f->V, src, sizeof(double) * ncells_padded());
+    return 0;
+}
+
+int refls_get_field(int id, double* dst) {
+    field* f = field_by_id(id);
+    if (!f) return -1;
+    std::memcpy(dst, f->V, sizeof(double) * ncells_padded());
+    return 0;
+}
+
+void refls_set_dt(double dt) { P->dt = dt; }
+void refls_set_count(int c) { P->count = c; }
+double refls_psi() { return P->psi; }
+double refls_dxm() { return P->DXM; }
+double refls_volume1() { return P->volume1; }
+double refls_volume2() { return P->volume2; }
+
+// Metric arrays as the reference derives them from the node coordinates
+// (src/grid.cpp:55-100): which 0..8 = DXN,DYN,DZN,DXP,DYP,DZP,XP,YP,ZP.
+int refls_get_metric(int which, double* dst, int n) {
+    double* src[9] = {P->DXN, P->DYN, P->DZN, P->DXP, P->DYP, P->DZP, P->XP, P->YP, P->ZP};
+    if (which < 0 || which > 8) return -1;
+    std::memcpy(dst, src[which], sizeof(double) * n);
+    return 0;
+}
+
+// WENO coefficient tables for axis 0..2 (uf=0 node tables): qf [n][6][2],
+// cf [n][6], isf [n][6][3], for index IP = -1+5 .. knox+5 (as built by
+// src/weno_nug_func_precalc_*.cpp).  n entries starting at table index 0.
+int refls_get_weno_tables(int axis, double* qf, double* cf, double* isf, int n) {
+    double**** q = axis == 0 ? weno_nug_func::qfx : axis == 1 ? weno_nug_func::qfy : weno_nug_func::qfz;
+    double*** c = axis == 0 ? weno_nug_func::cfx : axis == 1 ? weno_nug_func::cfy : weno_nug_func::cfz;
+    double**** s = axis == 0 ? weno_nug_func::isfx : axis == 1 ? weno_nug_func::isfy : weno_nug_func::isfz;
+    for (int t = 0; t < n; ++t)
+        for (int r = 0; r < 6; ++r) {
+            qf[(t * 6 + r) * 2 + 0] = q[t][0][r][0];
+            qf[(t * 6 + r) * 2 + 1] = q[t][0][r][1];
+            cf[t * 6 + r] = c[t][0][r];
+            for (int m = 0; m < 3; ++m) isf[(t * 6 + r) * 3 + m] = s[t][0][r][m];
+        }
+    return 0;
+}
+
+// L = convection operator of src/weno_hj_df_nug.cpp:58-91 (ipol=4) applied to
+// field `src` with the stored velocities; the caller's L is zeroed first as
+// src/levelset_RK3.cpp:115-116 does.
+int refls_weno_L(const double* src, double* L) {
+    std::memcpy(TMP->V, src, sizeof(double) * ncells_padded());
+    for (long n = 0; n < ncells_padded(); ++n) A->L.V[n] = 0.0;
+    CONV->start(P, A, *TMP, 4, A->u, A->v, A->w);
+    std::memcpy(L, A->L.V, sizeof(double) * ncells_padded());
+    return 0;
+}
+
+// L = reinitialisation operator (src/reinidisc_f.cpp:37-127 or
+// src/reinidisc_fsf.cpp:37-141) applied to `src`.
+int refls_reinidisc_L(const double* src, double* L) {
+    std::memcpy(TMP->V, src, sizeof(double) * ncells_padded());
+    for (long n = 0; n < ncells_padded(); ++n) A->L.V[n] = 0.0;
+    DISC->start(P, A, PGC, *TMP, A->L, 4);
+    std::memcpy(L, A->L.V, sizeof(double) * ncells_padded());
+    return 0;
+}
+
+// Ghost fill of a level-set field: ghostcell::start4 with gcv 52
+// (src/gc_start.cpp:146-185).
+int refls_ghost_fill(double* f) {
+    std::memcpy(TMP->V, f, sizeof(double) * ncells_padded());
+    PGC->start4(P, *TMP, 52);
+    std::memcpy(f, TMP->V, sizeof(double) * ncells_padded());
+    return 0;
+}
+
+// F44 reinitialisation pseudo-steps on phi (src/reini_RK3.cpp:84-143).
+int refls_reini() {
+    REINI->start(A, P, A->phi, PGC, FLOW);
+    return 0;
+}
+
+// One physical level-set step on phi with the current dt and velocities
+// (src/levelset_RK3.cpp:103-172), including reinitialisation and the
+// density/volume update.
+int refls_step() {
+    convection* pc = CONV;
+    LS->start(A, P, pc, nullptr, PGC, FLOW, REINI, PART, A->phi);
+    return 0;
+}
+
+// Density/volume update only (src/fluid_update_fsf.cpp:39-104).
+int refls_update() {
+    LS->update(P, A, PGC, A->phi);
+    return 0;
+}
+
+}  // extern "C"
