@@ -1,0 +1,250 @@
+"""ctypes bindings for the two CPU oracles (test infrastructure only).
+
+* ``PortOracle`` wraps ``oracle/liboracle.so``: the project's C restatement of
+  the reference's level-set path (``oracle/ls_oracle.c``).  Re-entrant.
+* ``RefOracle`` wraps ``oracle/_ref/libreef3d_ref.so``: the reference's own
+  sources compiled with ``oracle/Makefile.ref`` and driven through
+  ``oracle/ref_harness.cpp``.  One grid per process (the reference keeps loop
+  indices and WENO tables in static members), so callers run it in a fresh
+  process per grid.
+
+Both work on the reference's padded field layout (margin 3 on every side, k
+contiguous): arrays of shape ``(nx+6, ny+6, nz+6)`` in C order.
+Only tests, the smoke check and the CPU-baseline leg of the benchmark use
+this module.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libreef3d_ref.so")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.c_int
+
+
+def _dp(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def padded_shape(nx, ny, nz):
+    return (nx + 6, ny + 6, nz + 6)
+
+
+def uniform_nodes(n, length=1.0, origin=0.0):
+    """Node coordinates for indices -5..n+5 of a uniform axis (n+11 values),
+    x_i = origin + i*(length/n)."""
+    h = length / n
+    return np.array([origin + i * h for i in range(-5, n + 6)], dtype=np.float64)
+
+
+class PortOracle:
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = ctypes.CDLL(PORT_LIB)
+            lib.lso_new.restype = ctypes.c_void_p
+            lib.lso_new.argtypes = [_I, _I, _I, _D, _D, _D, ctypes.c_double, _I, ctypes.c_double, _I,
+                                    ctypes.c_double]
+            lib.lso_delete.argtypes = [ctypes.c_void_p]
+            lib.lso_ncell.restype = ctypes.c_long
+            lib.lso_ncell.argtypes = [ctypes.c_void_p]
+            for fn in ("lso_psi", "lso_dxm"):
+                getattr(lib, fn).restype = ctypes.c_double
+                getattr(lib, fn).argtypes = [ctypes.c_void_p]
+            lib.lso_get_metric.argtypes = [ctypes.c_void_p, _I, _D, _I]
+            lib.lso_get_weno_tables.argtypes = [ctypes.c_void_p, _I, _D, _D, _D, _I]
+            lib.lso_weno_L.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, _D]
+            lib.lso_reinidisc_L.argtypes = [ctypes.c_void_p, _D, _D]
+            lib.lso_ghost_fill.argtypes = [ctypes.c_void_p, _D]
+            lib.lso_reini.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, _I]
+            lib.lso_ls_step.argtypes = [ctypes.c_void_p, _D, _D, _D, _D, ctypes.c_double, _D, _D, _D]
+            lib.lso_volume.argtypes = [ctypes.c_void_p, _D, _D, _D]
+            lib.lso_cfl_dt.restype = ctypes.c_double
+            lib.lso_cfl_dt.argtypes = [ctypes.c_void_p, _D, _D, _D]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3):
+        self.lib()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.shape = padded_shape(nx, ny, nz)
+        self.f44 = f44
+        self._xn = np.ascontiguousarray(xn, dtype=np.float64)
+        self._yn = np.ascontiguousarray(yn, dtype=np.float64)
+        self._zn = np.ascontiguousarray(zn, dtype=np.float64)
+        self.h = self._lib.lso_new(nx, ny, nz, _dp(self._xn), _dp(self._yn), _dp(self._zn),
+                                   f43, f44, f45, f49, n47)
+        if not self.h:
+            raise ValueError("lso_new failed")
+
+    def __del__(self):
+        if getattr(self, "h", None) and self._lib is not None:
+            self._lib.lso_delete(self.h)
+            self.h = None
+
+    def zeros(self):
+        return np.zeros(self.shape, dtype=np.float64)
+
+    @property
+    def psi(self):
+        return self._lib.lso_psi(self.h)
+
+    @property
+    def dxm(self):
+        return self._lib.lso_dxm(self.h)
+
+    def metric(self, which, n):
+        out = np.zeros(n)
+        self._lib.lso_get_metric(self.h, which, _dp(out), n)
+        return out
+
+    def weno_tables(self, axis, n):
+        qf, cf, isf = np.zeros(n * 12), np.zeros(n * 6), np.zeros(n * 18)
+        self._lib.lso_get_weno_tables(self.h, axis, _dp(qf), _dp(cf), _dp(isf), n)
+        return qf, cf, isf
+
+    def weno_L(self, phi, u, v, w):
+        L = self.zeros()
+        self._lib.lso_weno_L(self.h, _dp(phi), _dp(u), _dp(v), _dp(w), _dp(L))
+        return L
+
+    def reinidisc_L(self, f):
+        L = self.zeros()
+        self._lib.lso_reinidisc_L(self.h, _dp(f), _dp(L))
+        return L
+
+    def ghost_fill(self, f):
+        f = np.array(f, dtype=np.float64, order="C", copy=True)
+        self._lib.lso_ghost_fill(self.h, _dp(f))
+        return f
+
+    def reini(self, f, iters):
+        f = np.array(f, dtype=np.float64, order="C", copy=True)
+        a1, a2, L = self.zeros(), self.zeros(), self.zeros()
+        self._lib.lso_reini(self.h, _dp(f), _dp(a1), _dp(a2), _dp(L), iters)
+        return f
+
+    def step(self, phi, u, v, w, dt):
+        phi = np.array(phi, dtype=np.float64, order="C", copy=True)
+        a1, a2, L = self.zeros(), self.zeros(), self.zeros()
+        self._lib.lso_ls_step(self.h, _dp(phi), _dp(u), _dp(v), _dp(w), dt, _dp(a1), _dp(a2), _dp(L))
+        return phi
+
+    def volume(self, phi):
+        v1, v2 = ctypes.c_double(), ctypes.c_double()
+        self._lib.lso_volume(self.h, _dp(np.ascontiguousarray(phi)), ctypes.byref(v1), ctypes.byref(v2))
+        return v1.value, v2.value
+
+    def cfl_dt(self, u, v, w):
+        return self._lib.lso_cfl_dt(self.h, _dp(u), _dp(v), _dp(w))
+
+
+class RefOracle:
+    """The reference's own objects; at most one per process."""
+
+    _lib = None
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(REF_LIB)
+
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1):
+        if RefOracle._lib is not None:
+            raise RuntimeError("the reference oracle holds one grid per process")
+        lib = ctypes.CDLL(REF_LIB)
+        lib.refls_init.argtypes = [_I, _I, _I, _D, _D, _D, _I, ctypes.c_double, ctypes.c_double, _I]
+        lib.refls_padded_size.restype = ctypes.c_long
+        lib.refls_set_field.argtypes = [_I, _D]
+        lib.refls_get_field.argtypes = [_I, _D]
+        lib.refls_set_dt.argtypes = [ctypes.c_double]
+        lib.refls_set_count.argtypes = [_I]
+        for fn in ("refls_psi", "refls_dxm", "refls_volume1", "refls_volume2"):
+            getattr(lib, fn).restype = ctypes.c_double
+        lib.refls_get_metric.argtypes = [_I, _D, _I]
+        lib.refls_get_weno_tables.argtypes = [_I, _D, _D, _D, _I]
+        lib.refls_weno_L.argtypes = [_D, _D]
+        lib.refls_reinidisc_L.argtypes = [_D, _D]
+        lib.refls_ghost_fill.argtypes = [_D]
+        lib.refls_cfl_dt.restype = ctypes.c_double
+        lib.refls_cfl_dt.argtypes = [ctypes.c_double]
+        RefOracle._lib = lib
+        self._lib = lib
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.shape = padded_shape(nx, ny, nz)
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xn, yn, zn)]
+        rc = lib.refls_init(nx, ny, nz, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]), f44, f43, f45, f49)
+        if rc != 0:
+            raise RuntimeError("refls_init failed")
+        assert lib.refls_padded_size() == int(np.prod(self.shape))
+
+    def zeros(self):
+        return np.zeros(self.shape, dtype=np.float64)
+
+    def set_field(self, fid, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._lib.refls_set_field(fid, _dp(a))
+
+    def get_field(self, fid):
+        a = self.zeros()
+        self._lib.refls_get_field(fid, _dp(a))
+        return a
+
+    def set_state(self, phi, u, v, w):
+        for fid, arr in ((0, phi), (1, u), (2, v), (3, w)):
+            self.set_field(fid, arr)
+
+    @property
+    def psi(self):
+        return self._lib.refls_psi()
+
+    @property
+    def dxm(self):
+        return self._lib.refls_dxm()
+
+    def metric(self, which, n):
+        out = np.zeros(n)
+        self._lib.refls_get_metric(which, _dp(out), n)
+        return out
+
+    def weno_tables(self, axis, n):
+        qf, cf, isf = np.zeros(n * 12), np.zeros(n * 6), np.zeros(n * 18)
+        self._lib.refls_get_weno_tables(axis, _dp(qf), _dp(cf), _dp(isf), n)
+        return qf, cf, isf
+
+    def weno_L(self, phi):
+        L = self.zeros()
+        self._lib.refls_weno_L(_dp(np.ascontiguousarray(phi)), _dp(L))
+        return L
+
+    def reinidisc_L(self, f):
+        L = self.zeros()
+        self._lib.refls_reinidisc_L(_dp(np.ascontiguousarray(f)), _dp(L))
+        return L
+
+    def ghost_fill(self, f):
+        f = np.array(f, dtype=np.float64, order="C", copy=True)
+        self._lib.refls_ghost_fill(_dp(f))
+        return f
+
+    def reini(self):
+        self._lib.refls_reini()
+        return self.get_field(0)
+
+    def step(self, dt):
+        self._lib.refls_set_dt(dt)
+        self._lib.refls_step()
+        return self.get_field(0)
+
+    def cfl_dt(self, n47):
+        return self._lib.refls_cfl_dt(n47)
+
+    def volume(self):
+        self._lib.refls_update()
+        return self._lib.refls_volume1(), self._lib.refls_volume2()

@@ -32,6 +32,11 @@
 #include "concentration.h"
 #include "fluid_update_fsf.h"
 #include "patchBC_void.h"
+#include "mgcslice1.h"
+#include "ietimestep.h"
+#include "kepsilon_void.h"
+#include "mgcslice2.h"
+#include "mgcslice4.h"
 
 #include <cstring>
 #include <vector>
@@ -50,6 +55,8 @@ reinidisc* DISC = nullptr;
 heat* HEAT = nullptr;
 concentration* CONC = nullptr;
 field4* TMP = nullptr;
+ietimestep* TSTEP = nullptr;
+turbulence* TURB = nullptr;
 
 long ncells_padded() { return (long)P->imax * P->jmax * P->kmax; }
 
@@ -241,6 +248,25 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
         gridgen.fill_dgc3(p);
         gridgen.fill_dgc4(p);
     }
+    {   // body of driver::makegrid2D (src/driver_makgrid_2D.cpp:31-74): the
+        // slice ghost lists sized here are allocated by every fdm
+        PGC->gcslflagx(p, p->flagslice4);
+        mgcslice1 m1(p);
+        mgcslice2 m2(p);
+        mgcslice4 m4(p);
+        m1.makemgc(p); PGC->gcslflagx(p, p->flagslice1);
+        m1.gcb_seed(p); m1.mgcsetup(p); m1.fillmgc(p); m1.gcdirfill(p);
+        m2.makemgc(p); PGC->gcslflagx(p, p->flagslice2);
+        m2.gcb_seed(p); m2.mgcsetup(p); m2.fillmgc(p); m2.gcdirfill(p);
+        m4.makemgc(p);
+        m4.gcb_seed(p); m4.mgcsetup(p); m4.fillmgc(p); m4.gcdirfill(p);
+        m1.make_ggc(p); m1.fill_ggc(p);
+        m2.make_ggc(p); m2.fill_ggc(p);
+        m4.make_ggc(p); m4.fill_ggc(p);
+        PGC->gcsl_setbc1(p); PGC->gcsl_setbc2(p); PGC->gcsl_setbc4(p);
+        PGC->gcsl_setbcio(p);
+        PGC->dgcslini1(p); PGC->dgcslini2(p); PGC->dgcslini4(p);
+    }
 
     A = new fdm(p);
     PGC->fdm_update(A);
@@ -261,6 +287,8 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     if (f49 == 1) DISC = new reinidisc_f(p);
     else DISC = new reinidisc_fsf(p);
     TMP = new field4(p);
+    TSTEP = new ietimestep(p);
+    TURB = new kepsilon_void(p, A, PGC);
     p->count = 1;
     p->dt = 0.0;
     return 0;
@@ -363,6 +391,15 @@ int refls_step() {
     convection* pc = CONV;
     LS->start(A, P, pc, nullptr, PGC, FLOW, REINI, PART, A->phi);
     return 0;
+}
+
+// Adaptive time step from the stored velocities with CFL factor n47
+// (src/ietimestep.cpp:38-206; maxF=maxG=maxH=0 for a prescribed velocity).
+double refls_cfl_dt(double n47) {
+    P->N47 = n47;
+    A->maxF = A->maxG = A->maxH = 0.0;
+    TSTEP->start(A, P, PGC, TURB);
+    return P->dt;
 }
 
 // Density/volume update only (src/fluid_update_fsf.cpp:39-104).
