@@ -1,0 +1,145 @@
+/* reef3d_b200 -- B200-native level-set transport for REEF3D.
+ *
+ * C-ABI of the shared library libreef3d_b200.so.  Plain pointers and sizes
+ * only; every entry point returns an int status (R3D_OK on success) and
+ * never throws.  The text of the last error of a handle is available from
+ * r3d_last_error(); errors raised before a handle exists go to the
+ * thread's last error, r3d_last_error(NULL).
+ *
+ * One handle = one level-set instance (one grid) whose fields live in device
+ * memory of the GPU current at creation.  Calls on one handle are not
+ * thread-safe; distinct handles may be used from distinct threads.
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the REEF3D source tree).
+ */
+#ifndef REEF3D_B200_H
+#define REEF3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define R3D_OK 0
+#define R3D_EINVAL 1     /* bad argument (size, id, layout, null pointer) */
+#define R3D_ENOMEM 2     /* device or host allocation failed / over budget */
+#define R3D_EDEVICE 3    /* CUDA runtime error */
+#define R3D_ETIMEOUT 4   /* a bounded device wait gave up */
+#define R3D_ESTATE 5     /* call not valid in the handle's current state */
+
+/* arithmetic of an instance */
+#define R3D_FP64 0       /* plain FP64: same operations and order as the reference */
+#define R3D_FP32 1       /* FP32 stencils and RK stages, FP64 reductions */
+
+/* field ids (the fdm members the path reads and writes, src/fdm.h) */
+#define R3D_PHI 0        /* a->phi, level set (cell centres) */
+#define R3D_U 1          /* a->u, x velocity on x faces (i+1/2) */
+#define R3D_V 2          /* a->v, y velocity on y faces */
+#define R3D_W 3          /* a->w, z velocity on z faces */
+#define R3D_L 4          /* a->L, right-hand side of the last operator call */
+#define R3D_WORK1 5      /* RK stage buffer (ark1 / frk1) */
+#define R3D_WORK2 6      /* RK stage buffer (ark2 / frk2) */
+
+/* host array layouts for upload/download */
+#define R3D_LAYOUT_REEF3D 0  /* the reference's padded field: (nx+6)(ny+6)(nz+6) doubles,
+                                index (i+3)(ny+6)(nz+6)+(j+3)(nz+6)+(k+3), k contiguous
+                                (src/field_base.h:32-47); 2D grids keep the 6 y ghost planes */
+#define R3D_LAYOUT_DENSE 1   /* interior cells only, nx*ny*nz doubles, x contiguous:
+                                index i + nx*(j + ny*k) */
+
+typedef struct r3d_handle r3d_handle;
+
+/* Grid and control flags of one instance.  Node coordinates follow the
+ * DIVEMesh grid the reference reads (src/read_grid.cpp:417-433): n+11 values
+ * for node indices -5..n+5.  ny == 1 selects the 2D x-z form (j_dir = 0).
+ * Flags carry the reference's control-file meaning (src/ini.cpp:400-416,
+ * 587-596): f43 reinit time-step factor, f44 reinit pseudo-steps per
+ * physical step, f45 interface thickness factor, f49 reinit form (1 every
+ * cell, 0 freeze cells next to the interface), n47 CFL factor. */
+typedef struct {
+    int nx, ny, nz;
+    const double* xn;
+    const double* yn;
+    const double* zn;
+    double f43;
+    int f44;
+    double f45;
+    int f49;
+    double n47;
+    int precision;      /* R3D_FP64 or R3D_FP32 */
+} r3d_grid_desc;
+
+/* Create an instance on the current CUDA device: allocates the level set,
+ * two stage buffers, L, the three velocity fields and reduction scratch,
+ * builds the grid metrics and WENO coefficient tables the way
+ * src/grid.cpp:55-148 and src/weno_nug_func_precalc_*.cpp do, and zeroes
+ * every field.  Replaces the construction of levelset_RK3, weno_hj_df_nug
+ * and reini_RK3 (src/driver_logic_cfd.cpp:145-146,377-385). */
+int r3d_create(const r3d_grid_desc* desc, r3d_handle** out);
+int r3d_destroy(r3d_handle* h);
+const char* r3d_last_error(const r3d_handle* h);
+
+/* Device bytes an instance of this description holds (for admission). */
+int r3d_footprint(const r3d_grid_desc* desc, size_t* bytes);
+
+/* Host <-> device field copies (explicit copy-in/copy-out of the
+ * reference's field objects, src/field_base.h:28-54).  Synchronous. */
+int r3d_upload(r3d_handle* h, int field, const double* host, int layout);
+int r3d_download(r3d_handle* h, int field, double* host, int layout);
+
+/* Time step used by r3d_ls_step when dt <= 0 is passed there. */
+int r3d_set_dt(r3d_handle* h, double dt);
+/* Adaptive time step from the stored velocities, FP64 on the device:
+ * src/ietimestep.cpp:38-206 for a prescribed velocity (N50=1, no source
+ * term).  Stores it as the handle's dt and returns it in *dt (may be NULL). */
+int r3d_cfl_dt(r3d_handle* h, double* dt);
+
+/* One physical level-set step: three WENO5-HJ convection RK stages with
+ * ghost fill, then f44 reinitialisation pseudo-steps, then the volume
+ * integral.  Replaces levelset_RK3::start (src/levelset_RK3.cpp:103-172)
+ * with picard, particles, ioflow hooks and solid forcing void, as in the
+ * reference's default configuration.  dt <= 0 uses the handle's dt.
+ * Asynchronous on the handle's stream. */
+int r3d_ls_step(r3d_handle* h, double dt);
+/* n steps, each preceded by r3d_cfl_dt when adaptive != 0 (the timestep
+ * control of src/driver_loop_cfd.cpp:104-105), all on the device. */
+int r3d_ls_run(r3d_handle* h, int nsteps, int adaptive);
+
+/* Reinitialisation only: `iters` pseudo-steps on the level set
+ * (reini_RK3::start, src/reini_RK3.cpp:84-143; iters <= 0 uses f44). */
+int r3d_reinit(r3d_handle* h, int iters);
+
+/* Operator-level drop-ins on device fields:
+ *  r3d_convection_L: L(field_in) = -u.grad(field_in) by WENO5-HJ, written
+ *    to R3D_L (convection::start with ipol 4 on a zeroed L,
+ *    src/weno_hj_df_nug.cpp:58-111).
+ *  r3d_reinidisc_L: reinitialisation operator (reinidisc::start,
+ *    src/reinidisc_f.cpp:37-127 / src/reinidisc_fsf.cpp:37-141).
+ *  r3d_ghost_fill: wall ghost fill of a field (ghostcell::start4 with a
+ *    level-set gcv, src/gc_start.cpp:146-185). */
+int r3d_convection_L(r3d_handle* h, int field_in);
+int r3d_reinidisc_L(r3d_handle* h, int field_in);
+int r3d_ghost_fill(r3d_handle* h, int field);
+
+/* Volume sums of the smoothed Heaviside (fluid_update_fsf::start,
+ * src/fluid_update_fsf.cpp:39-74), FP64.  Synchronous. */
+int r3d_volume(r3d_handle* h, double* volume1, double* volume2);
+
+/* Volume sums accumulated by the last r3d_ls_step / r3d_ls_run step
+ * (fused into the step's final stage).  Synchronous. */
+int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2);
+
+/* Wait for the handle's stream. */
+int r3d_sync(r3d_handle* h);
+/* The handle's cudaStream_t, as void*. */
+int r3d_stream(r3d_handle* h, void** stream);
+/* Kernel launches issued on this handle since creation. */
+int r3d_launch_count(const r3d_handle* h, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

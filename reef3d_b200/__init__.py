@@ -1,0 +1,235 @@
+"""reef3d_b200: B200-native level-set transport for REEF3D.
+
+Python host layer over the C-ABI of ``libreef3d_b200.so``
+(``include/reef3d_b200.h``).  The library is built in-tree by
+``reef3d_b200/build.py``; importing this package loads it and raises if it
+is missing (there is no CPU fallback).
+
+``LevelSet`` owns one device-resident instance.  ``reef3d_b200.compat``
+mirrors the reference's class interfaces (levelset_RK3, weno_hj_df_nug,
+reini_RK3, reinidisc_f/fsf, ghostcell::start4) on host arrays in the
+reference's field layout.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libreef3d_b200.so")
+
+R3D_OK, R3D_EINVAL, R3D_ENOMEM, R3D_EDEVICE, R3D_ETIMEOUT, R3D_ESTATE = 0, 1, 2, 3, 4, 5
+FP64, FP32 = 0, 1
+PHI, U, V, W, L, WORK1, WORK2 = range(7)
+LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
+
+_ERRNAMES = {1: "EINVAL", 2: "ENOMEM", 3: "EDEVICE", 4: "ETIMEOUT", 5: "ESTATE"}
+
+
+class R3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"r3d error {_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("xn", ctypes.POINTER(ctypes.c_double)), ("yn", ctypes.POINTER(ctypes.c_double)),
+        ("zn", ctypes.POINTER(ctypes.c_double)),
+        ("f43", ctypes.c_double), ("f44", ctypes.c_int), ("f45", ctypes.c_double), ("f49", ctypes.c_int),
+        ("n47", ctypes.c_double), ("precision", ctypes.c_int),
+    ]
+
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_H = ctypes.c_void_p
+
+# every symbol the C-ABI exports (include/reef3d_b200.h)
+EXPORTS = {
+    "r3d_create": ([ctypes.POINTER(GridDesc), ctypes.POINTER(_H)], ctypes.c_int),
+    "r3d_destroy": ([_H], ctypes.c_int),
+    "r3d_last_error": ([_H], ctypes.c_char_p),
+    "r3d_footprint": ([ctypes.POINTER(GridDesc), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+    "r3d_upload": ([_H, ctypes.c_int, _D, ctypes.c_int], ctypes.c_int),
+    "r3d_download": ([_H, ctypes.c_int, _D, ctypes.c_int], ctypes.c_int),
+    "r3d_set_dt": ([_H, ctypes.c_double], ctypes.c_int),
+    "r3d_cfl_dt": ([_H, _D], ctypes.c_int),
+    "r3d_ls_step": ([_H, ctypes.c_double], ctypes.c_int),
+    "r3d_ls_run": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_reinit": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_convection_L": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_reinidisc_L": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_ghost_fill": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_volume": ([_H, _D, _D], ctypes.c_int),
+    "r3d_last_volume": ([_H, _D, _D], ctypes.c_int),
+    "r3d_sync": ([_H], ctypes.c_int),
+    "r3d_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "r3d_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+}
+
+
+def load_library(path=LIB_PATH):
+    """Load libreef3d_b200.so (fails loudly if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: run `python reef3d_b200/build.py` (no CPU fallback exists)")
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc, h=None):
+    if rc != R3D_OK:
+        msg = _lib.r3d_last_error(h)
+        raise R3DError(rc, msg.decode() if msg else "")
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def uniform_nodes(n, length=1.0, origin=0.0):
+    """Node coordinates for node indices -5..n+5 of a uniform axis (n+11
+    values), x_i = origin + i*(length/n), as a DIVEMesh grid stores them."""
+    h = length / n
+    return np.array([origin + i * h for i in range(-5, n + 6)], dtype=np.float64)
+
+
+def make_desc(nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3, precision=FP64):
+    xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xn, yn, zn)]
+    for a, n in zip(xs, (nx, ny, nz)):
+        if a.shape != (n + 11,):
+            raise ValueError(f"node array of an axis with {n} cells needs {n + 11} values, got {a.shape}")
+    d = GridDesc(nx, ny, nz, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]), f43, f44, f45, f49, n47, precision)
+    d._keep = xs
+    return d
+
+
+def footprint(nx, ny, nz, precision=FP32):
+    """Device bytes of one instance (fields, tables, scratch)."""
+    load_library()
+    d = make_desc(nx, ny, nz, uniform_nodes(nx), uniform_nodes(ny), uniform_nodes(nz), precision=precision)
+    out = ctypes.c_size_t()
+    _check(_lib.r3d_footprint(ctypes.byref(d), ctypes.byref(out)))
+    return out.value
+
+
+class LevelSet:
+    """One device-resident level-set instance (the state levelset_RK3,
+    weno_hj_df_nug and reini_RK3 act on in the reference)."""
+
+    def __init__(self, nx, ny, nz, xn=None, yn=None, zn=None, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3,
+                 precision=FP64):
+        load_library()
+        xn = uniform_nodes(nx) if xn is None else xn
+        yn = uniform_nodes(ny) if yn is None else yn
+        zn = uniform_nodes(nz) if zn is None else zn
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.f44, self.precision = f44, precision
+        self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision)
+        h = _H()
+        _check(_lib.r3d_create(ctypes.byref(self.desc), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and _lib is not None:
+            _lib.r3d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- shapes
+    @property
+    def reef3d_shape(self):
+        return (self.nx + 6, self.ny + 6, self.nz + 6)
+
+    @property
+    def dense_shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    def _shape(self, layout):
+        return self.reef3d_shape if layout == LAYOUT_REEF3D else self.dense_shape
+
+    # -- host copies
+    def upload(self, field, arr, layout=LAYOUT_REEF3D):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != self._shape(layout):
+            raise ValueError(f"expected shape {self._shape(layout)}, got {a.shape}")
+        _check(_lib.r3d_upload(self.h, field, _dp(a), layout), self.h)
+
+    def download(self, field, layout=LAYOUT_REEF3D, out=None):
+        a = np.zeros(self._shape(layout), dtype=np.float64) if out is None else out
+        _check(_lib.r3d_download(self.h, field, _dp(a), layout), self.h)
+        return a
+
+    def upload_ptr(self, field, ptr, layout=LAYOUT_REEF3D):
+        """Upload from a raw host pointer (e.g. pinned memory)."""
+        _check(_lib.r3d_upload(self.h, field, ctypes.cast(ptr, _D), layout), self.h)
+
+    def download_ptr(self, field, ptr, layout=LAYOUT_REEF3D):
+        _check(_lib.r3d_download(self.h, field, ctypes.cast(ptr, _D), layout), self.h)
+
+    # -- path
+    def set_dt(self, dt):
+        _check(_lib.r3d_set_dt(self.h, dt), self.h)
+
+    def cfl_dt(self):
+        v = ctypes.c_double()
+        _check(_lib.r3d_cfl_dt(self.h, ctypes.byref(v)), self.h)
+        return v.value
+
+    def step(self, dt=0.0):
+        _check(_lib.r3d_ls_step(self.h, dt), self.h)
+
+    def run(self, nsteps, adaptive=True):
+        _check(_lib.r3d_ls_run(self.h, nsteps, 1 if adaptive else 0), self.h)
+
+    def reinit(self, iters=0):
+        _check(_lib.r3d_reinit(self.h, iters), self.h)
+
+    def convection_L(self, field=PHI):
+        _check(_lib.r3d_convection_L(self.h, field), self.h)
+
+    def reinidisc_L(self, field=PHI):
+        _check(_lib.r3d_reinidisc_L(self.h, field), self.h)
+
+    def ghost_fill(self, field=PHI):
+        _check(_lib.r3d_ghost_fill(self.h, field), self.h)
+
+    def volume(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.r3d_volume(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
+        return a.value, b.value
+
+    def last_volume(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.r3d_last_volume(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
+        return a.value, b.value
+
+    def sync(self):
+        _check(_lib.r3d_sync(self.h), self.h)
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        _check(_lib.r3d_stream(self.h, ctypes.byref(s)), self.h)
+        return s.value
+
+    def launch_count(self):
+        c = ctypes.c_longlong()
+        _check(_lib.r3d_launch_count(self.h, ctypes.byref(c)), self.h)
+        return c.value

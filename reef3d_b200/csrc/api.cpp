@@ -1,0 +1,465 @@
+// C-ABI of libreef3d_b200.so (declared in include/reef3d_b200.h).
+#include "reef3d_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "r3d_internal.h"
+
+using namespace r3d;
+
+struct r3d_handle {
+    Layout L{};
+    r3d_grid_desc desc{};
+    HostMetrics M;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void* field[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* metrics64 = nullptr;
+    float* metrics32 = nullptr;
+    KGrid<double> g64{};
+    KGrid<float> g32{};
+    Scratch S{};
+    double* staging = nullptr;
+    size_t staging_bytes = 0;
+    long long launches = 0;
+    double dt_host = 0.0;
+    bool have_last_volume = false;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_thread_err;
+
+int fail(r3d_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_thread_err = msg;
+    return code;
+}
+
+int cuda_fail(r3d_handle* h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(h, R3D_EDEVICE, m);
+}
+
+#define R3D_CUDA(h, call)                                  \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+bool fp32(const r3d_handle* h) { return h->desc.precision == R3D_FP32; }
+size_t elem(const r3d_handle* h) { return fp32(h) ? sizeof(float) : sizeof(double); }
+
+int check_desc(const r3d_grid_desc* d, std::string& why) {
+    if (!d) { why = "null descriptor"; return R3D_EINVAL; }
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1) { why = "grid sizes must be >= 1"; return R3D_EINVAL; }
+    if (d->nx > 65535 * 32 || d->ny > 65535 || d->nz > 65535) { why = "grid size beyond launch limits"; return R3D_EINVAL; }
+    if (!d->xn || !d->yn || !d->zn) { why = "node coordinates missing"; return R3D_EINVAL; }
+    if (d->precision != R3D_FP64 && d->precision != R3D_FP32) { why = "precision must be R3D_FP64 or R3D_FP32"; return R3D_EINVAL; }
+    if (d->f44 < 0) { why = "f44 must be >= 0"; return R3D_EINVAL; }
+    if (d->f49 != 0 && d->f49 != 1) { why = "f49 must be 0 or 1"; return R3D_EINVAL; }
+    const int n[3] = {d->nx, d->ny, d->nz};
+    const double* x[3] = {d->xn, d->yn, d->zn};
+    for (int a = 0; a < 3; ++a)
+        for (int t = 0; t < n[a] + 10; ++t)
+            if (!(x[a][t + 1] > x[a][t])) { why = "node coordinates must increase strictly"; return R3D_EINVAL; }
+    return R3D_OK;
+}
+
+// device bytes: 7 fields + metric tables + scratch (staging excluded: it is
+// allocated on first host copy)
+size_t footprint(const r3d_grid_desc* d, const Layout& L) {
+    const size_t e = d->precision == R3D_FP32 ? 4 : 8;
+    size_t b = 7 * (size_t)L.ncell * e;
+    size_t tab = 0;
+    const int n[3] = {d->nx, d->ny, d->nz};
+    for (int a = 0; a < 3; ++a) tab += 2 * (size_t)(n[a] + 21) + (size_t)(n[a] + 8) * 36;
+    b += tab * (8 + 4);
+    const long long blocks = (long long)((d->nx + 31) / 32) * ((d->ny + 3) / 4 + 4) * (d->nz + 4);
+    b += (size_t)(blocks + (long long)d->ny * d->nz + 64) * 16 + 256;
+    return b;
+}
+
+template <typename T>
+void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
+    g.L = h->L;
+    size_t off = 0;
+    host.clear();
+    for (int a = 0; a < 3; ++a) {
+        const size_t o_dxp = off;
+        for (double v : h->M.dxp[a]) host.push_back((T)v);
+        off = host.size();
+        const size_t o_dxn = off;
+        for (double v : h->M.dxn[a]) host.push_back((T)v);
+        off = host.size();
+        const size_t o_qf = off;
+        for (double v : h->M.qf[a]) host.push_back((T)v);
+        off = host.size();
+        const size_t o_cf = off;
+        for (double v : h->M.cf[a]) host.push_back((T)v);
+        off = host.size();
+        const size_t o_isf = off;
+        for (double v : h->M.isf[a]) host.push_back((T)v);
+        off = host.size();
+        g.dxp[a] = base + o_dxp;
+        g.dxn[a] = base + o_dxn;
+        g.qf[a] = base + o_qf;
+        g.cf[a] = base + o_cf;
+        g.isf[a] = base + o_isf;
+    }
+    g.f43 = h->desc.f43;
+    g.f49 = h->desc.f49;
+    g.psi = h->M.psi;
+    for (int a = 0; a < 3; ++a) {
+        g.h[a] = h->M.uniform ? (float)h->M.h[a] : 0.0f;
+        g.rh[a] = h->M.uniform ? (float)(1.0 / h->M.h[a]) : 0.0f;
+    }
+    g.eps_u = 1.0e-6f;
+}
+
+size_t metric_count(const r3d_handle* h) {
+    size_t c = 0;
+    for (int a = 0; a < 3; ++a)
+        c += h->M.dxp[a].size() + h->M.dxn[a].size() + h->M.qf[a].size() + h->M.cf[a].size() + h->M.isf[a].size();
+    return c;
+}
+
+void release(r3d_handle* h) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void*& p : h->field) { if (p) cudaFree(p); p = nullptr; }
+    if (h->metrics64) cudaFree(h->metrics64);
+    if (h->metrics32) cudaFree(h->metrics32);
+    if (h->S.partial) cudaFree(h->S.partial);
+    if (h->S.vmax) cudaFree(h->S.vmax);
+    if (h->staging) cudaFree(h->staging);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaSetDevice(cur);
+}
+
+Fields fields_of(r3d_handle* h) {
+    Fields f{};
+    f.phi = h->field[R3D_PHI];
+    f.u = h->field[R3D_U];
+    f.v = h->field[R3D_V];
+    f.w = h->field[R3D_W];
+    f.L = h->field[R3D_L];
+    f.a1 = h->field[R3D_WORK1];
+    f.a2 = h->field[R3D_WORK2];
+    return f;
+}
+
+int ensure_staging(r3d_handle* h) {
+    const size_t need = sizeof(double) * (size_t)(h->L.nx + 6) * (h->L.ny + 6) * (h->L.nz + 6);
+    if (h->staging_bytes >= need) return R3D_OK;
+    if (h->staging) cudaFree(h->staging);
+    h->staging = nullptr;
+    h->staging_bytes = 0;
+    if (cudaMalloc(&h->staging, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, R3D_ENOMEM, "staging allocation failed");
+    }
+    h->staging_bytes = need;
+    return R3D_OK;
+}
+
+size_t host_count(const r3d_handle* h, int layout) {
+    if (layout == R3D_LAYOUT_REEF3D) return (size_t)(h->L.nx + 6) * (h->L.ny + 6) * (h->L.nz + 6);
+    return (size_t)h->L.nx * h->L.ny * h->L.nz;
+}
+
+struct DeviceGuard {
+    int prev = 0;
+    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); if (prev != dev) cudaSetDevice(dev); }
+    ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
+};
+
+int enqueue_step(r3d_handle* h) {
+    const Fields f = fields_of(h);
+    const int f44 = h->desc.f44;
+    long long n = 0;
+    for (int s = 1; s <= 3; ++s) {
+        const bool vol = (f44 == 0 && s == 3);
+        n += fp32(h) ? launch_conv_stage_f32(h->g32, f, s, h->S, vol, h->stream)
+                     : launch_conv_stage_f64(h->g64, f, s, h->S, vol, h->stream);
+    }
+    for (int q = 0; q < f44; ++q)
+        for (int s = 1; s <= 3; ++s) {
+            const bool vol = (q == f44 - 1 && s == 3);
+            n += fp32(h) ? launch_reini_stage_f32(h->g32, f, s, h->S, vol, h->stream)
+                         : launch_reini_stage_f64(h->g64, f, s, h->S, vol, h->stream);
+        }
+    n += launch_volume_reduce(h->L, h->S, volume_blocks(h->L), h->stream);
+    h->launches += n;
+    h->have_last_volume = true;
+    return R3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* r3d_last_error(const r3d_handle* h) { return h ? h->err.c_str() : g_thread_err.c_str(); }
+
+int r3d_footprint(const r3d_grid_desc* desc, size_t* bytes) {
+    std::string why;
+    if (int rc = check_desc(desc, why)) return fail(nullptr, rc, why);
+    if (!bytes) return fail(nullptr, R3D_EINVAL, "null output");
+    *bytes = footprint(desc, make_layout(desc->nx, desc->ny, desc->nz));
+    return R3D_OK;
+}
+
+int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
+    std::string why;
+    if (!out) return fail(nullptr, R3D_EINVAL, "null output handle");
+    *out = nullptr;
+    if (int rc = check_desc(desc, why)) return fail(nullptr, rc, why);
+    r3d_handle* h = new (std::nothrow) r3d_handle();
+    if (!h) return fail(nullptr, R3D_ENOMEM, "host allocation failed");
+    h->desc = *desc;
+    h->desc.xn = h->desc.yn = h->desc.zn = nullptr;
+    cudaGetDevice(&h->device);
+    h->L = make_layout(desc->nx, desc->ny, desc->nz);
+    build_metrics(desc->nx, desc->ny, desc->nz, desc->xn, desc->yn, desc->zn, desc->f45, h->M);
+
+    auto bail = [&](int code, const std::string& m) {
+        g_thread_err = m;
+        release(h);
+        delete h;
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(R3D_EDEVICE, "stream creation failed (no usable CUDA device?)");
+    }
+    const size_t fbytes = (size_t)h->L.ncell * elem(h);
+    for (int id = 0; id < 7; ++id) {
+        if (cudaMalloc(&h->field[id], fbytes) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(R3D_ENOMEM, "device field allocation failed");
+        }
+        cudaMemsetAsync(h->field[id], 0, fbytes, h->stream);
+    }
+    const size_t mc = metric_count(h);
+    if (cudaMalloc(&h->metrics64, mc * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->metrics32, mc * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(R3D_ENOMEM, "metric allocation failed");
+    }
+    std::vector<double> m64;
+    std::vector<float> m32;
+    fill_kgrid<double>(h, h->g64, h->metrics64, m64);
+    fill_kgrid<float>(h, h->g32, h->metrics32, m32);
+    cudaMemcpy(h->metrics64, m64.data(), m64.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->metrics32, m32.data(), m32.size() * sizeof(float), cudaMemcpyHostToDevice);
+
+    const long long nb = volume_blocks(h->L);
+    const long long np = (nb > (long long)h->L.ny * h->L.nz ? nb : (long long)h->L.ny * h->L.nz) + 64;
+    if (cudaMalloc(&h->S.partial, (size_t)np * 2 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->S.vmax, 256) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(R3D_ENOMEM, "scratch allocation failed");
+    }
+    h->S.npartial = np;
+    h->S.dt = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 64);
+    h->S.vol = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 128);
+    cudaMemsetAsync(h->S.vmax, 0, 256, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return bail(R3D_EDEVICE, std::string("initialisation: ") + cudaGetErrorString(e));
+    *out = h;
+    return R3D_OK;
+}
+
+int r3d_destroy(r3d_handle* h) {
+    if (!h) return R3D_OK;
+    release(h);
+    delete h;
+    return R3D_OK;
+}
+
+int r3d_upload(r3d_handle* h, int field, const double* host, int layout) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
+    if (layout != R3D_LAYOUT_REEF3D && layout != R3D_LAYOUT_DENSE) return fail(h, R3D_EINVAL, "bad layout");
+    if (!host) return fail(h, R3D_EINVAL, "null host pointer");
+    DeviceGuard dg(h->device);
+    if (int rc = ensure_staging(h)) return rc;
+    const size_t n = host_count(h, layout);
+    R3D_CUDA(h, cudaMemcpyAsync(h->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    h->launches += launch_import(h->L, h->staging, layout, h->field[field], fp32(h), h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
+int r3d_download(r3d_handle* h, int field, double* host, int layout) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
+    if (layout != R3D_LAYOUT_REEF3D && layout != R3D_LAYOUT_DENSE) return fail(h, R3D_EINVAL, "bad layout");
+    if (!host) return fail(h, R3D_EINVAL, "null host pointer");
+    DeviceGuard dg(h->device);
+    if (int rc = ensure_staging(h)) return rc;
+    const size_t n = host_count(h, layout);
+    if (layout == R3D_LAYOUT_REEF3D) R3D_CUDA(h, cudaMemsetAsync(h->staging, 0, n * sizeof(double), h->stream));
+    h->launches += launch_export(h->L, h->field[field], fp32(h), layout, h->staging, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    R3D_CUDA(h, cudaMemcpyAsync(host, h->staging, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
+int r3d_set_dt(r3d_handle* h, double dt) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, R3D_EINVAL, "dt must be positive and finite");
+    DeviceGuard dg(h->device);
+    h->dt_host = dt;
+    h->launches += launch_set_scalar(h->S.dt, dt, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_cfl_dt(r3d_handle* h, double* dt) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    DeviceGuard dg(h->device);
+    h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h), h->M.dxmin_cfl,
+                              h->desc.n47, h->S, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    double v = 0.0;
+    R3D_CUDA(h, cudaMemcpyAsync(&v, h->S.dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->dt_host = v;
+    if (dt) *dt = v;
+    return R3D_OK;
+}
+
+int r3d_ls_step(r3d_handle* h, double dt) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    DeviceGuard dg(h->device);
+    if (dt > 0.0) {
+        if (int rc = r3d_set_dt(h, dt)) return rc;
+    } else if (!(h->dt_host > 0.0)) {
+        return fail(h, R3D_ESTATE, "no time step set (pass dt > 0, r3d_set_dt or r3d_cfl_dt first)");
+    }
+    enqueue_step(h);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_ls_run(r3d_handle* h, int nsteps, int adaptive) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (nsteps < 0) return fail(h, R3D_EINVAL, "nsteps must be >= 0");
+    DeviceGuard dg(h->device);
+    if (!adaptive && !(h->dt_host > 0.0)) return fail(h, R3D_ESTATE, "no time step set");
+    for (int n = 0; n < nsteps; ++n) {
+        if (adaptive)
+            h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h),
+                                      h->M.dxmin_cfl, h->desc.n47, h->S, h->stream);
+        enqueue_step(h);
+    }
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_reinit(r3d_handle* h, int iters) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    DeviceGuard dg(h->device);
+    const int it = iters > 0 ? iters : h->desc.f44;
+    const Fields f = fields_of(h);
+    for (int q = 0; q < it; ++q)
+        for (int s = 1; s <= 3; ++s)
+            h->launches += fp32(h) ? launch_reini_stage_f32(h->g32, f, s, h->S, false, h->stream)
+                                   : launch_reini_stage_f64(h->g64, f, s, h->S, false, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_convection_L(r3d_handle* h, int field_in) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (field_in != R3D_PHI && field_in != R3D_WORK1 && field_in != R3D_WORK2)
+        return fail(h, R3D_EINVAL, "convection input must be a level-set field");
+    DeviceGuard dg(h->device);
+    const Fields f = fields_of(h);
+    h->launches += fp32(h) ? launch_conv_L_f32(h->g32, h->field[field_in], f, h->stream)
+                           : launch_conv_L_f64(h->g64, h->field[field_in], f, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_reinidisc_L(r3d_handle* h, int field_in) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (field_in != R3D_PHI && field_in != R3D_WORK1 && field_in != R3D_WORK2)
+        return fail(h, R3D_EINVAL, "reinitialisation input must be a level-set field");
+    DeviceGuard dg(h->device);
+    const Fields f = fields_of(h);
+    h->launches += fp32(h) ? launch_reini_L_f32(h->g32, h->field[field_in], f, h->stream)
+                           : launch_reini_L_f64(h->g64, h->field[field_in], f, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_ghost_fill(r3d_handle* h, int field) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
+    DeviceGuard dg(h->device);
+    h->launches += launch_ghost_fill(h->L, h->field[field], fp32(h), h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_volume(r3d_handle* h, double* volume1, double* volume2) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    DeviceGuard dg(h->device);
+    const double* dxn = h->g64.dxn[0];
+    const double* dyn = h->g64.dxn[1];
+    const double* dzn = h->g64.dxn[2];
+    h->launches += launch_volume_direct(h->L, h->field[R3D_PHI], fp32(h), dxn, dyn, dzn, h->M.psi, h->S, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    double v[2] = {0.0, 0.0};
+    R3D_CUDA(h, cudaMemcpyAsync(v, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (volume1) *volume1 = v[0];
+    if (volume2) *volume2 = v[1];
+    return R3D_OK;
+}
+
+int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!h->have_last_volume) return fail(h, R3D_ESTATE, "no step has run yet");
+    DeviceGuard dg(h->device);
+    double v[2] = {0.0, 0.0};
+    R3D_CUDA(h, cudaMemcpyAsync(v, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (volume1) *volume1 = v[0];
+    if (volume2) *volume2 = v[1];
+    return R3D_OK;
+}
+
+int r3d_sync(r3d_handle* h) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    DeviceGuard dg(h->device);
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
+int r3d_stream(r3d_handle* h, void** stream) {
+    if (!h || !stream) return fail(h, R3D_EINVAL, "null argument");
+    *stream = (void*)h->stream;
+    return R3D_OK;
+}
+
+int r3d_launch_count(const r3d_handle* h, long long* count) {
+    if (!h || !count) return fail(nullptr, R3D_EINVAL, "null argument");
+    *count = h->launches;
+    return R3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// Internal declarations shared by the host API (api.cpp) and the kernel
+// translation units.  Not part of the public C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace r3d {
+
+// Device field layout: x contiguous ("i-contiguous"), padded by ghost cells.
+// A cell (i,j,k) of the interior lives at
+//     (k + gz) * sz + (j + gy) * sy + (i + gx)
+// with gx = 4 (3 ghost cells plus one slot so the interior starts 16-byte
+// aligned for FP32 and FP64 alike), gy = gz = 3.  A 2D grid (ny == 1) keeps
+// no y ghost planes (gy = 0, py = 1): the reference never writes them on
+// this path.  Faces: u(i) is the x face i+1/2, v(j) the y face j+1/2, w(k)
+// the z face k+1/2 (the staggering of src/flux_HJ_CDS2.cpp:59-127).
+struct Layout {
+    int nx, ny, nz;
+    int gx, gy, gz;
+    int px, py, pz;
+    long long sy, sz;
+    long long ncell;  // px*py*pz
+    bool two_d;
+};
+
+Layout make_layout(int nx, int ny, int nz);
+
+// Per-axis metric and WENO table offsets inside one device buffer of
+// doubles (FP64) and one of floats (FP32).  Index t = cell index + 5, the
+// reference's 1D indexing (src/iterators1D.h:25-60).
+struct AxisTables {
+    long long dxp, dxn;          // n + 21 entries each
+    long long qf, cf, isf;       // (n+8)*12, (n+8)*6, (n+8)*18 entries
+};
+
+struct HostMetrics {
+    int n[3];
+    std::vector<double> xn[3], xp[3], dxn[3], dxp[3];
+    std::vector<double> qf[3], cf[3], isf[3];
+    double dxm_mean;   // src/grid.cpp:102-148
+    double dym, dzm;   // DIVEMesh header spacings (first node spacing)
+    double psi;        // src/ini_psi.cpp:33-37
+    double dxmin_cfl;  // min over cells of MIN3(DXN,DYN,DZN) (src/ietimestep.cpp:160-166)
+    bool uniform;      // every spacing equal to the first within 1e-12 relative
+    double h[3];       // uniform spacing per axis
+};
+
+// Builds the metrics exactly as the reference does (src/grid.cpp:55-148,
+// src/weno_nug_func_precalc_qf.cpp, _cf.cpp, _isf.cpp, src/ini_psi.cpp).
+void build_metrics(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,
+                   double f45, HostMetrics& m);
+
+// Kernel-side view of an instance (passed by value).
+template <typename T>
+struct KGrid {
+    Layout L;
+    const T* dxp[3];
+    const T* dxn[3];
+    const T* qf[3];
+    const T* cf[3];
+    const T* isf[3];
+    double f43;
+    int f49;
+    double psi;
+    // uniform-grid FP32 form
+    float h[3], rh[3];
+    float eps_u;  // WENO psi (1e-6); rescaled by h^2 per axis for undivided differences
+};
+
+struct Fields {
+    void* phi;
+    void* a1;
+    void* a2;
+    void* L;
+    void* u;
+    void* v;
+    void* w;
+};
+
+// Scratch in device memory: FP64 reduction partials and scalars.
+struct Scratch {
+    double* partial;        // per-block volume partial sums (2 per block)
+    long long npartial;     // capacity in blocks
+    unsigned long long* vmax;  // |u|,|v|,|w| maxima as ordered bit patterns
+    double* dt;             // current time step (read by the stage kernels)
+    double* vol;            // volume1, volume2
+};
+
+// ---- launchers (kernels_f64.cu / kernels_f32.cu / kernels_common.cu)
+// All launchers enqueue on `st` and return the number of kernels launched.
+int launch_conv_stage_f64(const KGrid<double>& g, const Fields& f, int stage, const Scratch& s,
+                          bool volume, cudaStream_t st);
+int launch_reini_stage_f64(const KGrid<double>& g, const Fields& f, int stage, const Scratch& s,
+                           bool volume, cudaStream_t st);
+int launch_conv_L_f64(const KGrid<double>& g, const void* in, const Fields& f, cudaStream_t st);
+int launch_reini_L_f64(const KGrid<double>& g, const void* in, const Fields& f, cudaStream_t st);
+
+int launch_conv_stage_f32(const KGrid<float>& g, const Fields& f, int stage, const Scratch& s,
+                          bool volume, cudaStream_t st);
+int launch_reini_stage_f32(const KGrid<float>& g, const Fields& f, int stage, const Scratch& s,
+                           bool volume, cudaStream_t st);
+int launch_conv_L_f32(const KGrid<float>& g, const void* in, const Fields& f, cudaStream_t st);
+int launch_reini_L_f32(const KGrid<float>& g, const void* in, const Fields& f, cudaStream_t st);
+
+long long volume_blocks(const Layout& L);
+int launch_volume_reduce(const Layout& L, const Scratch& s, long long nblocks, cudaStream_t st);
+int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const double* dxn,
+                         const double* dyn, const double* dzn, double psi, const Scratch& s,
+                         cudaStream_t st);
+int launch_cfl(const Layout& L, const void* u, const void* v, const void* w, bool fp32,
+               double dxmin, double n47, const Scratch& s, cudaStream_t st);
+int launch_ghost_fill(const Layout& L, void* f, bool fp32, cudaStream_t st);
+// host layout <-> device layout (src is a device staging copy of the host array)
+int launch_import(const Layout& L, const double* staging, int layout, void* dst, bool fp32,
+                  cudaStream_t st);
+int launch_export(const Layout& L, const void* src, bool fp32, int layout, double* staging,
+                  cudaStream_t st);
+int launch_zero(void* p, size_t bytes, cudaStream_t st);
+int launch_set_scalar(double* dst, double value, cudaStream_t st);
+
+}  // namespace r3d

@@ -1,0 +1,175 @@
+// FP64 stencil arithmetic of the level-set path, written in the reference's
+// operation order.  Included only by translation units compiled with
+// -fmad=false, so every product and sum rounds separately as in the
+// reference built without FMA contraction; double division and sqrt are
+// IEEE round-to-nearest on the device as on the host.
+#pragma once
+
+#include "r3d_internal.h"
+
+namespace r3d {
+namespace f64 {
+
+// WENO5 derivative from the divided differences q1..q5 of the upwind set,
+// node tables of index t.  Minus side: IS src/weno_nug_func.h:48-60,
+// weights :133-143, reconstruction src/weno_hj_df_nug.cpp:155-159.  Plus
+// side: :61-73, :144-153, :186-190.  epsilon = 0, psi = 1e-6
+// (src/weno_nug_func.cpp:26).
+__device__ __forceinline__ double weno5(const double* __restrict__ Q, const double* __restrict__ C,
+                                        const double* __restrict__ S, bool plus, double q1, double q2,
+                                        double q3, double q4, double q5) {
+    const double psi = 1.0e-6, eps = 0.0;
+    const double dq12 = q1 - q2, dq23 = q2 - q3, dq32 = q3 - q2;
+    const double dq34 = q3 - q4, dq43 = q4 - q3, dq54 = q5 - q4;
+    const double is1 = __ldg(S + 0) * dq54 * dq54 + __ldg(S + 1) * (dq54) * (dq34) + __ldg(S + 2) * dq34 * dq34;
+    const double is2 = __ldg(S + 3) * dq23 * dq23 + __ldg(S + 4) * (dq43) * (dq23) + __ldg(S + 5) * dq43 * dq43;
+    const double is3 = __ldg(S + 6) * dq12 * dq12 + __ldg(S + 7) * (dq32) * (dq12) + __ldg(S + 8) * dq32 * dq32;
+    const double a = is1 + psi, b = is2 + psi, c = is3 + psi;
+    const double c0 = __ldg(C + 0), c1 = __ldg(C + 1), c2 = __ldg(C + 2);
+    const double sum = c0 / (a * a) + c1 / (b * b) + c2 / (c * c);
+    const double w1 = c0 / (eps + (a * a) * sum);
+    const double w2 = c1 / (eps + (b * b) * sum);
+    const double w3 = c2 / (eps + (c * c) * sum);
+    const double Q0 = __ldg(Q + 0), Q1 = __ldg(Q + 1), Q2 = __ldg(Q + 2);
+    const double Q3 = __ldg(Q + 3), Q4 = __ldg(Q + 4), Q5 = __ldg(Q + 5);
+    if (!plus)
+        return w1 * (q4 + Q0 * (q3 - q4) - Q1 * (q5 - q4))
+             + w2 * (q3 + Q2 * (q4 - q3) - Q3 * (q2 - q3))
+             + w3 * (q2 + Q4 * (q1 - q2) + Q5 * (q3 - q2));
+    return w1 * (q4 + Q0 * (q3 - q4) + Q1 * (q5 - q4))
+         + w2 * (q3 + Q2 * (q2 - q3) - Q3 * (q4 - q3))
+         + w3 * (q2 + Q4 * (q3 - q2) - Q5 * (q1 - q2));
+}
+
+// Upwind-biased derivative along one axis (stride s) at linear index c,
+// cell index t = idx+5.  Minus stencil src/weno_hj_df_nug.cpp:344-351, plus
+// stencil :371-378 (shared with src/ddweno_nug_sf.cpp:225-277).
+__device__ __forceinline__ double deriv(const double* __restrict__ f, long long c, long long s,
+                                        const double* __restrict__ dp, const double* __restrict__ qf,
+                                        const double* __restrict__ cf, const double* __restrict__ isf, int t,
+                                        bool plus) {
+    double q1, q2, q3, q4, q5;
+    if (!plus) {
+        const double fm3 = __ldg(f + c - 3 * s), fm2 = __ldg(f + c - 2 * s), fm1 = __ldg(f + c - s);
+        const double f0 = __ldg(f + c), fp1 = __ldg(f + c + s), fp2 = __ldg(f + c + 2 * s);
+        q1 = (fm2 - fm3) / __ldg(dp + t - 3);
+        q2 = (fm1 - fm2) / __ldg(dp + t - 2);
+        q3 = (f0 - fm1) / __ldg(dp + t - 1);
+        q4 = (fp1 - f0) / __ldg(dp + t);
+        q5 = (fp2 - fp1) / __ldg(dp + t + 1);
+    } else {
+        const double fm2 = __ldg(f + c - 2 * s), fm1 = __ldg(f + c - s), f0 = __ldg(f + c);
+        const double fp1 = __ldg(f + c + s), fp2 = __ldg(f + c + 2 * s), fp3 = __ldg(f + c + 3 * s);
+        q1 = (fm1 - fm2) / __ldg(dp + t - 2);
+        q2 = (f0 - fm1) / __ldg(dp + t - 1);
+        q3 = (fp1 - f0) / __ldg(dp + t);
+        q4 = (fp2 - fp1) / __ldg(dp + t + 1);
+        q5 = (fp3 - fp2) / __ldg(dp + t + 2);
+    }
+    const int side = plus ? 1 : 0;
+    return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
+                 isf + (long long)t * 18 + side * 9, plus, q1, q2, q3, q4, q5);
+}
+
+// -u.grad(f) at interior cell (i,j,k): src/weno_hj_df_nug.cpp:93-111 with the
+// cell-centre velocities of src/flux_HJ_CDS2.cpp:59-127 (2D: no y term,
+// src/flux_HJ_CDS2_2D.cpp).  Returned as the reference's a->L value
+// (0.0 + L).
+template <bool TWO_D>
+__device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* __restrict__ f,
+                                         const double* __restrict__ u, const double* __restrict__ v,
+                                         const double* __restrict__ w, long long c, int i, int j, int k) {
+    const long long sy = g.L.sy, sz = g.L.sz;
+    const double iadvec = 0.5 * (__ldg(u + c) + __ldg(u + c - 1));
+    const double kadvec = 0.5 * (__ldg(w + c) + __ldg(w + c - sz));
+    double grad = 0.0;
+    if (iadvec > 0.0) grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, false);
+    if (iadvec < 0.0) grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, true);
+    double l = -iadvec * grad;
+    if (!TWO_D) {
+        const double jadvec = 0.5 * (__ldg(v + c) + __ldg(v + c - sy));
+        grad = 0.0;
+        if (jadvec > 0.0) grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, false);
+        if (jadvec < 0.0) grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, true);
+        l -= jadvec * grad;
+    }
+    grad = 0.0;
+    if (kadvec > 0.0) grad = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5, false);
+    if (kadvec < 0.0) grad = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5, true);
+    l -= kadvec * grad;
+    double acc = 0.0;
+    acc += l;
+    return acc;
+}
+
+// F49=0 interface test (src/reinidisc_fsf.cpp:70-72).  In 2D the y
+// neighbours are ghost planes the reference never writes (zero).
+template <bool TWO_D>
+__device__ __forceinline__ bool same_sign(const double* __restrict__ f, long long c, long long sy,
+                                          long long sz) {
+    const double f0 = __ldg(f + c), xp = __ldg(f + c + 1), xm = __ldg(f + c - 1);
+    const double yp = TWO_D ? 0.0 : __ldg(f + c + sy), ym = TWO_D ? 0.0 : __ldg(f + c - sy);
+    const double zp = __ldg(f + c + sz), zm = __ldg(f + c - sz);
+    return (f0 >= 0.0 && xp >= 0.0 && xm >= 0.0 && yp >= 0.0 && ym >= 0.0 && zp >= 0.0 && zm >= 0.0) ||
+           (f0 < 0.0 && xp < 0.0 && xm < 0.0 && yp < 0.0 && ym < 0.0 && zp < 0.0 && zm < 0.0);
+}
+
+// Reinitialisation right-hand side at (i,j,k): src/reinidisc_f.cpp:58-127
+// (and the body of src/reinidisc_fsf.cpp:74-139).
+template <bool TWO_D>
+__device__ __forceinline__ double reini_L(const KGrid<double>& g, const double* __restrict__ f, long long c,
+                                          int i, int j, int k) {
+    const long long sy = g.L.sy, sz = g.L.sz;
+    const int ti = i + 5, tj = j + 5, tk = k + 5;
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    const double lsv = __ldg(f + c);
+    double lsSig = lsv / sqrt(lsv * lsv);
+    if (fabs(lsv) < 1.0e-8) lsSig = 1.0;
+
+    const double xmin = (lsv - __ldg(f + c - 1)) / __ldg(g.dxp[0] + ti - 1);
+    const double xplus = (__ldg(f + c + 1) - lsv) / __ldg(g.dxp[0] + ti);
+    if (xmin * lsSig > 0.0 && xplus * lsSig > -xmin * lsSig)
+        dx = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], ti, false);
+    if (xplus * lsSig < 0.0 && xmin * lsSig < -xplus * lsSig)
+        dx = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], ti, true);
+    if (xplus * lsSig > 0.0 && xmin * lsSig < 0.0) dx = 0.0;
+
+    if (!TWO_D) {
+        const double ymin = (lsv - __ldg(f + c - sy)) / __ldg(g.dxp[1] + tj - 1);
+        const double yplus = (__ldg(f + c + sy) - lsv) / __ldg(g.dxp[1] + tj);
+        if (ymin * lsSig > 0.0 && yplus * lsSig > -ymin * lsSig)
+            dy = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], tj, false);
+        if (yplus * lsSig < 0.0 && ymin * lsSig < -yplus * lsSig)
+            dy = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], tj, true);
+        if (yplus * lsSig > 0.0 && ymin * lsSig < 0.0) dy = 0.0;
+    }
+
+    const double zmin = (lsv - __ldg(f + c - sz)) / __ldg(g.dxp[2] + tk - 1);
+    const double zplus = (__ldg(f + c + sz) - lsv) / __ldg(g.dxp[2] + tk);
+    if (zmin * lsSig > 0.0 && zplus * lsSig > -zmin * lsSig)
+        dz = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], tk, false);
+    if (zplus * lsSig < 0.0 && zmin * lsSig < -zplus * lsSig)
+        dz = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], tk, true);
+    if (zplus * lsSig > 0.0 && zmin * lsSig < 0.0) dz = 0.0;
+
+    const double dnorm = sqrt(dx * dx + dy * dy + dz * dz);
+    double deltax;
+    if (TWO_D) deltax = (1.0 / 2.0) * (__ldg(g.dxn[0] + ti) + __ldg(g.dxn[2] + tk));
+    else deltax = (1.0 / 3.0) * (__ldg(g.dxn[0] + ti) + __ldg(g.dxn[1] + tj) + __ldg(g.dxn[2] + tk));
+    double sign = lsv / sqrt(lsv * lsv + dnorm * dnorm * deltax * deltax);
+    if (sign != sign) sign = 1.0;
+    return -(sign * dnorm - sign);
+}
+
+// Reinit pseudo time step of a cell (src/reini_RK3.cpp:150-160).
+template <bool TWO_D>
+__device__ __forceinline__ double reini_dt(const KGrid<double>& g, int i, int j, int k) {
+    const double a = __ldg(g.dxp[0] + i + 5), c = __ldg(g.dxp[2] + k + 5);
+    if (TWO_D) return g.f43 * (a < c ? a : c);
+    const double b = __ldg(g.dxp[1] + j + 5);
+    const double m = a < b ? a : b;
+    return g.f43 * (m < c ? m : c);
+}
+
+}  // namespace f64
+}  // namespace r3d

@@ -1,0 +1,43 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+GOLDEN_CASES = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load_golden(name):
+    import numpy as np
+    with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(scope="session")
+def port_lib():
+    """The C restatement oracle, built on demand (test infrastructure)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile")], check=True, cwd=ROOT)
+    from oracle.bindings import PortOracle
+    PortOracle.lib()
+    return PortOracle
+
+
+def velocity_at(g, t):
+    """Stored velocity of a golden case at time t (the vortex cases scale the
+    spatial field by cos(pi t / 3), as tests/golden/make_golden.py did)."""
+    import numpy as np
+    u, v, w = g["u"], g["v"], g["w"]
+    if str(g["vel_scale"]) == "vortex":
+        f = np.cos(np.pi * t / 3.0)
+        u, v, w = u * f, v * f, w * f
+    return np.ascontiguousarray(u), np.ascontiguousarray(v), np.ascontiguousarray(w)

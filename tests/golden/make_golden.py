@@ -1,0 +1,125 @@
+"""Generates the golden vectors in this folder by running the REFERENCE's own
+level-set code (oracle/_ref, built by oracle/Makefile.ref from the reference
+sources) on small seeded cases.  One process per case: the reference keeps
+its grid tables in static members.
+
+    make -f oracle/Makefile.ref REF=/root/reference -j8
+    python tests/golden/make_golden.py
+
+Each case file holds the inputs (node coordinates, control flags, phi, u, v,
+w in the reference's padded layout) and the reference's outputs: WENO node
+tables and metrics, the convection operator L, the reinitialisation operator
+L, the wall ghost fill, the CFL time step, one full level-set step (or a
+short trajectory with the time step recomputed before every step) and the
+volume sums after it.
+"""
+import math
+import multiprocessing as mp
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+
+def stretched(n, amp):
+    from oracle.bindings import uniform_nodes
+    x = uniform_nodes(n)
+    return x + amp * np.sin(2 * np.pi * x) / n
+
+
+def random_case(name, nx, ny, nz, f49, stretch, seed):
+    rng = np.random.default_rng(seed)
+    xn, yn, zn = stretched(nx, stretch), stretched(ny, stretch), stretched(nz, stretch)
+    shape = (nx + 6, ny + 6, nz + 6)
+    ii = 0.5 * (xn[2:-3] + xn[3:-2])
+    jj = 0.5 * (yn[2:-3] + yn[3:-2])
+    kk = 0.5 * (zn[2:-3] + zn[3:-2])
+    X, Y, Z = np.meshgrid(ii, jj, kk, indexing="ij")
+    if ny == 1:
+        phi = np.sqrt((X - 0.5) ** 2 + (Z - 0.55) ** 2) - 0.23
+    else:
+        phi = np.sqrt((X - 0.5) ** 2 + (Y - 0.45) ** 2 + (Z - 0.55) ** 2) - 0.23
+    phi = phi + 0.01 * rng.standard_normal(shape)
+    phi[1 + 3, :, 2 + 3] = 0.0  # exact zeros exercise the sign branches
+    u = rng.standard_normal(shape)
+    v = rng.standard_normal(shape)
+    w = rng.standard_normal(shape)
+    u[::3] = 0.0  # exact zero velocity: the advec == 0 branch
+    return dict(name=name, nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w,
+                f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.125, steps=1, vel_scale=None)
+
+
+def setup_case(name, which, n, steps):
+    from reef3d_b200 import setups
+    c = setups.slotted_disk(n) if which == "disk" else setups.vortex3d(n)
+    d = dict(name=name, nx=c.nx, ny=c.ny, nz=c.nz, xn=c.xn, yn=c.yn, zn=c.zn, phi=c.phi, u=c.u, v=c.v,
+             w=c.w, f43=c.f43, f44=c.f44, f45=c.f45, f49=c.f49, n47=c.n47, steps=steps,
+             vel_scale="vortex" if which == "vortex" else None)
+    return d
+
+
+CASES = [
+    lambda: random_case("box3d_uniform_f49_1", 9, 7, 8, 1, 0.0, 1),
+    lambda: random_case("box3d_stretched_f49_0", 9, 7, 8, 0, 0.3, 2),
+    lambda: random_case("box2d_uniform_f49_1", 12, 1, 10, 1, 0.0, 3),
+    lambda: random_case("box2d_stretched_f49_0", 12, 1, 10, 0, 0.3, 4),
+    lambda: setup_case("vortex3d_n12_3steps", "vortex", 12, 3),
+    lambda: setup_case("slotted2d_n24_3steps", "disk", 24, 3),
+]
+
+
+def run_case(idx):
+    from oracle.bindings import RefOracle
+    c = CASES[idx]()
+    nx, ny, nz = c["nx"], c["ny"], c["nz"]
+    ref = RefOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
+                    f49=c["f49"])
+    out = {k: c[k] for k in ("nx", "ny", "nz", "xn", "yn", "zn", "phi", "u", "v", "w", "f43", "f44", "f45",
+                              "f49", "n47", "steps")}
+    for a, n in enumerate((nx, ny, nz)):
+        qf, cf, isf = ref.weno_tables(a, n + 8)
+        out[f"qf{a}"], out[f"cf{a}"], out[f"isf{a}"] = qf, cf, isf
+        for w, name in ((a, "dxn"), (a + 3, "dxp")):
+            out[f"{name}{a}"] = ref.metric(w, n + 11)
+    out["psi"] = ref.psi
+    out["vel_scale"] = np.array(c["vel_scale"] or "none")
+    phi, u, v, w = c["phi"], c["u"], c["v"], c["w"]
+    ref.set_state(phi, u, v, w)
+    out["weno_L"] = ref.weno_L(phi)
+    out["reinidisc_L"] = ref.reinidisc_L(phi)
+    out["ghost"] = ref.ghost_fill(phi)
+    T = 3.0
+    t = 0.0
+    traj, dts, vols = [], [], []
+    for s in range(c["steps"]):
+        if c["vel_scale"] == "vortex":
+            f = math.cos(math.pi * t / T)
+            ref.set_field(1, u * f)
+            ref.set_field(2, v * f)
+            ref.set_field(3, w * f)
+        dt = ref.cfl_dt(c["n47"])
+        ph = ref.step(dt)
+        traj.append(ph)
+        dts.append(dt)
+        vols.append(ref.volume())
+        t += dt
+    out["step_phi"] = np.array(traj)
+    out["step_dt"] = np.array(dts)
+    out["step_volume"] = np.array(vols)
+    np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), **out)
+    return c["name"]
+
+
+def main():
+    ctx = mp.get_context("spawn")
+    for i in range(len(CASES)):
+        with ctx.Pool(1) as pool:
+            print("wrote", pool.apply(run_case, (i,)))
+
+
+if __name__ == "__main__":
+    main()
