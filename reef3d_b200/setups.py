@@ -30,6 +30,15 @@ def _mesh(a, b, c):
     return np.meshgrid(a, b, c, indexing="ij")
 
 
+def _zero_y_ghosts(a):
+    """2D (ny == 1): the y ghost planes of the reference's padded field hold
+    zeros (nothing on the path writes them; the F49=0 reinitialisation test
+    reads them, src/reinidisc_fsf.cpp:70-72)."""
+    a[:, :3, :] = 0.0
+    a[:, 4:, :] = 0.0
+    return a
+
+
 class Case:
     """Grid, control flags and fields of one instance."""
 
@@ -93,6 +102,7 @@ def slotted_disk(n=128, cfl=0.1):
     xc, yc, zc = centres(xn), centres(yn), centres(zn)
     X, Y, Z = _mesh(xc, yc, zc)
     phi = slotted_disk_sdf(X, Z)
+    _zero_y_ghosts(phi)
     _, _, Zu = _mesh(faces(xn), yc, zc)
     u = 2.0 * math.pi * (0.5 - Zu)
     Xw, _, _ = _mesh(xc, yc, faces(zn))
@@ -199,6 +209,8 @@ def random_instance(rng, n_edge_choices=None, two_d=None, name="ensemble", f44=2
     xc, yc, zc = centres(xn), centres(yn), centres(zn)
     X, Y, Z = _mesh(xc, yc, zc)
     phi = sphere_union_sdf(X, Y, Z, cs, rs, two_d)
+    if two_d:
+        _zero_y_ghosts(phi)
     Xu, Yu, Zu = _mesh(faces(xn), yc, zc)
     u = taylor_green(Xu, Yu, Zu, modes, 0, two_d)
     if two_d:
