@@ -1,0 +1,389 @@
+"""Benchmark of the level-set transport path (WENO5-HJ convection in TVD-RK3
+stages + PDE reinitialisation) on the 3D single-vortex deformation, 256^3
+cells, CFL 0.25, 2 reinitialisation pseudo-steps per step.
+
+One step = one physical time step over the whole grid: the FP64 CFL
+reduction, 3 fused convection stages, 2 x 3 fused reinitialisation stages
+and the FP64 volume integral, with the vortex velocity following the device
+clock (u(x,t) = u(x) cos(pi t / 3)).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun, one rank per GPU; every rank advances its own
+instance (replicas, no collective on the data path), `value` is the
+aggregate over ranks with the max-over-ranks device time.
+"""
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS_EDGE = 256
+METRIC = "level-set cell-updates/s (RK3+reinit), FP64 plain vs FP32 batched; p50/p99 latency"
+WORKLOAD = "3D single-vortex deformation 256^3, CFL 0.25, F44=2 reinit pseudo-steps, T=3"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--edge", type=int, default=N_CELLS_EDGE)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- CPU side
+def _ref_worker(args):
+    edge, steps, fast = args
+    from oracle.bindings import RefOracle
+    from reef3d_b200 import setups
+    c = setups.vortex3d(edge)
+    o = RefOracle(edge, edge, edge, c.xn, c.yn, c.zn, f43=c.f43, f44=c.f44, f45=c.f45, f49=c.f49, fast=fast)
+    o.set_state(c.phi, c.u, c.v, c.w)
+    dt = o.cfl_dt(c.n47)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(dt)
+    return time.perf_counter() - t0, edge ** 3 * steps
+
+
+def host_has_avx2_fma():
+    try:
+        flags = open("/proc/cpuinfo").read()
+        return " avx2" in flags and " fma" in flags
+    except OSError:
+        return False
+
+
+def reference_cpu(procs, edge, steps):
+    """The reference's own level-set step (oracle/_ref) on the host cores:
+    one single-threaded process per core (the reference's only parallel mode
+    is MPI), each advancing its own grid.  Returns (cell-updates/s, info)."""
+    from oracle.bindings import REF_LIB, REF_LIB_FAST
+    fast = host_has_avx2_fma() and os.path.exists(REF_LIB_FAST)
+    if not os.path.exists(REF_LIB) and not fast:
+        return None, {"unavailable": "oracle/_ref was not built (needs the reference sources)"}
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(edge, steps, fast)] * procs)
+    wall = time.perf_counter() - t0
+    slowest = max(r[0] for r in res)
+    cells = sum(r[1] for r in res)
+    return cells / slowest, {"cores": procs, "kind": "reference",
+                             "build": "-O3 -mavx2 -mfma" if fast else "-O2 -ffp-contract=off",
+                             "sample": f"{procs} processes x vortex {edge}^3 x {steps} steps (same per-cell work as "
+                                       f"256^3), slowest process timed; wall {wall:.1f}s"}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    edge = 96
+    steps_per = max(1, min(args.steps, 3))
+    rate, info = reference_cpu(procs, edge, steps_per)
+    base = {"metric": METRIC, "impl": "reference", "n_gpus": args.gpus, "steps": steps_per,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD, "edge": args.edge}}
+    if rate is None:
+        print(json.dumps({"impl": "reference", "unavailable": info["unavailable"]}))
+        return
+    base.update({"value": rate, "unit": "cell-updates/s",
+                 "ms_per_step": 1e3 * (N_CELLS_EDGE ** 3) / rate,
+                 "cpu_baseline": dict(value=rate, unit="cell-updates/s", **info),
+                 "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    print(json.dumps(base))
+
+
+# --------------------------------------------------------------- GPU side
+def device_time(ls, fn, reps):
+    import torch
+    s = torch.cuda.ExternalStream(ls.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ls.sync()
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps  # ms
+
+
+def make_instance(case, precision):
+    import reef3d_b200 as r3d
+    n = case.nx
+    ls = r3d.LevelSet(n, n, n, case.xn, case.yn, case.zn, precision=precision, **case.flags())
+    for f, a in ((r3d.PHI, case.phi), (r3d.U, case.u), (r3d.V, case.v), (r3d.W, case.w)):
+        ls.upload(f, a)
+    ls.set_velocity_period(3.0)
+    ls.set_time(0.0)
+    return ls
+
+
+def timed_steps(ls, steps, warmup, dist_ctx):
+    """W untimed steps, then K steps between barriers, device-timed with
+    CUDA events on the instance's stream; per-step events give p50/p99."""
+    import torch
+    s = torch.cuda.ExternalStream(ls.stream())
+    ls.run(warmup, adaptive=True)
+    ls.sync()
+    dist_ctx.barrier()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    c0 = ls.launch_count()
+    evs[0].record(s)
+    for k in range(steps):
+        ls.run(1, adaptive=True)
+        evs[k + 1].record(s)
+    evs[-1].synchronize()
+    torch.cuda.synchronize()
+    dist_ctx.barrier()
+    launches = ls.launch_count() - c0
+    per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    total = evs[0].elapsed_time(evs[-1])
+    return total, per, launches
+
+
+def stage_roofline(ls, cells, elem, peak_gbs, reps=20):
+    """Average device time of each fused stage kernel launched alone, and the
+    HBM roofline of the dominant one.  Algorithmic bytes per cell of a
+    stage: convection stage 2/3 reads phi^n, the stage input and u,v,w and
+    writes the output (6 words); reinit stage 2/3 reads f and the stage
+    input and writes the output (3 words)."""
+    import reef3d_b200 as r3d
+    ls.set_dt(ls.cfl_dt())
+    t_conv = device_time(ls, lambda: ls.stage(r3d.STAGE_CONVECTION, 2), reps)
+    t_rein = device_time(ls, lambda: ls.stage(r3d.STAGE_REINIT, 2), reps)
+    # one step runs 3 convection and 6 reinit stages
+    share_conv, share_rein = 3 * t_conv, 6 * t_rein
+    if share_rein >= share_conv:
+        name, t, words = "reinit_stage", t_rein, 3
+    else:
+        name, t, words = "convection_stage", t_conv, 6
+    alg = words * elem * cells
+    achieved = alg / (t * 1e-3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+            "frac": achieved / peak_gbs, "bytes_per_launch": alg, "ms_per_launch": t,
+            "conv_stage_ms": t_conv, "reinit_stage_ms": t_rein}
+
+
+def e2e_steps(case, precision, steps, warmup):
+    """Through the C-ABI with host buffers in the reference's layout: every
+    step uploads phi, u, v, w from pinned host memory, runs the step (CFL +
+    RK3 convection + reinitialisation + volume) and downloads phi."""
+    import torch
+
+    import reef3d_b200 as r3d
+    n = case.nx
+    shape = case.phi.shape
+    pinned = {}
+    for name, a in (("phi", case.phi), ("u", case.u), ("v", case.v), ("w", case.w)):
+        t = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        pinned[name] = t
+    out = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    ls = r3d.LevelSet(n, n, n, case.xn, case.yn, case.zn, precision=precision, **case.flags())
+    ids = (("phi", r3d.PHI), ("u", r3d.U), ("v", r3d.V), ("w", r3d.W))
+
+    def one():
+        for name, fid in ids:
+            ls.upload_ptr(fid, pinned[name].data_ptr())
+        ls.run(1, adaptive=True)
+        ls.download_ptr(r3d.PHI, out.data_ptr())
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one()
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    ls.close()
+    nbytes = pinned["phi"].numel() * 8
+    return n ** 3 * steps / el, 4 * nbytes, nbytes
+
+
+class DistCtx:
+    def __init__(self):
+        import torch
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if torch.cuda.is_available():
+            torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier(device_ids=[self.local])
+
+    def max(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+
+
+def run_ours(args):
+    import torch
+
+    import reef3d_b200 as r3d
+    from reef3d_b200 import setups
+
+    ctx = DistCtx()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    case = setups.vortex3d(args.edge)
+    cells = case.cells
+
+    # FP32 form (headline) -------------------------------------------------
+    ls32 = make_instance(case, r3d.FP32)
+    with ClockSampler(ctx.local) as clk:
+        total32, per32, launches32 = timed_steps(ls32, args.steps, args.warmup, ctx)
+    total32 = ctx.max(total32)
+    roof32 = stage_roofline(ls32, cells, 4, peak_gbs)
+    ls32.close()
+    # FP64 plain -----------------------------------------------------------
+    ls64 = make_instance(case, r3d.FP64)
+    total64, per64, launches64 = timed_steps(ls64, args.steps, args.warmup, ctx)
+    total64 = ctx.max(total64)
+    roof64 = stage_roofline(ls64, cells, 8, peak_gbs)
+    ls64.close()
+    # end to end through the C-ABI with host buffers ------------------------
+    e2e = None
+    if not args.no_e2e:
+        e2e_steps_n = max(2, min(args.steps, 10))
+        rate, h2d, d2h = e2e_steps(case, r3d.FP32, e2e_steps_n, 1)
+        e2e = {"value": rate * ctx.world, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps_n,
+               "path": "r3d_upload(phi,u,v,w) + r3d_ls_run(1) + r3d_download(phi), pinned host, FP32 form"}
+    cpu = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu:
+        rate, info = reference_cpu(min(os.cpu_count() or 1, 8), 96, 2)
+        if rate is not None:
+            cpu = dict(value=rate, unit="cell-updates/s", **info)
+        else:
+            cpu = info
+    value32 = cells * args.steps * ctx.world / (total32 * 1e-3)
+    value64 = cells * args.steps * ctx.world / (total64 * 1e-3)
+    out = {
+        "metric": METRIC, "value": value32, "unit": "cell-updates/s", "n_gpus": ctx.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "edge": args.edge, "cells_per_gpu": cells,
+                   "form": "FP32 stencils/RK, FP64 CFL/volume/interface band",
+                   "l2": "working set (phi, 2 stage buffers, u, v, w = 6 x 79 MB) larger than L2; no flush",
+                   "parallelism": f"replicas x{ctx.world}"},
+        "latency_ms": {"p50": float(np.percentile(per32, 50)), "p99": float(np.percentile(per32, 99)),
+                       "what": "per-step device time of the FP32 step"},
+        "fp64_plain": {"value": value64, "unit": "cell-updates/s", "ms_per_step": total64 / args.steps,
+                       "dtype": "f64", "p50_ms": float(np.percentile(per64, 50)),
+                       "p99_ms": float(np.percentile(per64, 99)), "roofline": roof64,
+                       "gpu_launches": launches64},
+        "fp32_over_fp64": value32 / value64,
+        "roofline": dict(roof32, traffic=None, peak_source=peak_src),
+        "gpu_launches": launches32,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    if ctx.rank == 0:
+        print(json.dumps(out))
+    ctx.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args, int(os.environ.get("RANK", "0")))
+        return
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

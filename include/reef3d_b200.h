@@ -132,6 +132,28 @@ int r3d_volume(r3d_handle* h, double* volume1, double* volume2);
  * (fused into the step's final stage).  Synchronous. */
 int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2);
 
+/* Factor applied to the stored face velocities by every convection stage
+ * and by r3d_cfl_dt (default 1, which leaves them bit-exact).  Lets a
+ * caller advance a velocity field u(x,t) = u(x) g(t) without re-uploading
+ * it; the reference multiplies the same way when it evaluates its analytic
+ * benchmark velocities (src/benchmark_vortex3D.cpp:77-95). */
+int r3d_set_velocity_scale(r3d_handle* h, double scale);
+/* With period T > 0 the factor follows the device clock:
+ * g = cos(pi t / T), recomputed after every step (0 turns it off). */
+int r3d_set_velocity_period(r3d_handle* h, double period);
+/* Device clock (the reference's p->simtime, advanced by dt every step,
+ * src/driver_loop_cfd.cpp:104). */
+int r3d_set_time(r3d_handle* h, double t);
+int r3d_get_time(r3d_handle* h, double* t);
+
+/* One fused RK stage on the device fields (stage 1..3): the convection
+ * stages of src/levelset_RK3.cpp:112-159 (phi -> WORK1 -> WORK2 -> phi) or
+ * the reinitialisation stages of src/reini_RK3.cpp:113-137, each with its
+ * wall ghost fill.  Used to time and test a single stage. */
+#define R3D_STAGE_CONVECTION 0
+#define R3D_STAGE_REINIT 1
+int r3d_stage(r3d_handle* h, int kind, int stage);
+
 /* Wait for the handle's stream. */
 int r3d_sync(r3d_handle* h);
 /* The handle's cudaStream_t, as void*. */

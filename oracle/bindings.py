@@ -21,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libreef3d_ref.so")
+REF_LIB_FAST = os.path.join(HERE, "_ref", "fast", "libreef3d_ref.so")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.c_int
@@ -155,10 +156,10 @@ class RefOracle:
     def available(cls):
         return os.path.exists(REF_LIB)
 
-    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1):
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False):
         if RefOracle._lib is not None:
             raise RuntimeError("the reference oracle holds one grid per process")
-        lib = ctypes.CDLL(REF_LIB)
+        lib = ctypes.CDLL(REF_LIB_FAST if fast else REF_LIB)
         lib.refls_init.argtypes = [_I, _I, _I, _D, _D, _D, _I, ctypes.c_double, ctypes.c_double, _I]
         lib.refls_padded_size.restype = ctypes.c_long
         lib.refls_set_field.argtypes = [_I, _D]

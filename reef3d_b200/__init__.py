@@ -22,6 +22,7 @@ R3D_OK, R3D_EINVAL, R3D_ENOMEM, R3D_EDEVICE, R3D_ETIMEOUT, R3D_ESTATE = 0, 1, 2,
 FP64, FP32 = 0, 1
 PHI, U, V, W, L, WORK1, WORK2 = range(7)
 LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
+STAGE_CONVECTION, STAGE_REINIT = 0, 1
 
 _ERRNAMES = {1: "EINVAL", 2: "ENOMEM", 3: "EDEVICE", 4: "ETIMEOUT", 5: "ESTATE"}
 
@@ -64,6 +65,11 @@ EXPORTS = {
     "r3d_ghost_fill": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_volume": ([_H, _D, _D], ctypes.c_int),
     "r3d_last_volume": ([_H, _D, _D], ctypes.c_int),
+    "r3d_set_velocity_scale": ([_H, ctypes.c_double], ctypes.c_int),
+    "r3d_set_velocity_period": ([_H, ctypes.c_double], ctypes.c_int),
+    "r3d_set_time": ([_H, ctypes.c_double], ctypes.c_int),
+    "r3d_get_time": ([_H, _D], ctypes.c_int),
+    "r3d_stage": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "r3d_sync": ([_H], ctypes.c_int),
     "r3d_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
@@ -220,6 +226,23 @@ class LevelSet:
         a, b = ctypes.c_double(), ctypes.c_double()
         _check(_lib.r3d_last_volume(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
         return a.value, b.value
+
+    def set_velocity_scale(self, scale):
+        _check(_lib.r3d_set_velocity_scale(self.h, scale), self.h)
+
+    def set_velocity_period(self, period):
+        _check(_lib.r3d_set_velocity_period(self.h, period), self.h)
+
+    def set_time(self, t):
+        _check(_lib.r3d_set_time(self.h, t), self.h)
+
+    def time(self):
+        v = ctypes.c_double()
+        _check(_lib.r3d_get_time(self.h, ctypes.byref(v)), self.h)
+        return v.value
+
+    def stage(self, kind, stage):
+        _check(_lib.r3d_stage(self.h, kind, stage), self.h)
 
     def sync(self):
         _check(_lib.r3d_sync(self.h), self.h)

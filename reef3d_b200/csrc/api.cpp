@@ -29,6 +29,7 @@ struct r3d_handle {
     size_t staging_bytes = 0;
     long long launches = 0;
     double dt_host = 0.0;
+    double period = 0.0;
     bool have_last_volume = false;
     std::string err;
 };
@@ -198,7 +199,7 @@ int enqueue_step(r3d_handle* h) {
             n += fp32(h) ? launch_reini_stage_f32(h->g32, f, s, h->S, vol, h->stream)
                          : launch_reini_stage_f64(h->g64, f, s, h->S, vol, h->stream);
         }
-    n += launch_volume_reduce(h->L, h->S, volume_blocks(h->L), h->stream);
+    n += launch_volume_reduce(h->L, h->S, volume_blocks(h->L), h->period, h->stream);
     h->launches += n;
     h->have_last_volume = true;
     return R3D_OK;
@@ -272,7 +273,10 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
     h->S.npartial = np;
     h->S.dt = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 64);
     h->S.vol = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 128);
+    h->S.t = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 160);
+    h->S.vscale = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 168);
     cudaMemsetAsync(h->S.vmax, 0, 256, h->stream);
+    launch_set_scalar(h->S.vscale, 1.0, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return bail(R3D_EDEVICE, std::string("initialisation: ") + cudaGetErrorString(e));
     *out = h;
@@ -388,8 +392,8 @@ int r3d_convection_L(r3d_handle* h, int field_in) {
         return fail(h, R3D_EINVAL, "convection input must be a level-set field");
     DeviceGuard dg(h->device);
     const Fields f = fields_of(h);
-    h->launches += fp32(h) ? launch_conv_L_f32(h->g32, h->field[field_in], f, h->stream)
-                           : launch_conv_L_f64(h->g64, h->field[field_in], f, h->stream);
+    h->launches += fp32(h) ? launch_conv_L_f32(h->g32, h->field[field_in], f, h->S, h->stream)
+                           : launch_conv_L_f64(h->g64, h->field[field_in], f, h->S, h->stream);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
@@ -440,6 +444,57 @@ int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2) {
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     if (volume1) *volume1 = v[0];
     if (volume2) *volume2 = v[1];
+    return R3D_OK;
+}
+
+int r3d_set_velocity_scale(r3d_handle* h, double scale) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!std::isfinite(scale)) return fail(h, R3D_EINVAL, "velocity scale must be finite");
+    DeviceGuard dg(h->device);
+    h->launches += launch_set_scalar(h->S.vscale, scale, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_set_velocity_period(r3d_handle* h, double period) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!(period >= 0.0) || !std::isfinite(period)) return fail(h, R3D_EINVAL, "period must be >= 0");
+    h->period = period;
+    return R3D_OK;
+}
+
+int r3d_set_time(r3d_handle* h, double t) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!std::isfinite(t)) return fail(h, R3D_EINVAL, "time must be finite");
+    DeviceGuard dg(h->device);
+    h->launches += launch_set_scalar(h->S.t, t, h->stream);
+    if (h->period > 0.0) h->launches += launch_set_scalar(h->S.vscale, std::cos(3.141592653589793 * t / h->period), h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_get_time(r3d_handle* h, double* t) {
+    if (!h || !t) return fail(h, R3D_EINVAL, "null argument");
+    DeviceGuard dg(h->device);
+    R3D_CUDA(h, cudaMemcpyAsync(t, h->S.t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
+int r3d_stage(r3d_handle* h, int kind, int stage) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if ((kind != R3D_STAGE_CONVECTION && kind != R3D_STAGE_REINIT) || stage < 1 || stage > 3)
+        return fail(h, R3D_EINVAL, "kind must be R3D_STAGE_CONVECTION or R3D_STAGE_REINIT, stage 1..3");
+    if (kind == R3D_STAGE_CONVECTION && !(h->dt_host > 0.0)) return fail(h, R3D_ESTATE, "no time step set");
+    DeviceGuard dg(h->device);
+    const Fields f = fields_of(h);
+    if (kind == R3D_STAGE_CONVECTION)
+        h->launches += fp32(h) ? launch_conv_stage_f32(h->g32, f, stage, h->S, false, h->stream)
+                               : launch_conv_stage_f64(h->g64, f, stage, h->S, false, h->stream);
+    else
+        h->launches += fp32(h) ? launch_reini_stage_f32(h->g32, f, stage, h->S, false, h->stream)
+                               : launch_reini_stage_f64(h->g64, f, stage, h->S, false, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
 

@@ -109,10 +109,12 @@ __global__ void vmax_kernel(Layout L, const T* __restrict__ u, const T* __restri
 // dt = N47 * MIN(1e10, 2/(sqrt(umax^2+vmax^2+wmax^2)/dx + sqrt(0/dx)))
 // (src/ietimestep.cpp:160-188 with maxF=maxG=maxH=0, evaluated at the
 // smallest cell length, where the reference's minimum over cells sits).
-__global__ void dt_kernel(const unsigned long long* vm, double dxmin, double n47, double* dt) {
-    const double umax = __longlong_as_double((long long)vm[0]);
-    const double vmax = __longlong_as_double((long long)vm[1]);
-    const double wmax = __longlong_as_double((long long)vm[2]);
+__global__ void dt_kernel(const unsigned long long* vm, const double* vscale, double dxmin, double n47, double* dt) {
+    // max |s*u| = |s| * max |u| exactly: rounding is monotone
+    const double sc = fabs(*vscale);
+    const double umax = sc * __longlong_as_double((long long)vm[0]);
+    const double vmax = sc * __longlong_as_double((long long)vm[1]);
+    const double wmax = sc * __longlong_as_double((long long)vm[2]);
     double cu = 1.0e10;
     const double cand = 2.0 / ((sqrt(umax * umax + vmax * vmax + wmax * wmax)) / dxmin + sqrt((4.0 * fabs(0.0)) / dxmin));
     cu = cu < cand ? cu : cand;
@@ -121,7 +123,8 @@ __global__ void dt_kernel(const unsigned long long* vm, double dxmin, double n47
 
 // --------------------------------------------------------------- volume
 // Second pass: one block sums the per-block partials in a fixed order.
-__global__ void volume_reduce_kernel(const double* __restrict__ partial, long long n, double* out) {
+__global__ void volume_reduce_kernel(const double* __restrict__ partial, long long n, double* out, double* t,
+                                     double* vscale, const double* dt, double period) {
     __shared__ double sa[1024], sb[1024];
     double a = 0.0, b = 0.0;
     for (long long t = threadIdx.x; t < n; t += blockDim.x) {
@@ -138,7 +141,14 @@ __global__ void volume_reduce_kernel(const double* __restrict__ partial, long lo
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) { out[0] = sa[0]; out[1] = sb[0]; }
+    if (threadIdx.x == 0) {
+        out[0] = sa[0];
+        out[1] = sb[0];
+        if (t) {
+            *t += *dt;
+            if (period > 0.0) *vscale = cos(3.141592653589793 * *t / period);
+        }
+    }
 }
 
 // Standalone volume of a field (first pass), one block per (j,k) row group.
@@ -213,12 +223,12 @@ int launch_cfl(const Layout& L, const void* u, const void* v, const void* w, boo
     else
         vmax_kernel<double><<<grid, block, 0, st>>>(L, static_cast<const double*>(u), static_cast<const double*>(v),
                                                     static_cast<const double*>(w), s.vmax);
-    dt_kernel<<<1, 1, 0, st>>>(s.vmax, dxmin, n47, s.dt);
+    dt_kernel<<<1, 1, 0, st>>>(s.vmax, s.vscale, dxmin, n47, s.dt);
     return 2;
 }
 
-int launch_volume_reduce(const Layout&, const Scratch& s, long long nblocks, cudaStream_t st) {
-    volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, nblocks, s.vol);
+int launch_volume_reduce(const Layout&, const Scratch& s, long long nblocks, double period, cudaStream_t st) {
+    volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, nblocks, s.vol, s.t, s.vscale, s.dt, period);
     return 1;
 }
 
@@ -231,7 +241,8 @@ int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const doub
     else
         volume_direct_kernel<double><<<grid, block, 0, st>>>(L, static_cast<const double*>(phi), dxn, dyn, dzn, psi,
                                                              s.partial);
-    volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.vol);
+    volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.vol, nullptr, nullptr, nullptr,
+                                             0.0);
     return 2;
 }
 

@@ -17,6 +17,7 @@ struct StageArgs32 {
     const float* v;
     const float* w;
     const double* dt;
+    const double* vscale;
     double* partial;
 };
 
@@ -28,10 +29,10 @@ __device__ __forceinline__ void load7(const float* __restrict__ f, long long c, 
 template <bool TWO_D, bool UNIFORM>
 __device__ __forceinline__ float conv_L(const KGrid<float>& g, const float* __restrict__ f,
                                         const float* __restrict__ u, const float* __restrict__ v,
-                                        const float* __restrict__ w, long long c, int i, int j, int k) {
+                                        const float* __restrict__ w, long long c, int i, int j, int k, float vs) {
     const long long sy = g.L.sy, sz = g.L.sz;
-    const float ia = 0.5f * (__ldg(u + c) + __ldg(u + c - 1));
-    const float ka = 0.5f * (__ldg(w + c) + __ldg(w + c - sz));
+    const float ia = 0.5f * vs * (__ldg(u + c) + __ldg(u + c - 1));
+    const float ka = 0.5f * vs * (__ldg(w + c) + __ldg(w + c - sz));
     float fv[7];
     float l = 0.0f;
     if (ia != 0.0f) {
@@ -41,7 +42,7 @@ __device__ __forceinline__ float conv_L(const KGrid<float>& g, const float* __re
         l -= ia * d;
     }
     if (!TWO_D) {
-        const float ja = 0.5f * (__ldg(v + c) + __ldg(v + c - sy));
+        const float ja = 0.5f * vs * (__ldg(v + c) + __ldg(v + c - sy));
         if (ja != 0.0f) {
             load7(f, c, sy, fv);
             const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ja < 0.0f, g.rh[1], g.eps_u * g.h[1] * g.h[1])
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, Stag
             Lc = reini_L<TWO_D, UNIFORM>(g, a.fs, c, i, j, k);
             dtc = reini_dt32<TWO_D>(g, i, j, k);
         } else {
-            Lc = conv_L<TWO_D, UNIFORM>(g, a.fs, a.u, a.v, a.w, c, i, j, k);
+            Lc = conv_L<TWO_D, UNIFORM>(g, a.fs, a.u, a.v, a.w, c, i, j, k, (float)*a.vscale);
             dtc = (float)*a.dt;
         }
         const float fn = a.fn[c];
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(kBX * kBY) operator_kernel32(KGrid<float> g, S
     if (i >= g.L.nx || j >= g.L.ny || k >= g.L.nz) return;
     const long long c = (long long)(k + g.L.gz) * g.L.sz + (long long)(j + g.L.gy) * g.L.sy + (i + g.L.gx);
     a.out[c] = REINI ? reini_L<TWO_D, UNIFORM>(g, a.fs, c, i, j, k)
-                     : conv_L<TWO_D, UNIFORM>(g, a.fs, a.u, a.v, a.w, c, i, j, k);
+                     : conv_L<TWO_D, UNIFORM>(g, a.fs, a.u, a.v, a.w, c, i, j, k, (float)*a.vscale);
 }
 
 dim3 grid_of32(const Layout& L) {
@@ -256,6 +257,7 @@ StageArgs32 args32(const Fields& f, int stage, const Scratch& s) {
     a.v = static_cast<const float*>(f.v);
     a.w = static_cast<const float*>(f.w);
     a.dt = s.dt;
+    a.vscale = s.vscale;
     a.partial = s.partial;
     return a;
 }
@@ -289,8 +291,9 @@ static void launch_op(const KGrid<float>& g, const StageArgs32& a, cudaStream_t 
     }
 }
 
-int launch_conv_L_f32(const KGrid<float>& g, const void* in, const Fields& f, cudaStream_t st) {
+int launch_conv_L_f32(const KGrid<float>& g, const void* in, const Fields& f, const Scratch& s, cudaStream_t st) {
     StageArgs32 a{};
+    a.vscale = s.vscale;
     a.fs = static_cast<const float*>(in);
     a.out = static_cast<float*>(f.L);
     a.u = static_cast<const float*>(f.u);

@@ -19,6 +19,7 @@ struct StageArgs {
     const double* v;
     const double* w;
     const double* dt;   // device time step (convection stages)
+    const double* vscale;  // device factor of the stored velocities
     double* partial;    // volume partials, 2 per block
 };
 
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel(KGrid<double> g, Stage
                 Lc = 0.0;
             dtc = f64::reini_dt<TWO_D>(g, i, j, k);
         } else {
-            Lc = f64::conv_L<TWO_D>(g, a.fs, a.u, a.v, a.w, c, i, j, k);
+            Lc = f64::conv_L<TWO_D>(g, a.fs, a.u, a.v, a.w, c, i, j, k, *a.vscale);
             dtc = *a.dt;
         }
         const double fn = a.fn[c];
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kBX * kBY) operator_kernel(KGrid<double> g, St
         if (g.f49 == 1 || f64::same_sign<TWO_D>(a.fs, c, g.L.sy, g.L.sz)) Lc = f64::reini_L<TWO_D>(g, a.fs, c, i, j, k);
         else Lc = 0.0;
     } else {
-        Lc = f64::conv_L<TWO_D>(g, a.fs, a.u, a.v, a.w, c, i, j, k);
+        Lc = f64::conv_L<TWO_D>(g, a.fs, a.u, a.v, a.w, c, i, j, k, *a.vscale);
     }
     a.out[c] = Lc;
 }
@@ -174,6 +175,7 @@ StageArgs stage_args(const Fields& f, int stage, const Scratch& s) {
     a.v = static_cast<const double*>(f.v);
     a.w = static_cast<const double*>(f.w);
     a.dt = s.dt;
+    a.vscale = s.vscale;
     a.partial = s.partial;
     return a;
 }
@@ -196,8 +198,9 @@ int launch_reini_stage_f64(const KGrid<double>& g, const Fields& f, int stage, c
     return 1;
 }
 
-int launch_conv_L_f64(const KGrid<double>& g, const void* in, const Fields& f, cudaStream_t st) {
+int launch_conv_L_f64(const KGrid<double>& g, const void* in, const Fields& f, const Scratch& s, cudaStream_t st) {
     StageArgs a{};
+    a.vscale = s.vscale;
     a.fs = static_cast<const double*>(in);
     a.out = static_cast<double*>(f.L);
     a.u = static_cast<const double*>(f.u);

@@ -89,6 +89,8 @@ struct Scratch {
     unsigned long long* vmax;  // |u|,|v|,|w| maxima as ordered bit patterns
     double* dt;             // current time step (read by the stage kernels)
     double* vol;            // volume1, volume2
+    double* t;              // simulated time (advanced by each step)
+    double* vscale;         // factor applied to the stored face velocities
 };
 
 // ---- launchers (kernels_f64.cu / kernels_f32.cu / kernels_common.cu)
@@ -97,18 +99,20 @@ int launch_conv_stage_f64(const KGrid<double>& g, const Fields& f, int stage, co
                           bool volume, cudaStream_t st);
 int launch_reini_stage_f64(const KGrid<double>& g, const Fields& f, int stage, const Scratch& s,
                            bool volume, cudaStream_t st);
-int launch_conv_L_f64(const KGrid<double>& g, const void* in, const Fields& f, cudaStream_t st);
+int launch_conv_L_f64(const KGrid<double>& g, const void* in, const Fields& f, const Scratch& s, cudaStream_t st);
 int launch_reini_L_f64(const KGrid<double>& g, const void* in, const Fields& f, cudaStream_t st);
 
 int launch_conv_stage_f32(const KGrid<float>& g, const Fields& f, int stage, const Scratch& s,
                           bool volume, cudaStream_t st);
 int launch_reini_stage_f32(const KGrid<float>& g, const Fields& f, int stage, const Scratch& s,
                            bool volume, cudaStream_t st);
-int launch_conv_L_f32(const KGrid<float>& g, const void* in, const Fields& f, cudaStream_t st);
+int launch_conv_L_f32(const KGrid<float>& g, const void* in, const Fields& f, const Scratch& s, cudaStream_t st);
 int launch_reini_L_f32(const KGrid<float>& g, const void* in, const Fields& f, cudaStream_t st);
 
 long long volume_blocks(const Layout& L);
-int launch_volume_reduce(const Layout& L, const Scratch& s, long long nblocks, cudaStream_t st);
+// also advances the device clock by dt and, with period > 0, sets the
+// velocity factor cos(pi t / period)
+int launch_volume_reduce(const Layout& L, const Scratch& s, long long nblocks, double period, cudaStream_t st);
 int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const double* dxn,
                          const double* dyn, const double* dzn, double psi, const Scratch& s,
                          cudaStream_t st);

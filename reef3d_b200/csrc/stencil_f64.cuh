@@ -75,19 +75,21 @@ __device__ __forceinline__ double deriv(const double* __restrict__ f, long long 
 // cell-centre velocities of src/flux_HJ_CDS2.cpp:59-127 (2D: no y term,
 // src/flux_HJ_CDS2_2D.cpp).  Returned as the reference's a->L value
 // (0.0 + L).
+// The stored face velocities are multiplied by vs (1 leaves them exact).
 template <bool TWO_D>
 __device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* __restrict__ f,
                                          const double* __restrict__ u, const double* __restrict__ v,
-                                         const double* __restrict__ w, long long c, int i, int j, int k) {
+                                         const double* __restrict__ w, long long c, int i, int j, int k,
+                                         double vs) {
     const long long sy = g.L.sy, sz = g.L.sz;
-    const double iadvec = 0.5 * (__ldg(u + c) + __ldg(u + c - 1));
-    const double kadvec = 0.5 * (__ldg(w + c) + __ldg(w + c - sz));
+    const double iadvec = 0.5 * (vs * __ldg(u + c) + vs * __ldg(u + c - 1));
+    const double kadvec = 0.5 * (vs * __ldg(w + c) + vs * __ldg(w + c - sz));
     double grad = 0.0;
     if (iadvec > 0.0) grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, false);
     if (iadvec < 0.0) grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, true);
     double l = -iadvec * grad;
     if (!TWO_D) {
-        const double jadvec = 0.5 * (__ldg(v + c) + __ldg(v + c - sy));
+        const double jadvec = 0.5 * (vs * __ldg(v + c) + vs * __ldg(v + c - sy));
         grad = 0.0;
         if (jadvec > 0.0) grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, false);
         if (jadvec < 0.0) grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, true);

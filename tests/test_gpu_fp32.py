@@ -1,0 +1,79 @@
+"""FP32 form (FP32 stencils and RK stages, FP64 reductions, FP64
+re-anchoring of the interface band in the reinitialisation) against the
+FP64 path.
+
+Tolerances: one step stays within 2e-5 of the FP64 oracle in relative
+max-norm (FP32 rounding of O(1) values through ~10^3 operations); over a
+full deformation period the FP32 run's L1 shape error and relative volume
+change stay within 1% of the FP64 run's own (plus an absolute floor of 1e-6
+for quantities that are themselves near zero)."""
+import math
+
+import numpy as np
+import pytest
+
+import reef3d_b200 as r3d
+from reef3d_b200 import setups
+from test_gpu_parity import random_state, relmax
+from test_oracle_golden import interior
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dims,stretch", [((40, 33, 27), 0.0), ((64, 1, 48), 0.0), ((30, 26, 22), 0.3)])
+def test_one_step_close_to_fp64(port_lib, dims, stretch):
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=7)
+    if stretch:
+        xn = xn + stretch * np.sin(2 * np.pi * xn) / nx
+        zn = zn + stretch * np.sin(2 * np.pi * zn) / nz
+        if ny > 1:
+            yn = yn + stretch * np.sin(2 * np.pi * yn) / ny
+    flags = dict(f43=0.5, f44=2, f45=2.1, f49=1, n47=0.125)
+    o = port_lib(nx, ny, nz, xn, yn, zn, **flags)
+    dt = o.cfl_dt(u, v, w)
+    ref = o.step(phi, u, v, w, dt)
+    with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=r3d.FP32, **flags) as ls:
+        for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+            ls.upload(f, a)
+        ls.step(dt)  # the FP64 oracle's time step (FP32 storage rounds the velocities)
+        got = ls.download(r3d.PHI)
+    err = relmax(interior(got, nx, ny, nz), interior(ref, nx, ny, nz))
+    assert err <= 2e-5, err
+
+
+def heaviside(phi, eps):
+    return np.where(phi > eps, 1.0, np.where(phi < -eps, 0.0,
+                    0.5 * (1 + phi / eps + np.sin(np.pi * phi / eps) / np.pi)))
+
+
+def run_vortex(n, precision, period=3.0):
+    c = setups.vortex3d(n)
+    with r3d.LevelSet(n, n, n, c.xn, c.yn, c.zn, precision=precision, **c.flags()) as ls:
+        for f, a in ((r3d.PHI, c.phi), (r3d.U, c.u), (r3d.V, c.v), (r3d.W, c.w)):
+            ls.upload(f, a)
+        ls.set_velocity_period(period)
+        ls.set_time(0.0)
+        v0 = ls.volume()[0]
+        steps = 0
+        while ls.time() < period and steps < 20000:
+            ls.run(1, adaptive=True)
+            steps += 1
+        phi = ls.download(r3d.PHI)
+        v1 = ls.volume()[0]
+    return c, phi, v0, v1, steps
+
+
+def test_vortex_period_fp32_matches_fp64_accuracy():
+    n = 32
+    c, p64, a64, b64, s64 = run_vortex(n, r3d.FP64)
+    _, p32, a32, b32, s32 = run_vortex(n, r3d.FP32)
+    assert abs(s64 - s32) <= 1
+    h = 1.0 / n
+    i0 = interior(c.phi, n, n, n)
+    e64 = np.sum(np.abs(heaviside(interior(p64, n, n, n), 1.5 * h) - heaviside(i0, 1.5 * h))) * h ** 3
+    e32 = np.sum(np.abs(heaviside(interior(p32, n, n, n), 1.5 * h) - heaviside(i0, 1.5 * h))) * h ** 3
+    dv64 = abs(b64 - a64) / abs(a64)
+    dv32 = abs(b32 - a32) / abs(a32)
+    assert abs(e32 - e64) <= 0.01 * e64 + 1e-6, (e32, e64)
+    assert abs(dv32 - dv64) <= 0.01 * dv64 + 1e-6, (dv32, dv64)

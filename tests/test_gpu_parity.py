@@ -86,6 +86,9 @@ def random_state(nx, ny, nz, seed):
     else:
         phi = np.sqrt((X - 0.45) ** 2 + (Y - 0.5) ** 2 + (Z - 0.55) ** 2) - 0.27
     phi = np.ascontiguousarray(phi + 0.002 * rng.standard_normal(phi.shape))
+    if ny == 1:  # 2D: the y ghost planes hold zeros (never written on the path)
+        phi[:, :3, :] = 0.0
+        phi[:, 4:, :] = 0.0
     vel = [np.ascontiguousarray(0.5 + rng.standard_normal(phi.shape)) for _ in range(3)]
     return xn, yn, zn, phi, vel
 
