@@ -154,7 +154,22 @@ int r3d_get_time(r3d_handle* h, double* t);
 #define R3D_STAGE_REINIT 1
 int r3d_stage(r3d_handle* h, int kind, int stage);
 
-/* Wait for the handle's stream. */
+/* Execution options of an instance (no effect on results beyond the
+ * rounding of the FP32 form):
+ *  R3D_OPT_TILED  1 = TMA-tiled FP32x2 stage kernels on 3D uniform FP32
+ *                 grids (default), 0 = one-cell-per-thread kernels;
+ *                 reading it returns whether the tiled path is in use.
+ *  R3D_OPT_CHUNK  z-planes per CTA of the tiled kernels (default 16).
+ *  R3D_OPT_BAND64 1 = FP64 re-anchoring of interface-band cells in the FP32
+ *                 reinitialisation (default), 0 = FP32 everywhere. */
+#define R3D_OPT_TILED 0
+#define R3D_OPT_CHUNK 1
+#define R3D_OPT_BAND64 2
+int r3d_set_option(r3d_handle* h, int option, int value);
+int r3d_get_option(r3d_handle* h, int option, int* value);
+
+/* Wait for the handle's stream; R3D_ETIMEOUT if a bounded device wait of a
+ * kernel gave up since the last check. */
 int r3d_sync(r3d_handle* h);
 /* The handle's cudaStream_t, as void*. */
 int r3d_stream(r3d_handle* h, void** stream);

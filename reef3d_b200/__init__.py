@@ -23,6 +23,7 @@ FP64, FP32 = 0, 1
 PHI, U, V, W, L, WORK1, WORK2 = range(7)
 LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
 STAGE_CONVECTION, STAGE_REINIT = 0, 1
+OPT_TILED, OPT_CHUNK, OPT_BAND64 = 0, 1, 2
 
 _ERRNAMES = {1: "EINVAL", 2: "ENOMEM", 3: "EDEVICE", 4: "ETIMEOUT", 5: "ESTATE"}
 
@@ -70,6 +71,8 @@ EXPORTS = {
     "r3d_set_time": ([_H, ctypes.c_double], ctypes.c_int),
     "r3d_get_time": ([_H, _D], ctypes.c_int),
     "r3d_stage": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_set_option": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_get_option": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_sync": ([_H], ctypes.c_int),
     "r3d_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
@@ -243,6 +246,14 @@ class LevelSet:
 
     def stage(self, kind, stage):
         _check(_lib.r3d_stage(self.h, kind, stage), self.h)
+
+    def set_option(self, option, value):
+        _check(_lib.r3d_set_option(self.h, option, int(value)), self.h)
+
+    def get_option(self, option):
+        v = ctypes.c_int()
+        _check(_lib.r3d_get_option(self.h, option, ctypes.byref(v)), self.h)
+        return v.value
 
     def sync(self):
         _check(_lib.r3d_sync(self.h), self.h)

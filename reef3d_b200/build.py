@@ -27,11 +27,12 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contr
 UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", ["-fmad=true"]),
+    ("kernels_f32_tile.cu", ["-fmad=true"]),
     ("kernels_common.cu", ["-fmad=false"]),
     ("grid_metrics.cpp", []),
     ("api.cpp", []),
 ]
-HEADERS = ["r3d_internal.h", "stencil_f64.cuh", "stencil_f32.cuh"]
+HEADERS = ["r3d_internal.h", "stencil_f64.cuh", "stencil_f32.cuh", "tile_host.h"]
 
 
 def nvcc():

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "r3d_internal.h"
+#include "tile_host.h"
 
 using namespace r3d;
 
@@ -31,6 +32,12 @@ struct r3d_handle {
     double dt_host = 0.0;
     double period = 0.0;
     bool have_last_volume = false;
+    // TMA-tiled FP32 path (3D uniform grids)
+    bool tile_ok = false;
+    int use_tile = 1;
+    int kc = 16;
+    int band64 = 1;
+    CUtensorMap map[3];  // stage inputs: phi, WORK1, WORK2
     std::string err;
 };
 
@@ -184,24 +191,77 @@ struct DeviceGuard {
     ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
 };
 
-int enqueue_step(r3d_handle* h) {
+bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile; }
+
+TileArgs tile_args(r3d_handle* h, int stage) {
+    TileArgs a{};
+    a.L = h->L;
+    a.fn = static_cast<const float*>(h->field[R3D_PHI]);
+    a.out = static_cast<float*>(stage == 1 ? h->field[R3D_WORK1] : stage == 2 ? h->field[R3D_WORK2] : h->field[R3D_PHI]);
+    a.u = static_cast<const float*>(h->field[R3D_U]);
+    a.v = static_cast<const float*>(h->field[R3D_V]);
+    a.w = static_cast<const float*>(h->field[R3D_W]);
+    a.dt = h->S.dt;
+    a.vscale = h->S.vscale;
+    a.partial = h->S.partial;
+    a.err = h->S.err;
+    double hmin = h->M.h[0];
+    for (int d = 0; d < 3; ++d) {
+        a.rh[d] = (float)(1.0 / h->M.h[d]);
+        a.eps[d] = (float)(1.0e-6 * h->M.h[d] * h->M.h[d]);
+        hmin = std::fmin(hmin, h->M.h[d]);
+    }
+    a.dtr = (float)(h->desc.f43 * hmin);
+    a.deltax = (float)((1.0 / 3.0) * (h->M.h[0] + h->M.h[1] + h->M.h[2]));
+    a.f49 = h->desc.f49;
+    a.band64 = h->band64;
+    a.psi = h->M.psi;
+    a.cellvol = h->M.h[0] * h->M.h[1] * h->M.h[2];
+    a.kc = h->kc;
+    return a;
+}
+
+long long stage_launch(r3d_handle* h, bool reini, int s, bool vol) {
     const Fields f = fields_of(h);
+    if (tiled(h)) return launch_tile_stage(h->map[s - 1], tile_args(h, s), reini, s, vol, h->stream);
+    if (fp32(h))
+        return reini ? launch_reini_stage_f32(h->g32, f, s, h->S, vol, h->stream)
+                     : launch_conv_stage_f32(h->g32, f, s, h->S, vol, h->stream);
+    return reini ? launch_reini_stage_f64(h->g64, f, s, h->S, vol, h->stream)
+                 : launch_conv_stage_f64(h->g64, f, s, h->S, vol, h->stream);
+}
+
+long long volume_block_count(const r3d_handle* h) {
+    if (tiled(h)) {
+        const dim3 g = tile_grid(h->L, h->kc);
+        return (long long)g.x * g.y * g.z;
+    }
+    return volume_blocks(h->L);
+}
+
+int enqueue_step(r3d_handle* h) {
     const int f44 = h->desc.f44;
     long long n = 0;
-    for (int s = 1; s <= 3; ++s) {
-        const bool vol = (f44 == 0 && s == 3);
-        n += fp32(h) ? launch_conv_stage_f32(h->g32, f, s, h->S, vol, h->stream)
-                     : launch_conv_stage_f64(h->g64, f, s, h->S, vol, h->stream);
-    }
+    for (int s = 1; s <= 3; ++s) n += stage_launch(h, false, s, f44 == 0 && s == 3);
     for (int q = 0; q < f44; ++q)
-        for (int s = 1; s <= 3; ++s) {
-            const bool vol = (q == f44 - 1 && s == 3);
-            n += fp32(h) ? launch_reini_stage_f32(h->g32, f, s, h->S, vol, h->stream)
-                         : launch_reini_stage_f64(h->g64, f, s, h->S, vol, h->stream);
-        }
-    n += launch_volume_reduce(h->L, h->S, volume_blocks(h->L), h->period, h->stream);
+        for (int s = 1; s <= 3; ++s) n += stage_launch(h, true, s, q == f44 - 1 && s == 3);
+    n += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
     h->launches += n;
     h->have_last_volume = true;
+    return R3D_OK;
+}
+
+// Reads and clears the device error flag raised by a bounded wait.
+int check_device_flag(r3d_handle* h) {
+    int flag = 0;
+    if (cudaMemcpy(&flag, h->S.err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaError_t e = cudaGetLastError();
+        return cuda_fail(h, e, "reading the device error flag");
+    }
+    if (flag) {
+        cudaMemset(h->S.err, 0, sizeof(int));
+        return fail(h, R3D_ETIMEOUT, "a device wait gave up (TMA copy did not complete)");
+    }
     return R3D_OK;
 }
 
@@ -275,10 +335,19 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
     h->S.vol = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 128);
     h->S.t = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 160);
     h->S.vscale = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 168);
+    h->S.err = reinterpret_cast<int*>(reinterpret_cast<char*>(h->S.vmax) + 192);
     cudaMemsetAsync(h->S.vmax, 0, 256, h->stream);
     launch_set_scalar(h->S.vscale, 1.0, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return bail(R3D_EDEVICE, std::string("initialisation: ") + cudaGetErrorString(e));
+    if (fp32(h) && !h->L.two_d && h->M.uniform) {
+        std::string why;
+        const int ids[3] = {R3D_PHI, R3D_WORK1, R3D_WORK2};
+        bool ok = true;
+        for (int q = 0; q < 3 && ok; ++q)
+            ok = encode_plane_map(h->L, static_cast<const float*>(h->field[ids[q]]), &h->map[q], &why) == 0;
+        h->tile_ok = ok;
+    }
     *out = h;
     return R3D_OK;
 }
@@ -318,7 +387,7 @@ int r3d_download(r3d_handle* h, int field, double* host, int layout) {
     R3D_CUDA(h, cudaGetLastError());
     R3D_CUDA(h, cudaMemcpyAsync(host, h->staging, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
-    return R3D_OK;
+    return check_device_flag(h);
 }
 
 int r3d_set_dt(r3d_handle* h, double dt) {
@@ -377,11 +446,8 @@ int r3d_reinit(r3d_handle* h, int iters) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     DeviceGuard dg(h->device);
     const int it = iters > 0 ? iters : h->desc.f44;
-    const Fields f = fields_of(h);
     for (int q = 0; q < it; ++q)
-        for (int s = 1; s <= 3; ++s)
-            h->launches += fp32(h) ? launch_reini_stage_f32(h->g32, f, s, h->S, false, h->stream)
-                                   : launch_reini_stage_f64(h->g64, f, s, h->S, false, h->stream);
+        for (int s = 1; s <= 3; ++s) h->launches += stage_launch(h, true, s, false);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
@@ -487,13 +553,7 @@ int r3d_stage(r3d_handle* h, int kind, int stage) {
         return fail(h, R3D_EINVAL, "kind must be R3D_STAGE_CONVECTION or R3D_STAGE_REINIT, stage 1..3");
     if (kind == R3D_STAGE_CONVECTION && !(h->dt_host > 0.0)) return fail(h, R3D_ESTATE, "no time step set");
     DeviceGuard dg(h->device);
-    const Fields f = fields_of(h);
-    if (kind == R3D_STAGE_CONVECTION)
-        h->launches += fp32(h) ? launch_conv_stage_f32(h->g32, f, stage, h->S, false, h->stream)
-                               : launch_conv_stage_f64(h->g64, f, stage, h->S, false, h->stream);
-    else
-        h->launches += fp32(h) ? launch_reini_stage_f32(h->g32, f, stage, h->S, false, h->stream)
-                               : launch_reini_stage_f64(h->g64, f, stage, h->S, false, h->stream);
+    h->launches += stage_launch(h, kind == R3D_STAGE_REINIT, stage, false);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
@@ -502,7 +562,30 @@ int r3d_sync(r3d_handle* h) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     DeviceGuard dg(h->device);
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
-    return R3D_OK;
+    return check_device_flag(h);
+}
+
+int r3d_set_option(r3d_handle* h, int option, int value) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    switch (option) {
+        case R3D_OPT_TILED: h->use_tile = value ? 1 : 0; return R3D_OK;
+        case R3D_OPT_CHUNK:
+            if (value < 1 || value > 4096) return fail(h, R3D_EINVAL, "chunk must be 1..4096 planes");
+            h->kc = value;
+            return R3D_OK;
+        case R3D_OPT_BAND64: h->band64 = value ? 1 : 0; return R3D_OK;
+        default: return fail(h, R3D_EINVAL, "unknown option");
+    }
+}
+
+int r3d_get_option(r3d_handle* h, int option, int* value) {
+    if (!h || !value) return fail(h, R3D_EINVAL, "null argument");
+    switch (option) {
+        case R3D_OPT_TILED: *value = tiled(h) ? 1 : 0; return R3D_OK;
+        case R3D_OPT_CHUNK: *value = h->kc; return R3D_OK;
+        case R3D_OPT_BAND64: *value = h->band64; return R3D_OK;
+        default: return fail(h, R3D_EINVAL, "unknown option");
+    }
 }
 
 int r3d_stream(r3d_handle* h, void** stream) {

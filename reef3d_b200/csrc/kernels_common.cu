@@ -83,23 +83,35 @@ __global__ void ghost_kernel(Layout L, T* f) {
 // Non-negative doubles order like their bit patterns, so an atomicMax on the
 // bits is an exact, order-independent max.
 template <typename T>
-__global__ void vmax_kernel(Layout L, const T* __restrict__ u, const T* __restrict__ v, const T* __restrict__ w,
-                            unsigned long long* out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
+__global__ void __launch_bounds__(256) vmax_kernel(Layout L, const T* __restrict__ u, const T* __restrict__ v,
+                                                   const T* __restrict__ w, unsigned long long* out) {
+    // grid-stride over the (j,k) rows; one atomic per block and component
     double mu = 0.0, mv = 0.0, mw = 0.0;
-    if (i < L.nx) {
-        const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
-        if (i < L.nx - 1) mu = fabs((double)u[c]);
-        if (j < L.ny - 1) mv = fabs((double)v[c]);
-        if (k < L.nz - 1) mw = fabs((double)w[c]);
+    const long long rows = (long long)L.ny * L.nz;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+        const long long base = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + L.gx;
+        for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
+            if (i < L.nx - 1) mu = fmax(mu, fabs((double)u[base + i]));
+            if (j < L.ny - 1) mv = fmax(mv, fabs((double)v[base + i]));
+            if (k < L.nz - 1) mw = fmax(mw, fabs((double)w[base + i]));
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         mu = fmax(mu, __shfl_down_sync(0xffffffffu, mu, o));
         mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
         mw = fmax(mw, __shfl_down_sync(0xffffffffu, mw, o));
     }
-    if ((threadIdx.x & 31) == 0) {
+    __shared__ double s[3][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { s[0][warp] = mu; s[1][warp] = mv; s[2][warp] = mw; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+            mu = fmax(mu, s[0][q]);
+            mv = fmax(mv, s[1][q]);
+            mw = fmax(mw, s[2][q]);
+        }
         atomicMax(out + 0, (unsigned long long)__double_as_longlong(mu));
         atomicMax(out + 1, (unsigned long long)__double_as_longlong(mv));
         atomicMax(out + 2, (unsigned long long)__double_as_longlong(mw));
@@ -216,7 +228,8 @@ int launch_ghost_fill(const Layout& L, void* f, bool fp32, cudaStream_t st) {
 int launch_cfl(const Layout& L, const void* u, const void* v, const void* w, bool fp32, double dxmin, double n47,
                const Scratch& s, cudaStream_t st) {
     cudaMemsetAsync(s.vmax, 0, 3 * sizeof(unsigned long long), st);
-    const dim3 grid((L.nx + 127) / 128, L.ny, L.nz), block(128);
+    const long long rows = (long long)L.ny * L.nz;
+    const dim3 grid((unsigned)(rows < 1184 ? rows : 1184)), block(256);
     if (fp32)
         vmax_kernel<float><<<grid, block, 0, st>>>(L, static_cast<const float*>(u), static_cast<const float*>(v),
                                                    static_cast<const float*>(w), s.vmax);

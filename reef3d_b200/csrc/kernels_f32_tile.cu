@@ -1,0 +1,460 @@
+// FP32 form, 3D uniform grids: TMA-tiled fused stage kernels.
+//
+// A CTA owns a 64 x 8 (x, y) column of cells and marches a chunk of kc
+// z-planes.  Each plane of the stage input is staged once into shared memory
+// by one TMA box copy (72 x 14 floats: the tile plus its 3-cell x/y halo,
+// x rounded down to a 16-byte boundary) into an 8-slot ring guarded by
+// mbarriers; the z neighbours of a thread's cells live in a 7-plane register
+// window.  Every thread computes two x-adjacent cells with packed FP32x2
+// arithmetic (Blackwell FFMA2/FADD2/FMUL2).  The WENO5-HJ upwind side and
+// the Godunov branch of the reinitialisation are chosen with selects: the
+// plus-side derivative is the minus-side formula on the mirrored difference
+// sequence, so one evaluation per axis serves both sides.
+//
+// Waits on the mbarriers are bounded: on a timeout the kernel raises the
+// instance's error flag, waits (bounded) for its copies in flight and
+// returns; the host reports R3D_ETIMEOUT.
+#include <cuda.h>
+
+#include <string>
+
+#include "stencil_f32.cuh"
+#include "tile_host.h"
+
+namespace r3d {
+
+namespace {
+
+constexpr int kTX = 64, kTY = 8, kThreads = 256;
+constexpr int kBoxX = kTX + 8, kBoxY = kTY + 6;
+constexpr int kSlots = 8;
+constexpr int kSlotFloats = 1024;  // 72*14 = 1008 floats, padded to 4 KB
+constexpr unsigned kBoxBytes = kBoxX * kBoxY * 4;
+constexpr long long kSpin = 1ll << 22;
+
+// ------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (long long it = 0; it < kSpin; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// plain (non-multicast) tiled TMA load of one box into this CTA's shared memory
+__device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// ------------------------------------------------------------ packed math
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+__device__ __forceinline__ float2 sel2(bool cx, bool cy, float2 a, float2 b) {
+    return make_float2(cx ? a.x : b.x, cy ? a.y : b.y);
+}
+
+// WENO5 (Jiang-Peng) derivative times h from the undivided differences
+// d1..d5 of the minus-side upwind set; the plus side passes the mirrored
+// set (d1..d5 = D2, D1, D0, D-1, D-2).  Ideal weights 0.1/0.6/0.3 for the
+// stencils (d1,d2,d3)/(d2,d3,d4)/(d3,d4,d5).
+__device__ __forceinline__ float2 weno5_2(float2 d1, float2 d2, float2 d3, float2 d4, float2 d5, float2 eps) {
+    const float2 a1 = sub2(d3, d4), b1 = sub2(d5, d4);
+    const float2 b2 = sub2(d2, d3), b3 = sub2(d1, d2);
+    const float2 k43 = f2(4.0f / 3.0f);
+    // IS1 = (10/3 a1 + 11/3 b1) a1 + 4/3 b1^2, IS2 = (4/3 a1 - 5/3 b2) a1 + 4/3 b2^2,
+    // IS3 = (10/3 b2 - 11/3 b3) b2 + 4/3 b3^2  (a2 = -a1, a3 = -b2)
+    const float2 is1 = fma2(fma2(f2(10.0f / 3.0f), a1, mul2(f2(11.0f / 3.0f), b1)), a1, mul2(mul2(k43, b1), b1));
+    const float2 is2 = fma2(fma2(k43, a1, mul2(f2(-5.0f / 3.0f), b2)), a1, mul2(mul2(k43, b2), b2));
+    const float2 is3 = fma2(fma2(f2(10.0f / 3.0f), b2, mul2(f2(-11.0f / 3.0f), b3)), b2, mul2(mul2(k43, b3), b3));
+    const float2 r1 = rcp2(add2(is1, eps)), r2 = rcp2(add2(is2, eps)), r3 = rcp2(add2(is3, eps));
+    const float2 al1 = mul2(mul2(f2(0.3f), r1), r1);
+    const float2 al2 = mul2(mul2(f2(0.6f), r2), r2);
+    const float2 al3 = mul2(mul2(f2(0.1f), r3), r3);
+    const float2 inv = rcp2(add2(add2(al1, al2), al3));
+    // p1 = d4 + a1/3 - b1/6, p2 = d3 - a1/3 - b2/6, p3 = d2 + b3/3 - 11/6 b2
+    const float2 p1 = fma2(f2(-1.0f / 6.0f), b1, fma2(f2(1.0f / 3.0f), a1, d4));
+    const float2 p2 = fma2(f2(-1.0f / 6.0f), b2, fma2(f2(-1.0f / 3.0f), a1, d3));
+    const float2 p3 = fma2(f2(-11.0f / 6.0f), b2, fma2(f2(1.0f / 3.0f), b3, d2));
+    return mul2(fma2(al3, p3, fma2(al2, p2, mul2(al1, p1))), inv);
+}
+
+// Upwind derivative (times h) of an axis from 7 packed values f[0..6]
+// (f[3] the cells), plus side where `plus` is set per cell.
+__device__ __forceinline__ float2 deriv2(const float2* f, bool px, bool py, float2 eps) {
+    const float2 D0 = sub2(f[1], f[0]), D1 = sub2(f[2], f[1]), D2 = sub2(f[3], f[2]);
+    const float2 D3 = sub2(f[4], f[3]), D4 = sub2(f[5], f[4]), D5 = sub2(f[6], f[5]);
+    // minus: (D0..D4); plus (mirrored): (D5, D4, D3, D2, D1)
+    return weno5_2(sel2(px, py, D5, D0), sel2(px, py, D4, D1), sel2(px, py, D3, D2), sel2(px, py, D2, D3),
+                   sel2(px, py, D1, D4), eps);
+}
+
+// Reinitialisation right-hand side of one cell in FP64 from its FP32
+// stencils (the interface band), the reference's branch structure.
+__device__ double reini_cell_fp64(const float* fx, const float* fy, const float* fz, const TileArgs& a) {
+    double X[7], Y[7], Z[7];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) { X[m] = fx[m]; Y[m] = fy[m]; Z[m] = fz[m]; }
+    const double rh[3] = {a.rh[0], a.rh[1], a.rh[2]};
+    const double hh[3] = {1.0 / (rh[0] * rh[0]), 1.0 / (rh[1] * rh[1]), 1.0 / (rh[2] * rh[2])};
+    return f32::reini_rhs_uniform<double, false>(X, Y, Z, rh, hh, 1.0e-6, (double)a.deltax);
+}
+
+template <bool REINI, int STAGE, bool VOLUME>
+__global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
+    // shared memory: ring of kSlots plane boxes, 3 boxes for the planes
+    // below the chunk, then the mbarriers
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* slots = reinterpret_cast<float*>(smem_raw);
+    float* below = slots + kSlots * kSlotFloats;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(below + 3 * kSlotFloats);
+    uint64_t* xbar = bar + kSlots;
+    __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
+
+    const Layout& L = a.L;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int i0 = blockIdx.x * kTX + 2 * tx;
+    const int j = blockIdx.y * kTY + ty;
+    const int k0 = blockIdx.z * a.kc;
+    const int k1 = min(k0 + a.kc, L.nz);
+    const int xbox = blockIdx.x * kTX + L.gx - 4;  // 16-byte aligned x start
+    const int ybox = blockIdx.y * kTY + L.gy - 3;
+    const int plast = k1 + 2;  // last plane staged in the ring
+    const bool act0 = i0 < L.nx && j < L.ny;
+    const bool act1 = i0 + 1 < L.nx && j < L.ny;
+    const long long col = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
+    const int own = (ty + 3) * kBoxX + 2 * tx + 4;  // the thread's two cells in a box
+
+    int issued = k0 - 1;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kSlots + 3; ++s) mbar_init(bar + s, 1);
+        mbar_fence_init();
+        for (int m = 0; m < 3; ++m) {
+            mbar_expect_tx(xbar + m, kBoxBytes);
+            tma_load_3d(below + m * kSlotFloats, &tmap, xbar + m, xbox, ybox, k0 - 3 + m + L.gz);
+        }
+        for (int p = k0; p <= min(k0 + kSlots - 1, plast); ++p) {
+            const int s = (p - k0) % kSlots;
+            mbar_expect_tx(bar + s, kBoxBytes);
+            tma_load_3d(slots + s * kSlotFloats, &tmap, bar + s, xbox, ybox, p + L.gz);
+            issued = p;
+        }
+    }
+    __syncthreads();
+
+    // z window: planes k-3..k+3 of the thread's two cells
+    float2 zw[7];
+    bool ok = true;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        ok = ok && mbar_wait_bounded(xbar + m, 0);
+        zw[m] = *reinterpret_cast<const float2*>(below + m * kSlotFloats + own);
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int p = k0 + m;  // p <= k0 + 2 <= plast always
+        ok = ok && mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
+        zw[3 + m] = *reinterpret_cast<const float2*>(slots + ((p - k0) % kSlots) * kSlotFloats + own);
+    }
+
+    const float vs = (float)*a.vscale;
+    const float dtc = REINI ? a.dtr : (float)*a.dt;
+    float2 wprev = make_float2(0.f, 0.f);
+    if (!REINI && act0) {
+        const long long c = (long long)(k0 - 1 + L.gz) * L.sz + col;
+        wprev = act1 ? *reinterpret_cast<const float2*>(a.w + c) : make_float2(a.w[c], 0.f);
+    }
+    double vol_a = 0.0, vol_b = 0.0;
+
+    bool aborted = __syncthreads_or(!ok);
+    for (int k = k0; k < k1 && !aborted; ++k) {
+        const int p = k + 3;
+        ok = mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
+        zw[6] = *reinterpret_cast<const float2*>(slots + ((p - k0) % kSlots) * kSlotFloats + own);
+        const float* sl = slots + ((k - k0) % kSlots) * kSlotFloats;
+
+        // x stencil: 10 values of the row, columns 2tx .. 2tx+9
+        float xv[10];
+        {
+            const float* r = sl + (ty + 3) * kBoxX + 2 * tx;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const float2 t = *reinterpret_cast<const float2*>(r + 2 * q);
+                xv[2 * q] = t.x;
+                xv[2 * q + 1] = t.y;
+            }
+        }
+        float2 fx[7], fy[7];
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+            fx[m] = make_float2(xv[m + 1], xv[m + 2]);
+            fy[m] = *reinterpret_cast<const float2*>(sl + (ty + m) * kBoxX + 2 * tx + 4);
+        }
+        const float2 f0 = fy[3];
+        const long long c = (long long)(k + L.gz) * L.sz + col;
+
+        float2 Lc;
+        if (!REINI) {
+            float2 uc = make_float2(0.f, 0.f), vc = uc, vm = uc, wc = uc;
+            float um = 0.f;
+            if (act0) {
+                if (act1) {
+                    uc = *reinterpret_cast<const float2*>(a.u + c);
+                    vc = *reinterpret_cast<const float2*>(a.v + c);
+                    vm = *reinterpret_cast<const float2*>(a.v + c - L.sy);
+                    wc = *reinterpret_cast<const float2*>(a.w + c);
+                } else {
+                    uc.x = a.u[c];
+                    vc.x = a.v[c];
+                    vm.x = a.v[c - L.sy];
+                    wc.x = a.w[c];
+                }
+                um = a.u[c - 1];
+            }
+            const float2 h2 = f2(0.5f * vs);
+            const float2 ia = mul2(h2, add2(make_float2(um, uc.x), uc));
+            const float2 ja = mul2(h2, add2(vc, vm));
+            const float2 ka = mul2(h2, add2(wc, wprev));
+            wprev = wc;
+            const float2 gx = mul2(f2(a.rh[0]), deriv2(fx, ia.x < 0.f, ia.y < 0.f, f2(a.eps[0])));
+            const float2 gy = mul2(f2(a.rh[1]), deriv2(fy, ja.x < 0.f, ja.y < 0.f, f2(a.eps[1])));
+            const float2 gz = mul2(f2(a.rh[2]), deriv2(zw, ka.x < 0.f, ka.y < 0.f, f2(a.eps[2])));
+            Lc = mul2(f2(-1.f), fma2(ka, gz, fma2(ja, gy, mul2(ia, gx))));
+        } else {
+            // Godunov selection per axis (src/reinidisc_f.cpp:70-109)
+            const float sgx = fabsf(f0.x) < 1.0e-8f ? 1.f : (f0.x > 0.f ? 1.f : -1.f);
+            const float sgy = fabsf(f0.y) < 1.0e-8f ? 1.f : (f0.y > 0.f ? 1.f : -1.f);
+            const float2* ax[3] = {fx, fy, zw};
+            float2 g2 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float2* f = ax[d];
+                const float2 xm = mul2(sub2(f0, f[2]), f2(a.rh[d]));
+                const float2 xp = mul2(sub2(f[4], f0), f2(a.rh[d]));
+                const float msx = xm.x * sgx, psx = xp.x * sgx, msy = xm.y * sgy, psy = xp.y * sgy;
+                const bool c1x = msx > 0.f && psx > -msx, c2x = psx < 0.f && msx < -psx;
+                const bool c1y = msy > 0.f && psy > -msy, c2y = psy < 0.f && msy < -psy;
+                float2 g = mul2(f2(a.rh[d]), deriv2(f, c2x, c2y, f2(a.eps[d])));
+                g.x = (c1x || c2x) ? g.x : 0.f;
+                g.y = (c1y || c2y) ? g.y : 0.f;
+                g2 = fma2(g, g, g2);
+            }
+            const float2 dn = make_float2(sqrt_approx(g2.x), sqrt_approx(g2.y));
+            const float2 dl = f2(a.deltax);
+            const float2 den = fma2(mul2(mul2(dn, dn), dl), dl, mul2(f0, f0));
+            float2 sg = mul2(f0, make_float2(rsqrtf(den.x), rsqrtf(den.y)));
+            if (sg.x != sg.x) sg.x = 1.f;
+            if (sg.y != sg.y) sg.y = 1.f;
+            Lc = sub2(sg, mul2(sg, dn));  // -(S |grad| - S)
+            // interface band: the 7-point stencil changes sign
+            const bool posx = f0.x >= 0.f && fx[2].x >= 0.f && fx[4].x >= 0.f && fy[2].x >= 0.f && fy[4].x >= 0.f &&
+                              zw[2].x >= 0.f && zw[4].x >= 0.f;
+            const bool negx = f0.x < 0.f && fx[2].x < 0.f && fx[4].x < 0.f && fy[2].x < 0.f && fy[4].x < 0.f &&
+                              zw[2].x < 0.f && zw[4].x < 0.f;
+            const bool posy = f0.y >= 0.f && fx[2].y >= 0.f && fx[4].y >= 0.f && fy[2].y >= 0.f && fy[4].y >= 0.f &&
+                              zw[2].y >= 0.f && zw[4].y >= 0.f;
+            const bool negy = f0.y < 0.f && fx[2].y < 0.f && fx[4].y < 0.f && fy[2].y < 0.f && fy[4].y < 0.f &&
+                              zw[2].y < 0.f && zw[4].y < 0.f;
+            const bool bandx = !(posx || negx), bandy = !(posy || negy);
+            if (a.f49 == 0) {
+                if (bandx) Lc.x = 0.f;  // src/reinidisc_fsf.cpp:70-72
+                if (bandy) Lc.y = 0.f;
+            } else if (a.band64) {
+                if (bandx || bandy) {
+                    float X[7], Y[7], Z[7];
+                    if (bandx) {
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) { X[m] = fx[m].x; Y[m] = fy[m].x; Z[m] = zw[m].x; }
+                        Lc.x = (float)reini_cell_fp64(X, Y, Z, a);
+                    }
+                    if (bandy) {
+#pragma unroll
+                        for (int m = 0; m < 7; ++m) { X[m] = fx[m].y; Y[m] = fy[m].y; Z[m] = zw[m].y; }
+                        Lc.y = (float)reini_cell_fp64(X, Y, Z, a);
+                    }
+                }
+            }
+        }
+
+        // RK combine (src/levelset_RK3.cpp:121-156, src/reini_RK3.cpp:118-135)
+        float2 val;
+        const float2 sdl = fma2(f2(dtc), Lc, f0);  // stage input + dt L
+        if (STAGE == 1) {
+            val = sdl;
+        } else {
+            float2 fn = make_float2(0.f, 0.f);
+            if (act0) fn = act1 ? *reinterpret_cast<const float2*>(a.fn + c) : make_float2(a.fn[c], 0.f);
+            if (STAGE == 2) val = fma2(f2(0.75f), fn, mul2(f2(0.25f), sdl));
+            else val = fma2(f2(1.0f / 3.0f), fn, mul2(f2(2.0f / 3.0f), sdl));
+        }
+        if (act0) {
+            if (act1) *reinterpret_cast<float2*>(a.out + c) = val;
+            else a.out[c] = val.x;
+            // wall ghost copies (src/gc_neumann.cpp:29-54)
+            if (i0 == 0) { a.out[c - 1] = val.x; a.out[c - 2] = val.x; a.out[c - 3] = val.x; }
+            if (act1 && i0 + 1 == L.nx - 1) { a.out[c + 2] = val.y; a.out[c + 3] = val.y; a.out[c + 4] = val.y; }
+            if (!act1) { a.out[c + 1] = val.x; a.out[c + 2] = val.x; a.out[c + 3] = val.x; }
+            const int nw = act1 ? 2 : 1;
+            if (j == 0)
+                for (int q = 1; q <= 3; ++q)
+                    for (int e = 0; e < nw; ++e) a.out[c - q * L.sy + e] = e ? val.y : val.x;
+            if (j == L.ny - 1)
+                for (int q = 1; q <= 3; ++q)
+                    for (int e = 0; e < nw; ++e) a.out[c + q * L.sy + e] = e ? val.y : val.x;
+            if (k == 0)
+                for (int q = 1; q <= 3; ++q)
+                    for (int e = 0; e < nw; ++e) a.out[c - q * L.sz + e] = e ? val.y : val.x;
+            if (k == L.nz - 1)
+                for (int q = 1; q <= 3; ++q)
+                    for (int e = 0; e < nw; ++e) a.out[c + q * L.sz + e] = e ? val.y : val.x;
+            if (VOLUME) {
+                // smoothed Heaviside in FP64 (src/fluid_update_fsf.cpp:50-71)
+                const double PI_REF = 3.14159265359;
+                for (int e = 0; e < nw; ++e) {
+                    const double ph = e ? val.y : val.x;
+                    double H = 0.0;
+                    if (ph > a.psi) H = 1.0;
+                    if (ph < -a.psi) H = 0.0;
+                    if (fabs(ph) <= a.psi) H = 0.5 * (1.0 + ph / a.psi + (1.0 / PI_REF) * sin((PI_REF * ph) / a.psi));
+                    vol_a += a.cellvol * H;
+                    vol_b += a.cellvol * (1.0 - H);
+                }
+            }
+        }
+
+        // every thread is done with the box of plane k: refill its slot
+        aborted = __syncthreads_or(!ok);
+        if (!aborted && threadIdx.x == 0 && k + kSlots <= plast) {
+            const int pn = k + kSlots;
+            const int s = (pn - k0) % kSlots;
+            fence_proxy_async();
+            mbar_expect_tx(bar + s, kBoxBytes);
+            tma_load_3d(slots + s * kSlotFloats, &tmap, bar + s, xbox, ybox, pn + L.gz);
+            issued = pn;
+        }
+#pragma unroll
+        for (int m = 0; m < 6; ++m) zw[m] = zw[m + 1];
+    }
+
+    if (aborted) {
+        if (threadIdx.x == 0) {
+            atomicExch(a.err, 1);
+            // wait (bounded) for every copy still in flight before leaving
+            for (int m = 0; m < 3; ++m) mbar_wait_bounded(xbar + m, 0);
+            for (int p = k0; p <= issued; ++p) mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
+        }
+        return;
+    }
+    if (VOLUME) {
+        for (int o = 16; o > 0; o >>= 1) {
+            vol_a += __shfl_down_sync(0xffffffffu, vol_a, o);
+            vol_b += __shfl_down_sync(0xffffffffu, vol_b, o);
+        }
+        if (tx == 0) { red_a[ty] = vol_a; red_b[ty] = vol_b; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sa = 0.0, sb = 0.0;
+            for (int q = 0; q < kThreads / 32; ++q) { sa += red_a[q]; sb += red_b[q]; }
+            const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            a.partial[2 * b] = sa;
+            a.partial[2 * b + 1] = sb;
+        }
+    }
+}
+
+}  // namespace
+
+int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::string* why) {
+    using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeFn encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            if (why) *why = "cuTensorMapEncodeTiled unavailable";
+            return 1;
+        }
+        encode = reinterpret_cast<EncodeFn>(fn);
+    }
+    // strides must be multiples of 16 bytes and the base 16-byte aligned
+    if ((L.px * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) {
+        if (why) *why = "field not 16-byte aligned for TMA";
+        return 1;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)L.px, (cuuint64_t)L.py, (cuuint64_t)L.pz};
+    const cuuint64_t strides[2] = {(cuuint64_t)L.px * 4, (cuuint64_t)L.px * L.py * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)kBoxX, (cuuint32_t)kBoxY, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        if (why) *why = "cuTensorMapEncodeTiled failed";
+        return 1;
+    }
+    return 0;
+}
+
+size_t tile_smem_bytes() { return (size_t)(kSlots + 3) * kSlotFloats * 4 + 16 * sizeof(uint64_t); }
+
+dim3 tile_grid(const Layout& L, int kc) {
+    return dim3((L.nx + kTX - 1) / kTX, (L.ny + kTY - 1) / kTY, (L.nz + kc - 1) / kc);
+}
+
+int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume, cudaStream_t st) {
+    const dim3 grid = tile_grid(a.L, a.kc), block(kThreads);
+    const size_t sm = tile_smem_bytes();
+#define R3D_TL(R, S, V) tile_kernel<R, S, V><<<grid, block, sm, st>>>(map, a)
+    if (reini) {
+        if (stage == 1) { if (volume) R3D_TL(true, 1, true); else R3D_TL(true, 1, false); }
+        else if (stage == 2) { if (volume) R3D_TL(true, 2, true); else R3D_TL(true, 2, false); }
+        else { if (volume) R3D_TL(true, 3, true); else R3D_TL(true, 3, false); }
+    } else {
+        if (stage == 1) { if (volume) R3D_TL(false, 1, true); else R3D_TL(false, 1, false); }
+        else if (stage == 2) { if (volume) R3D_TL(false, 2, true); else R3D_TL(false, 2, false); }
+        else { if (volume) R3D_TL(false, 3, true); else R3D_TL(false, 3, false); }
+    }
+#undef R3D_TL
+    return 1;
+}
+
+}  // namespace r3d

@@ -91,6 +91,7 @@ struct Scratch {
     double* vol;            // volume1, volume2
     double* t;              // simulated time (advanced by each step)
     double* vscale;         // factor applied to the stored face velocities
+    int* err;               // set by a kernel whose bounded wait gave up
 };
 
 // ---- launchers (kernels_f64.cu / kernels_f32.cu / kernels_common.cu)
@@ -125,6 +126,11 @@ int launch_import(const Layout& L, const double* staging, int layout, void* dst,
 int launch_export(const Layout& L, const void* src, bool fp32, int layout, double* staging,
                   cudaStream_t st);
 int launch_zero(void* p, size_t bytes, cudaStream_t st);
+
+// TMA-tiled FP32 stage kernels (kernels_f32_tile.cu), 3D uniform grids
+struct TileArgs;
+size_t tile_smem_bytes();
+dim3 tile_grid(const Layout& L, int kc);
 int launch_set_scalar(double* dst, double value, cudaStream_t st);
 
 }  // namespace r3d

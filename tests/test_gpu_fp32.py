@@ -77,3 +77,52 @@ def test_vortex_period_fp32_matches_fp64_accuracy():
     dv32 = abs(b32 - a32) / abs(a32)
     assert abs(e32 - e64) <= 0.01 * e64 + 1e-6, (e32, e64)
     assert abs(dv32 - dv64) <= 0.01 * dv64 + 1e-6, (dv32, dv64)
+
+
+@pytest.mark.parametrize("dims,kc", [((70, 21, 19), 16), ((64, 8, 16), 16), ((130, 9, 33), 7), ((33, 40, 5), 1),
+                                     ((64, 64, 64), 64), ((65, 17, 40), 3)])
+@pytest.mark.parametrize("f49", [1, 0])
+def test_tiled_path_vs_fp64(port_lib, dims, kc, f49):
+    """The TMA-tiled FP32x2 kernels on ragged sizes and chunkings: one step
+    within the FP32 tolerance of the FP64 oracle, ghost layers included,
+    and within FP32 rounding of the one-cell-per-thread FP32 kernels."""
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=nx * ny + kc)
+    flags = dict(f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.125)
+    o = port_lib(nx, ny, nz, xn, yn, zn, **flags)
+    dt = o.cfl_dt(u, v, w)
+    ref = o.step(phi, u, v, w, dt)
+    from test_oracle_golden import visible_mask
+    m = visible_mask(nx, ny, nz)
+    out = {}
+    for tiled in (1, 0):
+        with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=r3d.FP32, **flags) as ls:
+            ls.set_option(r3d.OPT_TILED, tiled)
+            ls.set_option(r3d.OPT_CHUNK, kc)
+            assert ls.get_option(r3d.OPT_TILED) == tiled
+            for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+                ls.upload(f, a)
+            ls.step(dt)
+            out[tiled] = ls.download(r3d.PHI)
+            ls.sync()
+    err_t = relmax(out[1][m], ref[m])
+    err_u = relmax(out[0][m], ref[m])
+    assert err_t <= 2e-5 and err_u <= 2e-5, (err_t, err_u)
+    assert relmax(out[1][m], out[0][m]) <= 2e-5
+
+
+def test_tiled_volume_and_band64_switch():
+    c = setups.vortex3d(48)
+    vols = {}
+    for band in (1, 0):
+        with r3d.LevelSet(48, 48, 48, c.xn, c.yn, c.zn, precision=r3d.FP32, **c.flags()) as ls:
+            assert ls.get_option(r3d.OPT_TILED) == 1
+            ls.set_option(r3d.OPT_BAND64, band)
+            for f, a in ((r3d.PHI, c.phi), (r3d.U, c.u), (r3d.V, c.v), (r3d.W, c.w)):
+                ls.upload(f, a)
+            ls.run(5, adaptive=True)
+            fused = ls.last_volume()
+            direct = ls.volume()
+            assert abs(fused[0] - direct[0]) <= 1e-9 * abs(direct[0])
+            vols[band] = direct[0]
+    assert abs(vols[1] - vols[0]) <= 1e-4 * abs(vols[0])
