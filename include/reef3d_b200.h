@@ -154,6 +154,17 @@ int r3d_get_time(r3d_handle* h, double* t);
 #define R3D_STAGE_REINIT 1
 int r3d_stage(r3d_handle* h, int kind, int stage);
 
+/* Device-side initial fields of the ensemble and serving workloads (the role
+ * of the reference's analytic benchmark setups, src/benchmark_*.cpp):
+ * phi = union of nspheres signed-distance spheres (circles in the x-z plane
+ * for 2D grids), spheres[4q..4q+3] = centre x, y, z and radius; the stored
+ * velocities = sum of nmodes Taylor-Green modes, modes[2q] = integer
+ * wavenumber k, modes[2q+1] = amplitude A:
+ *   u = A sin(k pi x) cos(k pi y) cos(k pi z), v = -A cos(k pi x) sin(k pi y) cos(k pi z), w = 0
+ *   (2D: u = A sin(k pi x) cos(k pi z), w = -A cos(k pi x) sin(k pi z)),
+ * evaluated on every stored cell at the staggered positions.  Synchronous. */
+int r3d_init_spheres_tg(r3d_handle* h, int nspheres, const double* spheres, int nmodes, const double* modes);
+
 /* Execution options of an instance (no effect on results beyond the
  * rounding of the FP32 form):
  *  R3D_OPT_TILED  1 = TMA-tiled FP32x2 stage kernels on 3D uniform FP32
@@ -175,6 +186,37 @@ int r3d_sync(r3d_handle* h);
 int r3d_stream(r3d_handle* h, void** stream);
 /* Kernel launches issued on this handle since creation. */
 int r3d_launch_count(const r3d_handle* h, long long* count);
+
+/* ---------------------------------------------------------------- batches
+ * Many FP32 instances of uneven sizes (2D and 3D mixed) advanced together:
+ * one persistent launch per RK stage over a packed tile list of all members,
+ * the whole step captured in a CUDA graph.  The reference has no
+ * counterpart (it runs one grid per process, src/weno_nug_func.h:198-202);
+ * each member's step is levelset_RK3::start (src/levelset_RK3.cpp:103-172)
+ * with its own CFL time step (src/ietimestep.cpp:38-206), clock and volume.
+ * A member's results do not depend on the other members.  While an
+ * instance is a member, calls on its handle first wait for the batch. */
+typedef struct r3d_batch r3d_batch;
+int r3d_batch_create(r3d_batch** out);
+int r3d_batch_destroy(r3d_batch* b);
+const char* r3d_batch_last_error(const r3d_batch* b);
+int r3d_batch_add(r3d_batch* b, r3d_handle* h);
+int r3d_batch_remove(r3d_batch* b, r3d_handle* h);
+int r3d_batch_size(const r3d_batch* b, int* n);
+/* Tile rows (2, 4, 8: tiles of 32 x rows cells, 32*rows threads) and
+ * persistent CTAs per SM. */
+int r3d_batch_set_config(r3d_batch* b, int rows, int ctas_per_sm);
+int r3d_batch_get_config(const r3d_batch* b, int* rows, int* ctas_per_sm);
+/* Times the candidate configurations on the batch (state-preserving) and
+ * caches the best per size class, in memory and in cache_path (may be
+ * NULL); a cached class is reused without timing. */
+int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows, int* ctas_per_sm);
+int r3d_batch_use_graph(r3d_batch* b, int on);
+/* nsteps adaptive steps of every member; asynchronous on the batch stream. */
+int r3d_batch_step(r3d_batch* b, int nsteps);
+int r3d_batch_sync(r3d_batch* b);
+int r3d_batch_stream(r3d_batch* b, void** stream);
+int r3d_batch_launch_count(const r3d_batch* b, long long* count);
 
 #ifdef __cplusplus
 }

@@ -71,11 +71,27 @@ EXPORTS = {
     "r3d_set_time": ([_H, ctypes.c_double], ctypes.c_int),
     "r3d_get_time": ([_H, _D], ctypes.c_int),
     "r3d_stage": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_init_spheres_tg": ([_H, ctypes.c_int, _D, ctypes.c_int, _D], ctypes.c_int),
     "r3d_set_option": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "r3d_get_option": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_sync": ([_H], ctypes.c_int),
     "r3d_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "r3d_batch_create": ([ctypes.POINTER(_H)], ctypes.c_int),
+    "r3d_batch_destroy": ([_H], ctypes.c_int),
+    "r3d_batch_last_error": ([_H], ctypes.c_char_p),
+    "r3d_batch_add": ([_H, _H], ctypes.c_int),
+    "r3d_batch_remove": ([_H, _H], ctypes.c_int),
+    "r3d_batch_size": ([_H, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "r3d_batch_set_config": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_batch_get_config": ([_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "r3d_batch_autotune": ([_H, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+                           ctypes.c_int),
+    "r3d_batch_use_graph": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_batch_step": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_batch_sync": ([_H], ctypes.c_int),
+    "r3d_batch_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "r3d_batch_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
 }
 
 
@@ -247,6 +263,13 @@ class LevelSet:
     def stage(self, kind, stage):
         _check(_lib.r3d_stage(self.h, kind, stage), self.h)
 
+    def init_spheres_tg(self, spheres, modes):
+        """Device-side initial fields: spheres = [(cx, cy, cz, r), ...],
+        modes = [(k, A), ...] (see r3d_init_spheres_tg)."""
+        sp = np.ascontiguousarray(np.asarray(spheres, dtype=np.float64).reshape(-1, 4))
+        mo = np.ascontiguousarray(np.asarray(modes, dtype=np.float64).reshape(-1, 2))
+        _check(_lib.r3d_init_spheres_tg(self.h, sp.shape[0], _dp(sp), mo.shape[0], _dp(mo)), self.h)
+
     def set_option(self, option, value):
         _check(_lib.r3d_set_option(self.h, option, int(value)), self.h)
 
@@ -266,4 +289,83 @@ class LevelSet:
     def launch_count(self):
         c = ctypes.c_longlong()
         _check(_lib.r3d_launch_count(self.h, ctypes.byref(c)), self.h)
+        return c.value
+
+
+def _bcheck(rc, b=None):
+    if rc != R3D_OK:
+        msg = _lib.r3d_batch_last_error(b)
+        raise R3DError(rc, msg.decode() if msg else "")
+
+
+class Batch:
+    """Many FP32 instances advanced together (one persistent launch per RK
+    stage over all members, the step replayed from a CUDA graph)."""
+
+    def __init__(self):
+        load_library()
+        b = _H()
+        _bcheck(_lib.r3d_batch_create(ctypes.byref(b)))
+        self.b = b
+        self.members = []
+
+    def close(self):
+        if getattr(self, "b", None) is not None and _lib is not None:
+            _lib.r3d_batch_destroy(self.b)
+            self.b = None
+            self.members = []
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, ls):
+        _bcheck(_lib.r3d_batch_add(self.b, ls.h), self.b)
+        self.members.append(ls)
+
+    def remove(self, ls):
+        _bcheck(_lib.r3d_batch_remove(self.b, ls.h), self.b)
+        self.members.remove(ls)
+
+    def size(self):
+        n = ctypes.c_int()
+        _bcheck(_lib.r3d_batch_size(self.b, ctypes.byref(n)), self.b)
+        return n.value
+
+    def set_config(self, rows, ctas_per_sm):
+        _bcheck(_lib.r3d_batch_set_config(self.b, rows, ctas_per_sm), self.b)
+
+    def config(self):
+        r, c = ctypes.c_int(), ctypes.c_int()
+        _bcheck(_lib.r3d_batch_get_config(self.b, ctypes.byref(r), ctypes.byref(c)), self.b)
+        return r.value, c.value
+
+    def autotune(self, cache_path=None):
+        r, c = ctypes.c_int(), ctypes.c_int()
+        p = cache_path.encode() if cache_path else None
+        _bcheck(_lib.r3d_batch_autotune(self.b, p, ctypes.byref(r), ctypes.byref(c)), self.b)
+        return r.value, c.value
+
+    def use_graph(self, on):
+        _bcheck(_lib.r3d_batch_use_graph(self.b, 1 if on else 0), self.b)
+
+    def step(self, nsteps=1):
+        _bcheck(_lib.r3d_batch_step(self.b, nsteps), self.b)
+
+    def sync(self):
+        _bcheck(_lib.r3d_batch_sync(self.b), self.b)
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        _bcheck(_lib.r3d_batch_stream(self.b, ctypes.byref(s)), self.b)
+        return s.value
+
+    def launch_count(self):
+        c = ctypes.c_longlong()
+        _bcheck(_lib.r3d_batch_launch_count(self.b, ctypes.byref(c)), self.b)
         return c.value

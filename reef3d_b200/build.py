@@ -28,11 +28,13 @@ UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", ["-fmad=true"]),
     ("kernels_f32_tile.cu", ["-fmad=true"]),
+    ("kernels_batch.cu", ["-fmad=true"]),
     ("kernels_common.cu", ["-fmad=false"]),
     ("grid_metrics.cpp", []),
     ("api.cpp", []),
+    ("batch.cpp", []),
 ]
-HEADERS = ["r3d_internal.h", "stencil_f64.cuh", "stencil_f32.cuh", "tile_host.h"]
+HEADERS = ["r3d_internal.h", "stencil_f64.cuh", "stencil_f32.cuh", "tile_host.h", "cell_f32.cuh", "handle.h", "batch_internal.h"]
 
 
 def nvcc():

@@ -8,38 +8,11 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
-#include "r3d_internal.h"
-#include "tile_host.h"
+#include "handle.h"
 
 using namespace r3d;
-
-struct r3d_handle {
-    Layout L{};
-    r3d_grid_desc desc{};
-    HostMetrics M;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    void* field[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    double* metrics64 = nullptr;
-    float* metrics32 = nullptr;
-    KGrid<double> g64{};
-    KGrid<float> g32{};
-    Scratch S{};
-    double* staging = nullptr;
-    size_t staging_bytes = 0;
-    long long launches = 0;
-    double dt_host = 0.0;
-    double period = 0.0;
-    bool have_last_volume = false;
-    // TMA-tiled FP32 path (3D uniform grids)
-    bool tile_ok = false;
-    int use_tile = 1;
-    int kc = 16;
-    int band64 = 1;
-    CUtensorMap map[3];  // stage inputs: phi, WORK1, WORK2
-    std::string err;
-};
 
 namespace {
 
@@ -185,9 +158,15 @@ size_t host_count(const r3d_handle* h, int layout) {
     return (size_t)h->L.nx * h->L.ny * h->L.nz;
 }
 
+// Makes the instance's device current for the call; if the instance is a
+// batch member, its work queued on the batch's stream completes first.
 struct DeviceGuard {
     int prev = 0;
-    explicit DeviceGuard(int dev) { cudaGetDevice(&prev); if (prev != dev) cudaSetDevice(dev); }
+    DeviceGuard(int dev, cudaStream_t batch = nullptr) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+        if (batch) cudaStreamSynchronize(batch);
+    }
     ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
 };
 
@@ -364,7 +343,7 @@ int r3d_upload(r3d_handle* h, int field, const double* host, int layout) {
     if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
     if (layout != R3D_LAYOUT_REEF3D && layout != R3D_LAYOUT_DENSE) return fail(h, R3D_EINVAL, "bad layout");
     if (!host) return fail(h, R3D_EINVAL, "null host pointer");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     if (int rc = ensure_staging(h)) return rc;
     const size_t n = host_count(h, layout);
     R3D_CUDA(h, cudaMemcpyAsync(h->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -379,7 +358,7 @@ int r3d_download(r3d_handle* h, int field, double* host, int layout) {
     if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
     if (layout != R3D_LAYOUT_REEF3D && layout != R3D_LAYOUT_DENSE) return fail(h, R3D_EINVAL, "bad layout");
     if (!host) return fail(h, R3D_EINVAL, "null host pointer");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     if (int rc = ensure_staging(h)) return rc;
     const size_t n = host_count(h, layout);
     if (layout == R3D_LAYOUT_REEF3D) R3D_CUDA(h, cudaMemsetAsync(h->staging, 0, n * sizeof(double), h->stream));
@@ -393,7 +372,7 @@ int r3d_download(r3d_handle* h, int field, double* host, int layout) {
 int r3d_set_dt(r3d_handle* h, double dt) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, R3D_EINVAL, "dt must be positive and finite");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     h->dt_host = dt;
     h->launches += launch_set_scalar(h->S.dt, dt, h->stream);
     R3D_CUDA(h, cudaGetLastError());
@@ -402,7 +381,7 @@ int r3d_set_dt(r3d_handle* h, double dt) {
 
 int r3d_cfl_dt(r3d_handle* h, double* dt) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h), h->M.dxmin_cfl,
                               h->desc.n47, h->S, h->stream);
     R3D_CUDA(h, cudaGetLastError());
@@ -416,7 +395,7 @@ int r3d_cfl_dt(r3d_handle* h, double* dt) {
 
 int r3d_ls_step(r3d_handle* h, double dt) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     if (dt > 0.0) {
         if (int rc = r3d_set_dt(h, dt)) return rc;
     } else if (!(h->dt_host > 0.0)) {
@@ -430,7 +409,7 @@ int r3d_ls_step(r3d_handle* h, double dt) {
 int r3d_ls_run(r3d_handle* h, int nsteps, int adaptive) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (nsteps < 0) return fail(h, R3D_EINVAL, "nsteps must be >= 0");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     if (!adaptive && !(h->dt_host > 0.0)) return fail(h, R3D_ESTATE, "no time step set");
     for (int n = 0; n < nsteps; ++n) {
         if (adaptive)
@@ -444,7 +423,7 @@ int r3d_ls_run(r3d_handle* h, int nsteps, int adaptive) {
 
 int r3d_reinit(r3d_handle* h, int iters) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     const int it = iters > 0 ? iters : h->desc.f44;
     for (int q = 0; q < it; ++q)
         for (int s = 1; s <= 3; ++s) h->launches += stage_launch(h, true, s, false);
@@ -456,7 +435,7 @@ int r3d_convection_L(r3d_handle* h, int field_in) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (field_in != R3D_PHI && field_in != R3D_WORK1 && field_in != R3D_WORK2)
         return fail(h, R3D_EINVAL, "convection input must be a level-set field");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     const Fields f = fields_of(h);
     h->launches += fp32(h) ? launch_conv_L_f32(h->g32, h->field[field_in], f, h->S, h->stream)
                            : launch_conv_L_f64(h->g64, h->field[field_in], f, h->S, h->stream);
@@ -468,7 +447,7 @@ int r3d_reinidisc_L(r3d_handle* h, int field_in) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (field_in != R3D_PHI && field_in != R3D_WORK1 && field_in != R3D_WORK2)
         return fail(h, R3D_EINVAL, "reinitialisation input must be a level-set field");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     const Fields f = fields_of(h);
     h->launches += fp32(h) ? launch_reini_L_f32(h->g32, h->field[field_in], f, h->stream)
                            : launch_reini_L_f64(h->g64, h->field[field_in], f, h->stream);
@@ -479,7 +458,7 @@ int r3d_reinidisc_L(r3d_handle* h, int field_in) {
 int r3d_ghost_fill(r3d_handle* h, int field) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_ghost_fill(h->L, h->field[field], fp32(h), h->stream);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
@@ -487,7 +466,7 @@ int r3d_ghost_fill(r3d_handle* h, int field) {
 
 int r3d_volume(r3d_handle* h, double* volume1, double* volume2) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     const double* dxn = h->g64.dxn[0];
     const double* dyn = h->g64.dxn[1];
     const double* dzn = h->g64.dxn[2];
@@ -504,7 +483,7 @@ int r3d_volume(r3d_handle* h, double* volume1, double* volume2) {
 int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (!h->have_last_volume) return fail(h, R3D_ESTATE, "no step has run yet");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     double v[2] = {0.0, 0.0};
     R3D_CUDA(h, cudaMemcpyAsync(v, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -516,7 +495,7 @@ int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2) {
 int r3d_set_velocity_scale(r3d_handle* h, double scale) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (!std::isfinite(scale)) return fail(h, R3D_EINVAL, "velocity scale must be finite");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_set_scalar(h->S.vscale, scale, h->stream);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
@@ -532,7 +511,7 @@ int r3d_set_velocity_period(r3d_handle* h, double period) {
 int r3d_set_time(r3d_handle* h, double t) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (!std::isfinite(t)) return fail(h, R3D_EINVAL, "time must be finite");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_set_scalar(h->S.t, t, h->stream);
     if (h->period > 0.0) h->launches += launch_set_scalar(h->S.vscale, std::cos(3.141592653589793 * t / h->period), h->stream);
     R3D_CUDA(h, cudaGetLastError());
@@ -541,7 +520,7 @@ int r3d_set_time(r3d_handle* h, double t) {
 
 int r3d_get_time(r3d_handle* h, double* t) {
     if (!h || !t) return fail(h, R3D_EINVAL, "null argument");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     R3D_CUDA(h, cudaMemcpyAsync(t, h->S.t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     return R3D_OK;
@@ -552,15 +531,49 @@ int r3d_stage(r3d_handle* h, int kind, int stage) {
     if ((kind != R3D_STAGE_CONVECTION && kind != R3D_STAGE_REINIT) || stage < 1 || stage > 3)
         return fail(h, R3D_EINVAL, "kind must be R3D_STAGE_CONVECTION or R3D_STAGE_REINIT, stage 1..3");
     if (kind == R3D_STAGE_CONVECTION && !(h->dt_host > 0.0)) return fail(h, R3D_ESTATE, "no time step set");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     h->launches += stage_launch(h, kind == R3D_STAGE_REINIT, stage, false);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
 
+int r3d_init_spheres_tg(r3d_handle* h, int nspheres, const double* spheres, int nmodes, const double* modes) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (nspheres < 1 || nspheres > 64 || nmodes < 0 || nmodes > 64 || !spheres || (nmodes && !modes))
+        return fail(h, R3D_EINVAL, "1..64 spheres and 0..64 modes");
+    DeviceGuard dg(h->device, h->batch_stream);
+    // centre and face coordinates of padded indices -3..n+2 per axis
+    std::vector<double> xc, xf;
+    for (int a = 0; a < 3; ++a) {
+        const int n = h->M.n[a];
+        for (int i = -3; i < n + 3; ++i) {
+            xc.push_back(h->M.xp[a][i + 5]);
+            xf.push_back(h->M.xn[a][i + 6]);
+        }
+    }
+    std::vector<double> buf;
+    buf.insert(buf.end(), xc.begin(), xc.end());
+    buf.insert(buf.end(), xf.begin(), xf.end());
+    buf.insert(buf.end(), spheres, spheres + 4 * nspheres);
+    if (nmodes) buf.insert(buf.end(), modes, modes + 2 * nmodes);
+    double* d = nullptr;
+    R3D_CUDA(h, cudaMallocAsync((void**)&d, buf.size() * sizeof(double), h->stream));
+    R3D_CUDA(h, cudaMemcpyAsync(d, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const double* dxc = d;
+    const double* dxf = d + xc.size();
+    const double* dsp = dxf + xf.size();
+    const double* dmo = dsp + 4 * nspheres;
+    h->launches += launch_init_fields(h->L, dxc, dxf, nspheres, dsp, nmodes, dmo, fp32(h), h->field[R3D_PHI],
+                                      h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    R3D_CUDA(h, cudaFreeAsync(d, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
 int r3d_sync(r3d_handle* h) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    DeviceGuard dg(h->device);
+    DeviceGuard dg(h->device, h->batch_stream);
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     return check_device_flag(h);
 }

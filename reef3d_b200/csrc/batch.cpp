@@ -1,0 +1,419 @@
+// Batched execution of many FP32 instances: one persistent launch per RK
+// stage over a packed tile list of all members, the whole step captured in
+// a CUDA graph and replayed, the tile shape and grid size picked by an
+// autotuner whose choice is cached per size class.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "batch_internal.h"
+#include "handle.h"
+
+using namespace r3d;
+
+struct r3d_batch {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<r3d_handle*> members;
+    // device state, rebuilt when the membership or the configuration changes
+    MemberDesc* d_members = nullptr;
+    long long* d_tile0 = nullptr;
+    double* d_vol = nullptr;
+    double* d_vmax = nullptr;
+    size_t cap_members = 0, cap_tiles = 0;
+    long long ntiles = 0;
+    int max_f44 = 0;
+    int rows = 4;
+    int ctas_per_sm = 8;
+    bool tuned = false;  // rows/ctas set explicitly or by the autotuner
+    bool dirty = true;
+    bool use_graph = true;
+    cudaGraphExec_t graph = nullptr;
+    long long launches = 0;
+    long long steps = 0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_batch_err;
+
+int bfail(r3d_batch* b, int code, const std::string& m) {
+    if (b) b->err = m;
+    else g_batch_err = m;
+    return code;
+}
+
+#define B_CUDA(b, call)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) return bfail(b, R3D_EDEVICE, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+void drop_graph(r3d_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+}
+
+MemberDesc describe(const r3d_handle* h) {
+    MemberDesc m{};
+    m.g = h->g32;
+    m.phi = static_cast<float*>(h->field[R3D_PHI]);
+    m.a1 = static_cast<float*>(h->field[R3D_WORK1]);
+    m.a2 = static_cast<float*>(h->field[R3D_WORK2]);
+    m.u = static_cast<const float*>(h->field[R3D_U]);
+    m.v = static_cast<const float*>(h->field[R3D_V]);
+    m.w = static_cast<const float*>(h->field[R3D_W]);
+    m.dt = h->S.dt;
+    m.vscale = h->S.vscale;
+    m.t = h->S.t;
+    m.vol = h->S.vol;
+    m.n47 = h->desc.n47;
+    m.dxmin = h->M.dxmin_cfl;
+    m.period = h->period;
+    m.f44 = h->desc.f44;
+    return m;
+}
+
+int rebuild(r3d_batch* b) {
+    drop_graph(b);
+    const size_t nm = b->members.size();
+    std::vector<MemberDesc> desc(nm);
+    std::vector<long long> tile0(nm + 1, 0);
+    b->max_f44 = 0;
+    for (size_t q = 0; q < nm; ++q) {
+        desc[q] = describe(b->members[q]);
+        tile0[q + 1] = tile0[q] + batch_tiles_of(b->members[q]->L, b->rows);
+        b->max_f44 = std::max(b->max_f44, b->members[q]->desc.f44);
+    }
+    b->ntiles = tile0[nm];
+    if (nm > b->cap_members) {
+        if (b->d_members) cudaFree(b->d_members);
+        if (b->d_tile0) cudaFree(b->d_tile0);
+        b->d_members = nullptr;
+        b->d_tile0 = nullptr;
+        const size_t cap = std::max<size_t>(nm, 2 * b->cap_members);
+        if (cudaMalloc(&b->d_members, cap * sizeof(MemberDesc)) != cudaSuccess ||
+            cudaMalloc(&b->d_tile0, (cap + 1) * sizeof(long long)) != cudaSuccess) {
+            cudaGetLastError();
+            b->cap_members = 0;
+            return bfail(b, R3D_ENOMEM, "batch descriptor allocation failed");
+        }
+        b->cap_members = cap;
+    }
+    if ((size_t)b->ntiles > b->cap_tiles) {
+        if (b->d_vol) cudaFree(b->d_vol);
+        if (b->d_vmax) cudaFree(b->d_vmax);
+        b->d_vol = b->d_vmax = nullptr;
+        const size_t cap = std::max<size_t>((size_t)b->ntiles, 2 * b->cap_tiles);
+        if (cudaMalloc(&b->d_vol, cap * 2 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&b->d_vmax, cap * 3 * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            b->cap_tiles = 0;
+            return bfail(b, R3D_ENOMEM, "batch reduction scratch allocation failed");
+        }
+        b->cap_tiles = cap;
+    }
+    if (nm) {
+        B_CUDA(b, cudaMemcpyAsync(b->d_members, desc.data(), nm * sizeof(MemberDesc), cudaMemcpyHostToDevice, b->stream));
+        B_CUDA(b, cudaMemcpyAsync(b->d_tile0, tile0.data(), (nm + 1) * sizeof(long long), cudaMemcpyHostToDevice, b->stream));
+        B_CUDA(b, cudaStreamSynchronize(b->stream));
+    }
+    b->dirty = false;
+    return R3D_OK;
+}
+
+BatchLaunch launch_of(const r3d_batch* b) {
+    BatchLaunch l{};
+    l.members = b->d_members;
+    l.tile0 = b->d_tile0;
+    l.nm = (int)b->members.size();
+    l.ntiles = b->ntiles;
+    l.vol_part = b->d_vol;
+    l.vmax_part = b->d_vmax;
+    l.rows = b->rows;
+    const long long want = (long long)b->ctas_per_sm * b->sms;
+    l.grid = (unsigned)std::max<long long>(1, std::min<long long>(want, b->ntiles));
+    return l;
+}
+
+// CFL, 3 convection stages, max(f44) reinit pseudo-steps, volume + clock.
+long long enqueue_batch_step(r3d_batch* b) {
+    const BatchLaunch l = launch_of(b);
+    long long n = 0;
+    n += launch_batch_cfl(l, b->stream);
+    for (int s = 1; s <= 3; ++s) n += launch_batch_stage(l, 1, s, 0, b->stream);
+    for (int q = 0; q < b->max_f44; ++q)
+        for (int s = 1; s <= 3; ++s) n += launch_batch_stage(l, 0, s, q, b->stream);
+    n += launch_batch_finish(l, b->stream);
+    return n;
+}
+
+int capture(r3d_batch* b) {
+    drop_graph(b);
+    cudaGraph_t g = nullptr;
+    B_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_batch_step(b);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess) return bfail(b, R3D_EDEVICE, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->graph = nullptr;
+        return bfail(b, R3D_EDEVICE, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    return R3D_OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+std::mutex g_tune_mu;
+std::map<std::string, std::pair<int, int>> g_tune_cache;
+
+std::string size_class(const r3d_batch* b) {
+    double c3 = 0, c2 = 0;
+    for (const r3d_handle* h : b->members) {
+        const double c = (double)h->L.nx * h->L.ny * h->L.nz;
+        (h->L.two_d ? c2 : c3) += c;
+    }
+    const double tot = c2 + c3;
+    std::ostringstream os;
+    os << (c3 >= c2 ? "3d" : "2d") << "-c" << (int)std::floor(std::log2(std::max(1.0, tot))) << "-m"
+       << (int)std::floor(std::log2(std::max<size_t>(1, b->members.size())));
+    return os.str();
+}
+
+void load_cache(const char* path) {
+    if (!path || !*path) return;
+    std::ifstream f(path);
+    std::string key;
+    int r, c;
+    while (f >> key >> r >> c) g_tune_cache[key] = {r, c};
+}
+
+void save_cache(const char* path) {
+    if (!path || !*path) return;
+    std::ofstream f(path, std::ios::trunc);
+    for (auto& kv : g_tune_cache) f << kv.first << " " << kv.second.first << " " << kv.second.second << "\n";
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* r3d_batch_last_error(const r3d_batch* b) { return b ? b->err.c_str() : g_batch_err.c_str(); }
+
+int r3d_batch_create(r3d_batch** out) {
+    if (!out) return bfail(nullptr, R3D_EINVAL, "null output");
+    *out = nullptr;
+    r3d_batch* b = new (std::nothrow) r3d_batch();
+    if (!b) return bfail(nullptr, R3D_ENOMEM, "host allocation failed");
+    cudaGetDevice(&b->device);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete b;
+        return bfail(nullptr, R3D_EDEVICE, "stream creation failed");
+    }
+    *out = b;
+    return R3D_OK;
+}
+
+int r3d_batch_destroy(r3d_batch* b) {
+    if (!b) return R3D_OK;
+    cudaStreamSynchronize(b->stream);
+    for (r3d_handle* h : b->members) h->batch_stream = nullptr;
+    drop_graph(b);
+    if (b->d_members) cudaFree(b->d_members);
+    if (b->d_tile0) cudaFree(b->d_tile0);
+    if (b->d_vol) cudaFree(b->d_vol);
+    if (b->d_vmax) cudaFree(b->d_vmax);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return R3D_OK;
+}
+
+int r3d_batch_add(r3d_batch* b, r3d_handle* h) {
+    if (!b || !h) return bfail(b, R3D_EINVAL, "null argument");
+    if (h->desc.precision != R3D_FP32) return bfail(b, R3D_EINVAL, "batches hold FP32 instances");
+    if (h->device != b->device) return bfail(b, R3D_EINVAL, "instance lives on another device");
+    if (h->batch_stream) return bfail(b, R3D_ESTATE, "instance already in a batch");
+    // the member's own queued work (uploads, settings) completes first
+    B_CUDA(b, cudaStreamSynchronize(h->stream));
+    b->members.push_back(h);
+    h->batch_stream = b->stream;
+    b->dirty = true;
+    return R3D_OK;
+}
+
+int r3d_batch_remove(r3d_batch* b, r3d_handle* h) {
+    if (!b || !h) return bfail(b, R3D_EINVAL, "null argument");
+    auto it = std::find(b->members.begin(), b->members.end(), h);
+    if (it == b->members.end()) return bfail(b, R3D_EINVAL, "not a member");
+    B_CUDA(b, cudaStreamSynchronize(b->stream));
+    b->members.erase(it);
+    h->batch_stream = nullptr;
+    b->dirty = true;
+    return R3D_OK;
+}
+
+int r3d_batch_size(const r3d_batch* b, int* n) {
+    if (!b || !n) return bfail(nullptr, R3D_EINVAL, "null argument");
+    *n = (int)b->members.size();
+    return R3D_OK;
+}
+
+int r3d_batch_set_config(r3d_batch* b, int rows, int ctas_per_sm) {
+    if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
+    if (rows != 2 && rows != 4 && rows != 8) return bfail(b, R3D_EINVAL, "rows must be 2, 4 or 8");
+    if (ctas_per_sm < 1 || ctas_per_sm * 32 * rows > 2048) return bfail(b, R3D_EINVAL, "ctas_per_sm out of range");
+    b->rows = rows;
+    b->ctas_per_sm = ctas_per_sm;
+    b->tuned = true;
+    b->dirty = true;
+    return R3D_OK;
+}
+
+int r3d_batch_get_config(const r3d_batch* b, int* rows, int* ctas_per_sm) {
+    if (!b || !rows || !ctas_per_sm) return bfail(nullptr, R3D_EINVAL, "null argument");
+    *rows = b->rows;
+    *ctas_per_sm = b->ctas_per_sm;
+    return R3D_OK;
+}
+
+int r3d_batch_use_graph(r3d_batch* b, int on) {
+    if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
+    b->use_graph = on != 0;
+    drop_graph(b);
+    return R3D_OK;
+}
+
+// Picks (rows, CTAs per SM) for the batch's size class by timing the first
+// convection and reinitialisation stages (they write only the stage buffer
+// WORK1, so the members' state is untouched), and caches the choice per
+// size class in memory and in `cache_path` (a text file; may be NULL).
+int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows_out, int* ctas_out) {
+    if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
+    if (b->members.empty()) return bfail(b, R3D_ESTATE, "empty batch");
+    const std::string key = size_class(b);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        if (g_tune_cache.empty()) load_cache(cache_path);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            int rc = r3d_batch_set_config(b, it->second.first, it->second.second);
+            if (rows_out) *rows_out = b->rows;
+            if (ctas_out) *ctas_out = b->ctas_per_sm;
+            return rc;
+        }
+    }
+    const int cand_rows[3] = {2, 4, 8};
+    const int cand_ctas[4] = {4, 8, 16, 32};
+    float best = 1e30f;
+    int br = 4, bc = 8;
+    cudaEvent_t e0, e1;
+    B_CUDA(b, cudaEventCreate(&e0));
+    B_CUDA(b, cudaEventCreate(&e1));
+    // the stages read dt: give every member a valid one first
+    b->rows = 4;
+    b->ctas_per_sm = 8;
+    if (int rc = rebuild(b)) return rc;
+    launch_batch_cfl(launch_of(b), b->stream);
+    for (int r : cand_rows)
+        for (int c : cand_ctas) {
+            if (c * 32 * r > 2048) continue;
+            b->rows = r;
+            b->ctas_per_sm = c;
+            if (int rc = rebuild(b)) return rc;
+            const BatchLaunch l = launch_of(b);
+            launch_batch_stage(l, 1, 1, 0, b->stream);  // warm
+            cudaEventRecord(e0, b->stream);
+            for (int rep = 0; rep < 3; ++rep) {
+                launch_batch_stage(l, 1, 1, 0, b->stream);
+                launch_batch_stage(l, 0, 1, 0, b->stream);
+            }
+            cudaEventRecord(e1, b->stream);
+            B_CUDA(b, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; br = r; bc = c; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    B_CUDA(b, cudaGetLastError());
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = {br, bc};
+        save_cache(cache_path);
+    }
+    int rc = r3d_batch_set_config(b, br, bc);
+    if (rows_out) *rows_out = br;
+    if (ctas_out) *ctas_out = bc;
+    return rc;
+}
+
+// nsteps physical steps of every member: per member the CFL time step from
+// its velocities, the three convection stages, its f44 reinitialisation
+// pseudo-steps, the volume integral and its clock (src/levelset_RK3.cpp
+// for every member at once).  Asynchronous on the batch's stream.
+int r3d_batch_step(r3d_batch* b, int nsteps) {
+    if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
+    if (nsteps < 0) return bfail(b, R3D_EINVAL, "nsteps must be >= 0");
+    if (b->members.empty() || nsteps == 0) return R3D_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != b->device) cudaSetDevice(b->device);
+    int rc = R3D_OK;
+    if (b->dirty) rc = rebuild(b);
+    if (!rc && b->use_graph && !b->graph) rc = capture(b);
+    if (!rc) {
+        for (int s = 0; s < nsteps; ++s) {
+            if (b->graph) {
+                if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) {
+                    rc = bfail(b, R3D_EDEVICE, "graph launch failed");
+                    break;
+                }
+            } else {
+                b->launches += enqueue_batch_step(b) - 0;
+            }
+        }
+        if (!rc) {
+            const long long per = 2 + 3 + 3 * b->max_f44 + 1;
+            if (b->graph) b->launches += per * nsteps;
+            b->steps += nsteps;
+            for (r3d_handle* h : b->members) h->have_last_volume = true;
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (!rc && e != cudaSuccess) rc = bfail(b, R3D_EDEVICE, cudaGetErrorString(e));
+    if (cur != b->device) cudaSetDevice(cur);
+    return rc;
+}
+
+int r3d_batch_sync(r3d_batch* b) {
+    if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
+    B_CUDA(b, cudaStreamSynchronize(b->stream));
+    return R3D_OK;
+}
+
+int r3d_batch_stream(r3d_batch* b, void** stream) {
+    if (!b || !stream) return bfail(b, R3D_EINVAL, "null argument");
+    *stream = (void*)b->stream;
+    return R3D_OK;
+}
+
+int r3d_batch_launch_count(const r3d_batch* b, long long* count) {
+    if (!b || !count) return bfail(nullptr, R3D_EINVAL, "null argument");
+    *count = b->launches;
+    return R3D_OK;
+}
+
+}  // extern "C"

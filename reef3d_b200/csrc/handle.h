@@ -1,0 +1,41 @@
+// The instance handle behind the C-ABI (shared by api.cpp and batch.cpp).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "reef3d_b200.h"
+#include "r3d_internal.h"
+#include "tile_host.h"
+
+struct r3d_handle {
+    r3d::Layout L{};
+    r3d_grid_desc desc{};
+    r3d::HostMetrics M;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    void* field[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* metrics64 = nullptr;
+    float* metrics32 = nullptr;
+    r3d::KGrid<double> g64{};
+    r3d::KGrid<float> g32{};
+    r3d::Scratch S{};
+    double* staging = nullptr;
+    size_t staging_bytes = 0;
+    long long launches = 0;
+    double dt_host = 0.0;
+    double period = 0.0;
+    bool have_last_volume = false;
+    // TMA-tiled FP32 path (3D uniform grids)
+    bool tile_ok = false;
+    int use_tile = 1;
+    int kc = 16;
+    int band64 = 1;
+    CUtensorMap map[3];  // stage inputs: phi, WORK1, WORK2
+    // set while the instance is a member of a batch: calls on the handle
+    // first wait for the batch's stream
+    cudaStream_t batch_stream = nullptr;
+    std::string err;
+};

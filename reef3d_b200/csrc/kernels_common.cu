@@ -261,7 +261,66 @@ int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const doub
 
 namespace {
 __global__ void set_scalar_kernel(double* dst, double value) { *dst = value; }
+
+// Initial fields of a sphere-union / Taylor-Green case on every stored cell
+// (interior and ghosts): phi = min over spheres of |x - c| - r (circles in
+// the x-z plane in 2D) at cell centres; u, v, w = sum of Taylor-Green modes
+// at the x, y, z faces.  xc/xf hold, per axis, the centre and face
+// coordinates of padded indices -3..n+2.
+template <typename T>
+__global__ void init_kernel(Layout L, const double* __restrict__ xc, const double* __restrict__ xf, int ns,
+                            const double* __restrict__ sph, int nm, const double* __restrict__ modes, T* phi, T* u,
+                            T* v, T* w) {
+    const int gyp = L.two_d ? 0 : 3;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - 3;
+    const int j = blockIdx.y - gyp;
+    const int k = blockIdx.z - 3;
+    if (i >= L.nx + 3) return;
+    const int nx6 = L.nx + 6, ny6 = L.ny + 6;
+    const double* cx = xc;
+    const double* cy = xc + nx6;
+    const double* cz = xc + nx6 + ny6;
+    const double* fx = xf;
+    const double* fy = xf + nx6;
+    const double* fz = xf + nx6 + ny6;
+    const double X = cx[i + 3], Y = cy[j + 3], Z = cz[k + 3];
+    double d = 1e30;
+    for (int s = 0; s < ns; ++s) {
+        const double ex = X - sph[4 * s], ey = Y - sph[4 * s + 1], ez = Z - sph[4 * s + 2];
+        const double e = (L.two_d ? sqrt(ex * ex + ez * ez) : sqrt(ex * ex + ey * ey + ez * ez)) - sph[4 * s + 3];
+        d = e < d ? e : d;
+    }
+    double uu = 0.0, vv = 0.0, ww = 0.0;
+    for (int m = 0; m < nm; ++m) {
+        const double kk = modes[2 * m] * 3.141592653589793, A = modes[2 * m + 1];
+        if (L.two_d) {
+            uu += A * sin(kk * fx[i + 3]) * cos(kk * Z);
+            ww += -A * cos(kk * X) * sin(kk * fz[k + 3]);
+        } else {
+            uu += A * sin(kk * fx[i + 3]) * cos(kk * Y) * cos(kk * Z);
+            vv += -A * cos(kk * X) * sin(kk * fy[j + 3]) * cos(kk * Z);
+        }
+    }
+    const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+    phi[c] = (T)d;
+    u[c] = (T)uu;
+    v[c] = (T)vv;
+    w[c] = (T)ww;
+}
 }  // namespace
+
+int launch_init_fields(const Layout& L, const double* xc, const double* xf, int ns, const double* sph, int nm,
+                       const double* modes, bool fp32, void* phi, void* u, void* v, void* w, cudaStream_t st) {
+    const int py = L.two_d ? 1 : L.ny + 6;
+    const dim3 grid((L.nx + 6 + 127) / 128, py, L.nz + 6), block(128);
+    if (fp32)
+        init_kernel<float><<<grid, block, 0, st>>>(L, xc, xf, ns, sph, nm, modes, (float*)phi, (float*)u, (float*)v,
+                                                   (float*)w);
+    else
+        init_kernel<double><<<grid, block, 0, st>>>(L, xc, xf, ns, sph, nm, modes, (double*)phi, (double*)u,
+                                                    (double*)v, (double*)w);
+    return 1;
+}
 
 // Writes a scalar into device memory as a kernel argument, so the value is
 // captured at enqueue time (also inside a CUDA graph).

@@ -2,10 +2,11 @@
 // and the reinitialisation of interface-band cells (cells whose 7-point
 // stencil changes sign) re-anchored in FP64 so the zero level set is moved
 // with FP64 arithmetic.  One fused pass per RK stage as in the FP64 path.
-#include "stencil_f32.cuh"
+#include "cell_f32.cuh"
 
 namespace r3d {
 namespace {
+using namespace f32c;
 
 constexpr int kBX = 32, kBY = 4;
 
@@ -20,121 +21,6 @@ struct StageArgs32 {
     const double* vscale;
     double* partial;
 };
-
-__device__ __forceinline__ void load7(const float* __restrict__ f, long long c, long long s, float* o) {
-#pragma unroll
-    for (int m = 0; m < 7; ++m) o[m] = __ldg(f + c + (m - 3) * s);
-}
-
-template <bool TWO_D, bool UNIFORM>
-__device__ __forceinline__ float conv_L(const KGrid<float>& g, const float* __restrict__ f,
-                                        const float* __restrict__ u, const float* __restrict__ v,
-                                        const float* __restrict__ w, long long c, int i, int j, int k, float vs) {
-    const long long sy = g.L.sy, sz = g.L.sz;
-    const float ia = 0.5f * vs * (__ldg(u + c) + __ldg(u + c - 1));
-    const float ka = 0.5f * vs * (__ldg(w + c) + __ldg(w + c - sz));
-    float fv[7];
-    float l = 0.0f;
-    if (ia != 0.0f) {
-        load7(f, c, 1, fv);
-        const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ia < 0.0f, g.rh[0], g.eps_u * g.h[0] * g.h[0])
-                                : f32::deriv_tables(fv, ia < 0.0f, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5);
-        l -= ia * d;
-    }
-    if (!TWO_D) {
-        const float ja = 0.5f * vs * (__ldg(v + c) + __ldg(v + c - sy));
-        if (ja != 0.0f) {
-            load7(f, c, sy, fv);
-            const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ja < 0.0f, g.rh[1], g.eps_u * g.h[1] * g.h[1])
-                                    : f32::deriv_tables(fv, ja < 0.0f, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5);
-            l -= ja * d;
-        }
-    }
-    if (ka != 0.0f) {
-        load7(f, c, sz, fv);
-        const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ka < 0.0f, g.rh[2], g.eps_u * g.h[2] * g.h[2])
-                                : f32::deriv_tables(fv, ka < 0.0f, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5);
-        l -= ka * d;
-    }
-    return l;
-}
-
-// Non-uniform reinitialisation RHS in FP32 with the node tables.
-template <bool TWO_D>
-__device__ __forceinline__ float reini_tables(const KGrid<float>& g, const float* fx, const float* fy,
-                                              const float* fz, int i, int j, int k) {
-    const float lsv = fx[3];
-    const float lsSig = (fabsf(lsv) < 1.0e-8f) ? 1.0f : (lsv > 0.0f ? 1.0f : -1.0f);
-    const float* fa[3] = {fx, fy, fz};
-    const int t[3] = {i + 5, j + 5, k + 5};
-    float gsum = 0.0f;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        if (TWO_D && a == 1) continue;
-        const float* f = fa[a];
-        const float xmin = __fdividef(lsv - f[2], __ldg(g.dxp[a] + t[a] - 1));
-        const float xplus = __fdividef(f[4] - lsv, __ldg(g.dxp[a] + t[a]));
-        float d = 0.0f;
-        if (xmin * lsSig > 0.0f && xplus * lsSig > -xmin * lsSig)
-            d = f32::deriv_tables(f, false, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t[a]);
-        if (xplus * lsSig < 0.0f && xmin * lsSig < -xplus * lsSig)
-            d = f32::deriv_tables(f, true, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t[a]);
-        if (xplus * lsSig > 0.0f && xmin * lsSig < 0.0f) d = 0.0f;
-        gsum += d * d;
-    }
-    const float dnorm = sqrtf(gsum);
-    const float deltax = TWO_D ? 0.5f * (__ldg(g.dxn[0] + t[0]) + __ldg(g.dxn[2] + t[2]))
-                               : (1.0f / 3.0f) * (__ldg(g.dxn[0] + t[0]) + __ldg(g.dxn[1] + t[1]) + __ldg(g.dxn[2] + t[2]));
-    float sign = lsv * rsqrtf(lsv * lsv + dnorm * dnorm * deltax * deltax);
-    if (sign != sign) sign = 1.0f;
-    return -(sign * dnorm - sign);
-}
-
-template <bool TWO_D, bool UNIFORM>
-__device__ __forceinline__ float reini_L(const KGrid<float>& g, const float* __restrict__ f, long long c, int i,
-                                         int j, int k) {
-    float fx[7], fy[7], fz[7];
-    load7(f, c, 1, fx);
-    load7(f, c, g.L.sz, fz);
-    if (!TWO_D) load7(f, c, g.L.sy, fy);
-    else {
-#pragma unroll
-        for (int m = 0; m < 7; ++m) fy[m] = 0.0f;
-        fy[3] = fx[3];
-    }
-    const float f0 = fx[3];
-    const bool pos = f0 >= 0.0f && fx[2] >= 0.0f && fx[4] >= 0.0f && fz[2] >= 0.0f && fz[4] >= 0.0f &&
-                     (TWO_D || (fy[2] >= 0.0f && fy[4] >= 0.0f));
-    const bool neg = f0 < 0.0f && fx[2] < 0.0f && fx[4] < 0.0f && fz[2] < 0.0f && fz[4] < 0.0f &&
-                     (TWO_D || (fy[2] < 0.0f && fy[4] < 0.0f));
-    const bool band = !(pos || neg);  // the zero level set crosses the 7-point stencil
-    // F49=0 freezes band cells (src/reinidisc_fsf.cpp:70-72); in 2D the
-    // reference's test also reads the never-written y ghost planes (zero),
-    // so no negative cell passes it there.
-    if (g.f49 == 0 && (band || (TWO_D && neg))) return 0.0f;
-    if (!UNIFORM) return reini_tables<TWO_D>(g, fx, fy, fz, i, j, k);
-    const float deltax = TWO_D ? 0.5f * (g.h[0] + g.h[2]) : (1.0f / 3.0f) * (g.h[0] + g.h[1] + g.h[2]);
-    if (band) {
-        // interface band: FP64 re-anchoring of the zero level set
-        double dx[7], dy[7], dz[7];
-#pragma unroll
-        for (int m = 0; m < 7; ++m) { dx[m] = fx[m]; dy[m] = fy[m]; dz[m] = fz[m]; }
-        const double rh[3] = {1.0 / g.h[0], 1.0 / g.h[1], 1.0 / g.h[2]};
-        const double hh[3] = {(double)g.h[0] * g.h[0], (double)g.h[1] * g.h[1], (double)g.h[2] * g.h[2]};
-        const double dlt = TWO_D ? 0.5 * ((double)g.h[0] + g.h[2]) : (1.0 / 3.0) * ((double)g.h[0] + g.h[1] + g.h[2]);
-        return (float)f32::reini_rhs_uniform<double, TWO_D>(dx, dy, dz, rh, hh, 1.0e-6, dlt);
-    }
-    const float hh[3] = {g.h[0] * g.h[0], g.h[1] * g.h[1], g.h[2] * g.h[2]};
-    return f32::reini_rhs_uniform<float, TWO_D>(fx, fy, fz, g.rh, hh, 1.0e-6f, deltax);
-}
-
-template <bool TWO_D>
-__device__ __forceinline__ float reini_dt32(const KGrid<float>& g, int i, int j, int k) {
-    const float a = __ldg(g.dxp[0] + i + 5), c = __ldg(g.dxp[2] + k + 5);
-    if (TWO_D) return (float)g.f43 * fminf(a, c);
-    const float b = __ldg(g.dxp[1] + j + 5);
-    return (float)g.f43 * fminf(fminf(a, b), c);
-}
 
 __device__ __forceinline__ void block_sum2(double a, double b, double* dst) {
     __shared__ double sa[32], sb[32];

@@ -197,9 +197,35 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
     float2 wprev = make_float2(0.f, 0.f);
     if (!REINI && act0) {
         const long long c = (long long)(k0 - 1 + L.gz) * L.sz + col;
-        wprev = act1 ? *reinterpret_cast<const float2*>(a.w + c) : make_float2(a.w[c], 0.f);
+        wprev = act1 ? __ldg(reinterpret_cast<const float2*>(a.w + c)) : make_float2(__ldg(a.w + c), 0.f);
     }
     double vol_a = 0.0, vol_b = 0.0;
+
+    // cell-local global operands of a plane (velocities, step start value),
+    // fetched one plane ahead so their latency overlaps the current plane
+    float2 nu = make_float2(0.f, 0.f), nv = nu, nvm = nu, nw = nu, nfn = nu;
+    float num = 0.f;
+    auto fetch = [&](int kk) {
+        if (!act0) return;
+        const long long cc = (long long)(kk + L.gz) * L.sz + col;
+        if (!REINI) {
+            if (act1) {
+                nu = __ldg(reinterpret_cast<const float2*>(a.u + cc));
+                nv = __ldg(reinterpret_cast<const float2*>(a.v + cc));
+                nvm = __ldg(reinterpret_cast<const float2*>(a.v + cc - L.sy));
+                nw = __ldg(reinterpret_cast<const float2*>(a.w + cc));
+            } else {
+                nu.x = __ldg(a.u + cc);
+                nv.x = __ldg(a.v + cc);
+                nvm.x = __ldg(a.v + cc - L.sy);
+                nw.x = __ldg(a.w + cc);
+            }
+            num = __ldg(a.u + cc - 1);
+        }
+        // the step start value may be this stage's output (stage 3): plain loads
+        if (STAGE != 1) nfn = act1 ? *reinterpret_cast<const float2*>(a.fn + cc) : make_float2(a.fn[cc], 0.f);
+    };
+    fetch(k0);
 
     bool aborted = __syncthreads_or(!ok);
     for (int k = k0; k < k1 && !aborted; ++k) {
@@ -229,23 +255,10 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
         const long long c = (long long)(k + L.gz) * L.sz + col;
 
         float2 Lc;
+        const float2 fn = nfn;
         if (!REINI) {
-            float2 uc = make_float2(0.f, 0.f), vc = uc, vm = uc, wc = uc;
-            float um = 0.f;
-            if (act0) {
-                if (act1) {
-                    uc = *reinterpret_cast<const float2*>(a.u + c);
-                    vc = *reinterpret_cast<const float2*>(a.v + c);
-                    vm = *reinterpret_cast<const float2*>(a.v + c - L.sy);
-                    wc = *reinterpret_cast<const float2*>(a.w + c);
-                } else {
-                    uc.x = a.u[c];
-                    vc.x = a.v[c];
-                    vm.x = a.v[c - L.sy];
-                    wc.x = a.w[c];
-                }
-                um = a.u[c - 1];
-            }
+            const float2 uc = nu, vc = nv, vm = nvm, wc = nw;
+            const float um = num;
             const float2 h2 = f2(0.5f * vs);
             const float2 ia = mul2(h2, add2(make_float2(um, uc.x), uc));
             const float2 ja = mul2(h2, add2(vc, vm));
@@ -317,8 +330,6 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
         if (STAGE == 1) {
             val = sdl;
         } else {
-            float2 fn = make_float2(0.f, 0.f);
-            if (act0) fn = act1 ? *reinterpret_cast<const float2*>(a.fn + c) : make_float2(a.fn[c], 0.f);
             if (STAGE == 2) val = fma2(f2(0.75f), fn, mul2(f2(0.25f), sdl));
             else val = fma2(f2(1.0f / 3.0f), fn, mul2(f2(2.0f / 3.0f), sdl));
         }
@@ -357,6 +368,7 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
             }
         }
 
+        if (k + 1 < k1) fetch(k + 1);
         // every thread is done with the box of plane k: refill its slot
         aborted = __syncthreads_or(!ok);
         if (!aborted && threadIdx.x == 0 && k + kSlots <= plast) {

@@ -132,5 +132,7 @@ struct TileArgs;
 size_t tile_smem_bytes();
 dim3 tile_grid(const Layout& L, int kc);
 int launch_set_scalar(double* dst, double value, cudaStream_t st);
+int launch_init_fields(const Layout& L, const double* xc, const double* xf, int ns, const double* sph, int nm,
+                       const double* modes, bool fp32, void* phi, void* u, void* v, void* w, cudaStream_t st);
 
 }  // namespace r3d

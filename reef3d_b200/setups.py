@@ -220,5 +220,8 @@ def random_instance(rng, n_edge_choices=None, two_d=None, name="ensemble", f44=2
         v = taylor_green(Xv, Yv, Zv, modes, 1, two_d)
     Xw, Yw, Zw = _mesh(xc, yc, faces(zn))
     w = taylor_green(Xw, Yw, Zw, modes, 2, two_d)
-    return Case(name, nx, ny, nz, xn, yn, zn, *(np.ascontiguousarray(a) for a in (phi, u, v, w)),
+    case = Case(name, nx, ny, nz, xn, yn, zn, *(np.ascontiguousarray(a) for a in (phi, u, v, w)),
                 f43=0.5, f44=f44, n47=cfl / 2.0)
+    case.spheres = [(float(c[0]), float(c[1]), float(c[2]), float(r)) for c, r in zip(cs, rs)]
+    case.modes = modes
+    return case
