@@ -187,7 +187,7 @@ TileArgs tile_args(r3d_handle* h, int stage) {
     double hmin = h->M.h[0];
     for (int d = 0; d < 3; ++d) {
         a.rh[d] = (float)(1.0 / h->M.h[d]);
-        a.eps[d] = (float)(1.0e-6 * h->M.h[d] * h->M.h[d]);
+        a.eps[d] = (float)(1.0 / (h->M.h[d] * h->M.h[d]));
         hmin = std::fmin(hmin, h->M.h[d]);
     }
     a.dtr = (float)(h->desc.f43 * hmin);

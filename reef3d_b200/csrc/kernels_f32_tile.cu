@@ -81,7 +81,7 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 // ------------------------------------------------------------ packed math
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
@@ -93,35 +93,48 @@ __device__ __forceinline__ float2 sel2(bool cx, bool cy, float2 a, float2 b) {
 // d1..d5 of the minus-side upwind set; the plus side passes the mirrored
 // set (d1..d5 = D2, D1, D0, D-1, D-2).  Ideal weights 0.1/0.6/0.3 for the
 // stencils (d1,d2,d3)/(d2,d3,d4)/(d3,d4,d5).
-__device__ __forceinline__ float2 weno5_2(float2 d1, float2 d2, float2 d3, float2 d4, float2 d5, float2 eps) {
+// The smoothness indicators are formed at the scale of divided differences
+// (IS coefficients times 1/h^2, so s = IS + psi with the reference's
+// psi = 1e-6 exactly as in src/weno_nug_func.h:133-143), and the nonlinear
+// weights w_r = (c_r/s_r^2) / sum_q (c_q/s_q^2) are evaluated as
+// c_r prod_{q!=r} s_q^2 / sum_q c_q prod_{p!=q} s_p^2 with one reciprocal.
+// ih2 = 1/h^2 of the axis.
+__device__ __forceinline__ float2 weno5_2(float2 d1, float2 d2, float2 d3, float2 d4, float2 d5, float ih2) {
     const float2 a1 = sub2(d3, d4), b1 = sub2(d5, d4);
     const float2 b2 = sub2(d2, d3), b3 = sub2(d1, d2);
-    const float2 k43 = f2(4.0f / 3.0f);
-    // IS1 = (10/3 a1 + 11/3 b1) a1 + 4/3 b1^2, IS2 = (4/3 a1 - 5/3 b2) a1 + 4/3 b2^2,
-    // IS3 = (10/3 b2 - 11/3 b3) b2 + 4/3 b3^2  (a2 = -a1, a3 = -b2)
-    const float2 is1 = fma2(fma2(f2(10.0f / 3.0f), a1, mul2(f2(11.0f / 3.0f), b1)), a1, mul2(mul2(k43, b1), b1));
-    const float2 is2 = fma2(fma2(k43, a1, mul2(f2(-5.0f / 3.0f), b2)), a1, mul2(mul2(k43, b2), b2));
-    const float2 is3 = fma2(fma2(f2(10.0f / 3.0f), b2, mul2(f2(-11.0f / 3.0f), b3)), b2, mul2(mul2(k43, b3), b3));
-    const float2 r1 = rcp2(add2(is1, eps)), r2 = rcp2(add2(is2, eps)), r3 = rcp2(add2(is3, eps));
-    const float2 al1 = mul2(mul2(f2(0.3f), r1), r1);
-    const float2 al2 = mul2(mul2(f2(0.6f), r2), r2);
-    const float2 al3 = mul2(mul2(f2(0.1f), r3), r3);
-    const float2 inv = rcp2(add2(add2(al1, al2), al3));
+    const float2 k43 = f2(ih2 * (4.0f / 3.0f)), k103 = f2(ih2 * (10.0f / 3.0f));
+    const float2 k113 = f2(ih2 * (11.0f / 3.0f)), k53 = f2(ih2 * (5.0f / 3.0f));
+    const float2 psi = f2(1.0e-6f);
+    // s1 = IS1 + psi = (10/3 a1 + 11/3 b1) a1 + 4/3 b1^2 + psi, etc.
+    // (IS2 = (4/3 a1 - 5/3 b2) a1 + 4/3 b2^2, IS3 = (10/3 b2 - 11/3 b3) b2 + 4/3 b3^2)
+    const float2 s1 = fma2(fma2(k103, a1, mul2(k113, b1)), a1, fma2(mul2(k43, b1), b1, psi));
+    const float2 s2 = fma2(fma2(k43, a1, mul2(make_float2(-k53.x, -k53.y), b2)), a1, fma2(mul2(k43, b2), b2, psi));
+    const float2 s3 = fma2(fma2(k103, b2, mul2(make_float2(-k113.x, -k113.y), b3)), b2, fma2(mul2(k43, b3), b3, psi));
+    // s lies in [1e-6, 1e6] (clamped above for fields far from a distance
+    // function): the products below stay inside the FP32 range
+    const float2 c1 = make_float2(fminf(s1.x, 1.0e6f), fminf(s1.y, 1.0e6f));
+    const float2 c2 = make_float2(fminf(s2.x, 1.0e6f), fminf(s2.y, 1.0e6f));
+    const float2 c3 = make_float2(fminf(s3.x, 1.0e6f), fminf(s3.y, 1.0e6f));
+    const float2 q1 = mul2(c1, c1), q2 = mul2(c2, c2), q3 = mul2(c3, c3);
+    const float2 n1 = mul2(mul2(f2(0.3f), q2), q3);
+    const float2 n2 = mul2(mul2(f2(0.6f), q1), q3);
+    const float2 n3 = mul2(mul2(f2(0.1f), q1), q2);
+    const float2 inv = rcp2(add2(add2(n1, n2), n3));
     // p1 = d4 + a1/3 - b1/6, p2 = d3 - a1/3 - b2/6, p3 = d2 + b3/3 - 11/6 b2
     const float2 p1 = fma2(f2(-1.0f / 6.0f), b1, fma2(f2(1.0f / 3.0f), a1, d4));
     const float2 p2 = fma2(f2(-1.0f / 6.0f), b2, fma2(f2(-1.0f / 3.0f), a1, d3));
     const float2 p3 = fma2(f2(-11.0f / 6.0f), b2, fma2(f2(1.0f / 3.0f), b3, d2));
-    return mul2(fma2(al3, p3, fma2(al2, p2, mul2(al1, p1))), inv);
+    return mul2(fma2(n3, p3, fma2(n2, p2, mul2(n1, p1))), inv);
 }
 
 // Upwind derivative (times h) of an axis from 7 packed values f[0..6]
 // (f[3] the cells), plus side where `plus` is set per cell.
-__device__ __forceinline__ float2 deriv2(const float2* f, bool px, bool py, float2 eps) {
+__device__ __forceinline__ float2 deriv2(const float2* f, bool px, bool py, float ih2) {
     const float2 D0 = sub2(f[1], f[0]), D1 = sub2(f[2], f[1]), D2 = sub2(f[3], f[2]);
     const float2 D3 = sub2(f[4], f[3]), D4 = sub2(f[5], f[4]), D5 = sub2(f[6], f[5]);
     // minus: (D0..D4); plus (mirrored): (D5, D4, D3, D2, D1)
     return weno5_2(sel2(px, py, D5, D0), sel2(px, py, D4, D1), sel2(px, py, D3, D2), sel2(px, py, D2, D3),
-                   sel2(px, py, D1, D4), eps);
+                   sel2(px, py, D1, D4), ih2);
 }
 
 // Reinitialisation right-hand side of one cell in FP64 from its FP32
@@ -264,9 +277,9 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
             const float2 ja = mul2(h2, add2(vc, vm));
             const float2 ka = mul2(h2, add2(wc, wprev));
             wprev = wc;
-            const float2 gx = mul2(f2(a.rh[0]), deriv2(fx, ia.x < 0.f, ia.y < 0.f, f2(a.eps[0])));
-            const float2 gy = mul2(f2(a.rh[1]), deriv2(fy, ja.x < 0.f, ja.y < 0.f, f2(a.eps[1])));
-            const float2 gz = mul2(f2(a.rh[2]), deriv2(zw, ka.x < 0.f, ka.y < 0.f, f2(a.eps[2])));
+            const float2 gx = mul2(f2(a.rh[0]), deriv2(fx, ia.x < 0.f, ia.y < 0.f, a.eps[0]));
+            const float2 gy = mul2(f2(a.rh[1]), deriv2(fy, ja.x < 0.f, ja.y < 0.f, a.eps[1]));
+            const float2 gz = mul2(f2(a.rh[2]), deriv2(zw, ka.x < 0.f, ka.y < 0.f, a.eps[2]));
             Lc = mul2(f2(-1.f), fma2(ka, gz, fma2(ja, gy, mul2(ia, gx))));
         } else {
             // Godunov selection per axis (src/reinidisc_f.cpp:70-109)
@@ -282,7 +295,7 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
                 const float msx = xm.x * sgx, psx = xp.x * sgx, msy = xm.y * sgy, psy = xp.y * sgy;
                 const bool c1x = msx > 0.f && psx > -msx, c2x = psx < 0.f && msx < -psx;
                 const bool c1y = msy > 0.f && psy > -msy, c2y = psy < 0.f && msy < -psy;
-                float2 g = mul2(f2(a.rh[d]), deriv2(f, c2x, c2y, f2(a.eps[d])));
+                float2 g = mul2(f2(a.rh[d]), deriv2(f, c2x, c2y, a.eps[d]));
                 g.x = (c1x || c2x) ? g.x : 0.f;
                 g.y = (c1y || c2y) ? g.y : 0.f;
                 g2 = fma2(g, g, g2);

@@ -19,7 +19,7 @@ struct TileArgs {
     double* partial;
     int* err;
     float rh[3];
-    float eps[3];
+    float eps[3];  // 1/h^2 per axis
     float dtr;
     float deltax;
     int f49;

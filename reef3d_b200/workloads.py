@@ -1,0 +1,130 @@
+"""The benchmark configurations beyond the headline vortex run: the 2D
+slotted-disc revolution, the batched ensemble and the serving load test.
+Each function runs on the current CUDA device and returns a dict for the
+benchmark's JSON line."""
+import math
+import time
+
+import numpy as np
+
+from . import FP32, FP64, PHI, U, V, W, Batch, LevelSet, setups, uniform_nodes
+
+
+def _events(stream_ptr):
+    import torch
+    s = torch.cuda.ExternalStream(stream_ptr)
+    return s, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def heaviside(phi, eps):
+    return np.where(phi > eps, 1.0, np.where(phi < -eps, 0.0, 0.5 * (1 + phi / eps + np.sin(np.pi * phi / eps) / np.pi)))
+
+
+def slotted_disk_revolution(n=128, precision=FP64):
+    """2D slotted disc, rigid rotation for one period (t = 1): device time,
+    cell-updates/s, L1 area error of the returned shape and relative volume
+    change."""
+    c = setups.slotted_disk(n)
+    with LevelSet(n, 1, n, c.xn, c.yn, c.zn, precision=precision, **c.flags()) as ls:
+        for f, a in ((PHI, c.phi), (U, c.u), (V, c.v), (W, c.w)):
+            ls.upload(f, a)
+        v0 = ls.volume()[0]
+        # the CFL step is constant (steady velocity): take it once, step to t = 1
+        dt = ls.cfl_dt()
+        nsteps = int(math.ceil(1.0 / dt - 1e-9))
+        dt = 1.0 / nsteps
+        ls.set_dt(dt)
+        s, e0, e1 = _events(ls.stream())
+        ls.sync()
+        e0.record(s)
+        for _ in range(nsteps):
+            ls.step()
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        phi = ls.download(PHI)
+        v1 = ls.volume()[0]
+    h = 1.0 / n
+    a0 = c.phi[3:3 + n, 3, 3:3 + n]
+    a1 = phi[3:3 + n, 3, 3:3 + n]
+    l1 = float(np.sum(np.abs(heaviside(a1, 1.5 * h) - heaviside(a0, 1.5 * h))) * h * h)
+    return {"workload": f"slotted disc 2D {n}x{n}, one revolution", "steps": nsteps, "ms": ms,
+            "cell_updates_per_s": n * n * nsteps / (ms * 1e-3), "l1_area_error": l1,
+            "relative_volume_change": abs(v1 - v0) / abs(v0), "precision": "fp64" if precision == FP64 else "fp32"}
+
+
+def ensemble_specs(seed=0, count=64, edges=tuple(range(64, 257, 32))):
+    """Parameters of the batched ensemble (same draw order as
+    setups.random_instance): 50/50 2D/3D, edges uniform in `edges`, 1-8
+    spheres, 4 Taylor-Green modes."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for q in range(count):
+        two_d = bool(rng.integers(0, 2))
+        nx = int(rng.choice(edges))
+        nz = int(rng.choice(edges))
+        ny = 1 if two_d else int(rng.choice(edges))
+        ns = int(rng.integers(1, 9))
+        cs = rng.uniform(0.2, 0.8, size=(ns, 3))
+        rs = rng.uniform(0.05, 0.2, size=ns)
+        modes = [(int(rng.integers(1, 4)), float(rng.normal(0.0, 0.5))) for _ in range(4)]
+        sph = [(float(c[0]), float(c[1]), float(c[2]), float(r)) for c, r in zip(cs, rs)]
+        specs.append(((nx, ny, nz), sph, modes))
+    return specs
+
+
+def make_instance(dims, sph, modes, precision=FP32, f44=2, cfl=0.25):
+    nx, ny, nz = dims
+    yn = uniform_nodes(1, 1.0 / nx) if ny == 1 else uniform_nodes(ny)
+    ls = LevelSet(nx, ny, nz, uniform_nodes(nx), yn, uniform_nodes(nz), f43=0.5, f44=f44, f45=2.1, f49=1,
+                  n47=cfl / 2.0, precision=precision)
+    ls.init_spheres_tg(sph, modes)
+    ls.set_time(0.0)
+    return ls
+
+
+def ensemble(steps=200, seed=0, count=64, autotune_cache=None, graph=True):
+    """64 instances (seed 0) advanced `steps` steps in one batch: device
+    time, aggregate cell-updates/s, launches per step and the tuned
+    configuration."""
+    specs = ensemble_specs(seed, count)
+    members = [make_instance(d, s, m) for d, s, m in specs]
+    cells = sum(d[0] * d[1] * d[2] for d, _, _ in specs)
+    with Batch() as b:
+        for m in members:
+            b.add(m)
+        t0 = time.perf_counter()
+        cfg = b.autotune(autotune_cache)
+        tune_s = time.perf_counter() - t0
+        b.use_graph(graph)
+        b.step(1)  # warm-up: builds and captures the graph
+        b.sync()
+        s, e0, e1 = _events(b.stream())
+        c0 = b.launch_count()
+        e0.record(s)
+        b.step(steps)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = b.launch_count() - c0
+    for m in members:
+        m.close()
+    n2 = sum(1 for d, _, _ in specs if d[1] == 1)
+    return {"workload": f"ensemble of {count} (seed {seed}), {n2} 2D + {count - n2} 3D, edges 64..256",
+            "steps": steps, "cells": cells, "ms": ms, "cell_updates_per_s": cells * steps / (ms * 1e-3),
+            "launches": launches, "config_rows_ctas": list(cfg), "autotune_s": tune_s, "graph": graph}
+
+
+def serving(njobs=48, rate=200.0, seed=1, budget=150e9, precision=FP32, autotune_cache=None):
+    from .serve import TransportServer, poisson_jobs, summarize
+    jobs = poisson_jobs(seed=seed, rate=rate, njobs=njobs)
+    srv = TransportServer(budget_bytes=budget, precision=precision, autotune_cache=autotune_cache)
+    try:
+        done = srv.serve(jobs, realtime=True)
+        out = summarize(done, srv.makespan)
+        out.update({"rate_jobs_per_s": rate, "seed": seed, "budget_gb": budget / 1e9,
+                    "peak_resident_gb": srv.peak_used / 1e9, "max_active": srv.max_active,
+                    "precision": "fp32 batched" if precision == FP32 else "fp64 plain"})
+    finally:
+        srv.close()
+    return out
