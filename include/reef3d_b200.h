@@ -187,6 +187,26 @@ int r3d_stream(r3d_handle* h, void** stream);
 /* Kernel launches issued on this handle since creation. */
 int r3d_launch_count(const r3d_handle* h, long long* count);
 
+/* Volume sums of a level set, allocating nothing (no counterpart in the
+ * reference: it is a variant of r3d_volume for callers that cannot allocate
+ * device memory at the time of the call -- a host code that has handed all
+ * of the GPU's memory to its own pool, or a time loop that must not take
+ * cudaMalloc's implicit device synchronisation).  phi: device array of
+ * nx*ny*nz doubles, dense x-contiguous layout (R3D_LAYOUT_DENSE); dx, dy,
+ * dz: uniform cell sizes; psi: interface half-thickness; out: device array
+ * of 2 doubles receiving volume1 and volume2 (the smoothed-Heaviside sums of
+ * src/fluid_update_fsf.cpp:50-74).  Asynchronous on `stream` (a
+ * cudaStream_t, NULL for the default stream).
+ * Its scratch is a fixed 1 MiB device array inside the library, kept by
+ * every GPU that loads it until the process exits: at most ny*nz = 65536
+ * rows (R3D_EINVAL beyond).  All calls share that array, so calls whose
+ * kernels may overlap on one GPU race and must be ordered by the caller.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.
+ * Errors: r3d_last_error(NULL). */
+int r3d_volume_dense_noalloc(const double* phi, int nx, int ny, int nz, double dx, double dy, double dz,
+                             double psi, double* out, void* stream);
+
 /* ---------------------------------------------------------------- batches
  * Many FP32 instances of uneven sizes (2D and 3D mixed) advanced together:
  * one persistent launch per RK stage over a packed tile list of all members,

@@ -77,6 +77,9 @@ EXPORTS = {
     "r3d_sync": ([_H], ctypes.c_int),
     "r3d_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "r3d_volume_dense_noalloc": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                  ctypes.c_void_p], ctypes.c_int),
     "r3d_batch_create": ([ctypes.POINTER(_H)], ctypes.c_int),
     "r3d_batch_destroy": ([_H], ctypes.c_int),
     "r3d_batch_last_error": ([_H], ctypes.c_char_p),

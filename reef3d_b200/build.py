@@ -29,6 +29,7 @@ UNITS = [
     ("kernels_f32.cu", ["-fmad=true"]),
     ("kernels_f32_tile.cu", ["-fmad=true"]),
     ("kernels_batch.cu", ["-fmad=true"]),
+    ("noalloc.cu", ["-fmad=false"]),
     ("kernels_common.cu", ["-fmad=false"]),
     ("grid_metrics.cpp", []),
     ("api.cpp", []),

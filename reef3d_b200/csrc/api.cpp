@@ -246,6 +246,11 @@ int check_device_flag(r3d_handle* h) {
 
 }  // namespace
 
+namespace r3d {
+// Error text of calls that have no handle (returned by r3d_last_error(NULL)).
+void set_thread_error(const char* msg) { g_thread_err = msg ? msg : ""; }
+}  // namespace r3d
+
 extern "C" {
 
 const char* r3d_last_error(const r3d_handle* h) { return h ? h->err.c_str() : g_thread_err.c_str(); }
