@@ -234,10 +234,32 @@ def stage_roofline(ls, cells, elem, peak_gbs, reps=20):
             "conv_stage_ms": t_conv, "reinit_stage_ms": t_rein}
 
 
+def tile_variants(ls, reps=10):
+    """Stage times of the tiled FP32 kernels under other chunkings and with
+    the FP64 interface band off (information for the tuning of R3D_OPT_*)."""
+    import reef3d_b200 as r3d
+    if not ls.get_option(r3d.OPT_TILED):
+        return None
+    out = {}
+    base_kc = ls.get_option(r3d.OPT_CHUNK)
+    for kc in (8, 16, 32, 64):
+        ls.set_option(r3d.OPT_CHUNK, kc)
+        out[f"kc{kc}"] = {"conv_ms": device_time(ls, lambda: ls.stage(r3d.STAGE_CONVECTION, 2), reps),
+                          "reinit_ms": device_time(ls, lambda: ls.stage(r3d.STAGE_REINIT, 2), reps)}
+    ls.set_option(r3d.OPT_CHUNK, base_kc)
+    ls.set_option(r3d.OPT_BAND64, 0)
+    out["band64_off_reinit_ms"] = device_time(ls, lambda: ls.stage(r3d.STAGE_REINIT, 2), reps)
+    ls.set_option(r3d.OPT_BAND64, 1)
+    return out
+
+
 def e2e_steps(case, precision, steps, warmup):
-    """Through the C-ABI with host buffers in the reference's layout: every
-    step uploads phi, u, v, w from pinned host memory, runs the step (CFL +
-    RK3 convection + reinitialisation + volume) and downloads phi."""
+    """Through the C-ABI with host buffers in the reference's layout, the
+    way the levelset_RK3 adapter of INTEGRATION.md drives it: the level set
+    stays on the device between steps; every step uploads the velocities
+    u, v, w the host's momentum solver owns (pinned host memory), runs the
+    step (CFL + RK3 convection + reinitialisation + volume) and downloads
+    phi for the host's density update."""
     import torch
 
     import reef3d_b200 as r3d
@@ -252,8 +274,10 @@ def e2e_steps(case, precision, steps, warmup):
     ls = r3d.LevelSet(n, n, n, case.xn, case.yn, case.zn, precision=precision, **case.flags())
     ids = (("phi", r3d.PHI), ("u", r3d.U), ("v", r3d.V), ("w", r3d.W))
 
+    ls.upload_ptr(r3d.PHI, pinned["phi"].data_ptr())
+
     def one():
-        for name, fid in ids:
+        for name, fid in ids[1:]:
             ls.upload_ptr(fid, pinned[name].data_ptr())
         ls.run(1, adaptive=True)
         ls.download_ptr(r3d.PHI, out.data_ptr())
@@ -268,40 +292,7 @@ def e2e_steps(case, precision, steps, warmup):
     el = time.perf_counter() - t0
     ls.close()
     nbytes = pinned["phi"].numel() * 8
-    return n ** 3 * steps / el, 4 * nbytes, nbytes
-
-
-class DistCtx:
-    def __init__(self):
-        import torch
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.dist = None
-        if torch.cuda.is_available():
-            torch.cuda.set_device(self.local)
-        if self.world > 1:
-            import datetime
-
-            import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-            self.dist = dist
-
-    def barrier(self):
-        if self.dist is not None:
-            self.dist.barrier(device_ids=[self.local])
-
-    def max(self, x):
-        if self.dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.dist is not None:
-            self.dist.destroy_process_group()
+    return n ** 3 * steps / el, 3 * nbytes, nbytes
 
 
 def run_ours(args):
@@ -310,7 +301,8 @@ def run_ours(args):
     import reef3d_b200 as r3d
     from reef3d_b200 import setups
 
-    ctx = DistCtx()
+    from reef3d_b200.replicas import Replicas
+    ctx = Replicas()
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -327,6 +319,7 @@ def run_ours(args):
         total32, per32, launches32 = timed_steps(ls32, args.steps, args.warmup, ctx)
     total32 = ctx.max(total32)
     roof32 = stage_roofline(ls32, cells, 4, peak_gbs)
+    variants = tile_variants(ls32)
     ls32.close()
     # FP64 plain -----------------------------------------------------------
     ls64 = make_instance(case, r3d.FP64)
@@ -341,7 +334,8 @@ def run_ours(args):
         rate, h2d, d2h = e2e_steps(case, r3d.FP32, e2e_steps_n, 1)
         e2e = {"value": rate * ctx.world, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": e2e_steps_n,
-               "path": "r3d_upload(phi,u,v,w) + r3d_ls_run(1) + r3d_download(phi), pinned host, FP32 form"}
+               "path": "r3d_upload(u,v,w) + r3d_ls_run(1) + r3d_download(phi) per step (phi resident), "
+                       "pinned host buffers in the reference layout, FP32 form"}
     cpu = None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu:
         rate, info = reference_cpu(min(os.cpu_count() or 1, 8), 96, 2)
@@ -367,6 +361,7 @@ def run_ours(args):
                        "gpu_launches": launches64},
         "fp32_over_fp64": value32 / value64,
         "roofline": dict(roof32, traffic=None, peak_source=peak_src),
+        "tile_variants": variants,
         "gpu_launches": launches32,
         "clocks": clk.summary(),
         "e2e": e2e,

@@ -172,7 +172,11 @@ struct DeviceGuard {
 
 bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile; }
 
-TileArgs tile_args(r3d_handle* h, int stage) {
+}  // namespace
+
+namespace r3d {
+// Tiled-kernel arguments of an instance for stage 1..3 (also used by batches).
+TileArgs make_tile_args(r3d_handle* h, int stage) {
     TileArgs a{};
     a.L = h->L;
     a.fn = static_cast<const float*>(h->field[R3D_PHI]);
@@ -199,6 +203,10 @@ TileArgs tile_args(r3d_handle* h, int stage) {
     a.kc = h->kc;
     return a;
 }
+}  // namespace r3d
+
+namespace {
+TileArgs tile_args(r3d_handle* h, int stage) { return r3d::make_tile_args(h, stage); }
 
 long long stage_launch(r3d_handle* h, bool reini, int s, bool vol) {
     const Fields f = fields_of(h);

@@ -27,6 +27,11 @@ struct r3d_batch {
     // device state, rebuilt when the membership or the configuration changes
     MemberDesc* d_members = nullptr;
     long long* d_tile0 = nullptr;
+    TiledMember* d_tiled = nullptr;   // members on the tiled kernels come first
+    CUtensorMap* d_maps = nullptr;    // 3 per tiled member
+    size_t cap_tiled = 0;
+    int n_tiled = 0;
+    long long t_tiled = 0;            // items of the tiled members: tiles [0, t_tiled)
     double* d_vol = nullptr;
     double* d_vmax = nullptr;
     size_t cap_members = 0, cap_tiles = 0;
@@ -84,18 +89,61 @@ MemberDesc describe(const r3d_handle* h) {
     return m;
 }
 
+bool on_tiles(const r3d_handle* h) { return h->tile_ok && h->use_tile; }
+
 int rebuild(r3d_batch* b) {
     drop_graph(b);
     const size_t nm = b->members.size();
+    // members on the tiled kernels first, the others after them
+    std::vector<r3d_handle*> order;
+    for (r3d_handle* h : b->members)
+        if (on_tiles(h)) order.push_back(h);
+    b->n_tiled = (int)order.size();
+    for (r3d_handle* h : b->members)
+        if (!on_tiles(h)) order.push_back(h);
     std::vector<MemberDesc> desc(nm);
     std::vector<long long> tile0(nm + 1, 0);
+    std::vector<TiledMember> tiled(b->n_tiled);
+    std::vector<CUtensorMap> maps(3 * (size_t)b->n_tiled);
     b->max_f44 = 0;
     for (size_t q = 0; q < nm; ++q) {
-        desc[q] = describe(b->members[q]);
-        tile0[q + 1] = tile0[q] + batch_tiles_of(b->members[q]->L, b->rows);
-        b->max_f44 = std::max(b->max_f44, b->members[q]->desc.f44);
+        r3d_handle* h = order[q];
+        desc[q] = describe(h);
+        const bool t = (int)q < b->n_tiled;
+        tile0[q + 1] = tile0[q] + (t ? tile_items_of(h->L, h->kc) : batch_tiles_of(h->L, b->rows));
+        b->max_f44 = std::max(b->max_f44, h->desc.f44);
+        if (t) {
+            TiledMember& m = tiled[q];
+            m.args = make_tile_args(h, 1);
+            m.phi = static_cast<float*>(h->field[R3D_PHI]);
+            m.a1 = static_cast<float*>(h->field[R3D_WORK1]);
+            m.a2 = static_cast<float*>(h->field[R3D_WORK2]);
+            m.f44 = h->desc.f44;
+            for (int s = 0; s < 3; ++s) maps[3 * q + s] = h->map[s];
+        }
     }
+    b->t_tiled = tile0[b->n_tiled];
     b->ntiles = tile0[nm];
+    if ((size_t)b->n_tiled > b->cap_tiled) {
+        if (b->d_tiled) cudaFree(b->d_tiled);
+        if (b->d_maps) cudaFree(b->d_maps);
+        b->d_tiled = nullptr;
+        b->d_maps = nullptr;
+        const size_t cap = std::max<size_t>((size_t)b->n_tiled, 2 * b->cap_tiled);
+        if (cudaMalloc(&b->d_tiled, cap * sizeof(TiledMember)) != cudaSuccess ||
+            cudaMalloc(&b->d_maps, 3 * cap * sizeof(CUtensorMap)) != cudaSuccess) {
+            cudaGetLastError();
+            b->cap_tiled = 0;
+            return bfail(b, R3D_ENOMEM, "batch tiled-member allocation failed");
+        }
+        b->cap_tiled = cap;
+    }
+    if (b->n_tiled) {
+        B_CUDA(b, cudaMemcpyAsync(b->d_tiled, tiled.data(), tiled.size() * sizeof(TiledMember),
+                                  cudaMemcpyHostToDevice, b->stream));
+        B_CUDA(b, cudaMemcpyAsync(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                                  b->stream));
+    }
     if (nm > b->cap_members) {
         if (b->d_members) cudaFree(b->d_members);
         if (b->d_tile0) cudaFree(b->d_tile0);
@@ -132,11 +180,13 @@ int rebuild(r3d_batch* b) {
     return R3D_OK;
 }
 
+// All members (for the per-member reductions).
 BatchLaunch launch_of(const r3d_batch* b) {
     BatchLaunch l{};
     l.members = b->d_members;
     l.tile0 = b->d_tile0;
     l.nm = (int)b->members.size();
+    l.t_begin = 0;
     l.ntiles = b->ntiles;
     l.vol_part = b->d_vol;
     l.vmax_part = b->d_vmax;
@@ -146,15 +196,41 @@ BatchLaunch launch_of(const r3d_batch* b) {
     return l;
 }
 
+// The members on the one-cell-per-thread kernels: tiles [t_tiled, ntiles).
+BatchLaunch cell_launch_of(const r3d_batch* b) {
+    BatchLaunch l = launch_of(b);
+    l.members = b->d_members + b->n_tiled;
+    l.tile0 = b->d_tile0 + b->n_tiled;
+    l.nm = (int)b->members.size() - b->n_tiled;
+    l.t_begin = b->t_tiled;
+    return l;
+}
+
+unsigned tiled_grid(const r3d_batch* b) {
+    const long long want = 2LL * b->sms;  // two 256-thread CTAs of 45 KB per SM
+    return (unsigned)std::max<long long>(1, std::min<long long>(want, b->t_tiled));
+}
+
+long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
+    long long n = 0;
+    if (b->n_tiled)
+        n += launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, reini, s, q, b->d_vol,
+                                     tiled_grid(b), b->stream);
+    if ((size_t)b->n_tiled < b->members.size())
+        n += launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, b->stream);
+    return n;
+}
+
 // CFL, 3 convection stages, max(f44) reinit pseudo-steps, volume + clock.
 long long enqueue_batch_step(r3d_batch* b) {
-    const BatchLaunch l = launch_of(b);
     long long n = 0;
-    n += launch_batch_cfl(l, b->stream);
-    for (int s = 1; s <= 3; ++s) n += launch_batch_stage(l, 1, s, 0, b->stream);
+    if (b->n_tiled) n += launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b), b->stream);
+    if ((size_t)b->n_tiled < b->members.size()) n += launch_batch_vmax(cell_launch_of(b), b->stream);
+    n += launch_batch_dt(launch_of(b), b->stream);
+    for (int s = 1; s <= 3; ++s) n += enqueue_stage(b, false, s, 0);
     for (int q = 0; q < b->max_f44; ++q)
-        for (int s = 1; s <= 3; ++s) n += launch_batch_stage(l, 0, s, q, b->stream);
-    n += launch_batch_finish(l, b->stream);
+        for (int s = 1; s <= 3; ++s) n += enqueue_stage(b, true, s, q);
+    n += launch_batch_finish(launch_of(b), b->stream);
     return n;
 }
 
@@ -236,6 +312,8 @@ int r3d_batch_destroy(r3d_batch* b) {
     if (b->d_tile0) cudaFree(b->d_tile0);
     if (b->d_vol) cudaFree(b->d_vol);
     if (b->d_vmax) cudaFree(b->d_vmax);
+    if (b->d_tiled) cudaFree(b->d_tiled);
+    if (b->d_maps) cudaFree(b->d_maps);
     cudaStreamDestroy(b->stream);
     delete b;
     return R3D_OK;
@@ -326,19 +404,20 @@ int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows_out, int*
     b->rows = 4;
     b->ctas_per_sm = 8;
     if (int rc = rebuild(b)) return rc;
-    launch_batch_cfl(launch_of(b), b->stream);
+    if (b->n_tiled) launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b), b->stream);
+    if ((size_t)b->n_tiled < b->members.size()) launch_batch_vmax(cell_launch_of(b), b->stream);
+    launch_batch_dt(launch_of(b), b->stream);
     for (int r : cand_rows)
         for (int c : cand_ctas) {
             if (c * 32 * r > 2048) continue;
             b->rows = r;
             b->ctas_per_sm = c;
             if (int rc = rebuild(b)) return rc;
-            const BatchLaunch l = launch_of(b);
-            launch_batch_stage(l, 1, 1, 0, b->stream);  // warm
+            enqueue_stage(b, false, 1, 0);  // warm
             cudaEventRecord(e0, b->stream);
             for (int rep = 0; rep < 3; ++rep) {
-                launch_batch_stage(l, 1, 1, 0, b->stream);
-                launch_batch_stage(l, 0, 1, 0, b->stream);
+                enqueue_stage(b, false, 1, 0);
+                enqueue_stage(b, true, 1, 0);
             }
             cudaEventRecord(e1, b->stream);
             B_CUDA(b, cudaEventSynchronize(e1));
@@ -386,8 +465,11 @@ int r3d_batch_step(r3d_batch* b, int nsteps) {
             }
         }
         if (!rc) {
-            const long long per = 2 + 3 + 3 * b->max_f44 + 1;
-            if (b->graph) b->launches += per * nsteps;
+            if (b->graph) {
+                const int kinds = (b->n_tiled ? 1 : 0) + ((size_t)b->n_tiled < b->members.size() ? 1 : 0);
+                const long long per = kinds + 1 + kinds * (3 + 3 * b->max_f44) + 1;
+                b->launches += per * nsteps;
+            }
             b->steps += nsteps;
             for (r3d_handle* h : b->members) h->have_last_volume = true;
         }

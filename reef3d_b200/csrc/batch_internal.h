@@ -28,7 +28,8 @@ struct BatchLaunch {
     const MemberDesc* members;
     const long long* tile0;  // first tile of each member, nm+1 entries
     int nm;
-    long long ntiles;
+    long long t_begin;       // first tile of these members in the batch's tile space
+    long long ntiles;        // one past the last tile
     double* vol_part;        // 2 per tile
     double* vmax_part;       // 3 per tile
     int rows;                // tile rows (2, 4 or 8); 32*rows threads per CTA
@@ -38,6 +39,8 @@ struct BatchLaunch {
 long long batch_tiles_of(const Layout& L, int rows);
 int launch_batch_stage(const BatchLaunch& b, int conv, int stage, int q, cudaStream_t st);
 int launch_batch_cfl(const BatchLaunch& b, cudaStream_t st);
+int launch_batch_vmax(const BatchLaunch& b, cudaStream_t st);   // per-tile maxima only
+int launch_batch_dt(const BatchLaunch& b, cudaStream_t st);     // per-member dt from the maxima
 int launch_batch_finish(const BatchLaunch& b, cudaStream_t st);
 
 }  // namespace r3d

@@ -39,3 +39,7 @@ struct r3d_handle {
     cudaStream_t batch_stream = nullptr;
     std::string err;
 };
+
+namespace r3d {
+TileArgs make_tile_args(r3d_handle* h, int stage);
+}

@@ -71,10 +71,10 @@ __device__ __forceinline__ void cta_sum2(double a, double b, double* dst) {
 template <int ROWS>
 __global__ void __launch_bounds__(32 * ROWS) batch_stage_kernel(const MemberDesc* __restrict__ members,
                                                                 const long long* __restrict__ tile0, int nm,
-                                                                long long ntiles, int conv, int stage, int q,
-                                                                double* __restrict__ partial) {
+                                                                long long t_begin, long long ntiles, int conv,
+                                                                int stage, int q, double* __restrict__ partial) {
     __shared__ MemberDesc sm;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (long long t = t_begin + blockIdx.x; t < ntiles; t += gridDim.x) {
         const int mi = find_member(tile0, nm, t);
         __syncthreads();
         if (threadIdx.x == 0) sm = members[mi];
@@ -145,10 +145,11 @@ __global__ void __launch_bounds__(32 * ROWS) batch_stage_kernel(const MemberDesc
 template <int ROWS>
 __global__ void __launch_bounds__(32 * ROWS) batch_vmax_kernel(const MemberDesc* __restrict__ members,
                                                                const long long* __restrict__ tile0, int nm,
-                                                               long long ntiles, double* __restrict__ partial) {
+                                                               long long t_begin, long long ntiles,
+                                                               double* __restrict__ partial) {
     __shared__ MemberDesc sm;
     __shared__ double s[3][ROWS];
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (long long t = t_begin + blockIdx.x; t < ntiles; t += gridDim.x) {
         const int mi = find_member(tile0, nm, t);
         __syncthreads();
         if (threadIdx.x == 0) sm = members[mi];
@@ -251,19 +252,34 @@ long long batch_tiles_of(const Layout& L, int rows) {
 int launch_batch_stage(const BatchLaunch& b, int conv, int stage, int q, cudaStream_t st) {
     const dim3 grid(b.grid), block(32 * b.rows);
     switch (b.rows) {
-        case 2: batch_stage_kernel<2><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.ntiles, conv, stage, q, b.vol_part); break;
-        case 8: batch_stage_kernel<8><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.ntiles, conv, stage, q, b.vol_part); break;
-        default: batch_stage_kernel<4><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.ntiles, conv, stage, q, b.vol_part); break;
+        case 2: batch_stage_kernel<2><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, conv, stage, q, b.vol_part); break;
+        case 8: batch_stage_kernel<8><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, conv, stage, q, b.vol_part); break;
+        default: batch_stage_kernel<4><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, conv, stage, q, b.vol_part); break;
     }
+    return 1;
+}
+
+int launch_batch_vmax(const BatchLaunch& b, cudaStream_t st) {
+    const dim3 grid(b.grid), block(32 * b.rows);
+    switch (b.rows) {
+        case 2: batch_vmax_kernel<2><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, b.vmax_part); break;
+        case 8: batch_vmax_kernel<8><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, b.vmax_part); break;
+        default: batch_vmax_kernel<4><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, b.vmax_part); break;
+    }
+    return 1;
+}
+
+int launch_batch_dt(const BatchLaunch& b, cudaStream_t st) {
+    batch_member_kernel<<<b.nm, 256, 0, st>>>(b.members, b.tile0, b.nm, 0, b.vmax_part, b.vol_part);
     return 1;
 }
 
 int launch_batch_cfl(const BatchLaunch& b, cudaStream_t st) {
     const dim3 grid(b.grid), block(32 * b.rows);
     switch (b.rows) {
-        case 2: batch_vmax_kernel<2><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.ntiles, b.vmax_part); break;
-        case 8: batch_vmax_kernel<8><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.ntiles, b.vmax_part); break;
-        default: batch_vmax_kernel<4><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.ntiles, b.vmax_part); break;
+        case 2: batch_vmax_kernel<2><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, b.vmax_part); break;
+        case 8: batch_vmax_kernel<8><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, b.vmax_part); break;
+        default: batch_vmax_kernel<4><<<grid, block, 0, st>>>(b.members, b.tile0, b.nm, b.t_begin, b.ntiles, b.vmax_part); break;
     }
     batch_member_kernel<<<b.nm, 256, 0, st>>>(b.members, b.tile0, b.nm, 0, b.vmax_part, b.vol_part);
     return 2;

@@ -39,6 +39,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
@@ -148,25 +151,31 @@ __device__ double reini_cell_fp64(const float* fx, const float* fy, const float*
     return f32::reini_rhs_uniform<double, false>(X, Y, Z, rh, hh, 1.0e-6, (double)a.deltax);
 }
 
-template <bool REINI, int STAGE, bool VOLUME>
-__global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
+// One work item: the 64 x 8 column (bx, by) over planes [bz*kc, bz*kc+kc)
+// of one instance.  Returns false when a bounded wait gave up (the error
+// flag is raised and the copies in flight have been waited for).  The
+// item's volume partials (when `volume`) go to partial_out[0..1].  The
+// mbarriers are initialised at the start of the item and invalidated at its
+// end, so a persistent CTA can run items back to back.
+template <bool REINI, int STAGE>
+__device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArgs& a, int bx, int by, int bz,
+                                          bool volume, unsigned char* smem_raw, double* red_a, double* red_b,
+                                          double* partial_out) {
     // shared memory: ring of kSlots plane boxes, 3 boxes for the planes
     // below the chunk, then the mbarriers
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     float* slots = reinterpret_cast<float*>(smem_raw);
     float* below = slots + kSlots * kSlotFloats;
     uint64_t* bar = reinterpret_cast<uint64_t*>(below + 3 * kSlotFloats);
     uint64_t* xbar = bar + kSlots;
-    __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
 
     const Layout& L = a.L;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int i0 = blockIdx.x * kTX + 2 * tx;
-    const int j = blockIdx.y * kTY + ty;
-    const int k0 = blockIdx.z * a.kc;
+    const int i0 = bx * kTX + 2 * tx;
+    const int j = by * kTY + ty;
+    const int k0 = bz * a.kc;
     const int k1 = min(k0 + a.kc, L.nz);
-    const int xbox = blockIdx.x * kTX + L.gx - 4;  // 16-byte aligned x start
-    const int ybox = blockIdx.y * kTY + L.gy - 3;
+    const int xbox = bx * kTX + L.gx - 4;  // 16-byte aligned x start
+    const int ybox = by * kTY + L.gy - 3;
     const int plast = k1 + 2;  // last plane staged in the ring
     const bool act0 = i0 < L.nx && j < L.ny;
     const bool act1 = i0 + 1 < L.nx && j < L.ny;
@@ -179,12 +188,12 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
         mbar_fence_init();
         for (int m = 0; m < 3; ++m) {
             mbar_expect_tx(xbar + m, kBoxBytes);
-            tma_load_3d(below + m * kSlotFloats, &tmap, xbar + m, xbox, ybox, k0 - 3 + m + L.gz);
+            tma_load_3d(below + m * kSlotFloats, tmap, xbar + m, xbox, ybox, k0 - 3 + m + L.gz);
         }
         for (int p = k0; p <= min(k0 + kSlots - 1, plast); ++p) {
             const int s = (p - k0) % kSlots;
             mbar_expect_tx(bar + s, kBoxBytes);
-            tma_load_3d(slots + s * kSlotFloats, &tmap, bar + s, xbox, ybox, p + L.gz);
+            tma_load_3d(slots + s * kSlotFloats, tmap, bar + s, xbox, ybox, p + L.gz);
             issued = p;
         }
     }
@@ -366,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
             if (k == L.nz - 1)
                 for (int q = 1; q <= 3; ++q)
                     for (int e = 0; e < nw; ++e) a.out[c + q * L.sz + e] = e ? val.y : val.x;
-            if (VOLUME) {
+            if (volume) {
                 // smoothed Heaviside in FP64 (src/fluid_update_fsf.cpp:50-71)
                 const double PI_REF = 3.14159265359;
                 for (int e = 0; e < nw; ++e) {
@@ -389,7 +398,7 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
             const int s = (pn - k0) % kSlots;
             fence_proxy_async();
             mbar_expect_tx(bar + s, kBoxBytes);
-            tma_load_3d(slots + s * kSlotFloats, &tmap, bar + s, xbox, ybox, pn + L.gz);
+            tma_load_3d(slots + s * kSlotFloats, tmap, bar + s, xbox, ybox, pn + L.gz);
             issued = pn;
         }
 #pragma unroll
@@ -403,9 +412,9 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
             for (int m = 0; m < 3; ++m) mbar_wait_bounded(xbar + m, 0);
             for (int p = k0; p <= issued; ++p) mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
         }
-        return;
+        return false;
     }
-    if (VOLUME) {
+    if (volume) {
         for (int o = 16; o > 0; o >>= 1) {
             vol_a += __shfl_down_sync(0xffffffffu, vol_a, o);
             vol_b += __shfl_down_sync(0xffffffffu, vol_b, o);
@@ -415,14 +424,152 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
         if (threadIdx.x == 0) {
             double sa = 0.0, sb = 0.0;
             for (int q = 0; q < kThreads / 32; ++q) { sa += red_a[q]; sb += red_b[q]; }
-            const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-            a.partial[2 * b] = sa;
-            a.partial[2 * b + 1] = sb;
+            partial_out[0] = sa;
+            partial_out[1] = sb;
         }
+    }
+    // every wait of the item has completed: retire the barriers
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int s = 0; s < kSlots + 3; ++s) mbar_inval(bar + s);
+    __syncthreads();
+    return true;
+}
+
+template <bool REINI, int STAGE, bool VOLUME>
+__global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
+    const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    tile_item<REINI, STAGE>(&tmap, a, blockIdx.x, blockIdx.y, blockIdx.z, VOLUME, smem_raw, red_a, red_b,
+                            a.partial + 2 * b);
+}
+
+// Persistent batched form: CTAs walk the work items of all tiled members
+// (member m owns items [tile0[m], tile0[m+1]); item = (bx, by, bz) of that
+// member).  Reinitialisation pseudo-step q is skipped by members with
+// f44 <= q; the last stage of a member's step adds its volume partials.
+template <bool REINI, int STAGE>
+__global__ void __launch_bounds__(kThreads, 2) batch_tile_kernel(const TiledMember* __restrict__ members,
+                                                                 const CUtensorMap* __restrict__ maps,
+                                                                 const long long* __restrict__ tile0, int nm,
+                                                                 int q, double* __restrict__ vol_part) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
+    __shared__ TileArgs sa;
+    __shared__ int s_member;
+    const long long nt = tile0[nm];
+    for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = nm - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (tile0[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            s_member = lo;
+            sa = members[lo].args;
+            sa.out = STAGE == 1 ? members[lo].a1 : STAGE == 2 ? members[lo].a2 : members[lo].phi;
+        }
+        __syncthreads();
+        const int m = s_member;
+        const int f44 = members[m].f44;
+        if (REINI && f44 <= q) {
+            __syncthreads();
+            continue;
+        }
+        const bool volume = STAGE == 3 && (REINI ? q == f44 - 1 : f44 == 0);
+        const long long lt = t - tile0[m];
+        const int ntx = (sa.L.nx + kTX - 1) / kTX, nty = (sa.L.ny + kTY - 1) / kTY;
+        const int bx = (int)(lt % ntx);
+        const int by = (int)((lt / ntx) % nty);
+        const int bz = (int)(lt / ((long long)ntx * nty));
+        if (!tile_item<REINI, STAGE>(maps + 3 * m + (STAGE - 1), sa, bx, by, bz, volume, smem_raw, red_a, red_b,
+                                     vol_part + 2 * t))
+            return;
+    }
+}
+
+// Face maxima over the cells of one item (x faces 0..nx-2, y 0..ny-2, z
+// 0..nz-2, src/ietimestep.cpp:72-88) for every tiled member's item.
+__global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMember* __restrict__ members,
+                                                                   const long long* __restrict__ tile0, int nm,
+                                                                   double* __restrict__ vmax_part) {
+    __shared__ double s[3][kThreads / 32];
+    const long long nt = tile0[nm];
+    for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
+        int lo = 0, hi = nm - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tile0[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const TileArgs& a = members[lo].args;
+        const Layout& L = a.L;
+        const long long lt = t - tile0[lo];
+        const int ntx = (L.nx + kTX - 1) / kTX, nty = (L.ny + kTY - 1) / kTY;
+        const int bx = (int)(lt % ntx), by = (int)((lt / ntx) % nty), bz = (int)(lt / ((long long)ntx * nty));
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        const int j = by * kTY + ty;
+        const int k0 = bz * a.kc, k1 = min(k0 + a.kc, L.nz);
+        double mu = 0.0, mv = 0.0, mw = 0.0;
+        if (j < L.ny)
+            for (int k = k0; k < k1; ++k)
+                for (int e = 0; e < 2; ++e) {
+                    const int i = bx * kTX + 2 * tx + e;
+                    if (i >= L.nx) continue;
+                    const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+                    if (i < L.nx - 1) mu = fmax(mu, fabs((double)a.u[c]));
+                    if (j < L.ny - 1) mv = fmax(mv, fabs((double)a.v[c]));
+                    if (k < L.nz - 1) mw = fmax(mw, fabs((double)a.w[c]));
+                }
+        for (int o = 16; o > 0; o >>= 1) {
+            mu = fmax(mu, __shfl_down_sync(0xffffffffu, mu, o));
+            mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+            mw = fmax(mw, __shfl_down_sync(0xffffffffu, mw, o));
+        }
+        if (tx == 0) { s[0][ty] = mu; s[1][ty] = mv; s[2][ty] = mw; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int q = 1; q < kThreads / 32; ++q) { mu = fmax(mu, s[0][q]); mv = fmax(mv, s[1][q]); mw = fmax(mw, s[2][q]); }
+            vmax_part[3 * t] = mu;
+            vmax_part[3 * t + 1] = mv;
+            vmax_part[3 * t + 2] = mw;
+        }
+        __syncthreads();
     }
 }
 
 }  // namespace
+
+long long tile_items_of(const Layout& L, int kc) {
+    const dim3 g = tile_grid(L, kc);
+    return (long long)g.x * g.y * g.z;
+}
+
+int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
+                            bool reini, int stage, int q, double* vol_part, unsigned grid, cudaStream_t st) {
+    const size_t sm = tile_smem_bytes();
+    const dim3 g(grid), block(kThreads);
+#define R3D_BT(R, S) batch_tile_kernel<R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part)
+    if (reini) {
+        if (stage == 1) R3D_BT(true, 1);
+        else if (stage == 2) R3D_BT(true, 2);
+        else R3D_BT(true, 3);
+    } else {
+        if (stage == 1) R3D_BT(false, 1);
+        else if (stage == 2) R3D_BT(false, 2);
+        else R3D_BT(false, 3);
+    }
+#undef R3D_BT
+    return 1;
+}
+
+int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, double* vmax_part,
+                           unsigned grid, cudaStream_t st) {
+    batch_tile_vmax_kernel<<<grid, kThreads, 0, st>>>(members, tile0, nm, vmax_part);
+    return 1;
+}
 
 int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::string* why) {
     using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,

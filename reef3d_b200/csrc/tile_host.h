@@ -29,9 +29,25 @@ struct TileArgs {
     int kc;
 };
 
+// A member of a batch that runs on the tiled kernels (3D, uniform, FP32).
+struct TiledMember {
+    TileArgs args;  // fn, u, v, w, dt, vscale, err, metrics, kc; out set per stage
+    float* phi;
+    float* a1;
+    float* a2;
+    int f44;
+};
+
 // Encodes the 3D tensor map of a padded FP32 field for the 72 x 14 x 1
 // plane boxes the tile kernels load.  Returns 0 on success.
 int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::string* why);
 int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume, cudaStream_t st);
+long long tile_items_of(const Layout& L, int kc);
+// Batched persistent tiled stage over the items of nm tiled members.
+int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
+                            bool reini, int stage, int q, double* vol_part, unsigned grid, cudaStream_t st);
+// Per-item face maxima of the tiled members (3 doubles per item).
+int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, double* vmax_part,
+                           unsigned grid, cudaStream_t st);
 
 }  // namespace r3d

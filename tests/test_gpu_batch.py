@@ -139,3 +139,20 @@ def test_device_init_matches_host_setup(seed):
         for f, a in ((r3d.PHI, c.phi), (r3d.U, c.u), (r3d.V, c.v), (r3d.W, c.w)):
             got = ls.download(f)
             assert np.max(np.abs(got[m] - a[m])) <= 1e-12
+
+
+def test_batched_tiled_member_equals_single_instance_run():
+    """A 3D uniform member runs the same tiled item code in a batch as a
+    single instance does on its own: identical level set and clock."""
+    rng = np.random.default_rng(9)
+    c = setups.random_instance(rng, two_d=False, edge=(70, 33, 41))
+    single = make_member(c)
+    assert single.get_option(r3d.OPT_TILED) == 1
+    single.set_time(0.0)
+    single.run(3, adaptive=True)
+    ref = single.download(r3d.PHI)
+    t_ref = single.time()
+    single.close()
+    res = run_batch([c] + cases(10, 3), 3)
+    assert np.array_equal(res[0][0], ref)
+    assert res[0][1] == t_ref
