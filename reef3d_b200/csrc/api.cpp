@@ -117,6 +117,7 @@ void release(r3d_handle* h) {
     cudaGetDevice(&cur);
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
     for (void*& p : h->field) { if (p) cudaFree(p); p = nullptr; }
     if (h->metrics64) cudaFree(h->metrics64);
     if (h->metrics32) cudaFree(h->metrics32);
@@ -419,16 +420,66 @@ int r3d_ls_step(r3d_handle* h, double dt) {
     return R3D_OK;
 }
 
+// The launches of one step of r3d_ls_run (CFL first when adaptive).
+void enqueue_run_step(r3d_handle* h, int adaptive) {
+    if (adaptive)
+        h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h), h->M.dxmin_cfl,
+                                  h->desc.n47, h->S, h->stream);
+    enqueue_step(h);
+}
+
+long long run_graph_key(const r3d_handle* h, int adaptive) {
+    long long k = adaptive ? 1 : 0;
+    k = k * 2 + (tiled(h) ? 1 : 0);
+    k = k * 2 + (h->band64 ? 1 : 0);
+    k = k * 8192 + h->kc;
+    return k;
+}
+
+void drop_step_graph(r3d_handle* h) {
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+    h->graph_key = -1;
+}
+
+// Captures one step into a CUDA graph (the step reads dt, the clock and the
+// velocity factor from device memory, so the same graph serves every step).
+int capture_step(r3d_handle* h, int adaptive) {
+    drop_step_graph(h);
+    cudaGraph_t g = nullptr;
+    R3D_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const long long before = h->launches;
+    enqueue_run_step(h, adaptive);
+    h->graph_launches = h->launches - before;
+    h->launches = before;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "step graph capture");
+    e = cudaGraphInstantiate(&h->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->step_graph = nullptr;
+        return cuda_fail(h, e, "step graph instantiate");
+    }
+    h->graph_key = run_graph_key(h, adaptive);
+    return R3D_OK;
+}
+
 int r3d_ls_run(r3d_handle* h, int nsteps, int adaptive) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (nsteps < 0) return fail(h, R3D_EINVAL, "nsteps must be >= 0");
     DeviceGuard dg(h->device, h->batch_stream);
     if (!adaptive && !(h->dt_host > 0.0)) return fail(h, R3D_ESTATE, "no time step set");
+    const bool use_graph = nsteps >= 2 || (h->step_graph && h->graph_key == run_graph_key(h, adaptive));
+    if (use_graph && !(h->step_graph && h->graph_key == run_graph_key(h, adaptive)))
+        if (int rc = capture_step(h, adaptive)) return rc;
     for (int n = 0; n < nsteps; ++n) {
-        if (adaptive)
-            h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h),
-                                      h->M.dxmin_cfl, h->desc.n47, h->S, h->stream);
-        enqueue_step(h);
+        if (use_graph) {
+            R3D_CUDA(h, cudaGraphLaunch(h->step_graph, h->stream));
+            h->launches += h->graph_launches;
+            h->have_last_volume = true;
+        } else {
+            enqueue_run_step(h, adaptive);
+        }
     }
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
@@ -517,6 +568,7 @@ int r3d_set_velocity_scale(r3d_handle* h, double scale) {
 int r3d_set_velocity_period(r3d_handle* h, double period) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (!(period >= 0.0) || !std::isfinite(period)) return fail(h, R3D_EINVAL, "period must be >= 0");
+    if (h->period != period) drop_step_graph(h);
     h->period = period;
     return R3D_OK;
 }

@@ -37,6 +37,11 @@ struct r3d_handle {
     // set while the instance is a member of a batch: calls on the handle
     // first wait for the batch's stream
     cudaStream_t batch_stream = nullptr;
+    // one captured step (CFL when adaptive + the step) replayed by r3d_ls_run;
+    // rebuilt when anything baked into it changes
+    cudaGraphExec_t step_graph = nullptr;
+    long long graph_key = -1;
+    long long graph_launches = 0;
     std::string err;
 };
 
