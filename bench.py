@@ -29,6 +29,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_CELLS_EDGE = 256
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the dominant FP32 kernel, the tiled reinitialisation stage 2, measured by ncu
+# on the 256^3 vortex (profiles/tile_stage_kernels_vortex.txt)
+NCU_TRAFFIC = {(256, "reinit_stage"): 144.57e6 + 48.61e6}
 METRIC = "level-set cell-updates/s (RK3+reinit), FP64 plain vs FP32 batched; p50/p99 latency"
 WORKLOAD = "3D single-vortex deformation 256^3, CFL 0.25, F44=2 reinit pseudo-steps, T=3"
 
@@ -42,6 +46,8 @@ def parse():
     ap.add_argument("--edge", type=int, default=N_CELLS_EDGE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other workloads (slotted disc, vortex accuracy, wave tank, ensemble, serving)")
     return ap.parse_args()
 
 
@@ -139,6 +145,49 @@ def reference_cpu(procs, edge, steps):
                              "build": "-O3 -mavx2 -mfma" if fast else "-O2 -ffp-contract=off",
                              "sample": f"{procs} processes x vortex {edge}^3 x {steps} steps (same per-cell work as "
                                        f"256^3), slowest process timed; wall {wall:.1f}s"}
+
+
+def _ref_disk_worker(args):
+    n, steps, fast = args
+    from oracle.bindings import RefOracle
+    from reef3d_b200 import setups
+    c = setups.slotted_disk(n)
+    o = RefOracle(n, 1, n, c.xn, c.yn, c.zn, f43=c.f43, f44=c.f44, f45=c.f45, f49=c.f49, fast=fast)
+    o.set_state(c.phi, c.u, c.v, c.w)
+    dt = o.cfl_dt(c.n47)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(dt)
+    return time.perf_counter() - t0
+
+
+def reference_disk_cpu(n=128, steps=300):
+    """The reference's own step on the 2D slotted disc, one core, a sample of
+    `steps` steps (the full revolution is ~5.7k steps)."""
+    from oracle.bindings import REF_LIB, REF_LIB_FAST
+    fast = host_has_avx2_fma() and os.path.exists(REF_LIB_FAST)
+    if not os.path.exists(REF_LIB) and not fast:
+        return None
+    with mp.get_context("spawn").Pool(1) as pool:
+        sec = pool.apply(_ref_disk_worker, ((n, steps, fast),))
+    return {"value": n * n * steps / sec, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+            "sample": f"{steps} steps of the {n}x{n} slotted disc"}
+
+
+def run_configs(ctx):
+    """The other workloads of the path, each on this GPU (rank 0 at N=1)."""
+    from reef3d_b200 import FP32, FP64, workloads
+    out = {}
+    disk = workloads.slotted_disk_revolution(128, FP64)
+    disk["cpu_reference"] = reference_disk_cpu()
+    out["slotted_disk_fp64"] = disk
+    out["slotted_disk_fp32"] = workloads.slotted_disk_revolution(128, FP32)
+    out["vortex_accuracy"] = workloads.vortex_accuracy(128)
+    out["wave_tank"] = workloads.wave_tank_run(500)
+    out["ensemble"] = workloads.ensemble(steps=200)
+    out["serving_fp32"] = workloads.serving(njobs=16)
+    out["serving_fp64"] = workloads.serving(njobs=16, precision=FP64)
+    return out
 
 
 def run_reference_arm(args, rank):
@@ -343,6 +392,9 @@ def run_ours(args):
             cpu = dict(value=rate, unit="cell-updates/s", **info)
         else:
             cpu = info
+    configs = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_configs:
+        configs = run_configs(ctx)
     value32 = cells * args.steps * ctx.world / (total32 * 1e-3)
     value64 = cells * args.steps * ctx.world / (total64 * 1e-3)
     out = {
@@ -360,12 +412,13 @@ def run_ours(args):
                        "p99_ms": float(np.percentile(per64, 99)), "roofline": roof64,
                        "gpu_launches": launches64},
         "fp32_over_fp64": value32 / value64,
-        "roofline": dict(roof32, traffic=None, peak_source=peak_src),
+        "roofline": dict(roof32, traffic=NCU_TRAFFIC.get((args.edge, roof32["kernel"])), peak_source=peak_src),
         "tile_variants": variants,
         "gpu_launches": launches32,
         "clocks": clk.summary(),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "configs": configs,
     }
     if ctx.rank == 0:
         print(json.dumps(out))

@@ -42,6 +42,8 @@ extern "C" {
 #define R3D_L 4          /* a->L, right-hand side of the last operator call */
 #define R3D_WORK1 5      /* RK stage buffer (ark1 / frk1) */
 #define R3D_WORK2 6      /* RK stage buffer (ark2 / frk2) */
+#define R3D_RO 7         /* a->ro, density (exists once r3d_set_fluid enabled it) */
+#define R3D_VISC 8       /* a->visc, kinematic viscosity (likewise) */
 
 /* host array layouts for upload/download */
 #define R3D_LAYOUT_REEF3D 0  /* the reference's padded field: (nx+6)(ny+6)(nz+6) doubles,
@@ -58,7 +60,14 @@ typedef struct r3d_handle r3d_handle;
  * Flags carry the reference's control-file meaning (src/ini.cpp:400-416,
  * 587-596): f43 reinit time-step factor, f44 reinit pseudo-steps per
  * physical step, f45 interface thickness factor, f49 reinit form (1 every
- * cell, 0 freeze cells next to the interface), n47 CFL factor. */
+ * cell, 0 freeze cells next to the interface), n47 CFL factor, f46 picard
+ * mass correction (0 off; 1 picard_f around each reinitialisation as
+ * reini_RK3 does, src/reini_RK3.cpp:65-69; 2 picard_f around each step as
+ * levelset_RK3 does, src/levelset_RK3.cpp:84-91; 3 picard_lsm there, whose
+ * target is the volume of the instance's first step, src/picard_lsm.cpp,
+ * with no inflow or outflow), f47 picard iterations.
+ * f46/f47 come last so that a zero-initialised descriptor leaves the
+ * correction off. */
 typedef struct {
     int nx, ny, nz;
     const double* xn;
@@ -70,6 +79,8 @@ typedef struct {
     int f49;
     double n47;
     int precision;      /* R3D_FP64 or R3D_FP32 */
+    int f46;            /* 0, 1 or 2 */
+    int f47;            /* >= 0 */
 } r3d_grid_desc;
 
 /* Create an instance on the current CUDA device: allocates the level set,
@@ -100,8 +111,11 @@ int r3d_cfl_dt(r3d_handle* h, double* dt);
 /* One physical level-set step: three WENO5-HJ convection RK stages with
  * ghost fill, then f44 reinitialisation pseudo-steps, then the volume
  * integral.  Replaces levelset_RK3::start (src/levelset_RK3.cpp:103-172)
- * with picard, particles, ioflow hooks and solid forcing void, as in the
- * reference's default configuration.  dt <= 0 uses the handle's dt.
+ * with particles, ioflow hooks and solid forcing void, as in the
+ * reference's default configuration; the picard mass correction runs as
+ * the descriptor's f46 selects (the volume integral then follows the
+ * correction, as fluid_update_fsf follows correct_ls at :171-174).
+ * dt <= 0 uses the handle's dt.
  * Asynchronous on the handle's stream. */
 int r3d_ls_step(r3d_handle* h, double dt);
 /* n steps, each preceded by r3d_cfl_dt when adaptive != 0 (the timestep
@@ -109,7 +123,8 @@ int r3d_ls_step(r3d_handle* h, double dt);
 int r3d_ls_run(r3d_handle* h, int nsteps, int adaptive);
 
 /* Reinitialisation only: `iters` pseudo-steps on the level set
- * (reini_RK3::start, src/reini_RK3.cpp:84-143; iters <= 0 uses f44). */
+ * (reini_RK3::start, src/reini_RK3.cpp:84-143; iters <= 0 uses f44), inside
+ * the picard volume/correction when f46 == 1 (:92, :140). */
 int r3d_reinit(r3d_handle* h, int iters);
 
 /* Operator-level drop-ins on device fields:
@@ -128,8 +143,23 @@ int r3d_ghost_fill(r3d_handle* h, int field);
  * src/fluid_update_fsf.cpp:39-74), FP64.  Synchronous. */
 int r3d_volume(r3d_handle* h, double* volume1, double* volume2);
 
+/* Density and viscosity update of fluid_update_fsf (src/fluid_update_fsf.cpp:
+ * 39-104): allocates R3D_RO and R3D_VISC and from then on ends every step
+ * with ro = ro_water H + ro_air (1-H), visc = visc_water H + visc_air (1-H)
+ * of the smoothed Heaviside H(phi; psi) on the interior, their wall ghost
+ * layers (a Neumann copy, gcval 1) and the volume sums -- the call
+ * levelset_RK3::start makes after the reinitialisation (src/levelset_RK3.cpp:
+ * 174).  The reference takes the constants from W1, W2, W3, W4 (defaults
+ * 998.2, 1.004e-6, 1.205, 1.41e-5, src/ini.cpp:831-834).  Synchronous.
+ * Not for batch members. */
+int r3d_set_fluid(r3d_handle* h, double ro_water, double visc_water, double ro_air, double visc_air);
+/* The update alone on the current level set (fluid_update_fsf::start),
+ * returning the volume sums; needs r3d_set_fluid.  Synchronous. */
+int r3d_fluid_update(r3d_handle* h, double* volume1, double* volume2);
+
 /* Volume sums accumulated by the last r3d_ls_step / r3d_ls_run step
- * (fused into the step's final stage).  Synchronous. */
+ * (fused into the step's final stage, or taken after the picard correction
+ * or by the fluid update when those are on).  Synchronous. */
 int r3d_last_volume(r3d_handle* h, double* volume1, double* volume2);
 
 /* Factor applied to the stored face velocities by every convection stage
@@ -141,6 +171,18 @@ int r3d_set_velocity_scale(r3d_handle* h, double scale);
 /* With period T > 0 the factor follows the device clock:
  * g = cos(pi t / T), recomputed after every step (0 turns it off). */
 int r3d_set_velocity_period(r3d_handle* h, double period);
+/* Velocity generator for wave-tank runs (no counterpart in the level-set
+ * path of the reference, whose velocities come from its momentum solver):
+ * before every step (and in r3d_cfl_dt) u and w are rewritten on every
+ * stored cell with the linear (Airy) orbital velocity of a wave
+ *   eta = amplitude cos(kw x - om t), kw = 2 pi / wavelength,
+ *   om = sqrt(gravity kw tanh(kw depth)), bed at z = 0:
+ *   u = a cosh(kw z) cos(kw x - om t), w = a sinh(kw z) sin(kw x - om t),
+ *   a = amplitude om / sinh(kw depth),
+ * at the device clock t (u on x faces, w on z faces); v is zeroed and the
+ * velocity factor set to 1.  wavelength <= 0 turns the generator off.
+ * Synchronous.  Not for batch members. */
+int r3d_set_velocity_airy(r3d_handle* h, double amplitude, double wavelength, double depth, double gravity);
 /* Device clock (the reference's p->simtime, advanced by dt every step,
  * src/driver_loop_cfd.cpp:104). */
 int r3d_set_time(r3d_handle* h, double t);
@@ -215,7 +257,9 @@ int r3d_volume_dense_noalloc(const double* phi, int nx, int ny, int nz, double d
  * each member's step is levelset_RK3::start (src/levelset_RK3.cpp:103-172)
  * with its own CFL time step (src/ietimestep.cpp:38-206), clock and volume.
  * A member's results do not depend on the other members.  While an
- * instance is a member, calls on its handle first wait for the batch. */
+ * instance is a member, calls on its handle first wait for the batch.
+ * Members are FP32 instances with f46 = 0 (no picard mass correction) and
+ * without the fluid update. */
 typedef struct r3d_batch r3d_batch;
 int r3d_batch_create(r3d_batch** out);
 int r3d_batch_destroy(r3d_batch* b);

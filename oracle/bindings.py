@@ -69,10 +69,12 @@ class PortOracle:
             lib.lso_volume.argtypes = [ctypes.c_void_p, _D, _D, _D]
             lib.lso_cfl_dt.restype = ctypes.c_double
             lib.lso_cfl_dt.argtypes = [ctypes.c_void_p, _D, _D, _D]
+            lib.lso_set_picard.argtypes = [ctypes.c_void_p, _I, _I]
+            lib.lso_fluid.argtypes = [ctypes.c_void_p, _D, _D, _D] + [ctypes.c_double] * 4
             cls._lib = lib
         return cls._lib
 
-    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3):
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3, f46=0, f47=10):
         self.lib()
         self.nx, self.ny, self.nz = nx, ny, nz
         self.shape = padded_shape(nx, ny, nz)
@@ -84,6 +86,7 @@ class PortOracle:
                                    f43, f44, f45, f49, n47)
         if not self.h:
             raise ValueError("lso_new failed")
+        self._lib.lso_set_picard(self.h, f46, f47)
 
     def __del__(self):
         if getattr(self, "h", None) and self._lib is not None:
@@ -146,6 +149,12 @@ class PortOracle:
     def cfl_dt(self, u, v, w):
         return self._lib.lso_cfl_dt(self.h, _dp(u), _dp(v), _dp(w))
 
+    def fluid(self, phi, w1=998.2, w2=1.004e-6, w3=1.205, w4=1.41e-5):
+        """(ro, visc) of fluid_update_fsf (defaults: the reference's W1..W4)."""
+        ro, visc = self.zeros(), self.zeros()
+        self._lib.lso_fluid(self.h, _dp(np.ascontiguousarray(phi)), _dp(ro), _dp(visc), w1, w2, w3, w4)
+        return ro, visc
+
 
 class RefOracle:
     """The reference's own objects; at most one per process."""
@@ -156,10 +165,12 @@ class RefOracle:
     def available(cls):
         return os.path.exists(REF_LIB)
 
-    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False):
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10):
         if RefOracle._lib is not None:
             raise RuntimeError("the reference oracle holds one grid per process")
         lib = ctypes.CDLL(REF_LIB_FAST if fast else REF_LIB)
+        lib.refls_set_picard.argtypes = [_I, _I]
+        lib.refls_set_picard(f46, f47)
         lib.refls_init.argtypes = [_I, _I, _I, _D, _D, _D, _I, ctypes.c_double, ctypes.c_double, _I]
         lib.refls_padded_size.restype = ctypes.c_long
         lib.refls_set_field.argtypes = [_I, _D]
@@ -237,6 +248,10 @@ class RefOracle:
     def reini(self):
         self._lib.refls_reini()
         return self.get_field(0)
+
+    def set_count(self, count):
+        """lexer::count, the time step counter (1 for the first step)."""
+        self._lib.refls_set_count(count)
 
     def step(self, dt):
         self._lib.refls_set_dt(dt)

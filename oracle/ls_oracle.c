@@ -358,8 +358,48 @@ static double reini_dt(const lso_grid* g, int i, int j, int k) {
     return g->f43 * MIN3V(g->dxp[ti], g->dyp[tj], g->dzp[tk]);
 }
 
-/* src/reini_RK3.cpp:113-138 */
+/* --------------------------------------------------- picard mass correction
+ * src/picard_f.cpp:36-56 (volcalc, volcalc2): volume of the smoothed
+ * Heaviside with epsi = F45*DXM and cell volume DXM^3, LOOP order. */
+static double picard_volume(const lso_grid* g, const double* f) {
+    const double epsi = g->f45 * g->dxm_mean;
+    double vol = 0.0, H = 0.0;
+    for (int i = 0; i < g->nx; ++i)
+        for (int j = 0; j < g->ny; ++j)
+            for (int k = 0; k < g->nz; ++k) {
+                const double b = f[lso_index(g, i, j, k)];
+                if (b > epsi) H = 1.0;
+                if (b < -epsi) H = 0.0;
+                if (fabs(b) <= epsi) H = 0.5 * (1.0 + b / epsi + (1.0 / LSO_PI) * sin((LSO_PI * b) / epsi));
+                vol += pow(g->dxm_mean, 3.0) * H;
+            }
+    return vol;
+}
+
+/* src/picard_f.cpp:82-113 (correct_ls): F47 uniform shifts of the interior
+ * by the difference of the equivalent-sphere radii; ghosts untouched. */
+static void picard_correct(const lso_grid* g, double* f, double vol1) {
+    for (int n = 0; n < g->f47; ++n) {
+        const double vol2 = picard_volume(g, f);
+        const double r1 = pow((0.75 / LSO_PI) * vol1, 1.0 / 3.0);
+        const double r2 = pow((0.75 / LSO_PI) * vol2, 1.0 / 3.0);
+        const double w = r1 - r2;
+        for (int i = 0; i < g->nx; ++i)
+            for (int j = 0; j < g->ny; ++j)
+                for (int k = 0; k < g->nz; ++k) f[lso_index(g, i, j, k)] += w;
+    }
+}
+
+void lso_set_picard(lso_grid* g, int f46, int f47) {
+    g->f46 = f46;
+    g->f47 = f47;
+    g->count = 0;
+    g->netvol = 0.0;
+}
+
+/* src/reini_RK3.cpp:113-138 (with picard_f when F46=1, :92 and :140) */
 void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, int iters) {
+    const double vol1 = g->f46 == 1 ? picard_volume(g, f) : 0.0;
     for (int q = 0; q < iters; ++q) {
         lso_reinidisc_L(g, f, L);
         for (int i = 0; i < g->nx; ++i)
@@ -386,11 +426,22 @@ void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, 
                 }
         lso_ghost_fill(g, f);
     }
+    if (g->f46 == 1) picard_correct(g, f, vol1);
 }
 
-/* src/levelset_RK3.cpp:112-161 then reini_RK3::start (F44 steps) */
-void lso_ls_step(const lso_grid* g, double* phi, const double* u, const double* v, const double* w,
+/* src/levelset_RK3.cpp:112-161 then reini_RK3::start (F44 steps), with
+ * picard_f around them when F46=2 (:110 and :171).  F46=3 (picard_lsm,
+ * src/picard_lsm.cpp:36-116): the target volume is the one of the first step
+ * (count == 1), carried as netvol; netvol += (Qi - Qo)*dt with Qi = Qo = 0 for
+ * the closed box.  g->count counts the steps like lexer::count. */
+void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, const double* w,
                  double dt, double* a1, double* a2, double* L) {
+    g->count += 1;
+    double vol1 = g->f46 >= 2 ? picard_volume(g, phi) : 0.0;
+    if (g->f46 == 3) {
+        if (g->count == 1) g->netvol = vol1;
+        g->netvol = g->netvol + 0.0 * dt - 0.0 * dt;
+    }
     lso_weno_L(g, phi, u, v, w, L);
     for (int i = 0; i < g->nx; ++i)
         for (int j = 0; j < g->ny; ++j)
@@ -416,6 +467,8 @@ void lso_ls_step(const lso_grid* g, double* phi, const double* u, const double* 
             }
     lso_ghost_fill(g, phi);
     lso_reini(g, phi, a1, a2, L, g->f44);
+    if (g->f46 == 2) picard_correct(g, phi, vol1);
+    if (g->f46 == 3) picard_correct(g, phi, g->netvol);
 }
 
 /* src/fluid_update_fsf.cpp:50-74 (porosity 1, every interior cell) */
@@ -434,6 +487,28 @@ void lso_volume(const lso_grid* g, const double* phi, double* vol1, double* vol2
             }
     *vol1 = v1;
     *vol2 = v2;
+}
+
+/* src/fluid_update_fsf.cpp:39-104: density and viscosity from the smoothed
+ * Heaviside on every interior cell (BASELOOP), then the wall ghost fill of
+ * both (gcval 1, a Neumann copy like the level set's, src/gc_epol4.cpp:90-93).
+ * W1 ro_water, W2 visc_water, W3 ro_air, W4 visc_air. */
+void lso_fluid(const lso_grid* g, const double* phi, double* ro, double* visc, double w1, double w2, double w3,
+               double w4) {
+    double H = 0.0;
+    for (int i = 0; i < g->nx; ++i)
+        for (int j = 0; j < g->ny; ++j)
+            for (int k = 0; k < g->nz; ++k) {
+                const long c = lso_index(g, i, j, k);
+                const double p = phi[c];
+                if (p > g->psi) H = 1.0;
+                if (p < -g->psi) H = 0.0;
+                if (fabs(p) <= g->psi) H = 0.5 * (1.0 + p / g->psi + (1.0 / LSO_PI) * sin((LSO_PI * p) / g->psi));
+                ro[c] = w1 * H + w3 * (1.0 - H);
+                visc[c] = w2 * H + w4 * (1.0 - H);
+            }
+    lso_ghost_fill(g, ro);
+    lso_ghost_fill(g, visc);
 }
 
 /* src/ietimestep.cpp:38-188 for a prescribed velocity (N50=1, no source

@@ -34,6 +34,9 @@ typedef struct {
     /* control flags (src/ini.cpp:400-416) */
     double f43, f45, n47;
     int f44, f49;
+    int f46, f47;       /* picard mass correction (0 off, 1 in reinit, 2 in the step, 3 picard_lsm) */
+    int count;          /* steps taken (lexer::count of the first step is 1) */
+    double netvol;      /* picard_lsm target volume */
     /* metrics, length n+1+4*marge like the reference (src/grid.cpp:55-100) */
     double *xn, *yn, *zn, *xp, *yp, *zp;
     double *dxn, *dyn, *dzn, *dxp, *dyp, *dzp;
@@ -64,13 +67,21 @@ void lso_ghost_fill(const lso_grid* g, double* f);
 void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, int iters);
 /* One physical step: 3 convection RK stages, then F44 reinit steps.
  * a1, a2, L are work fields of ncell doubles. */
-void lso_ls_step(const lso_grid* g, double* phi, const double* u, const double* v,
+void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v,
                  const double* w, double dt, double* a1, double* a2, double* L);
 /* Smoothed-Heaviside volume sums (volume1, volume2) over interior cells. */
 void lso_volume(const lso_grid* g, const double* phi, double* vol1, double* vol2);
 /* Next time step from the velocity maxima (src/ietimestep.cpp:38-188 with a
  * prescribed velocity: no source term, no turbulence). */
 double lso_cfl_dt(const lso_grid* g, const double* u, const double* v, const double* w);
+
+/* src/fluid_update_fsf.cpp:39-104: ro/visc with wall ghosts (w1..w4 = W1..W4). */
+void lso_fluid(const lso_grid* g, const double* phi, double* ro, double* visc, double w1, double w2, double w3,
+               double w4);
+
+/* Picard mass correction flags (src/picard_f.cpp, src/picard_lsm.cpp): f46 1, 2 or 3,
+ * f47 iterations.  Resets the step count. */
+void lso_set_picard(lso_grid* g, int f46, int f47);
 
 /* opaque handle helpers (used through ctypes) */
 lso_grid* lso_new(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,

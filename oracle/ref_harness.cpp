@@ -55,6 +55,7 @@ reinidisc* DISC = nullptr;
 heat* HEAT = nullptr;
 concentration* CONC = nullptr;
 field4* TMP = nullptr;
+int G_F46 = 0, G_F47 = 10;  // picard mass correction flags for the next refls_init
 ietimestep* TSTEP = nullptr;
 turbulence* TURB = nullptr;
 
@@ -69,6 +70,7 @@ field* field_by_id(int id) {
         case 4: return &A->L;
         case 5: return TMP;
         case 6: return &A->ro;
+        case 7: return &A->visc;
         default: return nullptr;
     }
 }
@@ -80,6 +82,12 @@ int ijk(int i, int j, int k) {
 }  // namespace
 
 extern "C" {
+
+// Picard mass correction of the next refls_init: f46 = 1 (in reini_RK3,
+// src/reini_RK3.cpp:92,140), 2 (picard_f in levelset_RK3,
+// src/levelset_RK3.cpp:110,171) or 3 (picard_lsm there), f47 iterations
+// (src/picard_f.cpp:82-113, src/picard_lsm.cpp:89-116).
+void refls_set_picard(int f46, int f47) { G_F46 = f46; G_F47 = f47; }
 
 // xn/yn/zn: node coordinates for index -5 .. n+5 (n+11 values), the same
 // arrays DIVEMesh writes (src/read_grid.cpp:417-433, marge=5).
@@ -97,7 +105,7 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
 
     // control flags on this path (defaults src/ini.cpp:400-416)
     p->F30 = 3; p->F35 = 5; p->F40 = 3;
-    p->F43 = f43; p->F44 = f44; p->F45 = f45; p->F46 = 0; p->F49 = f49; p->F50 = 2;
+    p->F43 = f43; p->F44 = f44; p->F45 = f45; p->F46 = G_F46; p->F47 = G_F47; p->F49 = f49; p->F50 = 2;
     p->X45 = 0; p->X48 = 0; p->M10 = 1; p->P12 = 1000000000;
 
     // --- what read_grid() assigns (src/read_grid.cpp:78-300)
@@ -291,6 +299,7 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     TURB = new kepsilon_void(p, A, PGC);
     p->count = 1;
     p->dt = 0.0;
+    p->Qi = p->Qo = 0.0;  // closed box: no discharge (read by picard_lsm, src/picard_lsm.cpp:95)
     return 0;
 }
 

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libreef3d_b200.so")
 
 R3D_OK, R3D_EINVAL, R3D_ENOMEM, R3D_EDEVICE, R3D_ETIMEOUT, R3D_ESTATE = 0, 1, 2, 3, 4, 5
 FP64, FP32 = 0, 1
-PHI, U, V, W, L, WORK1, WORK2 = range(7)
+PHI, U, V, W, L, WORK1, WORK2, RO, VISC = range(9)
 LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
 STAGE_CONVECTION, STAGE_REINIT = 0, 1
 OPT_TILED, OPT_CHUNK, OPT_BAND64 = 0, 1, 2
@@ -41,6 +41,7 @@ class GridDesc(ctypes.Structure):
         ("zn", ctypes.POINTER(ctypes.c_double)),
         ("f43", ctypes.c_double), ("f44", ctypes.c_int), ("f45", ctypes.c_double), ("f49", ctypes.c_int),
         ("n47", ctypes.c_double), ("precision", ctypes.c_int),
+        ("f46", ctypes.c_int), ("f47", ctypes.c_int),
     ]
 
 
@@ -66,6 +67,9 @@ EXPORTS = {
     "r3d_ghost_fill": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_volume": ([_H, _D, _D], ctypes.c_int),
     "r3d_last_volume": ([_H, _D, _D], ctypes.c_int),
+    "r3d_set_velocity_airy": ([_H] + [ctypes.c_double] * 4, ctypes.c_int),
+    "r3d_set_fluid": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+    "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_velocity_scale": ([_H, ctypes.c_double], ctypes.c_int),
     "r3d_set_velocity_period": ([_H, ctypes.c_double], ctypes.c_int),
     "r3d_set_time": ([_H, ctypes.c_double], ctypes.c_int),
@@ -131,12 +135,12 @@ def uniform_nodes(n, length=1.0, origin=0.0):
     return np.array([origin + i * h for i in range(-5, n + 6)], dtype=np.float64)
 
 
-def make_desc(nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3, precision=FP64):
+def make_desc(nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3, precision=FP64, f46=0, f47=10):
     xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (xn, yn, zn)]
     for a, n in zip(xs, (nx, ny, nz)):
         if a.shape != (n + 11,):
             raise ValueError(f"node array of an axis with {n} cells needs {n + 11} values, got {a.shape}")
-    d = GridDesc(nx, ny, nz, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]), f43, f44, f45, f49, n47, precision)
+    d = GridDesc(nx, ny, nz, _dp(xs[0]), _dp(xs[1]), _dp(xs[2]), f43, f44, f45, f49, n47, precision, f46, f47)
     d._keep = xs
     return d
 
@@ -155,14 +159,14 @@ class LevelSet:
     weno_hj_df_nug and reini_RK3 act on in the reference)."""
 
     def __init__(self, nx, ny, nz, xn=None, yn=None, zn=None, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3,
-                 precision=FP64):
+                 precision=FP64, f46=0, f47=10):
         load_library()
         xn = uniform_nodes(nx) if xn is None else xn
         yn = uniform_nodes(ny) if yn is None else yn
         zn = uniform_nodes(nz) if zn is None else zn
         self.nx, self.ny, self.nz = nx, ny, nz
         self.f44, self.precision = f44, precision
-        self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision)
+        self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision, f46, f47)
         h = _H()
         _check(_lib.r3d_create(ctypes.byref(self.desc), ctypes.byref(h)))
         self.h = h
@@ -249,8 +253,22 @@ class LevelSet:
         _check(_lib.r3d_last_volume(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
         return a.value, b.value
 
+    def set_fluid(self, ro_water=998.2, visc_water=1.004e-6, ro_air=1.205, visc_air=1.41e-5):
+        """Turn on the density/viscosity update of every step (fluid_update_fsf;
+        defaults are the reference's W1..W4)."""
+        _check(_lib.r3d_set_fluid(self.h, ro_water, visc_water, ro_air, visc_air), self.h)
+
+    def fluid_update(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.r3d_fluid_update(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
+        return a.value, b.value
+
     def set_velocity_scale(self, scale):
         _check(_lib.r3d_set_velocity_scale(self.h, scale), self.h)
+
+    def set_velocity_airy(self, amplitude, wavelength, depth, gravity=9.81):
+        """Regenerate u, w from the Airy wave at the device clock before every step."""
+        _check(_lib.r3d_set_velocity_airy(self.h, amplitude, wavelength, depth, gravity), self.h)
 
     def set_velocity_period(self, period):
         _check(_lib.r3d_set_velocity_period(self.h, period), self.h)

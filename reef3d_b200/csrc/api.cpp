@@ -46,6 +46,8 @@ int check_desc(const r3d_grid_desc* d, std::string& why) {
     if (d->precision != R3D_FP64 && d->precision != R3D_FP32) { why = "precision must be R3D_FP64 or R3D_FP32"; return R3D_EINVAL; }
     if (d->f44 < 0) { why = "f44 must be >= 0"; return R3D_EINVAL; }
     if (d->f49 != 0 && d->f49 != 1) { why = "f49 must be 0 or 1"; return R3D_EINVAL; }
+    if (d->f46 < 0 || d->f46 > 3) { why = "f46 must be 0, 1, 2 or 3"; return R3D_EINVAL; }
+    if (d->f46 != 0 && d->f47 < 0) { why = "f47 must be >= 0"; return R3D_EINVAL; }
     const int n[3] = {d->nx, d->ny, d->nz};
     const double* x[3] = {d->xn, d->yn, d->zn};
     for (int a = 0; a < 3; ++a)
@@ -124,6 +126,7 @@ void release(r3d_handle* h) {
     if (h->S.partial) cudaFree(h->S.partial);
     if (h->S.vmax) cudaFree(h->S.vmax);
     if (h->staging) cudaFree(h->staging);
+    if (h->coord) cudaFree(h->coord);
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaSetDevice(cur);
 }
@@ -144,6 +147,7 @@ int ensure_staging(r3d_handle* h) {
     const size_t need = sizeof(double) * (size_t)(h->L.nx + 6) * (h->L.ny + 6) * (h->L.nz + 6);
     if (h->staging_bytes >= need) return R3D_OK;
     if (h->staging) cudaFree(h->staging);
+    if (h->coord) cudaFree(h->coord);
     h->staging = nullptr;
     h->staging_bytes = 0;
     if (cudaMalloc(&h->staging, need) != cudaSuccess) {
@@ -227,13 +231,73 @@ long long volume_block_count(const r3d_handle* h) {
     return volume_blocks(h->L);
 }
 
+int check_field(r3d_handle* h, int field) {
+    if (field < 0 || field > R3D_VISC) return fail(h, R3D_EINVAL, "bad field id");
+    if (!h->field[field]) return fail(h, R3D_ESTATE, "ro/visc exist once r3d_set_fluid enabled them");
+    return R3D_OK;
+}
+
+// Airy velocity at the device clock (no-op unless r3d_set_velocity_airy).
+long long refresh_velocity(r3d_handle* h) {
+    if (!h->airy) return 0;
+    return launch_airy(h->L, h->field[R3D_U], h->field[R3D_W], fp32(h), h->coord, h->S.t, h->ap, h->sms,
+                       h->stream);
+}
+
+long long fluid_update(r3d_handle* h, bool clock) {
+    return launch_fluid_update(h->L, h->field[R3D_PHI], h->field[R3D_RO], h->field[R3D_VISC], fp32(h),
+                               h->g64.dxn[0], h->g64.dxn[1], h->g64.dxn[2], h->M.psi, h->fc, clock, h->period,
+                               h->S, h->stream);
+}
+
+// Picard constants (src/picard_f.cpp:30, :51): epsi = F45*DXM, cell volume DXM^3.
+double picard_epsi(const r3d_handle* h) { return h->desc.f45 * h->M.dxm_mean; }
+double picard_cellvol(const r3d_handle* h) { return std::pow(h->M.dxm_mean, 3.0); }
+
+long long picard_volcalc(r3d_handle* h) {
+    return launch_picard_volcalc(h->L, h->field[R3D_PHI], fp32(h), picard_epsi(h), picard_cellvol(h),
+                                 h->desc.f46 == 3, h->S, h->stream);
+}
+
+long long picard_correct(r3d_handle* h) {
+    return launch_picard_correct(h->L, h->field[R3D_PHI], fp32(h), picard_epsi(h), picard_cellvol(h),
+                                 h->desc.f47, h->desc.f46 == 3, h->S, h->stream);
+}
+
+// reini_RK3::start (src/reini_RK3.cpp:84-160): iters pseudo-steps of three
+// stages, inside picard volcalc/correct_ls when f46 == 1 (:92, :140).
+// fuse_volume: the last stage also writes the volume partials.
+long long enqueue_reinit(r3d_handle* h, int iters, bool fuse_volume) {
+    long long n = 0;
+    if (h->desc.f46 == 1) n += picard_volcalc(h);
+    for (int q = 0; q < iters; ++q)
+        for (int s = 1; s <= 3; ++s) n += stage_launch(h, true, s, fuse_volume && q == iters - 1 && s == 3);
+    if (h->desc.f46 == 1) n += picard_correct(h);
+    return n;
+}
+
+// levelset_RK3::start (src/levelset_RK3.cpp:103-174).  Without picard or
+// fluid update the volume partials come from the last stage; with picard
+// (f46 = 1, 2 or 3) the volume pass follows the correction, and with the
+// fluid update enabled that pass is fluid_update_fsf::start (:174), which
+// also writes ro and visc.  f46 = 2 (picard_f) and 3 (picard_lsm) wrap the
+// step (:84-91, :110, :171).
 int enqueue_step(r3d_handle* h) {
     const int f44 = h->desc.f44;
+    const bool pic = h->desc.f46 != 0 || h->fluid;
     long long n = 0;
-    for (int s = 1; s <= 3; ++s) n += stage_launch(h, false, s, f44 == 0 && s == 3);
-    for (int q = 0; q < f44; ++q)
-        for (int s = 1; s <= 3; ++s) n += stage_launch(h, true, s, q == f44 - 1 && s == 3);
-    n += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
+    const bool step_picard = h->desc.f46 >= 2;
+    if (step_picard) n += picard_volcalc(h);
+    for (int s = 1; s <= 3; ++s) n += stage_launch(h, false, s, !pic && f44 == 0 && s == 3);
+    n += enqueue_reinit(h, f44, !pic);
+    if (step_picard) n += picard_correct(h);
+    if (h->fluid)
+        n += fluid_update(h, true);
+    else if (pic)
+        n += launch_volume_direct_clock(h->L, h->field[R3D_PHI], fp32(h), h->g64.dxn[0], h->g64.dxn[1],
+                                        h->g64.dxn[2], h->M.psi, h->period, h->S, h->stream);
+    else
+        n += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
     h->launches += n;
     h->have_last_volume = true;
     return R3D_OK;
@@ -328,6 +392,7 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
     h->S.vol = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 128);
     h->S.t = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 160);
     h->S.vscale = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 168);
+    h->S.pic = reinterpret_cast<double*>(reinterpret_cast<char*>(h->S.vmax) + 208);
     h->S.err = reinterpret_cast<int*>(reinterpret_cast<char*>(h->S.vmax) + 192);
     cudaMemsetAsync(h->S.vmax, 0, 256, h->stream);
     launch_set_scalar(h->S.vscale, 1.0, h->stream);
@@ -354,7 +419,7 @@ int r3d_destroy(r3d_handle* h) {
 
 int r3d_upload(r3d_handle* h, int field, const double* host, int layout) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
+    if (int rc = check_field(h, field)) return rc;
     if (layout != R3D_LAYOUT_REEF3D && layout != R3D_LAYOUT_DENSE) return fail(h, R3D_EINVAL, "bad layout");
     if (!host) return fail(h, R3D_EINVAL, "null host pointer");
     DeviceGuard dg(h->device, h->batch_stream);
@@ -369,7 +434,7 @@ int r3d_upload(r3d_handle* h, int field, const double* host, int layout) {
 
 int r3d_download(r3d_handle* h, int field, double* host, int layout) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
+    if (int rc = check_field(h, field)) return rc;
     if (layout != R3D_LAYOUT_REEF3D && layout != R3D_LAYOUT_DENSE) return fail(h, R3D_EINVAL, "bad layout");
     if (!host) return fail(h, R3D_EINVAL, "null host pointer");
     DeviceGuard dg(h->device, h->batch_stream);
@@ -396,6 +461,7 @@ int r3d_set_dt(r3d_handle* h, double dt) {
 int r3d_cfl_dt(r3d_handle* h, double* dt) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     DeviceGuard dg(h->device, h->batch_stream);
+    h->launches += refresh_velocity(h);
     h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h), h->M.dxmin_cfl,
                               h->desc.n47, h->S, h->stream);
     R3D_CUDA(h, cudaGetLastError());
@@ -415,6 +481,7 @@ int r3d_ls_step(r3d_handle* h, double dt) {
     } else if (!(h->dt_host > 0.0)) {
         return fail(h, R3D_ESTATE, "no time step set (pass dt > 0, r3d_set_dt or r3d_cfl_dt first)");
     }
+    h->launches += refresh_velocity(h);
     enqueue_step(h);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
@@ -422,6 +489,7 @@ int r3d_ls_step(r3d_handle* h, double dt) {
 
 // The launches of one step of r3d_ls_run (CFL first when adaptive).
 void enqueue_run_step(r3d_handle* h, int adaptive) {
+    h->launches += refresh_velocity(h);
     if (adaptive)
         h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h), h->M.dxmin_cfl,
                                   h->desc.n47, h->S, h->stream);
@@ -489,8 +557,7 @@ int r3d_reinit(r3d_handle* h, int iters) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     DeviceGuard dg(h->device, h->batch_stream);
     const int it = iters > 0 ? iters : h->desc.f44;
-    for (int q = 0; q < it; ++q)
-        for (int s = 1; s <= 3; ++s) h->launches += stage_launch(h, true, s, false);
+    h->launches += enqueue_reinit(h, it, false);
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
@@ -521,7 +588,7 @@ int r3d_reinidisc_L(r3d_handle* h, int field_in) {
 
 int r3d_ghost_fill(r3d_handle* h, int field) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
-    if (field < 0 || field > 6) return fail(h, R3D_EINVAL, "bad field id");
+    if (int rc = check_field(h, field)) return rc;
     DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_ghost_fill(h->L, h->field[field], fp32(h), h->stream);
     R3D_CUDA(h, cudaGetLastError());
@@ -535,6 +602,41 @@ int r3d_volume(r3d_handle* h, double* volume1, double* volume2) {
     const double* dyn = h->g64.dxn[1];
     const double* dzn = h->g64.dxn[2];
     h->launches += launch_volume_direct(h->L, h->field[R3D_PHI], fp32(h), dxn, dyn, dzn, h->M.psi, h->S, h->stream);
+    R3D_CUDA(h, cudaGetLastError());
+    double v[2] = {0.0, 0.0};
+    R3D_CUDA(h, cudaMemcpyAsync(v, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (volume1) *volume1 = v[0];
+    if (volume2) *volume2 = v[1];
+    return R3D_OK;
+}
+
+int r3d_set_fluid(r3d_handle* h, double ro_water, double visc_water, double ro_air, double visc_air) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    DeviceGuard dg(h->device, h->batch_stream);
+    if (!h->fluid) {
+        const size_t fbytes = (size_t)h->L.ncell * elem(h);
+        for (int id : {R3D_RO, R3D_VISC}) {
+            if (cudaMalloc(&h->field[id], fbytes) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(h, R3D_ENOMEM, "ro/visc allocation failed");
+            }
+            R3D_CUDA(h, cudaMemsetAsync(h->field[id], 0, fbytes, h->stream));
+        }
+    }
+    h->fc = r3d::FluidConst{ro_water, visc_water, ro_air, visc_air};
+    h->fluid = true;
+    drop_step_graph(h);
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
+int r3d_fluid_update(r3d_handle* h, double* volume1, double* volume2) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!h->fluid) return fail(h, R3D_ESTATE, "r3d_set_fluid has not enabled the fluid update");
+    DeviceGuard dg(h->device, h->batch_stream);
+    h->launches += fluid_update(h, false);
     R3D_CUDA(h, cudaGetLastError());
     double v[2] = {0.0, 0.0};
     R3D_CUDA(h, cudaMemcpyAsync(v, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -565,9 +667,53 @@ int r3d_set_velocity_scale(r3d_handle* h, double scale) {
     return R3D_OK;
 }
 
+int r3d_set_velocity_airy(r3d_handle* h, double amplitude, double wavelength, double depth, double gravity) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    DeviceGuard dg(h->device, h->batch_stream);
+    drop_step_graph(h);
+    if (!(wavelength > 0.0)) {
+        h->airy = false;
+        return R3D_OK;
+    }
+    if (!(depth > 0.0) || !(gravity > 0.0) || !std::isfinite(amplitude) || !std::isfinite(wavelength))
+        return fail(h, R3D_EINVAL, "Airy wave needs depth > 0, gravity > 0 and finite amplitude/wavelength");
+    if (airy_prepare(h->L)) return fail(h, R3D_EINVAL, "grid too long in x or z for the Airy generator");
+    if (!h->coord) {
+        std::vector<double> c;
+        for (int a : {0, 2}) {
+            const int n = h->M.n[a];
+            for (int i = -3; i < n + 3; ++i) c.push_back(h->M.xp[a][i + 5]);  // centres
+            for (int i = -3; i < n + 3; ++i) c.push_back(h->M.xn[a][i + 6]);  // faces i+1/2
+        }
+        // order expected by the kernel: x centres, x faces, z centres, z faces
+        if (cudaMalloc(&h->coord, c.size() * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            h->coord = nullptr;
+            return fail(h, R3D_ENOMEM, "coordinate table allocation failed");
+        }
+        R3D_CUDA(h, cudaMemcpy(h->coord, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) == cudaSuccess && sms > 0)
+        h->sms = sms;
+    const double kw = 2.0 * 3.141592653589793 / wavelength;
+    const double om = std::sqrt(gravity * kw * std::tanh(kw * depth));
+    h->ap = r3d::AiryParams{amplitude * om / std::sinh(kw * depth), kw, om};
+    h->airy = true;
+    h->period = 0.0;
+    h->launches += launch_set_scalar(h->S.vscale, 1.0, h->stream);
+    R3D_CUDA(h, cudaMemsetAsync(h->field[R3D_V], 0, (size_t)h->L.ncell * elem(h), h->stream));
+    h->launches += refresh_velocity(h);
+    R3D_CUDA(h, cudaGetLastError());
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
 int r3d_set_velocity_period(r3d_handle* h, double period) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (!(period >= 0.0) || !std::isfinite(period)) return fail(h, R3D_EINVAL, "period must be >= 0");
+    if (h->airy && period > 0.0) return fail(h, R3D_ESTATE, "the Airy generator sets the velocity itself");
     if (h->period != period) drop_step_graph(h);
     h->period = period;
     return R3D_OK;

@@ -16,7 +16,15 @@ struct r3d_handle {
     r3d::HostMetrics M;
     int device = 0;
     cudaStream_t stream = nullptr;
-    void* field[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // fields 0..6 always; 7 (ro) and 8 (visc) once r3d_set_fluid enabled them
+    void* field[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool fluid = false;
+    r3d::FluidConst fc{};
+    // Airy wave velocity regenerated at the device clock before every step
+    bool airy = false;
+    r3d::AiryParams ap{};
+    double* coord = nullptr;  // x centres, x faces, z centres, z faces
+    int sms = 148;
     double* metrics64 = nullptr;
     float* metrics32 = nullptr;
     r3d::KGrid<double> g64{};

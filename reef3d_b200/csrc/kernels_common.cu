@@ -200,7 +200,260 @@ __global__ void volume_direct_kernel(Layout L, const T* __restrict__ phi, const 
     }
 }
 
+// ------------------------------------------------------- Airy velocity
+// Linear (Airy) wave orbital velocity at the device clock t, written on
+// every stored cell (interior and ghost layers):
+//   u = a cosh(kw z_c) cos(kw x_f - om t)   (x faces, cell-centre z)
+//   w = a sinh(kw z_f) sin(kw x_c - om t)   (z faces, cell-centre x)
+// with a = amp om / sinh(kw depth), the bed at z = 0.  The field is
+// separable, so each block first tabulates the x and z factors in shared
+// memory (coord: x centres, x faces, z centres, z faces of padded indices
+// -3..n+2) and then writes rows with two multiplies per value.
+template <typename T>
+__global__ void __launch_bounds__(256) airy_kernel(Layout L, T* __restrict__ u, T* __restrict__ w,
+                                                   const double* __restrict__ coord, const double* __restrict__ t,
+                                                   AiryParams ap) {
+    extern __shared__ double tab[];
+    const int nx6 = L.nx + 6, nz6 = L.nz + 6;
+    double* xu = tab;
+    double* xw = tab + nx6;
+    double* zu = tab + 2 * nx6;
+    double* zw = tab + 2 * nx6 + nz6;
+    const double tt = *t;
+    for (int i = threadIdx.x; i < nx6; i += blockDim.x) {
+        xu[i] = cos(ap.kw * coord[nx6 + i] - ap.om * tt);
+        xw[i] = sin(ap.kw * coord[i] - ap.om * tt);
+    }
+    for (int k = threadIdx.x; k < nz6; k += blockDim.x) {
+        zu[k] = ap.a * cosh(ap.kw * coord[2 * nx6 + k]);
+        zw[k] = ap.a * sinh(ap.kw * coord[2 * nx6 + nz6 + k]);
+    }
+    __syncthreads();
+    const int py = L.two_d ? 1 : L.ny + 6;
+    const long long rows = (long long)py * nz6;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        const int jj = (int)(r % py), kk = (int)(r / py);
+        const long long base = (long long)kk * L.sz + (long long)jj * L.sy + (L.gx - 3);
+        for (int i = threadIdx.x; i < nx6; i += blockDim.x) {
+            u[base + i] = static_cast<T>(zu[kk] * xu[i]);
+            w[base + i] = static_cast<T>(zw[kk] * xw[i]);
+        }
+    }
+}
+
+// --------------------------------------------------------- fluid update
+// fluid_update_fsf::start (src/fluid_update_fsf.cpp:39-104) on one (j,k)
+// row per block: smoothed Heaviside of phi, ro = W1 H + W3 (1-H),
+// visc = W2 H + W4 (1-H) on the interior, the wall ghost layers of both
+// (gcval 1: a Neumann copy into the three layers, src/gc_epol4.cpp:90-93,
+// src/gc_neumann.cpp:29-54; 2D skips y), and the volume partials of
+// volume_direct_kernel.
+template <typename T>
+__global__ void fluid_kernel(Layout L, const T* __restrict__ phi, T* __restrict__ ro, T* __restrict__ visc,
+                             const double* __restrict__ dxn, const double* __restrict__ dyn,
+                             const double* __restrict__ dzn, double psi, FluidConst fc, double* partial) {
+    const double PI_REF = 3.14159265359;  // src/definitions.h:37
+    const int j = blockIdx.y, k = blockIdx.z;
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
+        const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+        const double p = (double)phi[c];
+        double H = 0.0;
+        if (p > psi) H = 1.0;
+        if (p < -psi) H = 0.0;
+        if (fabs(p) <= psi) H = 0.5 * (1.0 + p / psi + (1.0 / PI_REF) * sin((PI_REF * p) / psi));
+        const T r = static_cast<T>(fc.ro_water * H + fc.ro_air * (1.0 - H));
+        const T m = static_cast<T>(fc.visc_water * H + fc.visc_air * (1.0 - H));
+        ro[c] = r;
+        visc[c] = m;
+        for (int q = 1; q <= 3; ++q) {
+            if (i == 0) { ro[c - q] = r; visc[c - q] = m; }
+            if (i == L.nx - 1) { ro[c + q] = r; visc[c + q] = m; }
+            if (!L.two_d && j == 0) { ro[c - q * L.sy] = r; visc[c - q * L.sy] = m; }
+            if (!L.two_d && j == L.ny - 1) { ro[c + q * L.sy] = r; visc[c + q * L.sy] = m; }
+            if (k == 0) { ro[c - q * L.sz] = r; visc[c - q * L.sz] = m; }
+            if (k == L.nz - 1) { ro[c + q * L.sz] = r; visc[c + q * L.sz] = m; }
+        }
+        const double vol = dxn[i + 5] * dyn[j + 5] * dzn[k + 5];
+        a += vol * (H - (1.0 - 1.0));
+        b += vol * (1.0 - H - (1.0 - 1.0));
+    }
+    __shared__ double sa[256], sb[256];
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sa[threadIdx.x] += sa[threadIdx.x + s];
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const long long blk = (long long)k * gridDim.y + j;
+        partial[2 * blk] = sa[0];
+        partial[2 * blk + 1] = sb[0];
+    }
+}
+
+// --------------------------------------------------------------- picard
+// One pass of the picard mass correction over the interior, one block per
+// (j,k) row (src/picard_f.cpp:36-113).  SHIFT: the row is first moved by
+// s.pic[1] (correct_ls's "LOOP b += w", :109-110; the ghost cells keep their
+// values as there).  SUM: the row's smoothed-Heaviside volume of the (moved)
+// values goes to partial[row] (volcalc/volcalc2, :36-76).  One pass thus
+// serves one iteration's update and the next iteration's volume.
+template <typename T, bool SHIFT, bool SUM>
+__global__ void __launch_bounds__(256) picard_row_kernel(Layout L, T* __restrict__ phi,
+                                                         const double* __restrict__ pic, double epsi,
+                                                         double cellvol, double* __restrict__ partial) {
+    const double PI_REF = 3.14159265359;  // src/definitions.h:37
+    const int j = blockIdx.y, k = blockIdx.z;
+    const double w = SHIFT ? pic[1] : 0.0;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
+        const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+        T v = phi[c];
+        if (SHIFT) {
+            v = static_cast<T>(static_cast<double>(v) + w);
+            phi[c] = v;
+        }
+        if (SUM) {
+            const double b = static_cast<double>(v);
+            double H = 0.0;
+            if (b > epsi) H = 1.0;
+            if (b < -epsi) H = 0.0;
+            if (fabs(b) <= epsi) H = 0.5 * (1.0 + b / epsi + (1.0 / PI_REF) * sin((PI_REF * b) / epsi));
+            a += cellvol * H;
+        }
+    }
+    if (!SUM) return;
+    __shared__ double sa[256];
+    sa[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sa[threadIdx.x] += sa[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[(long long)k * gridDim.y + j] = sa[0];
+}
+
+// Fixed-order sum of the row volumes.  mode 0: pic[0] = volume (vol1 of
+// volcalc); with lsm (picard_lsm, src/picard_lsm.cpp:36-61) the step
+// counter pic[3] advances and the first step's volume becomes the target
+// netvol pic[2] (netvol += (Qi - Qo) dt is zero for a closed box).
+// mode 1: volume is vol2, pic[1] = w = r1 - r2 with the equivalent-sphere
+// radii r = ((3/4pi) vol)^(1/3) of the target (pic[0], or pic[2] with lsm)
+// and of vol2 (src/picard_f.cpp:99-102, src/picard_lsm.cpp:102-105).
+__global__ void picard_reduce_kernel(const double* __restrict__ partial, long long n, double* pic, int mode,
+                                     int lsm) {
+    const double PI_REF = 3.14159265359;
+    __shared__ double sa[1024];
+    double a = 0.0;
+    for (long long t = threadIdx.x; t < n; t += blockDim.x) a += partial[t];
+    sa[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sa[threadIdx.x] += sa[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (mode == 0) {
+            pic[0] = sa[0];
+            if (lsm) {
+                pic[3] += 1.0;
+                if (pic[3] == 1.0) pic[2] = sa[0];
+            }
+        } else {
+            const double r1 = pow((0.75 / PI_REF) * (lsm ? pic[2] : pic[0]), 1.0 / 3.0);
+            const double r2 = pow((0.75 / PI_REF) * sa[0], 1.0 / 3.0);
+            pic[1] = r1 - r2;
+        }
+    }
+}
+
+template <typename T, bool SHIFT, bool SUM>
+void picard_pass(const Layout& L, void* phi, double epsi, double cellvol, const Scratch& s, cudaStream_t st) {
+    const dim3 grid(1, L.ny, L.nz), block(256);
+    picard_row_kernel<T, SHIFT, SUM><<<grid, block, 0, st>>>(L, static_cast<T*>(phi), s.pic, epsi, cellvol, s.partial);
+}
+
+template <bool SHIFT, bool SUM>
+void picard_pass(const Layout& L, void* phi, bool fp32, double epsi, double cellvol, const Scratch& s,
+                 cudaStream_t st) {
+    if (fp32) picard_pass<float, SHIFT, SUM>(L, phi, epsi, cellvol, s, st);
+    else picard_pass<double, SHIFT, SUM>(L, phi, epsi, cellvol, s, st);
+}
+
 }  // namespace
+
+size_t airy_smem_bytes(const Layout& L) { return (size_t)(2 * (L.nx + 6) + 2 * (L.nz + 6)) * sizeof(double); }
+
+int launch_airy(const Layout& L, void* u, void* w, bool fp32, const double* coord, const double* t,
+                const AiryParams& ap, int sms, cudaStream_t st) {
+    const long long rows = (long long)(L.two_d ? 1 : L.ny + 6) * (L.nz + 6);
+    const int grid = (int)(rows < 4LL * sms ? rows : 4LL * sms);
+    const size_t smem = airy_smem_bytes(L);
+    if (fp32)
+        airy_kernel<float><<<grid, 256, smem, st>>>(L, static_cast<float*>(u), static_cast<float*>(w), coord, t, ap);
+    else
+        airy_kernel<double><<<grid, 256, smem, st>>>(L, static_cast<double*>(u), static_cast<double*>(w), coord, t,
+                                                     ap);
+    return 1;
+}
+
+int airy_prepare(const Layout& L) {
+    const size_t smem = airy_smem_bytes(L);
+    if (smem > 227 * 1024) return 1;
+    if (smem > 48 * 1024) {
+        if (cudaFuncSetAttribute(airy_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(airy_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess)
+            return 1;
+    }
+    return 0;
+}
+
+int launch_fluid_update(const Layout& L, const void* phi, void* ro, void* visc, bool fp32, const double* dxn,
+                        const double* dyn, const double* dzn, double psi, const FluidConst& fc, bool clock,
+                        double period, const Scratch& s, cudaStream_t st) {
+    const dim3 grid(1, L.ny, L.nz), block(256);
+    if (fp32)
+        fluid_kernel<float><<<grid, block, 0, st>>>(L, static_cast<const float*>(phi), static_cast<float*>(ro),
+                                                    static_cast<float*>(visc), dxn, dyn, dzn, psi, fc, s.partial);
+    else
+        fluid_kernel<double><<<grid, block, 0, st>>>(L, static_cast<const double*>(phi), static_cast<double*>(ro),
+                                                     static_cast<double*>(visc), dxn, dyn, dzn, psi, fc, s.partial);
+    if (clock)
+        volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.vol, s.t, s.vscale, s.dt,
+                                                 period);
+    else
+        volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.vol, nullptr, nullptr,
+                                                 nullptr, 0.0);
+    return 2;
+}
+
+int launch_picard_volcalc(const Layout& L, const void* phi, bool fp32, double epsi, double cellvol, bool lsm,
+                          const Scratch& s, cudaStream_t st) {
+    picard_pass<false, true>(L, const_cast<void*>(phi), fp32, epsi, cellvol, s, st);
+    picard_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.pic, 0, lsm);
+    return 2;
+}
+
+int launch_picard_correct(const Layout& L, void* phi, bool fp32, double epsi, double cellvol, int f47, bool lsm,
+                          const Scratch& s, cudaStream_t st) {
+    if (f47 <= 0) return 0;
+    const long long rows = (long long)L.ny * L.nz;
+    picard_pass<false, true>(L, phi, fp32, epsi, cellvol, s, st);
+    picard_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, rows, s.pic, 1, lsm);
+    for (int n = 1; n < f47; ++n) {
+        picard_pass<true, true>(L, phi, fp32, epsi, cellvol, s, st);
+        picard_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, rows, s.pic, 1, lsm);
+    }
+    picard_pass<true, false>(L, phi, fp32, epsi, cellvol, s, st);
+    return 2 * f47 + 1;
+}
 
 int launch_import(const Layout& L, const double* staging, int layout, void* dst, bool fp32, cudaStream_t st) {
     const int py = L.two_d ? 1 : L.ny + 6;
@@ -256,6 +509,19 @@ int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const doub
                                                              s.partial);
     volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.vol, nullptr, nullptr, nullptr,
                                              0.0);
+    return 2;
+}
+
+int launch_volume_direct_clock(const Layout& L, const void* phi, bool fp32, const double* dxn, const double* dyn,
+                               const double* dzn, double psi, double period, const Scratch& s, cudaStream_t st) {
+    const dim3 grid(1, L.ny, L.nz), block(256);
+    if (fp32)
+        volume_direct_kernel<float><<<grid, block, 0, st>>>(L, static_cast<const float*>(phi), dxn, dyn, dzn, psi,
+                                                            s.partial);
+    else
+        volume_direct_kernel<double><<<grid, block, 0, st>>>(L, static_cast<const double*>(phi), dxn, dyn, dzn, psi,
+                                                             s.partial);
+    volume_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.vol, s.t, s.vscale, s.dt, period);
     return 2;
 }
 

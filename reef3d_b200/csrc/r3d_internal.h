@@ -92,6 +92,7 @@ struct Scratch {
     double* t;              // simulated time (advanced by each step)
     double* vscale;         // factor applied to the stored face velocities
     int* err;               // set by a kernel whose bounded wait gave up
+    double* pic;            // picard: step-start volume, shift w, picard_lsm target, step count
 };
 
 // ---- launchers (kernels_f64.cu / kernels_f32.cu / kernels_common.cu)
@@ -117,6 +118,44 @@ int launch_volume_reduce(const Layout& L, const Scratch& s, long long nblocks, d
 int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const double* dxn,
                          const double* dyn, const double* dzn, double psi, const Scratch& s,
                          cudaStream_t st);
+// Airy wave velocity generator: a = amp om / sinh(kw depth), kw = 2 pi /
+// wavelength, om = sqrt(g kw tanh(kw depth)).
+struct AiryParams {
+    double a, kw, om;
+};
+// Writes u and w of the Airy field at the device time *t on every stored
+// cell; coord = x centres, x faces, z centres, z faces (padded indices
+// -3..n+2).  airy_prepare sets the kernels' shared-memory limit (nonzero:
+// the grid is too long in x or z for the shared-memory tables).
+int airy_prepare(const Layout& L);
+int launch_airy(const Layout& L, void* u, void* w, bool fp32, const double* coord, const double* t,
+                const AiryParams& ap, int sms, cudaStream_t st);
+
+// Fluid constants of fluid_update_fsf (W1..W4, src/ini.cpp:831-834).
+struct FluidConst {
+    double ro_water, visc_water, ro_air, visc_air;
+};
+// Density/viscosity update with volume sums (src/fluid_update_fsf.cpp:39-104);
+// clock: the volume pass also advances the device clock like
+// launch_volume_reduce.
+int launch_fluid_update(const Layout& L, const void* phi, void* ro, void* visc, bool fp32, const double* dxn,
+                        const double* dyn, const double* dzn, double psi, const FluidConst& fc, bool clock,
+                        double period, const Scratch& s, cudaStream_t st);
+
+// Picard mass correction (src/picard_f.cpp:36-113; lsm: src/picard_lsm.cpp)
+// on the interior of phi: epsi = f45*DXM, cellvol = DXM^3 (host pow).
+// launch_picard_volcalc stores the smoothed-Heaviside volume in s.pic[0]
+// (lsm: the first step's one also in s.pic[2]); launch_picard_correct runs
+// f47 iterations of "volume, w = r(target) - r(vol2), phi += w".
+int launch_picard_volcalc(const Layout& L, const void* phi, bool fp32, double epsi, double cellvol, bool lsm,
+                          const Scratch& s, cudaStream_t st);
+int launch_picard_correct(const Layout& L, void* phi, bool fp32, double epsi, double cellvol, int f47, bool lsm,
+                          const Scratch& s, cudaStream_t st);
+// Volume pass of r3d_volume that also advances the device clock like
+// launch_volume_reduce (used when the step's last stage cannot fuse it).
+int launch_volume_direct_clock(const Layout& L, const void* phi, bool fp32, const double* dxn,
+                               const double* dyn, const double* dzn, double psi, double period,
+                               const Scratch& s, cudaStream_t st);
 int launch_cfl(const Layout& L, const void* u, const void* v, const void* w, bool fp32,
                double dxmin, double n47, const Scratch& s, cudaStream_t st);
 int launch_ghost_fill(const Layout& L, void* f, bool fp32, cudaStream_t st);

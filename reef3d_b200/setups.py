@@ -133,17 +133,22 @@ def vortex3d(n=256, cfl=0.25, T=3.0):
                 f43=0.5, f44=2, n47=cfl / 2.0, t_end=T, vel_time=lambda t: math.cos(math.pi * t / T))
 
 
-def wave_tank(nx=1024, ny=128, nz=256, dx=0.01, depth=0.5, amp=0.05, wavelength=2.0, t=0.0, cfl=0.2, g=9.81):
+def wave_tank(nx=1024, ny=128, nz=256, dx=0.01, depth=0.5, amp=0.05, wavelength=2.0, t=0.0, cfl=0.2, g=9.81,
+              velocity=True):
     """Wave-tank-shaped free surface: phi = z - (depth + amp cos(kx)) with the
-    linear (Airy) orbital velocity of that wave at time t, bed at z=0."""
+    linear (Airy) orbital velocity of that wave at time t, bed at z=0.
+    velocity=False leaves u, v, w as None (for instances whose velocity the
+    device's Airy generator writes)."""
     xn = uniform_nodes(nx, nx * dx)
     yn = uniform_nodes(ny, ny * dx)
     zn = uniform_nodes(nz, nz * dx)
     xc, yc, zc = centres(xn), centres(yn), centres(zn)
     k = 2.0 * math.pi / wavelength
     om = math.sqrt(g * k * math.tanh(k * depth))
-    X, _, Z = _mesh(xc, yc, zc)
-    phi = Z - (depth + amp * np.cos(k * X))
+    phi = (zc[None, None, :] - (depth + amp * np.cos(k * xc))[:, None, None]) * np.ones((1, len(yc), 1))
+    if not velocity:
+        return Case("wave_tank", nx, ny, nz, xn, yn, zn, np.ascontiguousarray(phi), None, None, None,
+                    f43=0.5, f44=1, n47=cfl / 2.0)
     a = amp * om / math.sinh(k * depth)
     uf = a * np.cosh(k * zc)[None, :] * np.cos(k * faces(xn) - om * t)[:, None]
     wf = a * np.sinh(k * faces(zn))[None, :] * np.sin(k * xc - om * t)[:, None]

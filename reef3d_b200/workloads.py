@@ -1,5 +1,7 @@
 """The benchmark configurations beyond the headline vortex run: the 2D
-slotted-disc revolution, the batched ensemble and the serving load test.
+slotted-disc revolution, the vortex accuracy run (FP32 form against the FP64
+path over a full period), the wave tank with the Airy velocity generator,
+the batched ensemble and the serving load test.
 Each function runs on the current CUDA device and returns a dict for the
 benchmark's JSON line."""
 import math
@@ -51,6 +53,93 @@ def slotted_disk_revolution(n=128, precision=FP64):
     return {"workload": f"slotted disc 2D {n}x{n}, one revolution", "steps": nsteps, "ms": ms,
             "cell_updates_per_s": n * n * nsteps / (ms * 1e-3), "l1_area_error": l1,
             "relative_volume_change": abs(v1 - v0) / abs(v0), "precision": "fp64" if precision == FP64 else "fp32"}
+
+
+def _vortex_period(n, precision, T=3.0):
+    """Vortex to t = T with the fixed step T/N, N = ceil(T / dt_peak) (dt_peak:
+    the CFL step of the peak velocity at t = 0).  Returns (case, phi(T),
+    volume1 at 0 and T, steps, device ms)."""
+    c = setups.vortex3d(n)
+    with LevelSet(n, n, n, c.xn, c.yn, c.zn, precision=precision, **c.flags()) as ls:
+        for f, a in ((PHI, c.phi), (U, c.u), (V, c.v), (W, c.w)):
+            ls.upload(f, a)
+        ls.set_velocity_period(T)
+        ls.set_time(0.0)
+        v0 = ls.volume()[0]
+        nsteps = int(math.ceil(T / ls.cfl_dt() - 1e-9))
+        ls.set_dt(T / nsteps)
+        s, e0, e1 = _events(ls.stream())
+        ls.sync()
+        e0.record(s)
+        ls.run(nsteps, adaptive=False)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        phi = ls.download(PHI)
+        v1 = ls.volume()[0]
+    return c, phi, v0, v1, nsteps, ms
+
+
+def vortex_accuracy(n=128, T=3.0):
+    """Shape error and volume change of the FP32 form and of the FP64 path
+    over a full vortex period (the shape returns to the initial sphere at
+    t = T), and the FP32 result against the FP64 one: L1 of the smoothed
+    Heaviside H(phi; 1.5 h) times the cell volume, L-infinity of phi over the
+    band |phi_FP64| < 3h, relative change of volume1."""
+    h = 1.0 / n
+    res = {}
+    runs = {}
+    for name, prec in (("fp64", FP64), ("fp32", FP32)):
+        c, phi, v0, v1, nsteps, ms = _vortex_period(n, prec, T)
+        a = phi[3:3 + n, 3:3 + n, 3:3 + n]
+        runs[name] = a
+        a0 = c.phi[3:3 + n, 3:3 + n, 3:3 + n]
+        res[name] = {"steps": nsteps, "ms": ms, "cell_updates_per_s": n ** 3 * nsteps / (ms * 1e-3),
+                     "l1_shape_error": float(np.sum(np.abs(heaviside(a, 1.5 * h) - heaviside(a0, 1.5 * h))) * h ** 3),
+                     "linf_shape_error_band": float(np.max(np.abs(a - a0)[np.abs(a0) < 3 * h])),
+                     "relative_volume_change": abs(v1 - v0) / abs(v0)}
+    a32, a64 = runs["fp32"], runs["fp64"]
+    band = np.abs(a64) < 3 * h
+    res["fp32_vs_fp64"] = {
+        "l1_heaviside": float(np.sum(np.abs(heaviside(a32, 1.5 * h) - heaviside(a64, 1.5 * h))) * h ** 3),
+        "linf_phi_band": float(np.max(np.abs(a32 - a64)[band])),
+        "shape_error_ratio": res["fp32"]["l1_shape_error"] / res["fp64"]["l1_shape_error"],
+        "volume_change_diff": abs(res["fp32"]["relative_volume_change"] - res["fp64"]["relative_volume_change"])}
+    res["workload"] = f"3D single vortex {n}^3 to t = T = {T}, CFL 0.25 of the peak velocity, fixed dt"
+    return res
+
+
+def wave_tank_run(steps=500, warmup=3, dims=(1024, 128, 256), precision=FP32):
+    """Wave tank 1024x128x256 (dx = 0.01 m, depth 0.5 m, wavelength 2 m,
+    amplitude 0.05 m), Airy orbital velocity regenerated on the device at the
+    start of every step, CFL 0.2, one reinitialisation pseudo-step per step,
+    `steps` steps in one captured-graph run: device time, cell-updates/s and
+    the relative change of volume1."""
+    nx, ny, nz = dims
+    c = setups.wave_tank(nx, ny, nz, velocity=False)
+    with LevelSet(nx, ny, nz, c.xn, c.yn, c.zn, precision=precision, **c.flags()) as ls:
+        ls.upload(PHI, c.phi)
+        del c.phi
+        ls.set_time(0.0)
+        ls.set_velocity_airy(0.05, 2.0, 0.5, 9.81)
+        v0 = ls.volume()[0]
+        ls.run(warmup, adaptive=True)
+        s, e0, e1 = _events(ls.stream())
+        ls.sync()
+        c0 = ls.launch_count()
+        e0.record(s)
+        ls.run(steps, adaptive=True)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = ls.launch_count() - c0
+        v1 = ls.volume()[0]
+        t_end = ls.time()
+    cells = nx * ny * nz
+    return {"workload": f"wave tank {nx}x{ny}x{nz}, Airy velocity per step, CFL 0.2, F44=1", "steps": steps,
+            "ms": ms, "ms_per_step": ms / steps, "cell_updates_per_s": cells * steps / (ms * 1e-3),
+            "simulated_s": t_end, "relative_volume_change": abs(v1 - v0) / abs(v0), "launches": launches,
+            "precision": "fp32 form" if precision == FP32 else "fp64 plain"}
 
 
 def ensemble_specs(seed=0, count=64, edges=tuple(range(64, 257, 32))):

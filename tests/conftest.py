@@ -22,6 +22,13 @@ def load_golden(name):
         return {k: z[k] for k in z.files}
 
 
+def golden_flags(g):
+    """Control flags of a golden case (cases without picard entries ran with
+    the reference's default f46 = 0, f47 = 10)."""
+    return dict(f43=float(g["f43"]), f44=int(g["f44"]), f45=float(g["f45"]), f49=int(g["f49"]),
+                n47=float(g["n47"]), f46=int(g.get("f46", 0)), f47=int(g.get("f47", 10)))
+
+
 @pytest.fixture(scope="session")
 def port_lib():
     """The C restatement oracle, built on demand (test infrastructure)."""

@@ -4,14 +4,17 @@ sources) on small seeded cases.  One process per case: the reference keeps
 its grid tables in static members.
 
     make -f oracle/Makefile.ref REF=/root/reference -j8
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case name ...]   # default: every case
 
 Each case file holds the inputs (node coordinates, control flags, phi, u, v,
 w in the reference's padded layout) and the reference's outputs: WENO node
 tables and metrics, the convection operator L, the reinitialisation operator
 L, the wall ghost fill, the CFL time step, one full level-set step (or a
 short trajectory with the time step recomputed before every step) and the
-volume sums after it.
+volume sums after it, with the density and viscosity fields the step's
+fluid update wrote.  The picard cases run with the mass correction on
+(f46 = 1 in the reinitialisation, f46 = 2 around the step, f46 = 3 the
+picard_lsm form that keeps the first step's volume; f47 iterations).
 """
 import math
 import multiprocessing as mp
@@ -31,7 +34,7 @@ def stretched(n, amp):
     return x + amp * np.sin(2 * np.pi * x) / n
 
 
-def random_case(name, nx, ny, nz, f49, stretch, seed):
+def random_case(name, nx, ny, nz, f49, stretch, seed, f46=0, f47=10):
     rng = np.random.default_rng(seed)
     xn, yn, zn = stretched(nx, stretch), stretched(ny, stretch), stretched(nz, stretch)
     shape = (nx + 6, ny + 6, nz + 6)
@@ -55,15 +58,15 @@ def random_case(name, nx, ny, nz, f49, stretch, seed):
     w = rng.standard_normal(shape)
     u[::3] = 0.0  # exact zero velocity: the advec == 0 branch
     return dict(name=name, nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w,
-                f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.125, steps=1, vel_scale=None)
+                f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.125, steps=1, vel_scale=None, f46=f46, f47=f47)
 
 
-def setup_case(name, which, n, steps):
+def setup_case(name, which, n, steps, f46=0, f47=10):
     from reef3d_b200 import setups
     c = setups.slotted_disk(n) if which == "disk" else setups.vortex3d(n)
     d = dict(name=name, nx=c.nx, ny=c.ny, nz=c.nz, xn=c.xn, yn=c.yn, zn=c.zn, phi=c.phi, u=c.u, v=c.v,
              w=c.w, f43=c.f43, f44=c.f44, f45=c.f45, f49=c.f49, n47=c.n47, steps=steps,
-             vel_scale="vortex" if which == "vortex" else None)
+             vel_scale="vortex" if which == "vortex" else None, f46=f46, f47=f47)
     return d
 
 
@@ -74,6 +77,10 @@ CASES = [
     lambda: random_case("box2d_stretched_f49_0", 12, 1, 10, 0, 0.3, 4),
     lambda: setup_case("vortex3d_n12_3steps", "vortex", 12, 3),
     lambda: setup_case("slotted2d_n24_3steps", "disk", 24, 3),
+    lambda: random_case("picard2_box3d_stretched_f49_1", 9, 7, 8, 1, 0.3, 5, f46=2, f47=10),
+    lambda: setup_case("picard2_vortex3d_n12_3steps", "vortex", 12, 3, f46=2, f47=10),
+    lambda: setup_case("picard1_slotted2d_n24_3steps", "disk", 24, 3, f46=1, f47=4),
+    lambda: setup_case("picard3_vortex3d_n12_3steps", "vortex", 12, 3, f46=3, f47=10),
 ]
 
 
@@ -82,9 +89,9 @@ def run_case(idx):
     c = CASES[idx]()
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ref = RefOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                    f49=c["f49"])
+                    f49=c["f49"], f46=c["f46"], f47=c["f47"])
     out = {k: c[k] for k in ("nx", "ny", "nz", "xn", "yn", "zn", "phi", "u", "v", "w", "f43", "f44", "f45",
-                              "f49", "n47", "steps")}
+                              "f49", "n47", "steps", "f46", "f47")}
     for a, n in enumerate((nx, ny, nz)):
         qf, cf, isf = ref.weno_tables(a, n + 8)
         out[f"qf{a}"], out[f"cf{a}"], out[f"isf{a}"] = qf, cf, isf
@@ -99,7 +106,7 @@ def run_case(idx):
     out["ghost"] = ref.ghost_fill(phi)
     T = 3.0
     t = 0.0
-    traj, dts, vols = [], [], []
+    traj, dts, vols, ros, viscs = [], [], [], [], []
     for s in range(c["steps"]):
         if c["vel_scale"] == "vortex":
             f = math.cos(math.pi * t / T)
@@ -107,7 +114,10 @@ def run_case(idx):
             ref.set_field(2, v * f)
             ref.set_field(3, w * f)
         dt = ref.cfl_dt(c["n47"])
+        ref.set_count(s + 1)  # lexer::count of the driver loop (read by picard_lsm)
         ph = ref.step(dt)
+        ros.append(ref.get_field(6))   # fluid_update_fsf inside the step (W1..W4 defaults)
+        viscs.append(ref.get_field(7))
         traj.append(ph)
         dts.append(dt)
         vols.append(ref.volume())
@@ -115,16 +125,20 @@ def run_case(idx):
     out["step_phi"] = np.array(traj)
     out["step_dt"] = np.array(dts)
     out["step_volume"] = np.array(vols)
+    out["step_ro"] = np.array(ros)
+    out["step_visc"] = np.array(viscs)
     np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), **out)
     return c["name"]
 
 
-def main():
+def main(names=()):
     ctx = mp.get_context("spawn")
     for i in range(len(CASES)):
+        if names and CASES[i]()["name"] not in names:
+            continue
         with ctx.Pool(1) as pool:
             print("wrote", pool.apply(run_case, (i,)))
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

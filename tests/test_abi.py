@@ -45,6 +45,12 @@ def test_footprint_and_bad_descriptors():
     assert r3d._lib.r3d_footprint(ctypes.byref(d2), ctypes.byref(out)) == r3d.R3D_EINVAL
     with pytest.raises(ValueError):
         r3d.make_desc(8, 8, 8, r3d.uniform_nodes(7), r3d.uniform_nodes(8), r3d.uniform_nodes(8))
+    # picard flags: 0..3 accepted; other forms and negative iterations refused
+    for f46, f47, rc in ((2, 10, r3d.R3D_OK), (1, 0, r3d.R3D_OK), (3, 10, r3d.R3D_OK), (4, 10, r3d.R3D_EINVAL),
+                         (2, -1, r3d.R3D_EINVAL)):
+        d3 = r3d.make_desc(8, 8, 8, r3d.uniform_nodes(8), r3d.uniform_nodes(8), r3d.uniform_nodes(8),
+                           f46=f46, f47=f47)
+        assert r3d._lib.r3d_footprint(ctypes.byref(d3), ctypes.byref(out)) == rc
 
 
 def test_null_handle_calls_fail_cleanly():

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import reef3d_b200 as r3d
-from conftest import GOLDEN_CASES, load_golden, velocity_at
+from conftest import GOLDEN_CASES, golden_flags, load_golden, velocity_at
 from test_oracle_golden import interior, visible_mask
 
 pytestmark = pytest.mark.gpu
@@ -25,9 +25,8 @@ def relmax(a, b):
 
 
 def make_gpu(g, precision=r3d.FP64):
-    return r3d.LevelSet(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], f43=float(g["f43"]),
-                        f44=int(g["f44"]), f45=float(g["f45"]), f49=int(g["f49"]), n47=float(g["n47"]),
-                        precision=precision)
+    return r3d.LevelSet(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], precision=precision,
+                        **golden_flags(g))
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -72,6 +71,33 @@ def test_steps_vs_reference(name):
             rv1, rv2 = g["step_volume"][s]
             assert abs(v1 - rv1) <= RTOL * abs(rv1) and abs(v2 - rv2) <= RTOL * abs(rv2)
             t += dt
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_fluid_update_vs_reference(name):
+    """ro and visc written by the step's fluid update (fluid_update_fsf with
+    the reference's default W1..W4) against the reference's own fields."""
+    g = load_golden(name)
+    nx, ny, nz = int(g["nx"]), int(g["ny"]), int(g["nz"])
+    m = visible_mask(nx, ny, nz)
+    t = 0.0
+    with make_gpu(g) as ls:
+        ls.set_fluid()
+        ls.upload(r3d.PHI, g["phi"])
+        for s in range(int(g["steps"])):
+            u, v, w = velocity_at(g, t)
+            for f, a in ((r3d.U, u), (r3d.V, v), (r3d.W, w)):
+                ls.upload(f, a)
+            t += ls.cfl_dt()
+            ls.step()
+            for fid, key in ((r3d.RO, "step_ro"), (r3d.VISC, "step_visc")):
+                got, ref = ls.download(fid), g[key][s]
+                assert relmax(got[m], ref[m]) <= RTOL, (key, s)
+            assert relmax(ls.download(r3d.PHI)[m], g["step_phi"][s][m]) <= RTOL
+            v1, v2 = ls.last_volume()
+            rv1, rv2 = g["step_volume"][s]
+            assert abs(v1 - rv1) <= RTOL * abs(rv1) and abs(v2 - rv2) <= RTOL * abs(rv2)
+        assert ls.fluid_update() == ls.last_volume()
 
 
 def random_state(nx, ny, nz, seed):
