@@ -118,6 +118,19 @@ def _ref_worker(args):
     return time.perf_counter() - t0, edge ** 3 * steps
 
 
+def host_cpu():
+    """Model name and logical CPU count of the host."""
+    model = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{model}, {os.cpu_count()} logical CPUs"
+
+
 def host_has_avx2_fma():
     try:
         flags = open("/proc/cpuinfo").read()
@@ -141,7 +154,7 @@ def reference_cpu(procs, edge, steps):
     wall = time.perf_counter() - t0
     slowest = max(r[0] for r in res)
     cells = sum(r[1] for r in res)
-    return cells / slowest, {"cores": procs, "kind": "reference",
+    return cells / slowest, {"cores": procs, "kind": "reference", "host": host_cpu(),
                              "build": "-O3 -mavx2 -mfma" if fast else "-O2 -ffp-contract=off",
                              "sample": f"{procs} processes x vortex {edge}^3 x {steps} steps (same per-cell work as "
                                        f"256^3), slowest process timed; wall {wall:.1f}s"}
@@ -170,7 +183,7 @@ def reference_disk_cpu(n=128, steps=300):
         return None
     with mp.get_context("spawn").Pool(1) as pool:
         sec = pool.apply(_ref_disk_worker, ((n, steps, fast),))
-    return {"value": n * n * steps / sec, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+    return {"value": n * n * steps / sec, "unit": "cell-updates/s", "cores": 1, "kind": "reference", "host": host_cpu(),
             "sample": f"{steps} steps of the {n}x{n} slotted disc"}
 
 

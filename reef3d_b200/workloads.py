@@ -39,8 +39,7 @@ def slotted_disk_revolution(n=128, precision=FP64):
         s, e0, e1 = _events(ls.stream())
         ls.sync()
         e0.record(s)
-        for _ in range(nsteps):
-            ls.step()
+        ls.run(nsteps, adaptive=False)  # one captured step replayed
         e1.record(s)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
@@ -55,13 +54,17 @@ def slotted_disk_revolution(n=128, precision=FP64):
             "relative_volume_change": abs(v1 - v0) / abs(v0), "precision": "fp64" if precision == FP64 else "fp32"}
 
 
-def _vortex_period(n, precision, T=3.0):
+def _vortex_period(n, precision, T=3.0, perturb=0.0):
     """Vortex to t = T with the fixed step T/N, N = ceil(T / dt_peak) (dt_peak:
-    the CFL step of the peak velocity at t = 0).  Returns (case, phi(T),
-    volume1 at 0 and T, steps, device ms)."""
+    the CFL step of the peak velocity at t = 0).  perturb > 0 multiplies the
+    initial level set by 1 + perturb * N(0,1) (seeded).  Returns (case,
+    phi(T), volume1 at 0 and T, steps, device ms)."""
     c = setups.vortex3d(n)
+    phi0 = c.phi
+    if perturb > 0.0:
+        phi0 = np.ascontiguousarray(c.phi * (1.0 + perturb * np.random.default_rng(12).standard_normal(c.phi.shape)))
     with LevelSet(n, n, n, c.xn, c.yn, c.zn, precision=precision, **c.flags()) as ls:
-        for f, a in ((PHI, c.phi), (U, c.u), (V, c.v), (W, c.w)):
+        for f, a in ((PHI, phi0), (U, c.u), (V, c.v), (W, c.w)):
             ls.upload(f, a)
         ls.set_velocity_period(T)
         ls.set_time(0.0)
@@ -89,8 +92,8 @@ def vortex_accuracy(n=128, T=3.0):
     h = 1.0 / n
     res = {}
     runs = {}
-    for name, prec in (("fp64", FP64), ("fp32", FP32)):
-        c, phi, v0, v1, nsteps, ms = _vortex_period(n, prec, T)
+    for name, prec, eps in (("fp64", FP64, 0.0), ("fp32", FP32, 0.0), ("fp64_perturbed", FP64, 1e-12)):
+        c, phi, v0, v1, nsteps, ms = _vortex_period(n, prec, T, eps)
         a = phi[3:3 + n, 3:3 + n, 3:3 + n]
         runs[name] = a
         a0 = c.phi[3:3 + n, 3:3 + n, 3:3 + n]
@@ -105,6 +108,14 @@ def vortex_accuracy(n=128, T=3.0):
         "linf_phi_band": float(np.max(np.abs(a32 - a64)[band])),
         "shape_error_ratio": res["fp32"]["l1_shape_error"] / res["fp64"]["l1_shape_error"],
         "volume_change_diff": abs(res["fp32"]["relative_volume_change"] - res["fp64"]["relative_volume_change"])}
+    # the same comparison for an FP64 run whose initial level set differs by
+    # 1e-12 relative: the sensitivity of these metrics to any perturbation
+    ap = runs["fp64_perturbed"]
+    res["fp64_perturbed_vs_fp64"] = {
+        "l1_heaviside": float(np.sum(np.abs(heaviside(ap, 1.5 * h) - heaviside(a64, 1.5 * h))) * h ** 3),
+        "linf_phi_band": float(np.max(np.abs(ap - a64)[band])),
+        "shape_error_ratio": res["fp64_perturbed"]["l1_shape_error"] / res["fp64"]["l1_shape_error"],
+        "volume_change_diff": abs(res["fp64_perturbed"]["relative_volume_change"] - res["fp64"]["relative_volume_change"])}
     res["workload"] = f"3D single vortex {n}^3 to t = T = {T}, CFL 0.25 of the peak velocity, fixed dt"
     return res
 
