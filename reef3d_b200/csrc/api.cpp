@@ -404,7 +404,7 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
         bool ok = true;
         for (int q = 0; q < 3 && ok; ++q)
             ok = encode_plane_map(h->L, static_cast<const float*>(h->field[ids[q]]), &h->map[q], &why) == 0;
-        h->tile_ok = ok;
+        h->tile_ok = ok && tile_prepare();
     }
     *out = h;
     return R3D_OK;

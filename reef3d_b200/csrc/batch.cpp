@@ -206,8 +206,8 @@ BatchLaunch cell_launch_of(const r3d_batch* b) {
     return l;
 }
 
-unsigned tiled_grid(const r3d_batch* b) {
-    const long long want = 2LL * b->sms;  // two 256-thread CTAs of 45 KB per SM
+unsigned tiled_grid(const r3d_batch* b, bool reini) {
+    const long long want = (long long)tile_ctas_per_sm(reini) * b->sms;  // the co-resident CTAs
     return (unsigned)std::max<long long>(1, std::min<long long>(want, b->t_tiled));
 }
 
@@ -215,7 +215,7 @@ long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
     long long n = 0;
     if (b->n_tiled)
         n += launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, reini, s, q, b->d_vol,
-                                     tiled_grid(b), b->stream);
+                                     tiled_grid(b, reini), b->stream);
     if ((size_t)b->n_tiled < b->members.size())
         n += launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, b->stream);
     return n;
@@ -224,7 +224,7 @@ long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
 // CFL, 3 convection stages, max(f44) reinit pseudo-steps, volume + clock.
 long long enqueue_batch_step(r3d_batch* b) {
     long long n = 0;
-    if (b->n_tiled) n += launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b), b->stream);
+    if (b->n_tiled) n += launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b, false), b->stream);
     if ((size_t)b->n_tiled < b->members.size()) n += launch_batch_vmax(cell_launch_of(b), b->stream);
     n += launch_batch_dt(launch_of(b), b->stream);
     for (int s = 1; s <= 3; ++s) n += enqueue_stage(b, false, s, 0);
@@ -406,7 +406,7 @@ int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows_out, int*
     b->rows = 4;
     b->ctas_per_sm = 8;
     if (int rc = rebuild(b)) return rc;
-    if (b->n_tiled) launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b), b->stream);
+    if (b->n_tiled) launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b, false), b->stream);
     if ((size_t)b->n_tiled < b->members.size()) launch_batch_vmax(cell_launch_of(b), b->stream);
     launch_batch_dt(launch_of(b), b->stream);
     for (int r : cand_rows)

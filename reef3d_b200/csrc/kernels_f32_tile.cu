@@ -3,9 +3,9 @@
 // A CTA owns a 64 x 8 (x, y) column of cells and marches a chunk of kc
 // z-planes.  Each plane of the stage input is staged once into shared memory
 // by one TMA box copy (72 x 14 floats: the tile plus its 3-cell x/y halo,
-// x rounded down to a 16-byte boundary) into an 8-slot ring guarded by
-// mbarriers; the z neighbours of a thread's cells live in a 7-plane register
-// window.  Every thread computes two x-adjacent cells with packed FP32x2
+// x rounded down to a 16-byte boundary) into a 16-slot ring guarded by
+// mbarriers; the ring holds the seven planes of the z stencil as well as the
+// planes being prefetched.  Every thread computes two x-adjacent cells with packed FP32x2
 // arithmetic (Blackwell FFMA2/FADD2/FMUL2).  The WENO5-HJ upwind side and
 // the Godunov branch of the reinitialisation are chosen with selects: the
 // plus-side derivative is the minus-side formula on the mirrored difference
@@ -27,10 +27,18 @@ namespace {
 
 constexpr int kTX = 64, kTY = 8, kThreads = 256;
 constexpr int kBoxX = kTX + 8, kBoxY = kTY + 6;
-constexpr int kSlots = 8;
+constexpr int kRing = 16;          // plane boxes in shared memory (a power of two)
 constexpr int kSlotFloats = 1024;  // 72*14 = 1008 floats, padded to 4 KB
 constexpr unsigned kBoxBytes = kBoxX * kBoxY * 4;
 constexpr long long kSpin = 1ll << 22;
+// CTAs per SM the stage kernels are register-limited for (the ring takes
+// 64 KB of shared memory per CTA, so three fit an SM)
+#ifndef R3D_TILE_MINB_CONV
+#define R3D_TILE_MINB_CONV 3
+#endif
+#ifndef R3D_TILE_MINB_REINI
+#define R3D_TILE_MINB_REINI 3
+#endif
 
 // ------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -130,25 +138,68 @@ __device__ __forceinline__ float2 weno5_2(float2 d1, float2 d2, float2 d3, float
     return mul2(fma2(n3, p3, fma2(n2, p2, mul2(n1, p1))), inv);
 }
 
-// Upwind derivative (times h) of an axis from 7 packed values f[0..6]
-// (f[3] the cells), plus side where `plus` is set per cell.
-__device__ __forceinline__ float2 deriv2(const float2* f, bool px, bool py, float ih2) {
-    const float2 D0 = sub2(f[1], f[0]), D1 = sub2(f[2], f[1]), D2 = sub2(f[3], f[2]);
-    const float2 D3 = sub2(f[4], f[3]), D4 = sub2(f[5], f[4]), D5 = sub2(f[6], f[5]);
+// Upwind derivative (times h) of an axis from its six packed undivided
+// differences D[m] = f[m+1] - f[m] of the 7-point stencil f[0..6] (f[3] the
+// cells), plus side where `plus` is set per cell.
+__device__ __forceinline__ float2 deriv2(const float2* D, bool px, bool py, float ih2) {
     // minus: (D0..D4); plus (mirrored): (D5, D4, D3, D2, D1)
-    return weno5_2(sel2(px, py, D5, D0), sel2(px, py, D4, D1), sel2(px, py, D3, D2), sel2(px, py, D2, D3),
-                   sel2(px, py, D1, D4), ih2);
+    return weno5_2(sel2(px, py, D[5], D[0]), sel2(px, py, D[4], D[1]), sel2(px, py, D[3], D[2]),
+                   sel2(px, py, D[2], D[3]), sel2(px, py, D[1], D[4]), ih2);
+}
+
+__device__ __forceinline__ void diffs2(const float2* f, float2* D) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) D[m] = sub2(f[m + 1], f[m]);
+}
+
+// WENO5 (Jiang-Peng) derivative times h in FP64 from the undivided
+// differences d1..d5 of the minus-side upwind set (the plus side passes the
+// mirrored set), the weights with one division:
+// w_r = c_r prod_{q!=r} s_q^2 / sum_q c_q prod_{p!=q} s_p^2.
+__device__ __forceinline__ double weno5_d(double d1, double d2, double d3, double d4, double d5, double eps) {
+    const double a1 = d3 - d4, b1 = d5 - d4, b2 = d2 - d3, b3 = d1 - d2;
+    const double s1 = ((10.0 / 3.0) * a1 + (11.0 / 3.0) * b1) * a1 + (4.0 / 3.0) * b1 * b1 + eps;
+    const double s2 = ((4.0 / 3.0) * a1 - (5.0 / 3.0) * b2) * a1 + (4.0 / 3.0) * b2 * b2 + eps;
+    const double s3 = ((10.0 / 3.0) * b2 - (11.0 / 3.0) * b3) * b2 + (4.0 / 3.0) * b3 * b3 + eps;
+    const double q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
+    const double n1 = 0.3 * q2 * q3, n2 = 0.6 * q1 * q3, n3 = 0.1 * q1 * q2;
+    const double p1 = d4 + (1.0 / 3.0) * a1 - (1.0 / 6.0) * b1;
+    const double p2 = d3 - (1.0 / 3.0) * a1 - (1.0 / 6.0) * b2;
+    const double p3 = d2 + (1.0 / 3.0) * b3 - (11.0 / 6.0) * b2;
+    return (n1 * p1 + n2 * p2 + n3 * p3) / (n1 + n2 + n3);
 }
 
 // Reinitialisation right-hand side of one cell in FP64 from its FP32
-// stencils (the interface band), the reference's branch structure.
-__device__ double reini_cell_fp64(const float* fx, const float* fy, const float* fz, const TileArgs& a) {
-    double X[7], Y[7], Z[7];
+// stencils (the interface band): Godunov selection, one-sided WENO5 per
+// axis and the smoothed sign of src/reinidisc_f.cpp:58-127 on a uniform
+// grid.  X, Y, Z: the 7-point stencils along x, y, z (centre at [3]).
+__device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, const float* Z, const TileArgs& a) {
+    const double f0 = X[3];
+    const double sg = fabs(f0) < 1.0e-8 ? 1.0 : (f0 > 0.0 ? 1.0 : -1.0);
+    const float* ax[3] = {X, Y, Z};
+    double g2 = 0.0;
 #pragma unroll
-    for (int m = 0; m < 7; ++m) { X[m] = fx[m]; Y[m] = fy[m]; Z[m] = fz[m]; }
-    const double rh[3] = {a.rh[0], a.rh[1], a.rh[2]};
-    const double hh[3] = {1.0 / (rh[0] * rh[0]), 1.0 / (rh[1] * rh[1]), 1.0 / (rh[2] * rh[2])};
-    return f32::reini_rhs_uniform<double, false>(X, Y, Z, rh, hh, 1.0e-6, (double)a.deltax);
+    for (int d = 0; d < 3; ++d) {
+        const float* f = ax[d];
+        double D[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) D[m] = (double)f[m + 1] - (double)f[m];
+        const double ms = D[2] * sg, ps = D[3] * sg, sum = ms + ps;
+        const bool c1 = ms > 0.0 && sum > 0.0, c2 = ps < 0.0 && sum < 0.0;
+        if (c1 || c2) {
+            const double h = 1.0 / (double)a.rh[d];
+            const double eps = 1.0e-6 * h * h;
+            const double w = c2 ? weno5_d(D[5], D[4], D[3], D[2], D[1], eps)
+                                : weno5_d(D[0], D[1], D[2], D[3], D[4], eps);
+            const double gd = w * (double)a.rh[d];
+            g2 += gd * gd;
+        }
+    }
+    const double dn = sqrt(g2);
+    const double dl = a.deltax;
+    double S = f0 / sqrt(f0 * f0 + dn * dn * dl * dl);
+    if (S != S) S = 1.0;
+    return (float)(S - S * dn);  // -(S |grad| - S)
 }
 
 // One work item: the 64 x 8 column (bx, by) over planes [bz*kc, bz*kc+kc)
@@ -157,16 +208,17 @@ __device__ double reini_cell_fp64(const float* fx, const float* fy, const float*
 // item's volume partials (when `volume`) go to partial_out[0..1].  The
 // mbarriers are initialised at the start of the item and invalidated at its
 // end, so a persistent CTA can run items back to back.
+//
+// Shared memory is a ring of kRing plane boxes holding planes k-3 .. k+12
+// while plane k is computed: the x and y stencils come from plane k's box,
+// the z stencil from the thread's own column in the seven boxes k-3..k+3.
+// After plane k the box of plane k-3 is refilled with plane k+13.
 template <bool REINI, int STAGE>
 __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArgs& a, int bx, int by, int bz,
                                           bool volume, unsigned char* smem_raw, double* red_a, double* red_b,
                                           double* partial_out) {
-    // shared memory: ring of kSlots plane boxes, 3 boxes for the planes
-    // below the chunk, then the mbarriers
-    float* slots = reinterpret_cast<float*>(smem_raw);
-    float* below = slots + kSlots * kSlotFloats;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(below + 3 * kSlotFloats);
-    uint64_t* xbar = bar + kSlots;
+    float* ring = reinterpret_cast<float*>(smem_raw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ring + kRing * kSlotFloats);
 
     const Layout& L = a.L;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -176,60 +228,51 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     const int k1 = min(k0 + a.kc, L.nz);
     const int xbox = bx * kTX + L.gx - 4;  // 16-byte aligned x start
     const int ybox = by * kTY + L.gy - 3;
-    const int plast = k1 + 2;  // last plane staged in the ring
+    const int pfirst = k0 - 3;  // first plane staged (ring position 0)
+    const int plast = k1 + 2;   // last plane staged
     const bool act0 = i0 < L.nx && j < L.ny;
     const bool act1 = i0 + 1 < L.nx && j < L.ny;
     const long long col = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
     const int own = (ty + 3) * kBoxX + 2 * tx + 4;  // the thread's two cells in a box
+    // wall ghost layers this thread writes on every plane (x, y faces)
+    const bool gxlo = act0 && i0 == 0;
+    const bool gxhi2 = act1 && i0 + 1 == L.nx - 1;  // second cell is the last one
+    const bool gxhi1 = act0 && !act1;                // first cell is the last one
+    const bool gylo = act0 && j == 0, gyhi = act0 && j == L.ny - 1;
+    const bool gside = gxlo || gxhi2 || gxhi1 || gylo || gyhi;
 
-    int issued = k0 - 1;
+    int issued = pfirst - 1;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kSlots + 3; ++s) mbar_init(bar + s, 1);
+        for (int s = 0; s < kRing; ++s) mbar_init(bar + s, 1);
         mbar_fence_init();
-        for (int m = 0; m < 3; ++m) {
-            mbar_expect_tx(xbar + m, kBoxBytes);
-            tma_load_3d(below + m * kSlotFloats, tmap, xbar + m, xbox, ybox, k0 - 3 + m + L.gz);
-        }
-        for (int p = k0; p <= min(k0 + kSlots - 1, plast); ++p) {
-            const int s = (p - k0) % kSlots;
+        for (int p = pfirst; p <= min(pfirst + kRing - 1, plast); ++p) {
+            const int s = p - pfirst;
             mbar_expect_tx(bar + s, kBoxBytes);
-            tma_load_3d(slots + s * kSlotFloats, tmap, bar + s, xbox, ybox, p + L.gz);
+            tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, p + L.gz);
             issued = p;
         }
     }
     __syncthreads();
 
-    // z window: planes k-3..k+3 of the thread's two cells
-    float2 zw[7];
+    // planes k0-3 .. k0+2: the first window without its top plane
     bool ok = true;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        ok = ok && mbar_wait_bounded(xbar + m, 0);
-        zw[m] = *reinterpret_cast<const float2*>(below + m * kSlotFloats + own);
-    }
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const int p = k0 + m;  // p <= k0 + 2 <= plast always
-        ok = ok && mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
-        zw[3 + m] = *reinterpret_cast<const float2*>(slots + ((p - k0) % kSlots) * kSlotFloats + own);
-    }
+    for (int m = 0; m < 6; ++m) ok = ok && mbar_wait_bounded(bar + m, 0);
 
     const float vs = (float)*a.vscale;
     const float dtc = REINI ? a.dtr : (float)*a.dt;
+    long long c = (long long)(k0 + L.gz) * L.sz + col;
     float2 wprev = make_float2(0.f, 0.f);
-    if (!REINI && act0) {
-        const long long c = (long long)(k0 - 1 + L.gz) * L.sz + col;
-        wprev = act1 ? __ldg(reinterpret_cast<const float2*>(a.w + c)) : make_float2(__ldg(a.w + c), 0.f);
-    }
+    if (!REINI && act0)
+        wprev = act1 ? __ldg(reinterpret_cast<const float2*>(a.w + c - L.sz)) : make_float2(__ldg(a.w + c - L.sz), 0.f);
     double vol_a = 0.0, vol_b = 0.0;
 
     // cell-local global operands of a plane (velocities, step start value),
     // fetched one plane ahead so their latency overlaps the current plane
     float2 nu = make_float2(0.f, 0.f), nv = nu, nvm = nu, nw = nu, nfn = nu;
     float num = 0.f;
-    auto fetch = [&](int kk) {
+    auto fetch = [&](long long cc) {
         if (!act0) return;
-        const long long cc = (long long)(kk + L.gz) * L.sz + col;
         if (!REINI) {
             if (act1) {
                 nu = __ldg(reinterpret_cast<const float2*>(a.u + cc));
@@ -247,16 +290,18 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
         // the step start value may be this stage's output (stage 3): plain loads
         if (STAGE != 1) nfn = act1 ? *reinterpret_cast<const float2*>(a.fn + cc) : make_float2(a.fn[cc], 0.f);
     };
-    fetch(k0);
+    fetch(c);
 
     bool aborted = __syncthreads_or(!ok);
-    for (int k = k0; k < k1 && !aborted; ++k) {
-        const int p = k + 3;
-        ok = mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
-        zw[6] = *reinterpret_cast<const float2*>(slots + ((p - k0) % kSlots) * kSlotFloats + own);
-        const float* sl = slots + ((k - k0) % kSlots) * kSlotFloats;
+    for (int k = k0; k < k1 && !aborted; ++k, c += L.sz) {
+        const int n = k - k0;  // ring position of plane k-3
+        {
+            const int nt = n + 6;  // plane k+3
+            ok = mbar_wait_bounded(bar + (nt & (kRing - 1)), (nt / kRing) & 1);
+        }
+        const float* sl = ring + ((n + 3) & (kRing - 1)) * kSlotFloats;  // plane k
 
-        // x stencil: 10 values of the row, columns 2tx .. 2tx+9
+        // x stencil: the row's columns 2tx .. 2tx+9 (the cells at 2tx+4, 2tx+5)
         float xv[10];
         {
             const float* r = sl + (ty + 3) * kBoxX + 2 * tx;
@@ -267,14 +312,22 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                 xv[2 * q + 1] = t.y;
             }
         }
-        float2 fx[7], fy[7];
+        float2 Dx[6], Dy[6], Dz[6];
 #pragma unroll
-        for (int m = 0; m < 7; ++m) {
-            fx[m] = make_float2(xv[m + 1], xv[m + 2]);
-            fy[m] = *reinterpret_cast<const float2*>(sl + (ty + m) * kBoxX + 2 * tx + 4);
+        for (int m = 0; m < 6; ++m) Dx[m] = make_float2(xv[m + 2] - xv[m + 1], xv[m + 3] - xv[m + 2]);
+        float2 fy2, fy4, fz2, fz4;
+        {
+            float2 fy[7], fz[7];
+#pragma unroll
+            for (int m = 0; m < 7; ++m) {
+                fy[m] = *reinterpret_cast<const float2*>(sl + (ty + m) * kBoxX + 2 * tx + 4);
+                fz[m] = *reinterpret_cast<const float2*>(ring + ((n + m) & (kRing - 1)) * kSlotFloats + own);
+            }
+            diffs2(fy, Dy);
+            diffs2(fz, Dz);
+            fy2 = fy[2]; fy4 = fy[4]; fz2 = fz[2]; fz4 = fz[4];
         }
-        const float2 f0 = fy[3];
-        const long long c = (long long)(k + L.gz) * L.sz + col;
+        const float2 f0 = make_float2(xv[4], xv[5]);
 
         float2 Lc;
         const float2 fn = nfn;
@@ -286,25 +339,29 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             const float2 ja = mul2(h2, add2(vc, vm));
             const float2 ka = mul2(h2, add2(wc, wprev));
             wprev = wc;
-            const float2 gx = mul2(f2(a.rh[0]), deriv2(fx, ia.x < 0.f, ia.y < 0.f, a.eps[0]));
-            const float2 gy = mul2(f2(a.rh[1]), deriv2(fy, ja.x < 0.f, ja.y < 0.f, a.eps[1]));
-            const float2 gz = mul2(f2(a.rh[2]), deriv2(zw, ka.x < 0.f, ka.y < 0.f, a.eps[2]));
+            const float2 gx = mul2(f2(a.rh[0]), deriv2(Dx, ia.x < 0.f, ia.y < 0.f, a.eps[0]));
+            const float2 gy = mul2(f2(a.rh[1]), deriv2(Dy, ja.x < 0.f, ja.y < 0.f, a.eps[1]));
+            const float2 gz = mul2(f2(a.rh[2]), deriv2(Dz, ka.x < 0.f, ka.y < 0.f, a.eps[2]));
             Lc = mul2(f2(-1.f), fma2(ka, gz, fma2(ja, gy, mul2(ia, gx))));
         } else {
-            // Godunov selection per axis (src/reinidisc_f.cpp:70-109)
-            const float sgx = fabsf(f0.x) < 1.0e-8f ? 1.f : (f0.x > 0.f ? 1.f : -1.f);
-            const float sgy = fabsf(f0.y) < 1.0e-8f ? 1.f : (f0.y > 0.f ? 1.f : -1.f);
-            const float2* ax[3] = {fx, fy, zw};
+            // Godunov selection per axis (src/reinidisc_f.cpp:70-109) on the
+            // backward and forward differences D[2], D[3] times the sign s
+            // (the grid factor 1/h > 0 leaves every test unchanged):
+            //   upwind minus side: m > 0 && p > -m, i.e. m > 0 && m + p > 0
+            //   upwind plus side:  p < 0 && m < -p, i.e. p < 0 && m + p < 0
+            // (the sign of a rounded sum is the sign of the exact sum)
+            const float2 sg = make_float2(fabsf(f0.x) < 1.0e-8f ? 1.f : (f0.x > 0.f ? 1.f : -1.f),
+                                          fabsf(f0.y) < 1.0e-8f ? 1.f : (f0.y > 0.f ? 1.f : -1.f));
+            const float2* ax[3] = {Dx, Dy, Dz};
             float2 g2 = make_float2(0.f, 0.f);
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                const float2* f = ax[d];
-                const float2 xm = mul2(sub2(f0, f[2]), f2(a.rh[d]));
-                const float2 xp = mul2(sub2(f[4], f0), f2(a.rh[d]));
-                const float msx = xm.x * sgx, psx = xp.x * sgx, msy = xm.y * sgy, psy = xp.y * sgy;
-                const bool c1x = msx > 0.f && psx > -msx, c2x = psx < 0.f && msx < -psx;
-                const bool c1y = msy > 0.f && psy > -msy, c2y = psy < 0.f && msy < -psy;
-                float2 g = mul2(f2(a.rh[d]), deriv2(f, c2x, c2y, a.eps[d]));
+                const float2* D = ax[d];
+                const float2 ms = mul2(D[2], sg), ps = mul2(D[3], sg);
+                const float2 sum = add2(ms, ps);
+                const bool c1x = ms.x > 0.f && sum.x > 0.f, c2x = ps.x < 0.f && sum.x < 0.f;
+                const bool c1y = ms.y > 0.f && sum.y > 0.f, c2y = ps.y < 0.f && sum.y < 0.f;
+                float2 g = mul2(f2(a.rh[d]), deriv2(D, c2x, c2y, a.eps[d]));
                 g.x = (c1x || c2x) ? g.x : 0.f;
                 g.y = (c1y || c2y) ? g.y : 0.f;
                 g2 = fma2(g, g, g2);
@@ -312,35 +369,55 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             const float2 dn = make_float2(sqrt_approx(g2.x), sqrt_approx(g2.y));
             const float2 dl = f2(a.deltax);
             const float2 den = fma2(mul2(mul2(dn, dn), dl), dl, mul2(f0, f0));
-            float2 sg = mul2(f0, make_float2(rsqrtf(den.x), rsqrtf(den.y)));
-            if (sg.x != sg.x) sg.x = 1.f;
-            if (sg.y != sg.y) sg.y = 1.f;
-            Lc = sub2(sg, mul2(sg, dn));  // -(S |grad| - S)
-            // interface band: the 7-point stencil changes sign
-            const bool posx = f0.x >= 0.f && fx[2].x >= 0.f && fx[4].x >= 0.f && fy[2].x >= 0.f && fy[4].x >= 0.f &&
-                              zw[2].x >= 0.f && zw[4].x >= 0.f;
-            const bool negx = f0.x < 0.f && fx[2].x < 0.f && fx[4].x < 0.f && fy[2].x < 0.f && fy[4].x < 0.f &&
-                              zw[2].x < 0.f && zw[4].x < 0.f;
-            const bool posy = f0.y >= 0.f && fx[2].y >= 0.f && fx[4].y >= 0.f && fy[2].y >= 0.f && fy[4].y >= 0.f &&
-                              zw[2].y >= 0.f && zw[4].y >= 0.f;
-            const bool negy = f0.y < 0.f && fx[2].y < 0.f && fx[4].y < 0.f && fy[2].y < 0.f && fy[4].y < 0.f &&
-                              zw[2].y < 0.f && zw[4].y < 0.f;
-            const bool bandx = !(posx || negx), bandy = !(posy || negy);
+            float2 S = mul2(f0, make_float2(rsqrtf(den.x), rsqrtf(den.y)));
+            if (S.x != S.x) S.x = 1.f;
+            if (S.y != S.y) S.y = 1.f;
+            Lc = sub2(S, mul2(S, dn));  // -(S |grad| - S)
+            // interface band: the 7-point stencil changes sign, i.e. neither
+            // all values >= 0 (min >= 0) nor all < 0 (max < 0)
+            const float lox = fminf(fminf(fminf(f0.x, xv[3]), fminf(xv[5], fy2.x)), fminf(fminf(fy4.x, fz2.x), fz4.x));
+            const float hix = fmaxf(fmaxf(fmaxf(f0.x, xv[3]), fmaxf(xv[5], fy2.x)), fmaxf(fmaxf(fy4.x, fz2.x), fz4.x));
+            const float loy = fminf(fminf(fminf(f0.y, xv[4]), fminf(xv[6], fy2.y)), fminf(fminf(fy4.y, fz2.y), fz4.y));
+            const float hiy = fmaxf(fmaxf(fmaxf(f0.y, xv[4]), fmaxf(xv[6], fy2.y)), fmaxf(fmaxf(fy4.y, fz2.y), fz4.y));
+            const bool bandx = lox < 0.f && hix >= 0.f, bandy = loy < 0.f && hiy >= 0.f;
             if (a.f49 == 0) {
                 if (bandx) Lc.x = 0.f;  // src/reinidisc_fsf.cpp:70-72
                 if (bandy) Lc.y = 0.f;
             } else if (a.band64) {
-                if (bandx || bandy) {
-                    float X[7], Y[7], Z[7];
-                    if (bandx) {
+                // The warp's band cells (at most 64) are dealt out to its
+                // lanes, one FP64 evaluation each, stencils from shared
+                // memory; results go back to the owning lanes by shuffles.
+                const unsigned mx = __ballot_sync(0xffffffffu, act0 && bandx);
+                const unsigned my = __ballot_sync(0xffffffffu, act1 && bandy);
+                if (mx | my) {
+                    const int cx = __popc(mx), total = cx + __popc(my);
+                    const unsigned below = (1u << tx) - 1u;
+                    const int bxi = __popc(mx & below), byi = cx + __popc(my & below);
+                    for (int base = 0; base < total; base += 32) {
+                        float res = 0.f;
+                        const int b = base + tx;
+                        if (b < total) {
+                            const bool isy = b >= cx;
+                            // the lane holding the (b or b-cx)-th set bit of the mask
+                            unsigned msk = isy ? my : mx;
+                            for (int q = isy ? b - cx : b; q > 0; --q) msk &= msk - 1u;
+                            const int src = __ffs(msk) - 1;
+                            const int e = isy ? 1 : 0;
+                            const float* r = sl + (ty + 3) * kBoxX + 2 * src + e;
+                            const int o = (ty + 3) * kBoxX + 2 * src + 4 + e;
+                            float X[7], Y[7], Z[7];
 #pragma unroll
-                        for (int m = 0; m < 7; ++m) { X[m] = fx[m].x; Y[m] = fy[m].x; Z[m] = zw[m].x; }
-                        Lc.x = (float)reini_cell_fp64(X, Y, Z, a);
-                    }
-                    if (bandy) {
-#pragma unroll
-                        for (int m = 0; m < 7; ++m) { X[m] = fx[m].y; Y[m] = fy[m].y; Z[m] = zw[m].y; }
-                        Lc.y = (float)reini_cell_fp64(X, Y, Z, a);
+                            for (int m = 0; m < 7; ++m) {
+                                X[m] = r[m + 1];
+                                Y[m] = sl[(ty + m) * kBoxX + 2 * src + 4 + e];
+                                Z[m] = ring[((n + m) & (kRing - 1)) * kSlotFloats + o];
+                            }
+                            res = reini_cell_fp64(X, Y, Z, a);
+                        }
+                        const float rx = __shfl_sync(0xffffffffu, res, (bxi - base) & 31);
+                        const float ry = __shfl_sync(0xffffffffu, res, (byi - base) & 31);
+                        if (act0 && bandx && bxi >= base && bxi < base + 32) Lc.x = rx;
+                        if (act1 && bandy && byi >= base && byi < base + 32) Lc.y = ry;
                     }
                 }
             }
@@ -359,25 +436,28 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             if (act1) *reinterpret_cast<float2*>(a.out + c) = val;
             else a.out[c] = val.x;
             // wall ghost copies (src/gc_neumann.cpp:29-54)
-            if (i0 == 0) { a.out[c - 1] = val.x; a.out[c - 2] = val.x; a.out[c - 3] = val.x; }
-            if (act1 && i0 + 1 == L.nx - 1) { a.out[c + 2] = val.y; a.out[c + 3] = val.y; a.out[c + 4] = val.y; }
-            if (!act1) { a.out[c + 1] = val.x; a.out[c + 2] = val.x; a.out[c + 3] = val.x; }
-            const int nw = act1 ? 2 : 1;
-            if (j == 0)
-                for (int q = 1; q <= 3; ++q)
-                    for (int e = 0; e < nw; ++e) a.out[c - q * L.sy + e] = e ? val.y : val.x;
-            if (j == L.ny - 1)
-                for (int q = 1; q <= 3; ++q)
-                    for (int e = 0; e < nw; ++e) a.out[c + q * L.sy + e] = e ? val.y : val.x;
-            if (k == 0)
-                for (int q = 1; q <= 3; ++q)
-                    for (int e = 0; e < nw; ++e) a.out[c - q * L.sz + e] = e ? val.y : val.x;
-            if (k == L.nz - 1)
-                for (int q = 1; q <= 3; ++q)
-                    for (int e = 0; e < nw; ++e) a.out[c + q * L.sz + e] = e ? val.y : val.x;
+            if (gside || k == 0 || k == L.nz - 1) {
+                if (gxlo) { a.out[c - 1] = val.x; a.out[c - 2] = val.x; a.out[c - 3] = val.x; }
+                if (gxhi2) { a.out[c + 2] = val.y; a.out[c + 3] = val.y; a.out[c + 4] = val.y; }
+                if (gxhi1) { a.out[c + 1] = val.x; a.out[c + 2] = val.x; a.out[c + 3] = val.x; }
+                const int nw = act1 ? 2 : 1;
+                if (gylo)
+                    for (int q = 1; q <= 3; ++q)
+                        for (int e = 0; e < nw; ++e) a.out[c - q * L.sy + e] = e ? val.y : val.x;
+                if (gyhi)
+                    for (int q = 1; q <= 3; ++q)
+                        for (int e = 0; e < nw; ++e) a.out[c + q * L.sy + e] = e ? val.y : val.x;
+                if (k == 0)
+                    for (int q = 1; q <= 3; ++q)
+                        for (int e = 0; e < nw; ++e) a.out[c - q * L.sz + e] = e ? val.y : val.x;
+                if (k == L.nz - 1)
+                    for (int q = 1; q <= 3; ++q)
+                        for (int e = 0; e < nw; ++e) a.out[c + q * L.sz + e] = e ? val.y : val.x;
+            }
             if (volume) {
                 // smoothed Heaviside in FP64 (src/fluid_update_fsf.cpp:50-71)
                 const double PI_REF = 3.14159265359;
+                const int nw = act1 ? 2 : 1;
                 for (int e = 0; e < nw; ++e) {
                     const double ph = e ? val.y : val.x;
                     double H = 0.0;
@@ -390,27 +470,27 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             }
         }
 
-        if (k + 1 < k1) fetch(k + 1);
-        // every thread is done with the box of plane k: refill its slot
+        if (k + 1 < k1) fetch(c + L.sz);
+        // every thread is done with the box of plane k-3: refill it with k+13
         aborted = __syncthreads_or(!ok);
-        if (!aborted && threadIdx.x == 0 && k + kSlots <= plast) {
-            const int pn = k + kSlots;
-            const int s = (pn - k0) % kSlots;
+        if (!aborted && threadIdx.x == 0 && k + kRing - 3 <= plast) {
+            const int pn = k + kRing - 3;
+            const int s = n & (kRing - 1);
             fence_proxy_async();
             mbar_expect_tx(bar + s, kBoxBytes);
-            tma_load_3d(slots + s * kSlotFloats, tmap, bar + s, xbox, ybox, pn + L.gz);
+            tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, pn + L.gz);
             issued = pn;
         }
-#pragma unroll
-        for (int m = 0; m < 6; ++m) zw[m] = zw[m + 1];
     }
 
     if (aborted) {
         if (threadIdx.x == 0) {
             atomicExch(a.err, 1);
             // wait (bounded) for every copy still in flight before leaving
-            for (int m = 0; m < 3; ++m) mbar_wait_bounded(xbar + m, 0);
-            for (int p = k0; p <= issued; ++p) mbar_wait_bounded(bar + (p - k0) % kSlots, ((p - k0) / kSlots) & 1);
+            for (int p = pfirst; p <= issued; ++p) {
+                const int q = p - pfirst;
+                mbar_wait_bounded(bar + (q & (kRing - 1)), (q / kRing) & 1);
+            }
         }
         return false;
     }
@@ -431,13 +511,13 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     // every wait of the item has completed: retire the barriers
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int s = 0; s < kSlots + 3; ++s) mbar_inval(bar + s);
+        for (int s = 0; s < kRing; ++s) mbar_inval(bar + s);
     __syncthreads();
     return true;
 }
 
 template <bool REINI, int STAGE, bool VOLUME>
-__global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
+__global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
     const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
@@ -450,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(const __grid_constant
 // member).  Reinitialisation pseudo-step q is skipped by members with
 // f44 <= q; the last stage of a member's step adds its volume partials.
 template <bool REINI, int STAGE>
-__global__ void __launch_bounds__(kThreads, 2) batch_tile_kernel(const TiledMember* __restrict__ members,
+__global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV) batch_tile_kernel(const TiledMember* __restrict__ members,
                                                                  const CUtensorMap* __restrict__ maps,
                                                                  const long long* __restrict__ tile0, int nm,
                                                                  int q, double* __restrict__ vol_part) {
@@ -540,7 +620,42 @@ __global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMe
     }
 }
 
+// The ring needs more than the default 48 KB of dynamic shared memory, and a
+// full shared-memory carveout lets several CTAs share an SM.
+template <typename K>
+bool tile_attr(K kernel, int bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess &&
+           cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
+}
+
 }  // namespace
+
+int tile_ctas_per_sm(bool reini) { return reini ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV; }
+
+// Sets the attributes of every instantiation once per device.
+bool tile_prepare() {
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (dev >= 0 && dev < 64 && done[dev]) return true;
+    const int b = (int)tile_smem_bytes();
+    const bool ok =
+        tile_attr(tile_kernel<false, 1, false>, b) && tile_attr(tile_kernel<false, 2, false>, b) &&
+        tile_attr(tile_kernel<false, 3, false>, b) && tile_attr(tile_kernel<false, 1, true>, b) &&
+        tile_attr(tile_kernel<false, 2, true>, b) && tile_attr(tile_kernel<false, 3, true>, b) &&
+        tile_attr(tile_kernel<true, 1, false>, b) && tile_attr(tile_kernel<true, 2, false>, b) &&
+        tile_attr(tile_kernel<true, 3, false>, b) && tile_attr(tile_kernel<true, 1, true>, b) &&
+        tile_attr(tile_kernel<true, 2, true>, b) && tile_attr(tile_kernel<true, 3, true>, b) &&
+        tile_attr(batch_tile_kernel<false, 1>, b) && tile_attr(batch_tile_kernel<false, 2>, b) &&
+        tile_attr(batch_tile_kernel<false, 3>, b) && tile_attr(batch_tile_kernel<true, 1>, b) &&
+        tile_attr(batch_tile_kernel<true, 2>, b) && tile_attr(batch_tile_kernel<true, 3>, b);
+    if (!ok) {
+        cudaGetLastError();
+        return false;
+    }
+    if (dev >= 0 && dev < 64) done[dev] = true;
+    return true;
+}
 
 long long tile_items_of(const Layout& L, int kc) {
     const dim3 g = tile_grid(L, kc);
@@ -549,6 +664,7 @@ long long tile_items_of(const Layout& L, int kc) {
 
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
                             bool reini, int stage, int q, double* vol_part, unsigned grid, cudaStream_t st) {
+    tile_prepare();  // a failure here makes the launch below fail, which the caller reports
     const size_t sm = tile_smem_bytes();
     const dim3 g(grid), block(kThreads);
 #define R3D_BT(R, S) batch_tile_kernel<R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part)
@@ -606,13 +722,14 @@ int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::
     return 0;
 }
 
-size_t tile_smem_bytes() { return (size_t)(kSlots + 3) * kSlotFloats * 4 + 16 * sizeof(uint64_t); }
+size_t tile_smem_bytes() { return (size_t)kRing * kSlotFloats * 4 + kRing * sizeof(uint64_t); }
 
 dim3 tile_grid(const Layout& L, int kc) {
     return dim3((L.nx + kTX - 1) / kTX, (L.ny + kTY - 1) / kTY, (L.nz + kc - 1) / kc);
 }
 
 int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume, cudaStream_t st) {
+    tile_prepare();  // a failure here makes the launch below fail, which the caller reports
     const dim3 grid = tile_grid(a.L, a.kc), block(kThreads);
     const size_t sm = tile_smem_bytes();
 #define R3D_TL(R, S, V) tile_kernel<R, S, V><<<grid, block, sm, st>>>(map, a)

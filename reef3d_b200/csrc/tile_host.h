@@ -42,6 +42,11 @@ struct TiledMember {
 // plane boxes the tile kernels load.  Returns 0 on success.
 int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::string* why);
 int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume, cudaStream_t st);
+// Sets the tiled kernels' shared-memory attributes on the current device
+// (once per device); false when the device refuses them.
+bool tile_prepare();
+// CTAs per SM the stage kernels are built to co-reside (persistent grids)
+int tile_ctas_per_sm(bool reini);
 long long tile_items_of(const Layout& L, int kc);
 // Batched persistent tiled stage over the items of nm tiled members.
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
