@@ -118,6 +118,63 @@ __global__ void __launch_bounds__(256) vmax_kernel(Layout L, const T* __restrict
     }
 }
 
+// FP32 fields: the same face maxima over float4 chunks of the rows.  |x| of
+// a float compared as its bit pattern with the sign cleared is exact, and the
+// largest magnitude converted to double equals the maximum of the converted
+// magnitudes, so the result is the one vmax_kernel<float> gives.  Rows start
+// 16-byte aligned; a chunk past the last cell reads the row's padding, which
+// the masks discard.
+__global__ void __launch_bounds__(256) vmax_f32_kernel(Layout L, const float* __restrict__ u,
+                                                       const float* __restrict__ v, const float* __restrict__ w,
+                                                       unsigned long long* out) {
+    const int nq = (L.nx + 3) >> 2;
+    const long long items = (long long)L.ny * L.nz * nq;
+    unsigned mu = 0u, mv = 0u, mw = 0u;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < items;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(t % nq);
+        const long long r = t / nq;
+        const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+        const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + L.gx + 4 * q;
+        const float4 a = __ldg(reinterpret_cast<const float4*>(u + c));
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (4 * q + e < L.nx - 1) mu = max(mu, __float_as_uint(av[e]) & 0x7fffffffu);
+        if (j < L.ny - 1) {
+            const float4 b = __ldg(reinterpret_cast<const float4*>(v + c));
+            const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (4 * q + e < L.nx) mv = max(mv, __float_as_uint(bv[e]) & 0x7fffffffu);
+        }
+        if (k < L.nz - 1) {
+            const float4 d = __ldg(reinterpret_cast<const float4*>(w + c));
+            const float dv[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (4 * q + e < L.nx) mw = max(mw, __float_as_uint(dv[e]) & 0x7fffffffu);
+        }
+    }
+    mu = __reduce_max_sync(0xffffffffu, mu);
+    mv = __reduce_max_sync(0xffffffffu, mv);
+    mw = __reduce_max_sync(0xffffffffu, mw);
+    __shared__ unsigned s[3][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { s[0][warp] = mu; s[1][warp] = mv; s[2][warp] = mw; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+            mu = max(mu, s[0][q]);
+            mv = max(mv, s[1][q]);
+            mw = max(mw, s[2][q]);
+        }
+        atomicMax(out + 0, (unsigned long long)__double_as_longlong((double)__uint_as_float(mu)));
+        atomicMax(out + 1, (unsigned long long)__double_as_longlong((double)__uint_as_float(mv)));
+        atomicMax(out + 2, (unsigned long long)__double_as_longlong((double)__uint_as_float(mw)));
+    }
+}
+
 // dt = N47 * MIN(1e10, 2/(sqrt(umax^2+vmax^2+wmax^2)/dx + sqrt(0/dx)))
 // (src/ietimestep.cpp:160-188 with maxF=maxG=maxH=0, evaluated at the
 // smallest cell length, where the reference's minimum over cells sits).
@@ -483,10 +540,12 @@ int launch_cfl(const Layout& L, const void* u, const void* v, const void* w, boo
     cudaMemsetAsync(s.vmax, 0, 3 * sizeof(unsigned long long), st);
     const long long rows = (long long)L.ny * L.nz;
     const dim3 grid((unsigned)(rows < 1184 ? rows : 1184)), block(256);
-    if (fp32)
-        vmax_kernel<float><<<grid, block, 0, st>>>(L, static_cast<const float*>(u), static_cast<const float*>(v),
-                                                   static_cast<const float*>(w), s.vmax);
-    else
+    if (fp32) {
+        const long long items = rows * ((L.nx + 3) / 4);
+        const long long blocks = (items + 255) / 256;
+        vmax_f32_kernel<<<(unsigned)(blocks < 148 * 8 ? blocks : 148 * 8), 256, 0, st>>>(
+            L, static_cast<const float*>(u), static_cast<const float*>(v), static_cast<const float*>(w), s.vmax);
+    } else
         vmax_kernel<double><<<grid, block, 0, st>>>(L, static_cast<const double*>(u), static_cast<const double*>(v),
                                                     static_cast<const double*>(w), s.vmax);
     dt_kernel<<<1, 1, 0, st>>>(s.vmax, s.vscale, dxmin, n47, s.dt);

@@ -209,16 +209,23 @@ __device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, co
 // mbarriers are initialised at the start of the item and invalidated at its
 // end, so a persistent CTA can run items back to back.
 //
-// Shared memory is a ring of kRing plane boxes holding planes k-3 .. k+12
-// while plane k is computed: the x and y stencils come from plane k's box,
-// the z stencil from the thread's own column in the seven boxes k-3..k+3.
-// After plane k the box of plane k-3 is refilled with plane k+13.
+// Shared memory is a ring of kRing plane boxes: the x and y stencils of
+// plane k come from its box, the z stencil from the thread's own column in
+// the seven boxes k-3..k+3.  Each box has a "full" mbarrier (the TMA copy
+// landed).  After plane k the box of plane k-3 is refilled with plane k+13:
+// in the convection stages after a CTA barrier, in the reinitialisation
+// stages by the last warp to count itself out of the box (a per-box release
+// counter), so that warps there drift apart where their work differs
+// (interface-band cells in FP64) instead of meeting at a barrier every plane.
 template <bool REINI, int STAGE>
 __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArgs& a, int bx, int by, int bz,
                                           bool volume, unsigned char* smem_raw, double* red_a, double* red_b,
                                           double* partial_out) {
     float* ring = reinterpret_cast<float*>(smem_raw);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(ring + kRing * kSlotFloats);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ring + kRing * kSlotFloats);  // full
+    int* rel = reinterpret_cast<int*>(bar + kRing);                           // release counters
+    volatile int* s_abort = rel + kRing;
+    int* s_issued = rel + kRing + 1;                                          // last plane issued
 
     const Layout& L = a.L;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -241,15 +248,18 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     const bool gylo = act0 && j == 0, gyhi = act0 && j == L.ny - 1;
     const bool gside = gxlo || gxhi2 || gxhi1 || gylo || gyhi;
 
-    int issued = pfirst - 1;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kRing; ++s) mbar_init(bar + s, 1);
+        for (int s = 0; s < kRing; ++s) {
+            mbar_init(bar + s, 1);
+            rel[s] = 0;
+        }
+        *s_abort = 0;
         mbar_fence_init();
         for (int p = pfirst; p <= min(pfirst + kRing - 1, plast); ++p) {
             const int s = p - pfirst;
             mbar_expect_tx(bar + s, kBoxBytes);
             tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, p + L.gz);
-            issued = p;
+            *s_issued = p;
         }
     }
     __syncthreads();
@@ -258,6 +268,8 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     bool ok = true;
 #pragma unroll
     for (int m = 0; m < 6; ++m) ok = ok && mbar_wait_bounded(bar + m, 0);
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok) *s_abort = 1;
 
     const float vs = (float)*a.vscale;
     const float dtc = REINI ? a.dtr : (float)*a.dt;
@@ -292,12 +304,15 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     };
     fetch(c);
 
-    bool aborted = __syncthreads_or(!ok);
-    for (int k = k0; k < k1 && !aborted; ++k, c += L.sz) {
+    for (int k = k0; k < k1; ++k, c += L.sz) {
         const int n = k - k0;  // ring position of plane k-3
         {
             const int nt = n + 6;  // plane k+3
-            ok = mbar_wait_bounded(bar + (nt & (kRing - 1)), (nt / kRing) & 1);
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + (nt & (kRing - 1)), (nt / kRing) & 1));
+        }
+        if (REINI) {
+            if (!ok) *s_abort = 1;
+            if (__any_sync(0xffffffffu, *s_abort != 0)) break;
         }
         const float* sl = ring + ((n + 3) & (kRing - 1)) * kSlotFloats;  // plane k
 
@@ -423,6 +438,26 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             }
         }
 
+        // reinitialisation: the warp's shared-memory reads of this plane are
+        // done, so it counts itself out of the box of plane k-3 (before its
+        // global stores and loads, so the fence waits on nothing in flight),
+        // and the last warp out refills the box with plane k+13
+        if (REINI) __syncwarp();
+        if (REINI && tx == 0) {
+            const int s = n & (kRing - 1);
+            __threadfence_block();
+            if (atomicAdd(rel + s, 1) == kThreads / 32 - 1) {
+                __threadfence_block();
+                rel[s] = 0;
+                if (k + kRing - 3 <= plast) {
+                    fence_proxy_async();
+                    mbar_expect_tx(bar + s, kBoxBytes);
+                    tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, k + kRing - 3 + L.gz);
+                    atomicMax(s_issued, k + kRing - 3);
+                }
+            }
+        }
+
         // RK combine (src/levelset_RK3.cpp:121-156, src/reini_RK3.cpp:118-135)
         float2 val;
         const float2 sdl = fma2(f2(dtc), Lc, f0);  // stage input + dt L
@@ -471,23 +506,30 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
         }
 
         if (k + 1 < k1) fetch(c + L.sz);
-        // every thread is done with the box of plane k-3: refill it with k+13
-        aborted = __syncthreads_or(!ok);
-        if (!aborted && threadIdx.x == 0 && k + kRing - 3 <= plast) {
-            const int pn = k + kRing - 3;
-            const int s = n & (kRing - 1);
-            fence_proxy_async();
-            mbar_expect_tx(bar + s, kBoxBytes);
-            tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, pn + L.gz);
-            issued = pn;
+        if (!REINI) {
+            // convection (the same work in every warp): one CTA barrier per
+            // plane, after which thread 0 refills the box of plane k-3
+            if (__syncthreads_or(!ok || *s_abort != 0)) {
+                if (threadIdx.x == 0) *s_abort = 1;
+                break;
+            }
+            if (threadIdx.x == 0 && k + kRing - 3 <= plast) {
+                const int s = n & (kRing - 1);
+                fence_proxy_async();
+                mbar_expect_tx(bar + s, kBoxBytes);
+                tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, k + kRing - 3 + L.gz);
+                *s_issued = k + kRing - 3;
+            }
         }
     }
+    __syncthreads();
+    const bool aborted = *s_abort != 0;
 
     if (aborted) {
         if (threadIdx.x == 0) {
             atomicExch(a.err, 1);
             // wait (bounded) for every copy still in flight before leaving
-            for (int p = pfirst; p <= issued; ++p) {
+            for (int p = pfirst; p <= *s_issued; ++p) {
                 const int q = p - pfirst;
                 mbar_wait_bounded(bar + (q & (kRing - 1)), (q / kRing) & 1);
             }
@@ -722,7 +764,9 @@ int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::
     return 0;
 }
 
-size_t tile_smem_bytes() { return (size_t)kRing * kSlotFloats * 4 + kRing * sizeof(uint64_t); }
+size_t tile_smem_bytes() {
+    return (size_t)kRing * kSlotFloats * 4 + kRing * sizeof(uint64_t) + (kRing + 2) * sizeof(int);
+}
 
 dim3 tile_grid(const Layout& L, int kc) {
     return dim3((L.nx + kTX - 1) / kTX, (L.ny + kTY - 1) / kTY, (L.nz + kc - 1) / kc);

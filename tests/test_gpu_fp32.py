@@ -128,3 +128,18 @@ def test_tiled_volume_and_band64_switch():
             assert abs(fused[0] - direct[0]) <= 1e-9 * abs(direct[0])
             vols[band] = direct[0]
     assert abs(vols[1] - vols[0]) <= 1e-4 * abs(vols[0])
+
+
+@pytest.mark.parametrize("dims", [(40, 33, 27), (61, 1, 45), (37, 22, 19)])
+def test_cfl_dt_exact_on_fp32_velocities(port_lib, dims):
+    """The FP32 form's CFL step equals the reference formula evaluated on the
+    stored (FP32-rounded) velocities: the face maxima are exact."""
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=5)
+    u, v, w = (np.ascontiguousarray(a.astype(np.float32).astype(np.float64)) for a in (u, v, w))
+    flags = dict(f43=0.5, f44=2, f45=2.1, f49=1, n47=0.125)
+    o = port_lib(nx, ny, nz, xn, yn, zn, **flags)
+    with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=r3d.FP32, **flags) as ls:
+        for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+            ls.upload(f, a)
+        assert ls.cfl_dt() == o.cfl_dt(u, v, w)
