@@ -23,6 +23,10 @@ struct r3d_batch {
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
+    // the cell-kernel members run beside the tiled ones on this stream,
+    // forked from and joined back into `stream` by the two events
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::vector<r3d_handle*> members;
     // device state, rebuilt when the membership or the configuration changes
     MemberDesc* d_members = nullptr;
@@ -206,26 +210,53 @@ BatchLaunch cell_launch_of(const r3d_batch* b) {
     return l;
 }
 
-unsigned tiled_grid(const r3d_batch* b, bool reini) {
-    const long long want = (long long)tile_ctas_per_sm(reini) * b->sms;  // the co-resident CTAs
+unsigned tiled_grid(const r3d_batch* b) {
+    const long long want = (long long)batch_tile_ctas_per_sm() * b->sms;  // the co-resident CTAs
     return (unsigned)std::max<long long>(1, std::min<long long>(want, b->t_tiled));
 }
 
+// Enqueues the tiled members' launch on the batch stream and the cell-kernel
+// members' launch on the side stream, so the two (independent) groups run at
+// the same time; the side stream forks from and joins back into the batch
+// stream (also inside a graph capture).
+template <typename T, typename C>
+long long fork_join(r3d_batch* b, T tiled, C cells) {
+    const bool has_t = b->n_tiled > 0, has_c = (size_t)b->n_tiled < b->members.size();
+    if (has_t && has_c) {
+        cudaEventRecord(b->fork, b->stream);
+        cudaStreamWaitEvent(b->side, b->fork, 0);
+        const long long n = cells(b->side) + tiled(b->stream);
+        cudaEventRecord(b->join, b->side);
+        cudaStreamWaitEvent(b->stream, b->join, 0);
+        return n;
+    }
+    return (has_t ? tiled(b->stream) : 0) + (has_c ? cells(b->stream) : 0);
+}
+
 long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
-    long long n = 0;
-    if (b->n_tiled)
-        n += launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, reini, s, q, b->d_vol,
-                                     tiled_grid(b, reini), b->stream);
-    if ((size_t)b->n_tiled < b->members.size())
-        n += launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, b->stream);
-    return n;
+    return fork_join(
+        b,
+        [&](cudaStream_t st) {
+            return (long long)launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, reini, s, q,
+                                                      b->d_vol, tiled_grid(b), st);
+        },
+        [&](cudaStream_t st) { return (long long)launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, st); });
+}
+
+long long enqueue_vmax(r3d_batch* b) {
+    return fork_join(
+        b,
+        [&](cudaStream_t st) {
+            return (long long)launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax,
+                                                     tiled_grid(b), st);
+        },
+        [&](cudaStream_t st) { return (long long)launch_batch_vmax(cell_launch_of(b), st); });
 }
 
 // CFL, 3 convection stages, max(f44) reinit pseudo-steps, volume + clock.
 long long enqueue_batch_step(r3d_batch* b) {
     long long n = 0;
-    if (b->n_tiled) n += launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b, false), b->stream);
-    if ((size_t)b->n_tiled < b->members.size()) n += launch_batch_vmax(cell_launch_of(b), b->stream);
+    n += enqueue_vmax(b);
     n += launch_batch_dt(launch_of(b), b->stream);
     for (int s = 1; s <= 3; ++s) n += enqueue_stage(b, false, s, 0);
     for (int q = 0; q < b->max_f44; ++q)
@@ -294,8 +325,15 @@ int r3d_batch_create(r3d_batch** out) {
     if (!b) return bfail(nullptr, R3D_ENOMEM, "host allocation failed");
     cudaGetDevice(&b->device);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
+        if (b->join) cudaEventDestroy(b->join);
+        if (b->fork) cudaEventDestroy(b->fork);
+        if (b->side) cudaStreamDestroy(b->side);
+        if (b->stream) cudaStreamDestroy(b->stream);
         delete b;
         return bfail(nullptr, R3D_EDEVICE, "stream creation failed");
     }
@@ -314,6 +352,10 @@ int r3d_batch_destroy(r3d_batch* b) {
     if (b->d_vmax) cudaFree(b->d_vmax);
     if (b->d_tiled) cudaFree(b->d_tiled);
     if (b->d_maps) cudaFree(b->d_maps);
+    cudaStreamSynchronize(b->side);
+    cudaEventDestroy(b->join);
+    cudaEventDestroy(b->fork);
+    cudaStreamDestroy(b->side);
     cudaStreamDestroy(b->stream);
     delete b;
     return R3D_OK;
@@ -406,8 +448,7 @@ int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows_out, int*
     b->rows = 4;
     b->ctas_per_sm = 8;
     if (int rc = rebuild(b)) return rc;
-    if (b->n_tiled) launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax, tiled_grid(b, false), b->stream);
-    if ((size_t)b->n_tiled < b->members.size()) launch_batch_vmax(cell_launch_of(b), b->stream);
+    enqueue_vmax(b);
     launch_batch_dt(launch_of(b), b->stream);
     for (int r : cand_rows)
         for (int c : cand_ctas) {

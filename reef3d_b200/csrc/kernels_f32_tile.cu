@@ -39,6 +39,10 @@ constexpr long long kSpin = 1ll << 22;
 #ifndef R3D_TILE_MINB_REINI
 #define R3D_TILE_MINB_REINI 3
 #endif
+// the batched persistent form (its per-item arguments sit in shared memory)
+#ifndef R3D_TILE_MINB_BATCH
+#define R3D_TILE_MINB_BATCH 3
+#endif
 
 // ------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -572,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TI
 // member).  Reinitialisation pseudo-step q is skipped by members with
 // f44 <= q; the last stage of a member's step adds its volume partials.
 template <bool REINI, int STAGE>
-__global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV) batch_tile_kernel(const TiledMember* __restrict__ members,
+__global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kernel(const TiledMember* __restrict__ members,
                                                                  const CUtensorMap* __restrict__ maps,
                                                                  const long long* __restrict__ tile0, int nm,
                                                                  int q, double* __restrict__ vol_part) {
@@ -617,7 +621,7 @@ __global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TI
 __global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMember* __restrict__ members,
                                                                    const long long* __restrict__ tile0, int nm,
                                                                    double* __restrict__ vmax_part) {
-    __shared__ double s[3][kThreads / 32];
+    __shared__ unsigned s[3][kThreads / 32];
     const long long nt = tile0[nm];
     for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
         int lo = 0, hi = nm - 1;
@@ -633,30 +637,41 @@ __global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMe
         const int bx = (int)(lt % ntx), by = (int)((lt / ntx) % nty), bz = (int)(lt / ((long long)ntx * nty));
         const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
         const int j = by * kTY + ty;
+        const int i0 = bx * kTX + 2 * tx;
         const int k0 = bz * a.kc, k1 = min(k0 + a.kc, L.nz);
-        double mu = 0.0, mv = 0.0, mw = 0.0;
-        if (j < L.ny)
-            for (int k = k0; k < k1; ++k)
-                for (int e = 0; e < 2; ++e) {
-                    const int i = bx * kTX + 2 * tx + e;
-                    if (i >= L.nx) continue;
-                    const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
-                    if (i < L.nx - 1) mu = fmax(mu, fabs((double)a.u[c]));
-                    if (j < L.ny - 1) mv = fmax(mv, fabs((double)a.v[c]));
-                    if (k < L.nz - 1) mw = fmax(mw, fabs((double)a.w[c]));
+        // |x| compared as the float's bit pattern with the sign cleared (exact)
+        unsigned mu = 0u, mv = 0u, mw = 0u;
+        if (j < L.ny && i0 < L.nx) {
+            const bool two = i0 + 1 < L.nx;
+            const long long col = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
+            for (int k = k0; k < k1; ++k) {
+                const long long c = (long long)(k + L.gz) * L.sz + col;
+                float2 fu, fv, fw;
+                if (two) {
+                    fu = __ldg(reinterpret_cast<const float2*>(a.u + c));
+                    fv = __ldg(reinterpret_cast<const float2*>(a.v + c));
+                    fw = __ldg(reinterpret_cast<const float2*>(a.w + c));
+                } else {
+                    fu = make_float2(__ldg(a.u + c), 0.f);
+                    fv = make_float2(__ldg(a.v + c), 0.f);
+                    fw = make_float2(__ldg(a.w + c), 0.f);
                 }
-        for (int o = 16; o > 0; o >>= 1) {
-            mu = fmax(mu, __shfl_down_sync(0xffffffffu, mu, o));
-            mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
-            mw = fmax(mw, __shfl_down_sync(0xffffffffu, mw, o));
+                if (i0 < L.nx - 1) mu = max(mu, __float_as_uint(fu.x) & 0x7fffffffu);
+                if (i0 + 1 < L.nx - 1) mu = max(mu, __float_as_uint(fu.y) & 0x7fffffffu);
+                if (j < L.ny - 1) mv = max(mv, max(__float_as_uint(fv.x) & 0x7fffffffu, __float_as_uint(fv.y) & 0x7fffffffu));
+                if (k < L.nz - 1) mw = max(mw, max(__float_as_uint(fw.x) & 0x7fffffffu, __float_as_uint(fw.y) & 0x7fffffffu));
+            }
         }
+        mu = __reduce_max_sync(0xffffffffu, mu);
+        mv = __reduce_max_sync(0xffffffffu, mv);
+        mw = __reduce_max_sync(0xffffffffu, mw);
         if (tx == 0) { s[0][ty] = mu; s[1][ty] = mv; s[2][ty] = mw; }
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int q = 1; q < kThreads / 32; ++q) { mu = fmax(mu, s[0][q]); mv = fmax(mv, s[1][q]); mw = fmax(mw, s[2][q]); }
-            vmax_part[3 * t] = mu;
-            vmax_part[3 * t + 1] = mv;
-            vmax_part[3 * t + 2] = mw;
+            for (int q = 1; q < kThreads / 32; ++q) { mu = max(mu, s[0][q]); mv = max(mv, s[1][q]); mw = max(mw, s[2][q]); }
+            vmax_part[3 * t] = (double)__uint_as_float(mu);
+            vmax_part[3 * t + 1] = (double)__uint_as_float(mv);
+            vmax_part[3 * t + 2] = (double)__uint_as_float(mw);
         }
         __syncthreads();
     }
@@ -673,6 +688,7 @@ bool tile_attr(K kernel, int bytes) {
 }  // namespace
 
 int tile_ctas_per_sm(bool reini) { return reini ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV; }
+int batch_tile_ctas_per_sm() { return R3D_TILE_MINB_BATCH; }
 
 // Sets the attributes of every instantiation once per device.
 bool tile_prepare() {

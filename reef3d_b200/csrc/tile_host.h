@@ -47,6 +47,7 @@ int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int
 bool tile_prepare();
 // CTAs per SM the stage kernels are built to co-reside (persistent grids)
 int tile_ctas_per_sm(bool reini);
+int batch_tile_ctas_per_sm();
 long long tile_items_of(const Layout& L, int kc);
 // Batched persistent tiled stage over the items of nm tiled members.
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
