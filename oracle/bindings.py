@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libreef3d_ref.so")
 REF_LIB_FAST = os.path.join(HERE, "_ref", "fast", "libreef3d_ref.so")
+ADAPTER_LIB = os.path.join(HERE, "_ref", "libreef3d_adapter.so")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.c_int
@@ -165,10 +166,15 @@ class RefOracle:
     def available(cls):
         return os.path.exists(REF_LIB)
 
-    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10):
-        if RefOracle._lib is not None:
+    _loaded = set()
+
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10,
+                 path=None):
+        path = path or (REF_LIB_FAST if fast else REF_LIB)
+        if path in RefOracle._loaded:
             raise RuntimeError("the reference oracle holds one grid per process")
-        lib = ctypes.CDLL(REF_LIB_FAST if fast else REF_LIB)
+        RefOracle._loaded.add(path)
+        lib = ctypes.CDLL(path)
         lib.refls_set_picard.argtypes = [_I, _I]
         lib.refls_set_picard(f46, f47)
         lib.refls_init.argtypes = [_I, _I, _I, _D, _D, _D, _I, ctypes.c_double, ctypes.c_double, _I]
@@ -186,7 +192,6 @@ class RefOracle:
         lib.refls_ghost_fill.argtypes = [_D]
         lib.refls_cfl_dt.restype = ctypes.c_double
         lib.refls_cfl_dt.argtypes = [ctypes.c_double]
-        RefOracle._lib = lib
         self._lib = lib
         self.nx, self.ny, self.nz = nx, ny, nz
         self.shape = padded_shape(nx, ny, nz)
@@ -264,3 +269,52 @@ class RefOracle:
     def volume(self):
         self._lib.refls_update()
         return self._lib.refls_volume1(), self._lib.refls_volume2()
+
+
+class AdapterOracle(RefOracle):
+    """The reference's own objects plus the REEF3D-side adapter classes
+    (``reef3d_b200/adapters/reef3d_b200_adapters.h``) compiled into
+    ``oracle/_ref/libreef3d_adapter.so`` against the reference's headers.
+    The ``refls_*`` calls run the reference on the CPU, the ``gpu_*`` calls
+    run the adapters (and through them libreef3d_b200.so) on the same REEF3D
+    lexer/fdm/ghostcell objects.  One grid per process; needs a GPU."""
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(ADAPTER_LIB)
+
+    def __init__(self, *args, precision=0, resident=False, **kw):
+        super().__init__(*args, path=ADAPTER_LIB, **kw)
+        lib = self._lib
+        lib.refad_weno_L.argtypes = [_D, _D]
+        lib.refad_reinidisc_L.argtypes = [_D, _D]
+        lib.refad_create.argtypes = [_I, _I]
+        if lib.refad_create(precision, 1 if resident else 0) != 0:
+            raise RuntimeError("refad_create failed")
+
+    def gpu_step(self, dt):
+        """freesurface::start of levelset_RK3_gpu on a->phi."""
+        self._lib.refls_set_dt(dt)
+        self._lib.refad_step()
+        return self.get_field(0)
+
+    def gpu_update(self):
+        self._lib.refad_update()
+        return self._lib.refls_volume1(), self._lib.refls_volume2()
+
+    def gpu_weno_L(self, phi):
+        L = self.zeros()
+        self._lib.refad_weno_L(_dp(np.ascontiguousarray(phi)), _dp(L))
+        return L
+
+    def gpu_reinidisc_L(self, phi):
+        L = self.zeros()
+        self._lib.refad_reinidisc_L(_dp(np.ascontiguousarray(phi)), _dp(L))
+        return L
+
+    def gpu_reini(self):
+        self._lib.refad_reini()
+        return self.get_field(0)
+
+    def close(self):
+        self._lib.refad_destroy()

@@ -81,6 +81,15 @@ int ijk(int i, int j, int k) {
 
 }  // namespace
 
+// The harness's objects, for oracle/ref_adapter.cpp (the adapter test).
+namespace refh {
+lexer* lex() { return P; }
+fdm* fd() { return A; }
+ghostcell* gc() { return PGC; }
+ioflow* flow() { return FLOW; }
+field4* tmp() { return TMP; }
+}  // namespace refh
+
 extern "C" {
 
 // Picard mass correction of the next refls_init: f46 = 1 (in reini_RK3,

@@ -1,0 +1,251 @@
+// REEF3D-side adapter classes for the B200 level-set library.
+//
+// These are the classes a REEF3D maintainer adds to REEF3D's source tree to
+// run the level-set path on the GPU through include/reef3d_b200.h.  Each one
+// derives from the REEF3D interface it replaces and keeps that interface's
+// contract; the file compiles only inside a REEF3D build (it includes
+// REEF3D's headers) and links against libreef3d_b200.so:
+//
+//   levelset_RK3_gpu : freesurface   replaces levelset_RK3 (src/levelset_RK3.h)
+//   weno_hj_gpu      : convection    replaces weno_hj_df_nug (src/weno_hj_df_nug.h)
+//   reinidisc_gpu    : reinidisc     replaces reinidisc_f / reinidisc_fsf
+//   reini_RK3_gpu    : reini         replaces reini_RK3 (src/reini_RK3.h)
+//
+// Fields cross the boundary in REEF3D's own layout (field_base::V,
+// R3D_LAYOUT_REEF3D).  Errors: the library returns a status, the adapters
+// print r3d_last_error and stop the run with exit(1), as REEF3D does on a
+// fatal error.
+#pragma once
+
+#include <cstdlib>
+#include <iostream>
+#include <vector>
+
+#include "convection.h"
+#include "fdm.h"
+#include "field.h"
+#include "freesurface.h"
+#include "ghostcell.h"
+#include "lexer.h"
+#include "reef3d_b200.h"
+#include "reini.h"
+#include "reinidisc.h"
+
+namespace r3d_adapter {
+
+inline void check(r3d_handle* h, int rc) {
+    if (rc != R3D_OK) {
+        std::cout << "reef3d_b200: " << r3d_last_error(h) << std::endl;
+        std::exit(1);
+    }
+}
+
+// One device instance for the grid and control flags of a REEF3D run: the
+// node coordinates DIVEMesh wrote (p->XN etc., node indices -5..n+5) and the
+// level-set flags of the control file.  precision: R3D_FP64 (the reference's
+// arithmetic) or R3D_FP32 (the FP32 form).
+inline r3d_handle* make_handle(lexer* p, int precision) {
+    r3d_grid_desc d{};
+    d.nx = p->knox;
+    d.ny = p->knoy;
+    d.nz = p->knoz;
+    d.xn = p->XN;
+    d.yn = p->YN;
+    d.zn = p->ZN;
+    d.f43 = p->F43;
+    d.f44 = p->F44;
+    d.f45 = p->F45;
+    d.f49 = p->F49;
+    d.n47 = p->N47;
+    d.precision = precision;
+    d.f46 = p->F46;
+    d.f47 = p->F47;
+    r3d_handle* h = nullptr;
+    check(nullptr, r3d_create(&d, &h));
+    return h;
+}
+
+// Interior cell (i,j,k) of a REEF3D field array (src/field_base.h:47).
+inline long ijk(const lexer* p, int i, int j, int k) {
+    return (long)(i - p->imin) * p->jmax * p->kmax + (long)(j - p->jmin) * p->kmax + (k - p->kmin);
+}
+
+// Copies the cells the device owns -- the interior, plus the face ghost
+// layers when `faces` (a 2D grid has no y ghost planes on the device) --
+// from a full REEF3D-layout array into a field; every other cell of the
+// field keeps its value, as it would under the reference object.
+inline void copy_owned(const lexer* p, const std::vector<double>& src, field& f, bool faces) {
+    const int nx = p->knox, ny = p->knoy, nz = p->knoz;
+    const int gy = ny == 1 ? 0 : 3;
+    for (int i = -3; i < nx + 3; ++i)
+        for (int j = -gy; j < ny + gy; ++j)
+            for (int k = -3; k < nz + 3; ++k) {
+                const int outside = (i < 0 || i >= nx) + (j < 0 || j >= ny) + (k < 0 || k >= nz);
+                if (outside > (faces ? 1 : 0)) continue;
+                const long c = ijk(p, i, j, k);
+                f.V[c] = src[c];
+            }
+}
+
+inline void download_owned(r3d_handle* h, int id, const lexer* p, field& f, bool faces,
+                           std::vector<double>& buf) {
+    buf.resize((size_t)p->imax * p->jmax * p->kmax);
+    check(h, r3d_download(h, id, buf.data(), R3D_LAYOUT_REEF3D));
+    copy_owned(p, buf, f, faces);
+}
+
+// Ghost-cell type of the level set for ghostcell::start4, chosen from F50
+// as levelset_RK3 and reini_RK3 choose it (src/levelset_RK3.cpp:50-60,
+// src/reini_RK3.cpp:35-62).
+inline int gcval_phi(const lexer* p) { return 50 + (p->F50 >= 1 && p->F50 <= 4 ? p->F50 : 0); }
+inline int gcval_iniphi(const lexer* p) {
+    int g = 50;
+    if ((p->F61 > 1.0e-20 || p->F60 > 1.0e-20) && p->F50 == 1) g = 51;
+    if ((p->F62 > 1.0e-20 || p->F60 > 1.0e-20) && p->F50 == 2) g = 52;
+    if (((p->F61 > 1.0e-20 && p->F62 > 1.0e-20) || p->F60 > 1.0e-20) && p->F50 == 3) g = 53;
+    return g;
+}
+
+}  // namespace r3d_adapter
+
+// The device writes the interior and the face ghost layers of every field it
+// returns; the adapters then run REEF3D's own ghostcell::start4 on the host
+// copy, which also fills the edge and corner ghosts (dgcpol4) and, in a
+// multi-rank run, exchanges the halo.  (The device step itself knows walls
+// only: a REEF3D run split over several MPI ranks needs one device instance
+// per rank and a halo exchange per stage, which this library does not do.)
+
+// freesurface: one level-set step on the device (three WENO5-HJ convection
+// RK stages with the wall ghost fill, F44 reinitialisation pseudo-steps, the
+// picard correction the control file selects, the volume integral and the
+// density/viscosity update), src/levelset_RK3.cpp:103-178.  The level set
+// goes up at every call unless `resident` is set, in which case it stays on
+// the device after the first call (for runs where only this object writes
+// a->phi); the velocities go up at every call because the momentum solver
+// owns them on the host.  a->phi, a->ro, a->visc and p->volume1/2 come back.
+class levelset_RK3_gpu final : public freesurface {
+public:
+    levelset_RK3_gpu(lexer* p, fdm*, ghostcell*, int precision = R3D_FP64, bool resident = false)
+        : h(r3d_adapter::make_handle(p, precision)), resident(resident) {
+        r3d_adapter::check(h, r3d_set_fluid(h, p->W1, p->W2, p->W3, p->W4));
+    }
+    ~levelset_RK3_gpu() { r3d_destroy(h); }
+
+    void start(fdm* a, lexer* p, convection*, solver*, ghostcell* pgc, ioflow*, reini*, particle_corr*,
+               field& ls) override {
+        using r3d_adapter::check;
+        if (!resident || first) check(h, r3d_upload(h, R3D_PHI, ls.V, R3D_LAYOUT_REEF3D));
+        first = false;
+        check(h, r3d_upload(h, R3D_U, a->u.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_upload(h, R3D_V, a->v.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_upload(h, R3D_W, a->w.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_ls_step(h, p->dt));
+        r3d_adapter::download_owned(h, R3D_PHI, p, ls, true, buf);
+        r3d_adapter::download_owned(h, R3D_RO, p, a->ro, true, buf);
+        r3d_adapter::download_owned(h, R3D_VISC, p, a->visc, true, buf);
+        check(h, r3d_last_volume(h, &p->volume1, &p->volume2));
+        // the reference fills the ghosts of ls in the last reinitialisation
+        // stage; a picard correction after it moves the interior only
+        if (p->F46 == 0) pgc->start4(p, ls, r3d_adapter::gcval_phi(p));
+        pgc->start4(p, a->ro, 1);  // gcval_ro of fluid_update_fsf
+        pgc->start4(p, a->visc, 1);
+    }
+
+    // levelset_RK3::update: the density/viscosity update on a->phi
+    // (src/levelset_RK3.cpp:180-183).
+    void update(lexer* p, fdm* a, ghostcell* pgc, field&) override {
+        using r3d_adapter::check;
+        check(h, r3d_upload(h, R3D_PHI, a->phi.V, R3D_LAYOUT_REEF3D));
+        first = false;
+        check(h, r3d_fluid_update(h, &p->volume1, &p->volume2));
+        r3d_adapter::download_owned(h, R3D_RO, p, a->ro, true, buf);
+        r3d_adapter::download_owned(h, R3D_VISC, p, a->visc, true, buf);
+        pgc->start4(p, a->ro, 1);
+        pgc->start4(p, a->visc, 1);
+    }
+
+    r3d_handle* handle() { return h; }
+
+private:
+    r3d_handle* h;
+    bool resident;
+    bool first = true;
+    std::vector<double> buf;
+};
+
+// convection: the WENO5-HJ operator of the level set (ipol 4), accumulated
+// into a->L over the LOOP cells as weno_hj_df_nug::start does
+// (src/weno_hj_df_nug.cpp:58-110).
+class weno_hj_gpu final : public convection {
+public:
+    explicit weno_hj_gpu(lexer* p, int precision = R3D_FP64)
+        : h(r3d_adapter::make_handle(p, precision)), buf((size_t)p->imax * p->jmax * p->kmax) {}
+    ~weno_hj_gpu() { r3d_destroy(h); }
+
+    void start(lexer* p, fdm* a, field& f, int ipol, field& u, field& v, field& w) override {
+        using r3d_adapter::check;
+        if (ipol != 4) {
+            std::cout << "weno_hj_gpu: only the level set (ipol 4) is on the device" << std::endl;
+            std::exit(1);
+        }
+        check(h, r3d_upload(h, R3D_WORK1, f.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_upload(h, R3D_U, u.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_upload(h, R3D_V, v.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_upload(h, R3D_W, w.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_convection_L(h, R3D_WORK1));
+        check(h, r3d_download(h, R3D_L, buf.data(), R3D_LAYOUT_REEF3D));
+        for (int i = 0; i < p->knox; ++i)
+            for (int j = 0; j < p->knoy; ++j)
+                for (int k = 0; k < p->knoz; ++k) {
+                    const long c = r3d_adapter::ijk(p, i, j, k);
+                    if (p->flag4[c] > 0) a->L.V[c] += buf[c];
+                }
+    }
+
+private:
+    r3d_handle* h;
+    std::vector<double> buf;
+};
+
+// reinidisc: the reinitialisation right-hand side (reinidisc_f, or
+// reinidisc_fsf when F49 = 0), written to L over the interior
+// (src/reinidisc_f.cpp:37-127, src/reinidisc_fsf.cpp:37-141).
+class reinidisc_gpu final : public reinidisc {
+public:
+    explicit reinidisc_gpu(lexer* p, int precision = R3D_FP64) : h(r3d_adapter::make_handle(p, precision)) {}
+    ~reinidisc_gpu() { r3d_destroy(h); }
+
+    void start(lexer* p, fdm*, ghostcell*, field& f, field& L, int) override {
+        using r3d_adapter::check;
+        check(h, r3d_upload(h, R3D_WORK1, f.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_reinidisc_L(h, R3D_WORK1));
+        r3d_adapter::download_owned(h, R3D_L, p, L, false, buf);  // BASELOOP cells only
+    }
+
+private:
+    r3d_handle* h;
+    std::vector<double> buf;
+};
+
+// reini: the RK3 pseudo-time reinitialisation, 2 int(maxlength/(F43 DXM))
+// pseudo-steps on the first call of a run (p->count == 0) and F44 after
+// (src/reini_RK3.cpp:84-143), with the picard correction when F46 = 1.
+class reini_RK3_gpu final : public reini {
+public:
+    explicit reini_RK3_gpu(lexer* p, int precision = R3D_FP64) : h(r3d_adapter::make_handle(p, precision)) {}
+    ~reini_RK3_gpu() { r3d_destroy(h); }
+
+    void start(fdm*, lexer* p, field& f, ghostcell* pgc, ioflow*) override {
+        using r3d_adapter::check;
+        const int iters = p->count == 0 ? 2 * int(p->maxlength / (p->F43 * p->DXM)) : p->F44;
+        check(h, r3d_upload(h, R3D_PHI, f.V, R3D_LAYOUT_REEF3D));
+        check(h, r3d_reinit(h, iters));
+        r3d_adapter::download_owned(h, R3D_PHI, p, f, true, buf);
+        if (p->F46 != 1)  // (with picard the last shift leaves the ghosts as they were)
+            pgc->start4(p, f, p->count == 0 ? r3d_adapter::gcval_iniphi(p) : r3d_adapter::gcval_phi(p));
+    }
+
+private:
+    r3d_handle* h;
+    std::vector<double> buf;
+};
