@@ -64,13 +64,13 @@ def _interior(a, nx, ny, nz):
     return a[3:3 + nx, 3:3 + ny, 3:3 + nz]
 
 
-def _run(name):
+def _run(name, precision=0):
     sys.path.insert(0, ROOT)
     from oracle.bindings import AdapterOracle
     c = _case(name)
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                       f49=c["f49"], f46=c["f46"], f47=6)
+                       f49=c["f49"], f46=c["f46"], f47=6, precision=precision)
     out = {}
     ao.set_state(c["phi"], c["u"], c["v"], c["w"])
     out["weno_L"] = bool(np.array_equal(_interior(ao.weno_L(c["phi"]), nx, ny, nz),
@@ -122,3 +122,36 @@ def test_adapters_match_reference_objects(name):
     assert out["weno_L"] and out["reinidisc_L"] and out["reini"], out
     assert all(out["phi"]), out
     assert max(out["rel"]) <= 1e-12, out
+
+
+def _run_fp32(name):
+    """The free-surface adapter in the FP32 form against the reference's FP64
+    levelset_RK3 for three steps (each from the reference's state)."""
+    sys.path.insert(0, ROOT)
+    from oracle.bindings import AdapterOracle
+    c = _case(name)
+    nx, ny, nz = c["nx"], c["ny"], c["nz"]
+    ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
+                       f49=c["f49"], f46=c["f46"], f47=6, precision=1)
+    ao.set_state(c["phi"], c["u"], c["v"], c["w"])
+    phi, errs = c["phi"], []
+    for s in range(3):
+        ao.set_count(s + 1)
+        ao.set_field(0, phi)
+        dt = ao.cfl_dt(c["n47"])
+        ref = ao.step(dt)
+        ao.set_field(0, phi)
+        got = ao.gpu_step(dt)
+        errs.append(float(np.max(np.abs(_interior(got - ref, nx, ny, nz))) / np.max(np.abs(ref))))
+        phi = ref
+    ao.close()
+    return errs
+
+
+@pytest.mark.parametrize("name", ["vortex3d", "disk2d"])
+def test_fp32_adapter_within_fp32_tolerance(name):
+    """FP32 form through the same adapter: within 2e-5 relative max-norm of
+    the reference per step (the FP32 tolerance of test_gpu_fp32.py)."""
+    with mp.get_context("spawn").Pool(1) as pool:
+        errs = pool.apply(_run_fp32, (name,))
+    assert max(errs) <= 2e-5, errs
