@@ -38,6 +38,7 @@ struct r3d_batch {
     long long t_tiled = 0;            // items of the tiled members: tiles [0, t_tiled)
     double* d_vol = nullptr;
     double* d_vmax = nullptr;
+    unsigned* d_work = nullptr;       // item counters of the persistent tiled launches
     size_t cap_members = 0, cap_tiles = 0;
     long long ntiles = 0;
     int max_f44 = 0;
@@ -238,7 +239,7 @@ long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
         b,
         [&](cudaStream_t st) {
             return (long long)launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, reini, s, q,
-                                                      b->d_vol, tiled_grid(b), st);
+                                                      b->d_vol, b->d_work, tiled_grid(b), st);
         },
         [&](cudaStream_t st) { return (long long)launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, st); });
 }
@@ -325,7 +326,9 @@ int r3d_batch_create(r3d_batch** out) {
     if (!b) return bfail(nullptr, R3D_ENOMEM, "host allocation failed");
     cudaGetDevice(&b->device);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaMalloc(&b->d_work, 4 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(b->d_work, 0, 4 * sizeof(unsigned)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
@@ -334,6 +337,7 @@ int r3d_batch_create(r3d_batch** out) {
         if (b->fork) cudaEventDestroy(b->fork);
         if (b->side) cudaStreamDestroy(b->side);
         if (b->stream) cudaStreamDestroy(b->stream);
+        if (b->d_work) cudaFree(b->d_work);
         delete b;
         return bfail(nullptr, R3D_EDEVICE, "stream creation failed");
     }
@@ -357,6 +361,7 @@ int r3d_batch_destroy(r3d_batch* b) {
     cudaEventDestroy(b->fork);
     cudaStreamDestroy(b->side);
     cudaStreamDestroy(b->stream);
+    cudaFree(b->d_work);
     delete b;
     return R3D_OK;
 }

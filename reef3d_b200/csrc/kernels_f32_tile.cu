@@ -571,33 +571,44 @@ __global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TI
                             a.partial + 2 * b);
 }
 
-// Persistent batched form: CTAs walk the work items of all tiled members
+// Persistent batched form: CTAs take the work items of all tiled members
 // (member m owns items [tile0[m], tile0[m+1]); item = (bx, by, bz) of that
-// member).  Reinitialisation pseudo-step q is skipped by members with
+// member) one at a time from a global counter, so CTAs whose items hold
+// more work (FP64 interface band, wall ghosts) take fewer of them.  The
+// last CTA to leave resets the counter pair work[0..1] for the next launch
+// on the stream.  Reinitialisation pseudo-step q is skipped by members with
 // f44 <= q; the last stage of a member's step adds its volume partials.
 template <bool REINI, int STAGE>
 __global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kernel(const TiledMember* __restrict__ members,
                                                                  const CUtensorMap* __restrict__ maps,
                                                                  const long long* __restrict__ tile0, int nm,
-                                                                 int q, double* __restrict__ vol_part) {
+                                                                 int q, double* __restrict__ vol_part,
+                                                                 unsigned* __restrict__ work) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
     __shared__ TileArgs sa;
     __shared__ int s_member;
+    __shared__ long long s_t;
     const long long nt = tile0[nm];
-    for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
+    for (;;) {
         if (threadIdx.x == 0) {
-            int lo = 0, hi = nm - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (tile0[mid] <= t) lo = mid;
-                else hi = mid - 1;
+            const long long t0 = (long long)atomicAdd(work, 1u);
+            s_t = t0;
+            if (t0 < nt) {
+                int lo = 0, hi = nm - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (tile0[mid] <= t0) lo = mid;
+                    else hi = mid - 1;
+                }
+                s_member = lo;
+                sa = members[lo].args;
+                sa.out = STAGE == 1 ? members[lo].a1 : STAGE == 2 ? members[lo].a2 : members[lo].phi;
             }
-            s_member = lo;
-            sa = members[lo].args;
-            sa.out = STAGE == 1 ? members[lo].a1 : STAGE == 2 ? members[lo].a2 : members[lo].phi;
         }
         __syncthreads();
+        const long long t = s_t;
+        if (t >= nt) break;
         const int m = s_member;
         const int f44 = members[m].f44;
         if (REINI && f44 <= q) {
@@ -612,7 +623,15 @@ __global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kern
         const int bz = (int)(lt / ((long long)ntx * nty));
         if (!tile_item<REINI, STAGE>(maps + 3 * m + (STAGE - 1), sa, bx, by, bz, volume, smem_raw, red_a, red_b,
                                      vol_part + 2 * t))
-            return;
+            break;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(work + 1, 1u) == gridDim.x - 1) {
+            work[0] = 0u;
+            work[1] = 0u;
+            __threadfence();
+        }
     }
 }
 
@@ -721,11 +740,12 @@ long long tile_items_of(const Layout& L, int kc) {
 }
 
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
-                            bool reini, int stage, int q, double* vol_part, unsigned grid, cudaStream_t st) {
+                            bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
+                            cudaStream_t st) {
     tile_prepare();  // a failure here makes the launch below fail, which the caller reports
     const size_t sm = tile_smem_bytes();
     const dim3 g(grid), block(kThreads);
-#define R3D_BT(R, S) batch_tile_kernel<R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part)
+#define R3D_BT(R, S) batch_tile_kernel<R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part, work)
     if (reini) {
         if (stage == 1) R3D_BT(true, 1);
         else if (stage == 2) R3D_BT(true, 2);

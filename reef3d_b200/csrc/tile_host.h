@@ -50,8 +50,11 @@ int tile_ctas_per_sm(bool reini);
 int batch_tile_ctas_per_sm();
 long long tile_items_of(const Layout& L, int kc);
 // Batched persistent tiled stage over the items of nm tiled members.
+// work: two zero-initialised counters the launch takes items from (it leaves
+// them at zero for the next launch on the same stream).
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
-                            bool reini, int stage, int q, double* vol_part, unsigned grid, cudaStream_t st);
+                            bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
+                            cudaStream_t st);
 // Per-item face maxima of the tiled members (3 doubles per item).
 int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, double* vmax_part,
                            unsigned grid, cudaStream_t st);
