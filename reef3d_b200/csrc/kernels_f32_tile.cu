@@ -621,7 +621,10 @@ __global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kern
         const int bx = (int)(lt % ntx);
         const int by = (int)((lt / ntx) % nty);
         const int bz = (int)(lt / ((long long)ntx * nty));
-        if (!tile_item<REINI, STAGE>(maps + 3 * m + (STAGE - 1), sa, bx, by, bz, volume, smem_raw, red_a, red_b,
+        // the item's arguments in a thread-local copy: the plane loop reads
+        // them across CTA barriers, after which shared memory would be reread
+        const TileArgs a = sa;
+        if (!tile_item<REINI, STAGE>(maps + 3 * m + (STAGE - 1), a, bx, by, bz, volume, smem_raw, red_a, red_b,
                                      vol_part + 2 * t))
             break;
     }
