@@ -10,6 +10,10 @@ namespace r3d {
 namespace {
 
 constexpr int kBX = 32, kBY = 4;
+// resident blocks per SM the stage kernels are register-limited for
+#ifndef R3D_F64_MINB
+#define R3D_F64_MINB 8
+#endif
 
 struct StageArgs {
     const double* fn;   // step start value (phi^n / f): read at the cell only
@@ -94,7 +98,7 @@ __device__ __forceinline__ void heaviside_volume(const KGrid<double>& g, double 
 // Reinit stage s of src/reini_RK3.cpp:113-137: the same with the per-cell
 // pseudo time step.
 template <bool TWO_D, int STAGE, bool REINI, bool VOLUME>
-__global__ void __launch_bounds__(kBX * kBY) stage_kernel(KGrid<double> g, StageArgs a) {
+__global__ void __launch_bounds__(kBX * kBY, R3D_F64_MINB) stage_kernel(KGrid<double> g, StageArgs a) {
     int i, j, k;
     cell_of_thread(g.L, TWO_D, i, j, k);
     const bool active = i < g.L.nx && j < g.L.ny && k < g.L.nz;

@@ -32,40 +32,41 @@ __device__ __forceinline__ double weno5(const double* __restrict__ Q, const doub
     const double w3 = c2 / (eps + (c * c) * sum);
     const double Q0 = __ldg(Q + 0), Q1 = __ldg(Q + 1), Q2 = __ldg(Q + 2);
     const double Q3 = __ldg(Q + 3), Q4 = __ldg(Q + 4), Q5 = __ldg(Q + 5);
-    if (!plus)
-        return w1 * (q4 + Q0 * (q3 - q4) - Q1 * (q5 - q4))
-             + w2 * (q3 + Q2 * (q4 - q3) - Q3 * (q2 - q3))
-             + w3 * (q2 + Q4 * (q1 - q2) + Q5 * (q3 - q2));
-    return w1 * (q4 + Q0 * (q3 - q4) + Q1 * (q5 - q4))
-         + w2 * (q3 + Q2 * (q2 - q3) - Q3 * (q4 - q3))
-         + w3 * (q2 + Q4 * (q3 - q2) - Q5 * (q1 - q2));
+    // The two sides' reconstructions differ only in which differences enter
+    // and in two signs (minus side :155-159, plus side :186-190); selecting
+    // those operands keeps every rounding of either side:
+    //   w1 (q4 + Q0 (q3-q4) -+ Q1 (q5-q4))
+    //   w2 (q3 + Q2 x2 - Q3 y2)   x2, y2 = (q4-q3), (q2-q3)  [plus: swapped]
+    //   w3 (q2 + Q4 x3 +- Q5 y3)  x3, y3 = (q1-q2), (q3-q2)  [plus: swapped]
+    const double t1 = Q1 * (q5 - q4);
+    const double x2 = plus ? (q2 - q3) : (q4 - q3), y2 = plus ? (q4 - q3) : (q2 - q3);
+    const double x3 = plus ? (q3 - q2) : (q1 - q2), y3 = plus ? (q1 - q2) : (q3 - q2);
+    const double t3 = Q5 * y3;
+    return w1 * (q4 + Q0 * (q3 - q4) + (plus ? t1 : -t1))
+         + w2 * (q3 + Q2 * x2 - Q3 * y2)
+         + w3 * (q2 + Q4 * x3 + (plus ? -t3 : t3));
 }
 
 // Upwind-biased derivative along one axis (stride s) at linear index c,
 // cell index t = idx+5.  Minus stencil src/weno_hj_df_nug.cpp:344-351, plus
-// stencil :371-378 (shared with src/ddweno_nug_sf.cpp:225-277).
+// stencil :371-378 (shared with src/ddweno_nug_sf.cpp:225-277): the six
+// points f[c+(o+m)s], m = 0..5, with o = -3 (minus) or -2 (plus), and
+// q_m = (f_m - f_{m-1}) / DXP[t+o+m-1].  The side is a runtime value, so a
+// warp whose cells take different sides runs one evaluation, not both.
 __device__ __forceinline__ double deriv(const double* __restrict__ f, long long c, long long s,
                                         const double* __restrict__ dp, const double* __restrict__ qf,
                                         const double* __restrict__ cf, const double* __restrict__ isf, int t,
                                         bool plus) {
-    double q1, q2, q3, q4, q5;
-    if (!plus) {
-        const double fm3 = __ldg(f + c - 3 * s), fm2 = __ldg(f + c - 2 * s), fm1 = __ldg(f + c - s);
-        const double f0 = __ldg(f + c), fp1 = __ldg(f + c + s), fp2 = __ldg(f + c + 2 * s);
-        q1 = (fm2 - fm3) / __ldg(dp + t - 3);
-        q2 = (fm1 - fm2) / __ldg(dp + t - 2);
-        q3 = (f0 - fm1) / __ldg(dp + t - 1);
-        q4 = (fp1 - f0) / __ldg(dp + t);
-        q5 = (fp2 - fp1) / __ldg(dp + t + 1);
-    } else {
-        const double fm2 = __ldg(f + c - 2 * s), fm1 = __ldg(f + c - s), f0 = __ldg(f + c);
-        const double fp1 = __ldg(f + c + s), fp2 = __ldg(f + c + 2 * s), fp3 = __ldg(f + c + 3 * s);
-        q1 = (fm1 - fm2) / __ldg(dp + t - 2);
-        q2 = (f0 - fm1) / __ldg(dp + t - 1);
-        q3 = (fp1 - f0) / __ldg(dp + t);
-        q4 = (fp2 - fp1) / __ldg(dp + t + 1);
-        q5 = (fp3 - fp2) / __ldg(dp + t + 2);
-    }
+    const int o = plus ? -2 : -3;
+    const double* p = f + c + o * s;
+    const double* d = dp + t + o;
+    const double f0 = __ldg(p), f1 = __ldg(p + s), f2 = __ldg(p + 2 * s);
+    const double f3 = __ldg(p + 3 * s), f4 = __ldg(p + 4 * s), f5 = __ldg(p + 5 * s);
+    const double q1 = (f1 - f0) / __ldg(d);
+    const double q2 = (f2 - f1) / __ldg(d + 1);
+    const double q3 = (f3 - f2) / __ldg(d + 2);
+    const double q4 = (f4 - f3) / __ldg(d + 3);
+    const double q5 = (f5 - f4) / __ldg(d + 4);
     const int side = plus ? 1 : 0;
     return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
                  isf + (long long)t * 18 + side * 9, plus, q1, q2, q3, q4, q5);
@@ -84,20 +85,18 @@ __device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* _
     const long long sy = g.L.sy, sz = g.L.sz;
     const double iadvec = 0.5 * (vs * __ldg(u + c) + vs * __ldg(u + c - 1));
     const double kadvec = 0.5 * (vs * __ldg(w + c) + vs * __ldg(w + c - sz));
-    double grad = 0.0;
-    if (iadvec > 0.0) grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, false);
-    if (iadvec < 0.0) grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, true);
+    // advec > 0: minus side, < 0: plus side, == 0: no contribution (grad 0)
+    double grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, iadvec < 0.0);
+    if (iadvec == 0.0) grad = 0.0;
     double l = -iadvec * grad;
     if (!TWO_D) {
         const double jadvec = 0.5 * (vs * __ldg(v + c) + vs * __ldg(v + c - sy));
-        grad = 0.0;
-        if (jadvec > 0.0) grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, false);
-        if (jadvec < 0.0) grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, true);
+        grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, jadvec < 0.0);
+        if (jadvec == 0.0) grad = 0.0;
         l -= jadvec * grad;
     }
-    grad = 0.0;
-    if (kadvec > 0.0) grad = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5, false);
-    if (kadvec < 0.0) grad = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5, true);
+    grad = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5, kadvec < 0.0);
+    if (kadvec == 0.0) grad = 0.0;
     l -= kadvec * grad;
     double acc = 0.0;
     acc += l;
@@ -130,29 +129,38 @@ __device__ __forceinline__ double reini_L(const KGrid<double>& g, const double* 
 
     const double xmin = (lsv - __ldg(f + c - 1)) / __ldg(g.dxp[0] + ti - 1);
     const double xplus = (__ldg(f + c + 1) - lsv) / __ldg(g.dxp[0] + ti);
-    if (xmin * lsSig > 0.0 && xplus * lsSig > -xmin * lsSig)
-        dx = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], ti, false);
-    if (xplus * lsSig < 0.0 && xmin * lsSig < -xplus * lsSig)
-        dx = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], ti, true);
-    if (xplus * lsSig > 0.0 && xmin * lsSig < 0.0) dx = 0.0;
+    {
+        // minus side if c1, plus side if c2 (the later test wins, as there), else 0
+        const bool c1 = xmin * lsSig > 0.0 && xplus * lsSig > -xmin * lsSig;
+        const bool c2 = xplus * lsSig < 0.0 && xmin * lsSig < -xplus * lsSig;
+        dx = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], ti, c2);
+        if (!(c1 || c2)) dx = 0.0;
+        if (xplus * lsSig > 0.0 && xmin * lsSig < 0.0) dx = 0.0;
+    }
 
     if (!TWO_D) {
         const double ymin = (lsv - __ldg(f + c - sy)) / __ldg(g.dxp[1] + tj - 1);
         const double yplus = (__ldg(f + c + sy) - lsv) / __ldg(g.dxp[1] + tj);
-        if (ymin * lsSig > 0.0 && yplus * lsSig > -ymin * lsSig)
-            dy = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], tj, false);
-        if (yplus * lsSig < 0.0 && ymin * lsSig < -yplus * lsSig)
-            dy = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], tj, true);
-        if (yplus * lsSig > 0.0 && ymin * lsSig < 0.0) dy = 0.0;
+        {
+            // minus side if c1, plus side if c2 (the later test wins, as there), else 0
+            const bool c1 = ymin * lsSig > 0.0 && yplus * lsSig > -ymin * lsSig;
+            const bool c2 = yplus * lsSig < 0.0 && ymin * lsSig < -yplus * lsSig;
+            dy = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], tj, c2);
+            if (!(c1 || c2)) dy = 0.0;
+            if (yplus * lsSig > 0.0 && ymin * lsSig < 0.0) dy = 0.0;
+        }
     }
 
     const double zmin = (lsv - __ldg(f + c - sz)) / __ldg(g.dxp[2] + tk - 1);
     const double zplus = (__ldg(f + c + sz) - lsv) / __ldg(g.dxp[2] + tk);
-    if (zmin * lsSig > 0.0 && zplus * lsSig > -zmin * lsSig)
-        dz = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], tk, false);
-    if (zplus * lsSig < 0.0 && zmin * lsSig < -zplus * lsSig)
-        dz = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], tk, true);
-    if (zplus * lsSig > 0.0 && zmin * lsSig < 0.0) dz = 0.0;
+    {
+        // minus side if c1, plus side if c2 (the later test wins, as there), else 0
+        const bool c1 = zmin * lsSig > 0.0 && zplus * lsSig > -zmin * lsSig;
+        const bool c2 = zplus * lsSig < 0.0 && zmin * lsSig < -zplus * lsSig;
+        dz = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], tk, c2);
+        if (!(c1 || c2)) dz = 0.0;
+        if (zplus * lsSig > 0.0 && zmin * lsSig < 0.0) dz = 0.0;
+    }
 
     const double dnorm = sqrt(dx * dx + dy * dy + dz * dz);
     double deltax;
