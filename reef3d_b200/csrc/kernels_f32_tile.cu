@@ -177,7 +177,9 @@ __device__ __forceinline__ double weno5_d(double d1, double d2, double d3, doubl
 // stencils (the interface band): Godunov selection, one-sided WENO5 per
 // axis and the smoothed sign of src/reinidisc_f.cpp:58-127 on a uniform
 // grid.  X, Y, Z: the 7-point stencils along x, y, z (centre at [3]).
-__device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, const float* Z, const TileArgs& a) {
+__device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, const float* Z, float rhx, float rhy,
+                                              float rhz, float deltax) {
+    const float rh[3] = {rhx, rhy, rhz};
     const double f0 = X[3];
     const double sg = fabs(f0) < 1.0e-8 ? 1.0 : (f0 > 0.0 ? 1.0 : -1.0);
     const float* ax[3] = {X, Y, Z};
@@ -191,16 +193,16 @@ __device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, co
         const double ms = D[2] * sg, ps = D[3] * sg, sum = ms + ps;
         const bool c1 = ms > 0.0 && sum > 0.0, c2 = ps < 0.0 && sum < 0.0;
         if (c1 || c2) {
-            const double h = 1.0 / (double)a.rh[d];
+            const double h = 1.0 / (double)rh[d];
             const double eps = 1.0e-6 * h * h;
             const double w = c2 ? weno5_d(D[5], D[4], D[3], D[2], D[1], eps)
                                 : weno5_d(D[0], D[1], D[2], D[3], D[4], eps);
-            const double gd = w * (double)a.rh[d];
+            const double gd = w * (double)rh[d];
             g2 += gd * gd;
         }
     }
     const double dn = sqrt(g2);
-    const double dl = a.deltax;
+    const double dl = deltax;
     double S = f0 / sqrt(f0 * f0 + dn * dn * dl * dl);
     if (S != S) S = 1.0;
     return (float)(S - S * dn);  // -(S |grad| - S)
@@ -349,10 +351,13 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
         const float2 f0 = make_float2(xv[4], xv[5]);
 
         float2 Lc;
+        // this plane's operands, then the next plane's loads in flight
+        // through the whole computation of this one
         const float2 fn = nfn;
+        const float2 uc = nu, vc = nv, vm = nvm, wc = nw;
+        const float um = num;
+        if (k + 1 < k1) fetch(c + L.sz);
         if (!REINI) {
-            const float2 uc = nu, vc = nv, vm = nvm, wc = nw;
-            const float um = num;
             const float2 h2 = f2(0.5f * vs);
             const float2 ia = mul2(h2, add2(make_float2(um, uc.x), uc));
             const float2 ja = mul2(h2, add2(vc, vm));
@@ -431,7 +436,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                                 Y[m] = sl[(ty + m) * kBoxX + 2 * src + 4 + e];
                                 Z[m] = ring[((n + m) & (kRing - 1)) * kSlotFloats + o];
                             }
-                            res = reini_cell_fp64(X, Y, Z, a);
+                            res = reini_cell_fp64(X, Y, Z, a.rh[0], a.rh[1], a.rh[2], a.deltax);
                         }
                         const float rx = __shfl_sync(0xffffffffu, res, (bxi - base) & 31);
                         const float ry = __shfl_sync(0xffffffffu, res, (byi - base) & 31);
@@ -509,7 +514,6 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             }
         }
 
-        if (k + 1 < k1) fetch(c + L.sz);
         if (!REINI) {
             // convection (the same work in every warp): one CTA barrier per
             // plane, after which thread 0 refills the box of plane k-3
