@@ -197,7 +197,9 @@ def run_configs(ctx):
     out["slotted_disk_fp32"] = workloads.slotted_disk_revolution(128, FP32)
     out["vortex_accuracy"] = workloads.vortex_accuracy(128)
     out["wave_tank"] = workloads.wave_tank_run(500)
+    out["wave_tank_accuracy"] = workloads.wave_tank_accuracy(500)
     out["ensemble"] = workloads.ensemble(steps=200)
+    out["ensemble_accuracy"] = workloads.ensemble_accuracy(200)
     out["serving_fp32"] = workloads.serving(njobs=16)
     out["serving_fp64"] = workloads.serving(njobs=16, precision=FP64)
     return out

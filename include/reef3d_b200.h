@@ -177,8 +177,10 @@ int r3d_set_velocity_period(r3d_handle* h, double period);
  * stored cell with the linear (Airy) orbital velocity of a wave
  *   eta = amplitude cos(kw x - om t), kw = 2 pi / wavelength,
  *   om = sqrt(gravity kw tanh(kw depth)), bed at z = 0:
- *   u = a cosh(kw z) cos(kw x - om t), w = a sinh(kw z) sin(kw x - om t),
- *   a = amplitude om / sinh(kw depth),
+ *   u = a cosh(kw z') cos(kw x - om t), w = a sinh(kw z') sin(kw x - om t),
+ *   a = amplitude om / sinh(kw depth), z' = min(z, depth) (above the
+ *   still-water level the surface value, not the linear solution's
+ *   exponential growth into the air),
  * at the device clock t (u on x faces, w on z faces); v is zeroed and the
  * velocity factor set to 1.  wavelength <= 0 turns the generator off.
  * Synchronous.  Not for batch members. */

@@ -699,7 +699,7 @@ int r3d_set_velocity_airy(r3d_handle* h, double amplitude, double wavelength, do
         h->sms = sms;
     const double kw = 2.0 * 3.141592653589793 / wavelength;
     const double om = std::sqrt(gravity * kw * std::tanh(kw * depth));
-    h->ap = r3d::AiryParams{amplitude * om / std::sinh(kw * depth), kw, om};
+    h->ap = r3d::AiryParams{amplitude * om / std::sinh(kw * depth), kw, om, depth};
     h->airy = true;
     h->period = 0.0;
     h->launches += launch_set_scalar(h->S.vscale, 1.0, h->stream);

@@ -262,7 +262,9 @@ __global__ void volume_direct_kernel(Layout L, const T* __restrict__ phi, const 
 // every stored cell (interior and ghost layers):
 //   u = a cosh(kw z_c) cos(kw x_f - om t)   (x faces, cell-centre z)
 //   w = a sinh(kw z_f) sin(kw x_c - om t)   (z faces, cell-centre x)
-// with a = amp om / sinh(kw depth), the bed at z = 0.  The field is
+// with a = amp om / sinh(kw depth), the bed at z = 0, and z limited to the
+// still-water depth (the field above it is the one at the surface, instead of
+// the exponential growth of the linear solution into the air).  The field is
 // separable, so each block first tabulates the x and z factors in shared
 // memory (coord: x centres, x faces, z centres, z faces of padded indices
 // -3..n+2) and then writes rows with two multiplies per value.
@@ -282,8 +284,9 @@ __global__ void __launch_bounds__(256) airy_kernel(Layout L, T* __restrict__ u, 
         xw[i] = sin(ap.kw * coord[i] - ap.om * tt);
     }
     for (int k = threadIdx.x; k < nz6; k += blockDim.x) {
-        zu[k] = ap.a * cosh(ap.kw * coord[2 * nx6 + k]);
-        zw[k] = ap.a * sinh(ap.kw * coord[2 * nx6 + nz6 + k]);
+        // above the still-water level the surface value is carried upward
+        zu[k] = ap.a * cosh(ap.kw * fmin(coord[2 * nx6 + k], ap.depth));
+        zw[k] = ap.a * sinh(ap.kw * fmin(coord[2 * nx6 + nz6 + k], ap.depth));
     }
     __syncthreads();
     const int py = L.two_d ? 1 : L.ny + 6;

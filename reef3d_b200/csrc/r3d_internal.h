@@ -121,7 +121,7 @@ int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const doub
 // Airy wave velocity generator: a = amp om / sinh(kw depth), kw = 2 pi /
 // wavelength, om = sqrt(g kw tanh(kw depth)).
 struct AiryParams {
-    double a, kw, om;
+    double a, kw, om, depth;
 };
 // Writes u and w of the Airy field at the device time *t on every stored
 // cell; coord = x centres, x faces, z centres, z faces (padded indices

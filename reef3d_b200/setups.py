@@ -136,7 +136,8 @@ def vortex3d(n=256, cfl=0.25, T=3.0):
 def wave_tank(nx=1024, ny=128, nz=256, dx=0.01, depth=0.5, amp=0.05, wavelength=2.0, t=0.0, cfl=0.2, g=9.81,
               velocity=True):
     """Wave-tank-shaped free surface: phi = z - (depth + amp cos(kx)) with the
-    linear (Airy) orbital velocity of that wave at time t, bed at z=0.
+    linear (Airy) orbital velocity of that wave at time t, bed at z=0, carried
+    upward unchanged above the still-water level.
     velocity=False leaves u, v, w as None (for instances whose velocity the
     device's Airy generator writes)."""
     xn = uniform_nodes(nx, nx * dx)
@@ -150,8 +151,9 @@ def wave_tank(nx=1024, ny=128, nz=256, dx=0.01, depth=0.5, amp=0.05, wavelength=
         return Case("wave_tank", nx, ny, nz, xn, yn, zn, np.ascontiguousarray(phi), None, None, None,
                     f43=0.5, f44=1, n47=cfl / 2.0)
     a = amp * om / math.sinh(k * depth)
-    uf = a * np.cosh(k * zc)[None, :] * np.cos(k * faces(xn) - om * t)[:, None]
-    wf = a * np.sinh(k * faces(zn))[None, :] * np.sin(k * xc - om * t)[:, None]
+    # above the still-water level the surface value (see r3d_set_velocity_airy)
+    uf = a * np.cosh(k * np.minimum(zc, depth))[None, :] * np.cos(k * faces(xn) - om * t)[:, None]
+    wf = a * np.sinh(k * np.minimum(faces(zn), depth))[None, :] * np.sin(k * xc - om * t)[:, None]
     u = np.broadcast_to(uf[:, None, :], phi.shape)
     w = np.broadcast_to(wf[:, None, :], phi.shape)
     v = np.zeros(phi.shape)

@@ -153,6 +153,78 @@ def wave_tank_run(steps=500, warmup=3, dims=(1024, 128, 256), precision=FP32):
             "precision": "fp32 form" if precision == FP32 else "fp64 plain"}
 
 
+def _accuracy(a32, a64, a0, h, cellvol, v0s, v1s):
+    """FP32 result against the FP64 one on the same grid: L1 of the smoothed
+    Heaviside H(phi; 1.5 h) times the cell volume, L-infinity of phi over the
+    band |phi_FP64| < 3h, and each run's relative change of volume1; plus the
+    FP64 run's L1 distance from the initial shape for scale."""
+    band = np.abs(a64) < 3 * h
+    return {"l1_heaviside_fp32_vs_fp64": float(np.sum(np.abs(heaviside(a32, 1.5 * h) - heaviside(a64, 1.5 * h))) * cellvol),
+            "l1_heaviside_fp64_moved": float(np.sum(np.abs(heaviside(a64, 1.5 * h) - heaviside(a0, 1.5 * h))) * cellvol),
+            "linf_phi_band": float(np.max(np.abs(a32 - a64)[band])) if band.any() else 0.0,
+            "relative_volume_change_fp32": abs(v1s[0] - v0s[0]) / abs(v0s[0]),
+            "relative_volume_change_fp64": abs(v1s[1] - v0s[1]) / abs(v0s[1])}
+
+
+def wave_tank_accuracy(steps=500, dims=(1024, 128, 256)):
+    """The wave tank in the FP32 form and in FP64 with the same fixed step
+    (the FP64 CFL step at t = 0), compared after `steps` steps."""
+    nx, ny, nz = dims
+    c = setups.wave_tank(nx, ny, nz, velocity=False)
+    outs, v0s, v1s, dt = [], [], [], None
+    for prec in (FP64, FP32):
+        with LevelSet(nx, ny, nz, c.xn, c.yn, c.zn, precision=prec, **c.flags()) as ls:
+            ls.upload(PHI, c.phi)
+            ls.set_time(0.0)
+            ls.set_velocity_airy(0.05, 2.0, 0.5, 9.81)
+            if dt is None:
+                dt = ls.cfl_dt()
+            ls.set_dt(dt)
+            v0s.append(ls.volume()[0])
+            ls.run(steps, adaptive=False)
+            v1s.append(ls.volume()[0])
+            outs.append(ls.download(PHI)[3:3 + nx, 3:3 + ny, 3:3 + nz].copy())
+    h = 0.01
+    r = _accuracy(outs[1], outs[0], c.phi[3:3 + nx, 3:3 + ny, 3:3 + nz], h, h ** 3, v0s[::-1], v1s[::-1])
+    r.update({"steps": steps, "dt": dt, "workload": f"wave tank {nx}x{ny}x{nz}, fixed dt, FP32 form vs FP64"})
+    return r
+
+
+def ensemble_accuracy(steps=200, seed=0, picks=(2, 2)):
+    """Members of the ensemble (the first `picks[0]` 2D and `picks[1]` 3D
+    ones of seed 0) run alone in the FP32 form -- the arithmetic of their
+    batched steps -- and in FP64 with the same fixed step, compared after
+    `steps` steps."""
+    specs = ensemble_specs(seed)
+    chosen = [s for s in specs if s[0][1] == 1][:picks[0]] + [s for s in specs if s[0][1] > 1][:picks[1]]
+    res = []
+    for dims, sph, modes in chosen:
+        nx, ny, nz = dims
+        outs, v0s, v1s, dt = [], [], [], None
+        for prec in (FP64, FP32):
+            ls = make_instance(dims, sph, modes, precision=prec)
+            try:
+                if dt is None:
+                    dt = ls.cfl_dt()
+                ls.set_dt(dt)
+                v0s.append(ls.volume()[0])
+                if prec == FP64:
+                    phi0 = ls.download(PHI)[3:3 + nx, 3:3 + ny, 3:3 + nz].copy()
+                ls.run(steps, adaptive=False)
+                v1s.append(ls.volume()[0])
+                outs.append(ls.download(PHI)[3:3 + nx, 3:3 + ny, 3:3 + nz].copy())
+            finally:
+                ls.close()
+        axes = [nx, nz] if ny == 1 else [nx, ny, nz]
+        h = 1.0 / min(axes)                     # the coarsest spacing
+        cellvol = float(np.prod([1.0 / n for n in axes]))
+        r = _accuracy(outs[1], outs[0], phi0, h, cellvol, v0s[::-1], v1s[::-1])
+        r["dims"] = list(dims)
+        res.append(r)
+    return {"steps": steps, "members": res,
+            "workload": f"{picks[0]} 2D + {picks[1]} 3D members of the seed-{seed} ensemble, fixed dt, FP32 vs FP64"}
+
+
 def ensemble_specs(seed=0, count=64, edges=tuple(range(64, 257, 32))):
     """Parameters of the batched ensemble (same draw order as
     setups.random_instance): 50/50 2D/3D, edges uniform in `edges`, 1-8
