@@ -260,8 +260,8 @@ int r3d_volume_dense_noalloc(const double* phi, int nx, int ny, int nz, double d
  * with its own CFL time step (src/ietimestep.cpp:38-206), clock and volume.
  * A member's results do not depend on the other members.  While an
  * instance is a member, calls on its handle first wait for the batch.
- * Members are FP32 instances with f46 = 0 (no picard mass correction) and
- * without the fluid update. */
+ * Members are FP32 instances with f46 = 0 (no picard mass correction),
+ * without the fluid update and without the Airy velocity generator. */
 typedef struct r3d_batch r3d_batch;
 int r3d_batch_create(r3d_batch** out);
 int r3d_batch_destroy(r3d_batch* b);

@@ -371,6 +371,7 @@ int r3d_batch_add(r3d_batch* b, r3d_handle* h) {
     if (h->desc.precision != R3D_FP32) return bfail(b, R3D_EINVAL, "batches hold FP32 instances");
     if (h->desc.f46 != 0) return bfail(b, R3D_EINVAL, "batches hold instances without picard mass correction (f46 = 0)");
     if (h->fluid) return bfail(b, R3D_EINVAL, "batches hold instances without the fluid update");
+    if (h->airy) return bfail(b, R3D_EINVAL, "batches hold instances without the Airy velocity generator");
     if (h->device != b->device) return bfail(b, R3D_EINVAL, "instance lives on another device");
     if (h->batch_stream) return bfail(b, R3D_ESTATE, "instance already in a batch");
     // the member's own queued work (uploads, settings) completes first

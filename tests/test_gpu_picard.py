@@ -99,3 +99,19 @@ def test_picard_rejected_in_batches():
         with pytest.raises(r3d.R3DError):
             b.add(ls)
         b.close()
+
+
+@pytest.mark.parametrize("what", ["fluid", "airy"])
+def test_batch_refuses_per_instance_extras(what):
+    """The batched step has no fluid update and no velocity generator: an
+    instance that needs either is refused, not advanced without it."""
+    n = 16
+    with r3d.LevelSet(n, n, n, precision=r3d.FP32) as ls:
+        if what == "fluid":
+            ls.set_fluid()
+        else:
+            ls.set_velocity_airy(0.05, 2.0, 0.5)
+        b = r3d.Batch()
+        with pytest.raises(r3d.R3DError):
+            b.add(ls)
+        b.close()
