@@ -32,7 +32,7 @@ N_CELLS_EDGE = 256
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the dominant FP32 kernel, the tiled reinitialisation stage 2, measured by ncu
 # on the 256^3 vortex (profiles/tile_stage_kernels_vortex.txt)
-NCU_TRAFFIC = {(256, "reinit_stage"): 146.27e6 + 79.82e6}
+NCU_TRAFFIC = {(256, "reinit_stage"): 145.90e6 + 45.69e6}
 METRIC = "level-set cell-updates/s (RK3+reinit), FP64 plain vs FP32 batched; p50/p99 latency"
 WORKLOAD = "3D single-vortex deformation 256^3, CFL 0.25, F44=2 reinit pseudo-steps, T=3"
 
