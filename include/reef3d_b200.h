@@ -216,10 +216,18 @@ int r3d_init_spheres_tg(r3d_handle* h, int nspheres, const double* spheres, int 
  *                 reading it returns whether the tiled path is in use.
  *  R3D_OPT_CHUNK  z-planes per CTA of the tiled kernels (default 16).
  *  R3D_OPT_BAND64 1 = FP64 re-anchoring of interface-band cells in the FP32
- *                 reinitialisation (default), 0 = FP32 everywhere. */
+ *                 reinitialisation (default), 0 = FP32 everywhere.
+ *  R3D_OPT_WAIT_TEST  diagnostic for the bounded waits of the tiled kernels:
+ *                 1 makes every CTA of the next r3d_ls_step wait (with a
+ *                 short limit) for a copy that is never issued, so the
+ *                 kernels take their timeout path -- raise the error flag,
+ *                 wait for their own copies, return -- and the next
+ *                 r3d_sync reports R3D_ETIMEOUT; the instance stays usable.
+ *                 Cleared by that step.  No effect off the tiled path. */
 #define R3D_OPT_TILED 0
 #define R3D_OPT_CHUNK 1
 #define R3D_OPT_BAND64 2
+#define R3D_OPT_WAIT_TEST 3
 int r3d_set_option(r3d_handle* h, int option, int value);
 int r3d_get_option(r3d_handle* h, int option, int* value);
 

@@ -23,7 +23,7 @@ FP64, FP32 = 0, 1
 PHI, U, V, W, L, WORK1, WORK2, RO, VISC = range(9)
 LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
 STAGE_CONVECTION, STAGE_REINIT = 0, 1
-OPT_TILED, OPT_CHUNK, OPT_BAND64 = 0, 1, 2
+OPT_TILED, OPT_CHUNK, OPT_BAND64, OPT_WAIT_TEST = 0, 1, 2, 3
 
 _ERRNAMES = {1: "EINVAL", 2: "ENOMEM", 3: "EDEVICE", 4: "ETIMEOUT", 5: "ESTATE"}
 

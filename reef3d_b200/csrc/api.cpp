@@ -203,6 +203,8 @@ TileArgs make_tile_args(r3d_handle* h, int stage) {
     a.deltax = (float)((1.0 / 3.0) * (h->M.h[0] + h->M.h[1] + h->M.h[2]));
     a.f49 = h->desc.f49;
     a.band64 = h->band64;
+    a.wait_test = h->wait_test;
+    a.spin = h->wait_test ? (1ll << 12) : 0;
     a.psi = h->M.psi;
     a.cellvol = h->M.h[0] * h->M.h[1] * h->M.h[2];
     a.kc = h->kc;
@@ -483,6 +485,7 @@ int r3d_ls_step(r3d_handle* h, double dt) {
     }
     h->launches += refresh_velocity(h);
     enqueue_step(h);
+    h->wait_test = 0;  // a timeout-path test covers one step
     R3D_CUDA(h, cudaGetLastError());
     return R3D_OK;
 }
@@ -798,6 +801,7 @@ int r3d_set_option(r3d_handle* h, int option, int value) {
             h->kc = value;
             return R3D_OK;
         case R3D_OPT_BAND64: h->band64 = value ? 1 : 0; return R3D_OK;
+        case R3D_OPT_WAIT_TEST: h->wait_test = value ? 1 : 0; return R3D_OK;
         default: return fail(h, R3D_EINVAL, "unknown option");
     }
 }
@@ -808,6 +812,7 @@ int r3d_get_option(r3d_handle* h, int option, int* value) {
         case R3D_OPT_TILED: *value = tiled(h) ? 1 : 0; return R3D_OK;
         case R3D_OPT_CHUNK: *value = h->kc; return R3D_OK;
         case R3D_OPT_BAND64: *value = h->band64; return R3D_OK;
+        case R3D_OPT_WAIT_TEST: *value = h->wait_test; return R3D_OK;
         default: return fail(h, R3D_EINVAL, "unknown option");
     }
 }

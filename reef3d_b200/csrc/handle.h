@@ -41,6 +41,7 @@ struct r3d_handle {
     int use_tile = 1;
     int kc = 16;
     int band64 = 1;
+    int wait_test = 0;  // R3D_OPT_WAIT_TEST: armed for the next r3d_ls_step
     CUtensorMap map[3];  // stage inputs: phi, WORK1, WORK2
     // set while the instance is a member of a batch: calls on the handle
     // first wait for the batch's stream

@@ -70,8 +70,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (long long it = 0; it < kSpin; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit = kSpin) {
+    for (long long it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -271,9 +271,13 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     __syncthreads();
 
     // planes k0-3 .. k0+2: the first window without its top plane
+    const long long spin = a.spin > 0 ? a.spin : kSpin;
     bool ok = true;
 #pragma unroll
-    for (int m = 0; m < 6; ++m) ok = ok && mbar_wait_bounded(bar + m, 0);
+    for (int m = 0; m < 6; ++m) ok = ok && mbar_wait_bounded(bar + m, 0, spin);
+    // timeout-path test: the second completion of box 0 needs a refill that
+    // only the plane loop issues, so this wait gives up after `spin` tries
+    if (a.wait_test) ok = ok && mbar_wait_bounded(bar, 1, spin);
     ok = __all_sync(0xffffffffu, ok);
     if (!ok) *s_abort = 1;
 
@@ -314,7 +318,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
         const int n = k - k0;  // ring position of plane k-3
         {
             const int nt = n + 6;  // plane k+3
-            ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + (nt & (kRing - 1)), (nt / kRing) & 1));
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + (nt & (kRing - 1)), (nt / kRing) & 1, spin));
         }
         if (REINI) {
             if (!ok) *s_abort = 1;

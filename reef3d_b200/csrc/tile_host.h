@@ -24,6 +24,8 @@ struct TileArgs {
     float deltax;
     int f49;
     int band64;
+    int wait_test;   // nonzero: each item first waits for a copy that is never issued (timeout-path test)
+    long long spin;  // iteration limit of a bounded wait (0: the default)
     double psi;
     double cellvol;
     int kc;

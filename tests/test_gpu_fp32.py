@@ -173,3 +173,32 @@ def test_tiled_kernels_on_ragged_grids(port_lib, dims):
     assert err <= 2e-5, err
     m = visible_mask(nx, ny, nz)
     assert relmax(runs[0][1][m], runs[1][1][m]) <= 1e-5
+
+
+def test_bounded_wait_timeout_path_reports_and_recovers():
+    """The tiled kernels' bounded waits: with R3D_OPT_WAIT_TEST every CTA of
+    one step waits for a copy that is never issued; the kernels give up,
+    raise the instance's error flag and return, r3d_sync reports
+    R3D_ETIMEOUT, and the instance then steps exactly like a fresh one."""
+    n = 64
+    xn, yn, zn, phi, (u, v, w) = random_state(n, n, n, seed=9)
+    flags = dict(f43=0.5, f44=2, f45=2.1, f49=1, n47=0.125)
+    out = []
+    for stall in (True, False):
+        with r3d.LevelSet(n, n, n, xn, yn, zn, precision=r3d.FP32, **flags) as ls:
+            assert ls.get_option(r3d.OPT_TILED) == 1
+            for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+                ls.upload(f, a)
+            dt = ls.cfl_dt()
+            if stall:
+                ls.set_option(r3d.OPT_WAIT_TEST, 1)
+                ls.step(dt)
+                with pytest.raises(r3d.R3DError) as err:
+                    ls.sync()
+                assert err.value.code == r3d.R3D_ETIMEOUT
+                assert ls.get_option(r3d.OPT_WAIT_TEST) == 0
+                ls.upload(r3d.PHI, phi)
+            ls.step(dt)
+            ls.sync()
+            out.append(ls.download(r3d.PHI))
+    assert np.array_equal(out[0], out[1])
