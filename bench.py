@@ -356,7 +356,19 @@ def e2e_steps(case, precision, steps, warmup):
     el = time.perf_counter() - t0
     ls.close()
     nbytes = pinned["phi"].numel() * 8
-    return n ** 3 * steps / el, 3 * nbytes, nbytes
+    # the same host<->device traffic alone (three uploads, one download per
+    # step, pinned buffers, one stream): the link's share of the step
+    dev = torch.empty(shape, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(steps):
+        for name in ("u", "v", "w"):
+            dev.copy_(pinned[name], non_blocking=True)
+        out.copy_(dev, non_blocking=True)
+    torch.cuda.synchronize()
+    copy_ms = (time.perf_counter() - t1) * 1e3 / steps
+    del dev
+    return n ** 3 * steps / el, 3 * nbytes, nbytes, copy_ms, el * 1e3 / steps
 
 
 def run_ours(args):
@@ -395,9 +407,11 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         e2e_steps_n = max(2, min(args.steps, 10))
-        rate, h2d, d2h = e2e_steps(case, r3d.FP32, e2e_steps_n, 1)
+        rate, h2d, d2h, copy_ms, step_ms = e2e_steps(case, r3d.FP32, e2e_steps_n, 1)
         e2e = {"value": rate * ctx.world, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": e2e_steps_n,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps_n, "ms_per_step": step_ms,
+               "copies_alone_ms_per_step": copy_ms,
+               "link_gbs": (h2d + d2h) / (copy_ms * 1e-3) / 1e9,
                "path": "r3d_upload(u,v,w) + r3d_ls_run(1) + r3d_download(phi) per step (phi resident), "
                        "pinned host buffers in the reference layout, FP32 form"}
     cpu = None
