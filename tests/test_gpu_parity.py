@@ -153,15 +153,20 @@ def test_dense_layout_roundtrip():
         assert np.array_equal(b[3:3 + nx, 3:3 + ny, 3:3 + nz], a.transpose(2, 1, 0))
 
 
-@pytest.mark.parametrize("precision", [r3d.FP64, r3d.FP32])
-def test_graph_replayed_run_equals_direct_steps(precision):
+@pytest.mark.parametrize("precision,extras", [(r3d.FP64, False), (r3d.FP32, False), (r3d.FP64, True),
+                                              (r3d.FP32, True)])
+def test_graph_replayed_run_equals_direct_steps(precision, extras):
     """r3d_ls_run(n >= 2) replays one captured step; the result equals the
-    same steps launched one by one."""
+    same steps launched one by one (also with picard_lsm and the fluid
+    update in the step, whose counters and fields live on the device)."""
     nx, ny, nz = 36, 30, 28
     xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=21)
     out = []
     for graph in (True, False):
-        with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=precision, f43=0.5, f44=2, n47=0.125) as ls:
+        with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=precision, f43=0.5, f44=2, n47=0.125,
+                          f46=3 if extras else 0, f47=4) as ls:
+            if extras:
+                ls.set_fluid()
             for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
                 ls.upload(f, a)
             ls.set_velocity_period(3.0)
@@ -171,6 +176,9 @@ def test_graph_replayed_run_equals_direct_steps(precision):
             else:
                 for _ in range(4):
                     ls.run(1, adaptive=True)
-            out.append((ls.download(r3d.PHI), ls.time(), ls.last_volume()))
+            out.append((ls.download(r3d.PHI), ls.time(), ls.last_volume(),
+                        ls.download(r3d.RO) if extras else None))
     assert np.array_equal(out[0][0], out[1][0])
+    if extras:
+        assert np.array_equal(out[0][3], out[1][3])
     assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
