@@ -185,6 +185,50 @@ int r3d_set_velocity_period(r3d_handle* h, double period);
  * velocity factor set to 1.  wavelength <= 0 turns the generator off.
  * Synchronous.  Not for batch members. */
 int r3d_set_velocity_airy(r3d_handle* h, double amplitude, double wavelength, double depth, double gravity);
+/* Inflow and outflow boundaries with the level-set hooks of REEF3D's
+ * ioflow_f (B60 >= 1, src/driver_logic_cfd.cpp:509-510), which the
+ * closed box's ioflow_v leaves void.  The x-min face becomes an inflow
+ * boundary (boundary type 1) and the x-max face an outflow boundary (type
+ * 2); the other faces stay walls.  Per step (levelset_RK3::start,
+ * src/levelset_RK3.cpp:105-109):
+ *  - fsfinflow (src/ioflow_waterlevel.cpp:29-141): the inflow water level
+ *    phimean from the zero crossings of phi in the first ghost column
+ *    (else F56, or F60 when set) is imposed on the inflow ghosts when f50 is
+ *    2 or 4; the outflow level phiout is measured the same way on the last
+ *    interior column; with F62 set and B77 = 2 the outflow ghosts take the
+ *    level F62 (ramped from F60 over the first F64 steps);
+ *  - fsfrkin / fsfrkout (:143-177) on the RK buffers, also at the start of
+ *    every reinitialisation (src/reini_RK3.cpp:107-110);
+ *  - the ghost fill of the level set follows gcval 50+f50
+ *    (src/gc_epol4.cpp:26-58): the inflow face is a Neumann copy for f50 2
+ *    and 4 and untouched otherwise, the outflow face a Neumann copy for f50
+ *    1 and 4 and for 2 with B77 = 1, untouched otherwise.
+ * Values as the reference's control file gives them; "unset" is its
+ * default (F56 1e20, F60/F61/F62 -1e20).  qi, qo: the discharges picard_lsm
+ * adds to its target volume each step, netvol += Qi dt - Qo dt
+ * (src/picard_lsm.cpp:93), which the flow solver computes.  ioflow_f's
+ * phi_relax (src/ioflow_relax.cpp:49) acts only at step count 0, the
+ * reference's initialisation step, and is not part of a step here.
+ * Not for batch members; instances with inflow/outflow run the
+ * one-cell-per-thread kernels.  NULL restores the closed box.  Synchronous. */
+typedef struct {
+    int inflow;         /* 1: x-min face is an inflow boundary, 0: wall */
+    int outflow;        /* 1: x-max face is an outflow boundary, 0: wall */
+    int f50;            /* 1..4, level-set ghost rule gcval 50+f50 (src/levelset_RK3.cpp:50-60) */
+    int b77;            /* 1 or 2: outflow pressure-controlled / fixed water level */
+    double f56, f60, f61, f62;
+    int f64;            /* >= 0 */
+    double qi, qo;
+} r3d_ioflow_desc;
+int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io);
+/* Water levels phimean and phiout of the last step's fsfinflow (both may be
+ * NULL).  Synchronous. */
+int r3d_io_levels(r3d_handle* h, double* phimean, double* phiout);
+/* lexer::count of the next step (default: 1 for the first step of the
+ * instance).  The outflow ramp (F64) and picard_lsm's first-step target
+ * read it. */
+int r3d_set_step_count(r3d_handle* h, long long count);
+
 /* Device clock (the reference's p->simtime, advanced by dt every step,
  * src/driver_loop_cfd.cpp:104). */
 int r3d_set_time(r3d_handle* h, double t);

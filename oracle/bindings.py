@@ -33,6 +33,13 @@ def _dp(a):
     return a.ctypes.data_as(_D)
 
 
+# ioflow_f flags in refls_set_ioflow's argument order, with the reference's
+# defaults (src/ini.cpp:208-441; F50 = 2 the level-set default).
+IOFLOW_KEYS = ("inflow", "outflow", "f50", "b77", "f56", "f60", "f61", "f62", "f64", "qi", "qo")
+IOFLOW_DEFAULTS = dict(inflow=1, outflow=1, f50=2, b77=1, f56=1.0e20, f60=-1.0e20, f61=-1.0e20, f62=-1.0e20,
+                       f64=0, qi=0.0, qo=0.0)
+
+
 def padded_shape(nx, ny, nz):
     return (nx + 6, ny + 6, nz + 6)
 
@@ -72,10 +79,15 @@ class PortOracle:
             lib.lso_cfl_dt.argtypes = [ctypes.c_void_p, _D, _D, _D]
             lib.lso_set_picard.argtypes = [ctypes.c_void_p, _I, _I]
             lib.lso_fluid.argtypes = [ctypes.c_void_p, _D, _D, _D] + [ctypes.c_double] * 4
+            lib.lso_set_ioflow.argtypes = ([ctypes.c_void_p, _I, _I, _I, _I] + [ctypes.c_double] * 4 + [_I]
+                                           + [ctypes.c_double] * 2)
+            lib.lso_io_levels.argtypes = [ctypes.c_void_p, _D]
+            lib.lso_set_count.argtypes = [ctypes.c_void_p, _I]
             cls._lib = lib
         return cls._lib
 
-    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3, f46=0, f47=10):
+    def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, n47=0.3, f46=0, f47=10,
+                 ioflow=None):
         self.lib()
         self.nx, self.ny, self.nz = nx, ny, nz
         self.shape = padded_shape(nx, ny, nz)
@@ -88,6 +100,19 @@ class PortOracle:
         if not self.h:
             raise ValueError("lso_new failed")
         self._lib.lso_set_picard(self.h, f46, f47)
+        if ioflow is not None:
+            io = dict(IOFLOW_DEFAULTS, **ioflow)
+            self._lib.lso_set_ioflow(self.h, *(io[k] for k in IOFLOW_KEYS))
+
+    def io_levels(self):
+        """(phimean, phiout) after the last step's fsfinflow."""
+        out = np.zeros(2)
+        self._lib.lso_io_levels(self.h, _dp(out))
+        return float(out[0]), float(out[1])
+
+    def set_count(self, count):
+        """lexer::count the next step runs as."""
+        self._lib.lso_set_count(self.h, count)
 
     def __del__(self):
         if getattr(self, "h", None) and self._lib is not None:
@@ -169,7 +194,9 @@ class RefOracle:
     _loaded = set()
 
     def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10,
-                 path=None):
+                 path=None, ioflow=None):
+        """ioflow: None for the closed box, else a dict of IOFLOW_DEFAULTS'
+        keys: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags."""
         path = path or (REF_LIB_FAST if fast else REF_LIB)
         if path in RefOracle._loaded:
             raise RuntimeError("the reference oracle holds one grid per process")
@@ -177,6 +204,11 @@ class RefOracle:
         lib = ctypes.CDLL(path)
         lib.refls_set_picard.argtypes = [_I, _I]
         lib.refls_set_picard(f46, f47)
+        if ioflow is not None:
+            io = dict(IOFLOW_DEFAULTS, **ioflow)
+            lib.refls_set_ioflow.argtypes = [_I, _I, _I, _I] + [ctypes.c_double] * 4 + [_I] + [ctypes.c_double] * 2
+            lib.refls_set_ioflow(*(io[k] for k in IOFLOW_KEYS))
+        lib.refls_io_levels.argtypes = [_D]
         lib.refls_init.argtypes = [_I, _I, _I, _D, _D, _D, _I, ctypes.c_double, ctypes.c_double, _I]
         lib.refls_padded_size.restype = ctypes.c_long
         lib.refls_set_field.argtypes = [_I, _D]
@@ -269,6 +301,12 @@ class RefOracle:
     def volume(self):
         self._lib.refls_update()
         return self._lib.refls_volume1(), self._lib.refls_volume2()
+
+    def io_levels(self):
+        """(phimean, phiout) after the last step's fsfinflow."""
+        out = np.zeros(4)
+        self._lib.refls_io_levels(_dp(out))
+        return float(out[0]), float(out[1])
 
 
 class AdapterOracle(RefOracle):

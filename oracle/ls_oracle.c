@@ -329,12 +329,31 @@ void lso_reinidisc_L(const lso_grid* g, const double* f, double* L) {
  * gclabel_lsm=4 (src/gc_epol4.cpp:26-31, src/ghostcell.cpp:116), i.e. the
  * Neumann copy of src/gc_neumann.cpp:29-54 into the three face ghost layers.
  * 2D skips the y sides (src/gc_neumann.cpp:34-40). */
-void lso_ghost_fill(const lso_grid* g, double* f) {
+/* Ghost label of an x face for the level-set gcval 50+f50
+ * (src/gc_epol4.cpp:26-58): walls (type 21) always 4 (Neumann copy);
+ * inflow (type 1) 4 for gcv 52/54, else 0 (untouched); outflow (type 2) 4
+ * for gcv 51/54 and for 52 with B77 = 1, else 0. */
+static int x_face_filled(const lso_grid* g, int side) {
+    if (!g->io_on) return 1;
+    const int gcv = 50 + g->f50;
+    if (side == 1 && g->io_in) return gcv == 52 || gcv == 54;
+    if (side == 4 && g->io_out) return gcv == 51 || gcv == 54 || (gcv == 52 && g->b77 == 1);
+    return 1;
+}
+
+static void ghost_fill_gcv(const lso_grid* g, double* f, int level_set);
+
+void lso_ghost_fill(const lso_grid* g, double* f) { ghost_fill_gcv(g, f, 1); }
+
+/* level_set 0: gcval 1 of ro/visc, a Neumann copy on every face
+ * (src/gc_epol4.cpp:90-93), whatever the boundary type. */
+static void ghost_fill_gcv(const lso_grid* g, double* f, int level_set) {
+    const int fill_lo = !level_set || x_face_filled(g, 1), fill_hi = !level_set || x_face_filled(g, 4);
     for (int j = 0; j < g->ny; ++j)
         for (int k = 0; k < g->nz; ++k)
             for (int q = 0; q < LSO_MARGIN; ++q) {
-                f[lso_index(g, -q - 1, j, k)] = f[lso_index(g, 0, j, k)];
-                f[lso_index(g, g->nx + q, j, k)] = f[lso_index(g, g->nx - 1, j, k)];
+                if (fill_lo) f[lso_index(g, -q - 1, j, k)] = f[lso_index(g, 0, j, k)];
+                if (fill_hi) f[lso_index(g, g->nx + q, j, k)] = f[lso_index(g, g->nx - 1, j, k)];
             }
     if (g->jdir == 1)
         for (int i = 0; i < g->nx; ++i)
@@ -349,7 +368,112 @@ void lso_ghost_fill(const lso_grid* g, double* f) {
                 f[lso_index(g, i, j, -q - 1)] = f[lso_index(g, i, j, 0)];
                 f[lso_index(g, i, j, g->nz + q)] = f[lso_index(g, i, j, g->nz - 1)];
             }
+    /* With an inflow face, fsfinflow reads the edge ghost (-1, j, nz) above
+     * the top inflow cell; start4 leaves there the copy of cell (0, j, nz-1)
+     * that dgcpol4 writes into the first diagonal ghost layer
+     * (src/gc_dgcpol4.cpp:28-50, Y40 = 3). */
+    if (level_set && g->io_on && g->io_in)
+        for (int j = 0; j < g->ny; ++j) f[lso_index(g, -1, j, g->nz)] = f[lso_index(g, 0, j, g->nz - 1)];
 }
+
+/* ------------------------------------------------------------ ioflow hooks
+ * ioflow_f::fsfinflow (src/ioflow_waterlevel.cpp:29-141): the water level
+ * at the inflow from the zero crossings of the first ghost column over the
+ * inflow cells (list order: j outer, k inner, the order of the boundary
+ * list), imposed on the inflow ghosts for F50 = 2 or 4; the outflow level
+ * from the last interior column; with F62 set and B77 = 2 the outflow
+ * ghosts take the (ramped) outflow level. */
+static void io_fsfinflow(lso_grid* g, double* phi) {
+    g->phimean = g->f56;
+    if (g->f60 > -1.0e20) { g->phimean = g->f60; g->phiout = g->f60; }
+    if (g->f62 > -1.0e20) g->phiout = g->f62;
+    int count = 0;
+    double zval = 0.0;
+    if (g->io_in) {
+        for (int j = 0; j < g->ny; ++j)
+            for (int k = 0; k < g->nz; ++k) {
+                const double a = phi[lso_index(g, -1, j, k)], b = phi[lso_index(g, -1, j, k + 1)];
+                if (a >= 0.0 && b < 0.0) {
+                    zval += -(a * g->dzp[k + LSO_MARGE]) / (b - a) + g->zp[k + LSO_MARGE];
+                    ++count;
+                }
+            }
+        if (count > 0) {
+            g->phimean = zval / (double)count;
+            if (g->f50 == 2 || g->f50 == 4)
+                for (int j = 0; j < g->ny; ++j)
+                    for (int k = 0; k < g->nz; ++k)
+                        for (int q = 1; q <= 3; ++q) phi[lso_index(g, -q, j, k)] = g->phimean - g->zp[k + LSO_MARGE];
+        }
+    }
+    count = 0;
+    zval = 0.0;
+    if (g->io_out) {
+        const int i = g->nx - 1;
+        for (int j = 0; j < g->ny; ++j)
+            for (int k = 0; k < g->nz; ++k) {
+                const double a = phi[lso_index(g, i, j, k)], b = phi[lso_index(g, i, j, k + 1)];
+                if (a >= 0.0 && b < 0.0) {
+                    zval += -(a * g->dzp[k + LSO_MARGE]) / (b - a) + g->zp[k + LSO_MARGE];
+                    ++count;
+                }
+            }
+        if (count > 0) g->phiout = zval / (double)count;
+    }
+    double wsfout = g->phimean;
+    if (g->f62 > 1.0e-20) {
+        if (g->f64 == 0) wsfout = g->f62;
+        if (g->f64 > 0) {
+            double f = 1.0;
+            if (g->count < g->f64) f = 0.5 * cos(LSO_PI + LSO_PI * (double)g->count / (double)g->f64) + 0.5;
+            wsfout = f * g->f62 + (1.0 - f) * g->f60;
+        }
+    }
+    if (g->io_out && g->f62 > -1.0e20 && g->b77 == 2)
+        for (int j = 0; j < g->ny; ++j)
+            for (int k = 0; k < g->nz; ++k)
+                for (int q = 1; q <= 3; ++q) phi[lso_index(g, g->nx - 1 + q, j, k)] = wsfout - g->zp[k + LSO_MARGE];
+}
+
+/* ioflow_f::fsfrkin and fsfrkout (src/ioflow_waterlevel.cpp:143-177): the
+ * RK buffer's inflow ghosts copy phi's; its outflow ghosts copy phi's, or
+ * hold F62 - z with F62 set and B77 = 2. */
+static void io_fsfrk(const lso_grid* g, const double* phi, double* f) {
+    if (!g->io_on) return;
+    for (int j = 0; j < g->ny; ++j)
+        for (int k = 0; k < g->nz; ++k)
+            for (int q = 1; q <= 3; ++q) {
+                if (g->io_in) f[lso_index(g, -q, j, k)] = phi[lso_index(g, -q, j, k)];
+                if (g->io_out) {
+                    const long c = lso_index(g, g->nx - 1 + q, j, k);
+                    if (g->f62 < -1.0e19 || g->b77 != 2) f[c] = phi[c];
+                    if (g->f62 > -1.0e20 && g->b77 == 2) f[c] = g->f62 - g->zp[k + LSO_MARGE];
+                }
+            }
+}
+
+void lso_set_ioflow(lso_grid* g, int inflow, int outflow, int f50, int b77, double f56, double f60, double f61,
+                    double f62, int f64, double qi, double qo) {
+    g->io_on = 1;
+    g->io_in = inflow;
+    g->io_out = outflow;
+    g->f50 = f50;
+    g->b77 = b77;
+    g->f56 = f56;
+    g->f60 = f60;
+    g->f61 = f61;
+    g->f62 = f62;
+    g->f64 = f64;
+    g->qi = qi;
+    g->qo = qo;
+}
+
+void lso_io_levels(const lso_grid* g, double* out) {
+    out[0] = g->phimean;
+    out[1] = g->phiout;
+}
+
+void lso_set_count(lso_grid* g, int count) { g->count = count - 1; }
 
 /* reinit pseudo time step per cell (src/reini_RK3.cpp:150-160) */
 static double reini_dt(const lso_grid* g, int i, int j, int k) {
@@ -400,6 +524,8 @@ void lso_set_picard(lso_grid* g, int f46, int f47) {
 /* src/reini_RK3.cpp:113-138 (with picard_f when F46=1, :92 and :140) */
 void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, int iters) {
     const double vol1 = g->f46 == 1 ? picard_volume(g, f) : 0.0;
+    io_fsfrk(g, f, a1);
+    io_fsfrk(g, f, a2);
     for (int q = 0; q < iters; ++q) {
         lso_reinidisc_L(g, f, L);
         for (int i = 0; i < g->nx; ++i)
@@ -432,15 +558,21 @@ void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, 
 /* src/levelset_RK3.cpp:112-161 then reini_RK3::start (F44 steps), with
  * picard_f around them when F46=2 (:110 and :171).  F46=3 (picard_lsm,
  * src/picard_lsm.cpp:36-116): the target volume is the one of the first step
- * (count == 1), carried as netvol; netvol += (Qi - Qo)*dt with Qi = Qo = 0 for
- * the closed box.  g->count counts the steps like lexer::count. */
+ * (count == 1), carried as netvol; netvol += Qi*dt - Qo*dt (zero discharges
+ * for the closed box).  g->count counts the steps like lexer::count.  With
+ * inflow / outflow faces the ioflow_f hooks run first (:105-109). */
 void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, const double* w,
                  double dt, double* a1, double* a2, double* L) {
     g->count += 1;
+    if (g->io_on) {
+        io_fsfinflow(g, phi);
+        io_fsfrk(g, phi, a1);
+        io_fsfrk(g, phi, a2);
+    }
     double vol1 = g->f46 >= 2 ? picard_volume(g, phi) : 0.0;
     if (g->f46 == 3) {
         if (g->count == 1) g->netvol = vol1;
-        g->netvol = g->netvol + 0.0 * dt - 0.0 * dt;
+        g->netvol = g->netvol + g->qi * dt - g->qo * dt;
     }
     lso_weno_L(g, phi, u, v, w, L);
     for (int i = 0; i < g->nx; ++i)
@@ -507,8 +639,8 @@ void lso_fluid(const lso_grid* g, const double* phi, double* ro, double* visc, d
                 ro[c] = w1 * H + w3 * (1.0 - H);
                 visc[c] = w2 * H + w4 * (1.0 - H);
             }
-    lso_ghost_fill(g, ro);
-    lso_ghost_fill(g, visc);
+    ghost_fill_gcv(g, ro, 0);
+    ghost_fill_gcv(g, visc, 0);
 }
 
 /* src/ietimestep.cpp:38-188 for a prescribed velocity (N50=1, no source

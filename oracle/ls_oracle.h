@@ -46,6 +46,12 @@ typedef struct {
     /* WENO node tables per axis (uf=0): qf[n][6][2], cf[n][6], isf[n][6][3],
      * n = cells+8, built like src/weno_nug_func_precalc_*.cpp */
     double *qf[3], *cf[3], *isf[3];
+    /* inflow (x-min, boundary type 1) / outflow (x-max, type 2) faces and
+     * ioflow_f's level-set flags (src/ioflow_waterlevel.cpp); io_on == 0 is
+     * the closed box with ioflow_v (every hook void) */
+    int io_on, io_in, io_out, f50, b77, f64;
+    double f56, f60, f61, f62, qi, qo;
+    double phimean, phiout;  /* water levels of the last fsfinflow */
 } lso_grid;
 
 /* xn/yn/zn: node coordinates for indices -5..n+5 (n+11 values). */
@@ -82,6 +88,17 @@ void lso_fluid(const lso_grid* g, const double* phi, double* ro, double* visc, d
 /* Picard mass correction flags (src/picard_f.cpp, src/picard_lsm.cpp): f46 1, 2 or 3,
  * f47 iterations.  Resets the step count. */
 void lso_set_picard(lso_grid* g, int f46, int f47);
+
+/* Inflow / outflow faces with ioflow_f's hooks (B60 >= 1): fsfinflow at the
+ * start of each step, fsfrkin/fsfrkout on the RK buffers of the step and of
+ * each reinitialisation, and the ghost rule of gcval 50+f50 on those faces
+ * (src/gc_epol4.cpp:26-58).  qi, qo: discharges of picard_lsm's netvol. */
+void lso_set_ioflow(lso_grid* g, int inflow, int outflow, int f50, int b77, double f56, double f60, double f61,
+                    double f62, int f64, double qi, double qo);
+/* out[0] = phimean, out[1] = phiout of the last step */
+void lso_io_levels(const lso_grid* g, double* out);
+/* lexer::count the next step runs as minus one (the step increments it) */
+void lso_set_count(lso_grid* g, int count);
 
 /* opaque handle helpers (used through ctypes) */
 lso_grid* lso_new(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,

@@ -27,6 +27,7 @@
 #include "reinidisc_f.h"
 #include "reinidisc_fsf.h"
 #include "ioflow_void.h"
+#include "ioflow_f.h"
 #include "particle_pls_void.h"
 #include "heat.h"
 #include "concentration.h"
@@ -56,6 +57,12 @@ heat* HEAT = nullptr;
 concentration* CONC = nullptr;
 field4* TMP = nullptr;
 int G_F46 = 0, G_F47 = 10;  // picard mass correction flags for the next refls_init
+// inflow (x-min) / outflow (x-max) boundaries and ioflow_f flags for the next
+// refls_init; io.on == 0 keeps the closed box and ioflow_v
+struct IoFlags {
+    int on = 0, inflow = 0, outflow = 0, f50 = 2, b77 = 1, f64 = 0;
+    double f56 = 1.0e20, f60 = -1.0e20, f61 = -1.0e20, f62 = -1.0e20, qi = 0.0, qo = 0.0;
+} G_IO;
 ietimestep* TSTEP = nullptr;
 turbulence* TURB = nullptr;
 
@@ -98,6 +105,19 @@ extern "C" {
 // (src/picard_f.cpp:82-113, src/picard_lsm.cpp:89-116).
 void refls_set_picard(int f46, int f47) { G_F46 = f46; G_F47 = f47; }
 
+// Inflow / outflow boundaries of the next refls_init.  inflow: the x-min face
+// is boundary type 1, outflow: the x-max face type 2 (the other faces stay
+// walls, type 21); the flow object becomes ioflow_f (B60 = 1,
+// src/driver_logic_cfd.cpp:509-510) with the level-set flags F50, B77,
+// F56, F60, F61, F62, F64 (src/ini.cpp:208-441) and discharges Qi, Qo.
+void refls_set_ioflow(int inflow, int outflow, int f50, int b77, double f56, double f60, double f61,
+                      double f62, int f64, double qi, double qo) {
+    G_IO.on = 1;
+    G_IO.inflow = inflow; G_IO.outflow = outflow; G_IO.f50 = f50; G_IO.b77 = b77;
+    G_IO.f56 = f56; G_IO.f60 = f60; G_IO.f61 = f61; G_IO.f62 = f62; G_IO.f64 = f64;
+    G_IO.qi = qi; G_IO.qo = qo;
+}
+
 // xn/yn/zn: node coordinates for index -5 .. n+5 (n+11 values), the same
 // arrays DIVEMesh writes (src/read_grid.cpp:417-433, marge=5).
 // f49 selects reinidisc_f (1) or reinidisc_fsf (0); f44 the reinit
@@ -115,6 +135,10 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     // control flags on this path (defaults src/ini.cpp:400-416)
     p->F30 = 3; p->F35 = 5; p->F40 = 3;
     p->F43 = f43; p->F44 = f44; p->F45 = f45; p->F46 = G_F46; p->F47 = G_F47; p->F49 = f49; p->F50 = 2;
+    if (G_IO.on) {
+        p->F50 = G_IO.f50; p->B60 = 1; p->B77 = G_IO.b77;
+        p->F56 = G_IO.f56; p->F60 = G_IO.f60; p->F61 = G_IO.f61; p->F62 = G_IO.f62; p->F64 = G_IO.f64;
+    }
     p->X45 = 0; p->X48 = 0; p->M10 = 1; p->P12 = 1000000000;
 
     // --- what read_grid() assigns (src/read_grid.cpp:78-300)
@@ -232,7 +256,9 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
         p->gcb4[q][1] = wall[4 * q + 1];
         p->gcb4[q][2] = wall[4 * q + 2];
         p->gcb4[q][3] = wall[4 * q + 3];
-        p->gcb4[q][4] = 21;
+        const int side = wall[4 * q + 3];
+        p->gcb4[q][4] = (G_IO.on && G_IO.inflow && side == 1) ? 1
+                        : (G_IO.on && G_IO.outflow && side == 4) ? 2 : 21;
     }
     p->Iarray(p->gcin, 0, 6); p->Iarray(p->gcout, 0, 6);
     p->Iarray(p->gcin4a, 0, 6); p->Iarray(p->gcout4a, 0, 6);
@@ -297,7 +323,8 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     CONV = new weno_hj_df_nug(p);
     // no patch boundaries: driver::patchBC_logic picks patchBC_void
     // (src/driver_logic_cfd.cpp:661-672)
-    FLOW = new ioflow_v(p, PGC, new patchBC_void(p));
+    if (G_IO.on) FLOW = new ioflow_f(p, PGC, new patchBC_void(p));
+    else FLOW = new ioflow_v(p, PGC, new patchBC_void(p));
     PART = new particle_pls_void();
     REINI = new reini_RK3(p, 0);
     LS = new levelset_RK3(p, A, PGC, HEAT, CONC);
@@ -309,6 +336,11 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     p->count = 1;
     p->dt = 0.0;
     p->Qi = p->Qo = 0.0;  // closed box: no discharge (read by picard_lsm, src/picard_lsm.cpp:95)
+    if (G_IO.on) {
+        p->Qi = G_IO.qi; p->Qo = G_IO.qo;
+        // inflow / outflow cell lists gcin, gcout (src/ioflow_util.cpp:30-81)
+        FLOW->gcio_update(p, A, PGC);
+    }
     return 0;
 }
 
@@ -339,6 +371,12 @@ double refls_psi() { return P->psi; }
 double refls_dxm() { return P->DXM; }
 double refls_volume1() { return P->volume1; }
 double refls_volume2() { return P->volume2; }
+// Water levels of the last ioflow_f::fsfinflow (src/ioflow_waterlevel.cpp:29-141).
+int refls_io_levels(double* out) {
+    out[0] = P->phimean; out[1] = P->phiout;
+    out[2] = P->gcin_count; out[3] = P->gcout_count;
+    return 0;
+}
 
 // Metric arrays as the reference derives them from the node coordinates
 // (src/grid.cpp:55-100): which 0..8 = DXN,DYN,DZN,DXP,DYP,DZP,XP,YP,ZP.
@@ -387,11 +425,12 @@ int refls_reinidisc_L(const double* src, double* L) {
     return 0;
 }
 
-// Ghost fill of a level-set field: ghostcell::start4 with gcv 52
-// (src/gc_start.cpp:146-185).
+// Ghost fill of a level-set field: ghostcell::start4 with the level set's
+// gcv 50+F50 (52 for the default F50 = 2; src/gc_start.cpp:146-185,
+// src/levelset_RK3.cpp:50-60).
 int refls_ghost_fill(double* f) {
     std::memcpy(TMP->V, f, sizeof(double) * ncells_padded());
-    PGC->start4(P, *TMP, 52);
+    PGC->start4(P, *TMP, 50 + P->F50);
     std::memcpy(f, TMP->V, sizeof(double) * ncells_padded());
     return 0;
 }

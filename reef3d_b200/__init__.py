@@ -45,6 +45,19 @@ class GridDesc(ctypes.Structure):
     ]
 
 
+class IoflowDesc(ctypes.Structure):
+    """r3d_ioflow_desc: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags."""
+    _fields_ = [
+        ("inflow", ctypes.c_int), ("outflow", ctypes.c_int), ("f50", ctypes.c_int), ("b77", ctypes.c_int),
+        ("f56", ctypes.c_double), ("f60", ctypes.c_double), ("f61", ctypes.c_double), ("f62", ctypes.c_double),
+        ("f64", ctypes.c_int), ("qi", ctypes.c_double), ("qo", ctypes.c_double),
+    ]
+
+
+# the reference's defaults of those flags (src/ini.cpp:208-441; F50 = 2)
+IOFLOW_DEFAULTS = dict(inflow=1, outflow=1, f50=2, b77=1, f56=1.0e20, f60=-1.0e20, f61=-1.0e20, f62=-1.0e20,
+                       f64=0, qi=0.0, qo=0.0)
+
 _lib = None
 _D = ctypes.POINTER(ctypes.c_double)
 _H = ctypes.c_void_p
@@ -70,6 +83,9 @@ EXPORTS = {
     "r3d_set_velocity_airy": ([_H] + [ctypes.c_double] * 4, ctypes.c_int),
     "r3d_set_fluid": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
+    "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
+    "r3d_io_levels": ([_H, _D, _D], ctypes.c_int),
+    "r3d_set_step_count": ([_H, ctypes.c_longlong], ctypes.c_int),
     "r3d_set_velocity_scale": ([_H, ctypes.c_double], ctypes.c_int),
     "r3d_set_velocity_period": ([_H, ctypes.c_double], ctypes.c_int),
     "r3d_set_time": ([_H, ctypes.c_double], ctypes.c_int),
@@ -265,6 +281,29 @@ class LevelSet:
 
     def set_velocity_scale(self, scale):
         _check(_lib.r3d_set_velocity_scale(self.h, scale), self.h)
+
+    def set_ioflow(self, **flags):
+        """Inflow / outflow faces with ioflow_f's hooks (r3d_set_ioflow):
+        keys of IOFLOW_DEFAULTS, unspecified ones at the reference's
+        defaults.  set_ioflow(off=True) restores the closed box."""
+        if flags.pop("off", False):
+            _check(_lib.r3d_set_ioflow(self.h, None), self.h)
+            return
+        unknown = set(flags) - set(IOFLOW_DEFAULTS)
+        if unknown:
+            raise TypeError(f"unknown ioflow flags {sorted(unknown)}")
+        d = IoflowDesc(**dict(IOFLOW_DEFAULTS, **flags))
+        _check(_lib.r3d_set_ioflow(self.h, ctypes.byref(d)), self.h)
+
+    def io_levels(self):
+        """(phimean, phiout) measured by the last step's fsfinflow."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.r3d_io_levels(self.h, ctypes.byref(a), ctypes.byref(b)), self.h)
+        return a.value, b.value
+
+    def set_step_count(self, count):
+        """lexer::count of the next step."""
+        _check(_lib.r3d_set_step_count(self.h, count), self.h)
 
     def set_velocity_airy(self, amplitude, wavelength, depth, gravity=9.81):
         """Regenerate u, w from the Airy wave at the device clock before every step."""

@@ -106,14 +106,77 @@ inline int gcval_iniphi(const lexer* p) {
     return g;
 }
 
+// Inflow / outflow faces of a run whose flow object is ioflow_f (B60 >= 1,
+// src/driver_logic_cfd.cpp:509-510) for the level-set gcv `gcv`: the
+// device models an inflow boundary on the whole x-min face and an outflow
+// boundary on the whole x-max face, with ioflow_f's hooks
+// (r3d_set_ioflow).  false: closed box (ioflow_v, or gcv 50, whose ghost
+// label is 4 on every face).  iowave and the gravity flow (B90, B180) have
+// relaxation zones and hooks of their own, not on the device.
+inline bool ioflow_desc(const lexer* p, int gcv, r3d_ioflow_desc* d) {
+    if (p->B90 >= 1 || p->B180 == 1 || p->B191 == 1 || p->B192 == 1) {
+        std::cout << "reef3d_b200: iowave / ioflow_gravity level-set hooks are not on the device" << std::endl;
+        std::exit(1);
+    }
+    if (p->B60 < 1 || gcv == 50) return false;
+    const int face = p->knoy * p->knoz;
+    for (int n = 0; n < p->gcin_count; ++n)
+        if (p->gcin[n][3] != 1 || p->gcin_count != face) {
+            std::cout << "reef3d_b200: the device's inflow boundary is the whole x-min face" << std::endl;
+            std::exit(1);
+        }
+    for (int n = 0; n < p->gcout_count; ++n)
+        if (p->gcout[n][3] != 4 || p->gcout_count != face) {
+            std::cout << "reef3d_b200: the device's outflow boundary is the whole x-max face" << std::endl;
+            std::exit(1);
+        }
+    *d = r3d_ioflow_desc{};
+    d->inflow = p->gcin_count > 0 ? 1 : 0;
+    d->outflow = p->gcout_count > 0 ? 1 : 0;
+    if (!d->inflow && !d->outflow) return false;
+    d->f50 = gcv - 50;
+    d->b77 = p->B77;
+    d->f56 = p->F56;
+    d->f60 = p->F60;
+    d->f61 = p->F61;
+    d->f62 = p->F62;
+    d->f64 = p->F64;
+    d->qi = p->Qi;
+    d->qo = p->Qo;
+    return true;
+}
+
+inline bool same_ioflow(const r3d_ioflow_desc& a, const r3d_ioflow_desc& b) {
+    return a.inflow == b.inflow && a.outflow == b.outflow && a.f50 == b.f50 && a.b77 == b.b77 && a.f56 == b.f56 &&
+           a.f60 == b.f60 && a.f61 == b.f61 && a.f62 == b.f62 && a.f64 == b.f64 && a.qi == b.qi && a.qo == b.qo;
+}
+
+// Brings the instance's inflow / outflow configuration and step count
+// (lexer::count, read by the outflow ramp and picard_lsm) up to date.
+struct IoflowState {
+    bool on = false;
+    r3d_ioflow_desc last{};
+    void sync(r3d_handle* h, const lexer* p, int gcv) {
+        r3d_ioflow_desc d{};
+        const bool now = ioflow_desc(p, gcv, &d);
+        if (now != on || (now && !same_ioflow(d, last))) {
+            check(h, r3d_set_ioflow(h, now ? &d : nullptr));
+            on = now;
+            last = d;
+        }
+        check(h, r3d_set_step_count(h, p->count));
+    }
+};
+
 }  // namespace r3d_adapter
 
 // The device writes the interior and the face ghost layers of every field it
 // returns; the adapters then run REEF3D's own ghostcell::start4 on the host
 // copy, which also fills the edge and corner ghosts (dgcpol4) and, in a
 // multi-rank run, exchanges the halo.  (The device step itself knows walls
-// only: a REEF3D run split over several MPI ranks needs one device instance
-// per rank and a halo exchange per stage, which this library does not do.)
+// and the inflow / outflow x faces of ioflow_f only: a REEF3D run split over
+// several MPI ranks needs one device instance per rank and a halo exchange
+// per stage, which this library does not do.)
 
 // freesurface: one level-set step on the device (three WENO5-HJ convection
 // RK stages with the wall ghost fill, F44 reinitialisation pseudo-steps, the
@@ -134,6 +197,7 @@ public:
     void start(fdm* a, lexer* p, convection*, solver*, ghostcell* pgc, ioflow*, reini*, particle_corr*,
                field& ls) override {
         using r3d_adapter::check;
+        io.sync(h, p, r3d_adapter::gcval_phi(p));
         if (!resident || first) check(h, r3d_upload(h, R3D_PHI, ls.V, R3D_LAYOUT_REEF3D));
         first = false;
         check(h, r3d_upload(h, R3D_U, a->u.V, R3D_LAYOUT_REEF3D));
@@ -170,6 +234,7 @@ private:
     r3d_handle* h;
     bool resident;
     bool first = true;
+    r3d_adapter::IoflowState io;
     std::vector<double> buf;
 };
 
@@ -238,6 +303,7 @@ public:
     void start(fdm*, lexer* p, field& f, ghostcell* pgc, ioflow*) override {
         using r3d_adapter::check;
         const int iters = p->count == 0 ? 2 * int(p->maxlength / (p->F43 * p->DXM)) : p->F44;
+        io.sync(h, p, p->count == 0 ? r3d_adapter::gcval_iniphi(p) : r3d_adapter::gcval_phi(p));
         check(h, r3d_upload(h, R3D_PHI, f.V, R3D_LAYOUT_REEF3D));
         check(h, r3d_reinit(h, iters));
         r3d_adapter::download_owned(h, R3D_PHI, p, f, true, buf);
@@ -247,5 +313,6 @@ public:
 
 private:
     r3d_handle* h;
+    r3d_adapter::IoflowState io;
     std::vector<double> buf;
 };

@@ -127,6 +127,7 @@ void release(r3d_handle* h) {
     if (h->S.vmax) cudaFree(h->S.vmax);
     if (h->staging) cudaFree(h->staging);
     if (h->coord) cudaFree(h->coord);
+    if (h->io_buf) cudaFree(h->io_buf);
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaSetDevice(cur);
 }
@@ -175,7 +176,9 @@ struct DeviceGuard {
     ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
 };
 
-bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile; }
+// The tiled kernels fill every face as a wall: instances with inflow /
+// outflow faces run the one-cell-per-thread kernels.
+bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile && !h->io; }
 
 }  // namespace
 
@@ -269,9 +272,19 @@ long long picard_correct(r3d_handle* h) {
 // reini_RK3::start (src/reini_RK3.cpp:84-160): iters pseudo-steps of three
 // stages, inside picard volcalc/correct_ls when f46 == 1 (:92, :140).
 // fuse_volume: the last stage also writes the volume partials.
+// ioflow_f hooks (no-op for the closed box): step = fsfinflow + fsfrkin/out
+// at the start of levelset_RK3::start, else fsfrkin/out alone as at the
+// start of reini_RK3::start.
+long long io_hooks(r3d_handle* h, bool step) {
+    if (!h->io) return 0;
+    return launch_io_hooks(h->L, h->field[R3D_PHI], h->field[R3D_WORK1], h->field[R3D_WORK2], fp32(h), h->iop,
+                           step, h->stream);
+}
+
 long long enqueue_reinit(r3d_handle* h, int iters, bool fuse_volume) {
     long long n = 0;
     if (h->desc.f46 == 1) n += picard_volcalc(h);
+    n += io_hooks(h, false);
     for (int q = 0; q < iters; ++q)
         for (int s = 1; s <= 3; ++s) n += stage_launch(h, true, s, fuse_volume && q == iters - 1 && s == 3);
     if (h->desc.f46 == 1) n += picard_correct(h);
@@ -289,9 +302,11 @@ int enqueue_step(r3d_handle* h) {
     const bool pic = h->desc.f46 != 0 || h->fluid;
     long long n = 0;
     const bool step_picard = h->desc.f46 >= 2;
+    n += io_hooks(h, true);
     if (step_picard) n += picard_volcalc(h);
     for (int s = 1; s <= 3; ++s) n += stage_launch(h, false, s, !pic && f44 == 0 && s == 3);
     n += enqueue_reinit(h, f44, !pic);
+    if (h->desc.f46 == 3 && h->io) n += launch_netvol(h->S, h->iod.qi, h->iod.qo, h->stream);
     if (step_picard) n += picard_correct(h);
     if (h->fluid)
         n += fluid_update(h, true);
@@ -667,6 +682,112 @@ int r3d_set_velocity_scale(r3d_handle* h, double scale) {
     DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_set_scalar(h->S.vscale, scale, h->stream);
     R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+namespace {
+void set_layout_io(r3d_handle* h, int mask) {
+    h->L.io = mask;
+    h->g64.L.io = mask;
+    h->g32.L.io = mask;
+}
+}  // namespace
+
+int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    DeviceGuard dg(h->device, h->batch_stream);
+    if (!io) {
+        drop_step_graph(h);
+        h->io = false;
+        set_layout_io(h, 0);
+        return R3D_OK;
+    }
+    if ((io->inflow != 0 && io->inflow != 1) || (io->outflow != 0 && io->outflow != 1))
+        return fail(h, R3D_EINVAL, "inflow and outflow must be 0 or 1");
+    if (io->f50 < 1 || io->f50 > 4) return fail(h, R3D_EINVAL, "f50 must be 1..4");
+    if (io->b77 != 1 && io->b77 != 2) return fail(h, R3D_EINVAL, "b77 must be 1 or 2");
+    if (io->f64 < 0 || io->f64 > (1 << 24)) return fail(h, R3D_EINVAL, "f64 must be 0..2^24");
+    drop_step_graph(h);
+    // state, ZP (index k + 5), ramp table of the outflow level (F64 > 0)
+    const std::vector<double>& zp = h->M.xp[2];
+    const size_t ramp_at = kIoStateLen + zp.size();
+    const size_t len = ramp_at + (size_t)std::max(io->f64, 1);
+    std::vector<double> host(len, 0.0);
+    if (h->io_buf) {  // keep the step count and levels of an earlier configuration
+        R3D_CUDA(h, cudaMemcpyAsync(host.data(), h->io_buf, kIoStateLen * sizeof(double), cudaMemcpyDeviceToHost,
+                                    h->stream));
+        R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    } else {
+        host[kIoCount] = (double)(h->next_count - 1);
+    }
+    for (size_t t = 0; t < zp.size(); ++t) host[kIoStateLen + t] = zp[t];
+    const double PI_REF = 3.14159265359;  // src/definitions.h:37
+    for (int c = 0; c < io->f64; ++c)  // src/ioflow_waterlevel.cpp:110-111
+        host[ramp_at + c] = 0.5 * std::cos(PI_REF + PI_REF * double(c) / double(io->f64)) + 0.5;
+    if (len > h->io_buf_len) {
+        if (h->io_buf) cudaFree(h->io_buf);
+        h->io_buf = nullptr;
+        h->io_buf_len = 0;
+        if (cudaMalloc(&h->io_buf, len * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            h->io = false;
+            set_layout_io(h, 0);
+            return fail(h, R3D_ENOMEM, "ioflow state allocation failed");
+        }
+        h->io_buf_len = len;
+    }
+    R3D_CUDA(h, cudaMemcpyAsync(h->io_buf, host.data(), len * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->iod = *io;
+    h->io = true;
+    IoParams p{};
+    p.inflow = io->inflow;
+    p.outflow = io->outflow;
+    p.f50 = io->f50;
+    p.b77 = io->b77;
+    p.f64 = io->f64;
+    p.f56 = io->f56;
+    p.f60 = io->f60;
+    p.f62 = io->f62;
+    p.zp = h->io_buf + kIoStateLen;
+    p.dzp = h->g64.dxp[2];
+    p.ramp = h->io_buf + ramp_at;
+    p.state = h->io_buf;
+    h->iop = p;
+    // ghost labels of gcval 50+f50 on the two x faces (src/gc_epol4.cpp:26-58)
+    const int gcv = 50 + io->f50;
+    int mask = 0;
+    if (io->inflow && !(gcv == 52 || gcv == 54)) mask |= kIoSkipLo;
+    if (io->outflow && !(gcv == 51 || gcv == 54 || (gcv == 52 && io->b77 == 1))) mask |= kIoSkipHi;
+    if (io->inflow) mask |= kIoEdge;
+    set_layout_io(h, mask);
+    return R3D_OK;
+}
+
+int r3d_io_levels(r3d_handle* h, double* phimean, double* phiout) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!h->io) return fail(h, R3D_ESTATE, "r3d_set_ioflow has not set inflow/outflow faces");
+    DeviceGuard dg(h->device, h->batch_stream);
+    double v[2] = {0.0, 0.0};
+    R3D_CUDA(h, cudaMemcpyAsync(v, h->io_buf, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (phimean) *phimean = v[kIoPhimean];
+    if (phiout) *phiout = v[kIoPhiout];
+    return R3D_OK;
+}
+
+int r3d_set_step_count(r3d_handle* h, long long count) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (count < 0 || count > (1LL << 50)) return fail(h, R3D_EINVAL, "count out of range");
+    DeviceGuard dg(h->device, h->batch_stream);
+    h->next_count = count;
+    const double c = (double)(count - 1);
+    // picard_lsm's step counter (s.pic[3]) and the hooks' one count the steps taken
+    launch_set_scalar(h->S.pic + 3, c, h->stream);
+    if (h->io_buf) launch_set_scalar(h->io_buf + kIoCount, c, h->stream);
+    h->launches += h->io_buf ? 2 : 1;
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     return R3D_OK;
 }
 

@@ -24,6 +24,13 @@ struct r3d_handle {
     bool airy = false;
     r3d::AiryParams ap{};
     double* coord = nullptr;  // x centres, x faces, z centres, z faces
+    // inflow / outflow faces with ioflow_f's hooks (r3d_set_ioflow)
+    bool io = false;
+    r3d_ioflow_desc iod{};
+    double* io_buf = nullptr;  // hook state, ZP, ramp table (r3d::IoParams)
+    size_t io_buf_len = 0;
+    r3d::IoParams iop{};
+    long long next_count = 1;  // lexer::count of the next step, for r3d_set_ioflow's first state
     int sms = 148;
     double* metrics64 = nullptr;
     float* metrics32 = nullptr;

@@ -55,6 +55,9 @@ __global__ void export_kernel(Layout L, const T* __restrict__ src, int layout, d
 }
 
 // ------------------------------------------------------------- ghost fill
+// ghostcell::start4 with a level-set gcv (src/gc_start.cpp:146-185): the
+// Neumann copy on every face whose ghost label is 4 (all walls; inflow /
+// outflow faces as Layout::io says) and the inflow edge ghost of dgcpol4.
 template <typename T>
 __global__ void ghost_kernel(Layout L, T* f) {
     // one thread per interior cell on any face
@@ -66,9 +69,10 @@ __global__ void ghost_kernel(Layout L, T* f) {
     if (!face) return;
     const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
     const T val = f[c];
+    if ((L.io & kIoEdge) && i == 0 && k == L.nz - 1) f[c - 1 + L.sz] = val;
     for (int q = 1; q <= 3; ++q) {
-        if (i == 0) f[c - q] = val;
-        if (i == L.nx - 1) f[c + q] = val;
+        if (i == 0 && !(L.io & kIoSkipLo)) f[c - q] = val;
+        if (i == L.nx - 1 && !(L.io & kIoSkipHi)) f[c + q] = val;
         if (!L.two_d && j == 0) f[c - q * L.sy] = val;
         if (!L.two_d && j == L.ny - 1) f[c + q * L.sy] = val;
         if (k == 0) f[c - q * L.sz] = val;
@@ -445,7 +449,173 @@ void picard_pass(const Layout& L, void* phi, bool fp32, double epsi, double cell
     else picard_pass<double, SHIFT, SUM>(L, phi, epsi, cellvol, s, st);
 }
 
+// --------------------------------------------------------- ioflow hooks
+constexpr int kIoThreads = 1024;
+
+// Zero-crossing water level of column i over the face's cells
+// (src/ioflow_waterlevel.cpp:48-58 inflow, :84-91 outflow): a cell counts
+// when phi(i,j,k) >= 0 > phi(i,j,k+1), with the height
+//     -(phi(i,j,k) DZP[k]) / (phi(i,j,k+1) - phi(i,j,k)) + ZP[k].
+// The cells are visited in the order of the reference's boundary list
+// (j outer, k inner); every thread forms the height of one cell, the block
+// compacts the crossings in that order and thread 0 adds them one by one,
+// so the FP64 sum rounds exactly as the reference's loop does.  zval is
+// valid in thread 0, count in every thread.
+template <typename T>
+__device__ void crossing_sum(const Layout& L, const T* __restrict__ phi, int i, const IoParams& p, double& zval,
+                             int& count) {
+    __shared__ double vals[kIoThreads];
+    __shared__ int wc[kIoThreads / 32];
+    const int n = L.ny * L.nz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    zval = 0.0;
+    count = 0;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int e = base + threadIdx.x;
+        bool hit = false;
+        double h = 0.0;
+        if (e < n) {
+            const int j = e / L.nz, k = e - j * L.nz;
+            const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+            const double a = static_cast<double>(phi[c]), b = static_cast<double>(phi[c + L.sz]);
+            if (a >= 0.0 && b < 0.0) {
+                hit = true;
+                h = -(a * p.dzp[k + 5]) / (b - a) + p.zp[k + 5];
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) wc[warp] = __popc(m);
+        __syncthreads();
+        int off = __popc(m & ((1u << lane) - 1u)), total = 0;
+        for (int w = 0; w < nwarp; ++w) {
+            if (w < warp) off += wc[w];
+            total += wc[w];
+        }
+        if (hit) vals[off] = h;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int q = 0; q < total; ++q) zval += vals[q];
+        count += total;
+        __syncthreads();
+    }
+}
+
+// ioflow_f::fsfinflow, the measuring half (src/ioflow_waterlevel.cpp:29-125):
+// advances the step count (lexer::count of this step), sets phimean from
+// F56/F60 or the inflow crossings, phiout from F60/F62 or the outflow
+// crossings, and the outflow level wsfout (F62, or its ramp from F60 over
+// F64 steps).  One block.
+template <typename T>
+__global__ void __launch_bounds__(kIoThreads) io_level_kernel(Layout L, const T* __restrict__ phi, IoParams p) {
+    double* st = p.state;
+    double phimean = p.f56, phiout = st[kIoPhiout];
+    if (p.f60 > -1.0e20) {
+        phimean = p.f60;
+        phiout = p.f60;
+    }
+    if (p.f62 > -1.0e20) phiout = p.f62;
+    double zval = 0.0;
+    int count = 0, found = 0;
+    if (p.inflow) {
+        crossing_sum(L, phi, -1, p, zval, count);
+        if (count > 0) {
+            phimean = zval / static_cast<double>(count);
+            found = 1;
+        }
+    }
+    if (p.outflow) {
+        crossing_sum(L, phi, L.nx - 1, p, zval, count);
+        if (count > 0) phiout = zval / static_cast<double>(count);
+    }
+    if (threadIdx.x != 0) return;
+    const double cnt = st[kIoCount] + 1.0;
+    double wsfout = phimean;
+    if (p.f62 > 1.0e-20) {
+        if (p.f64 == 0) wsfout = p.f62;
+        if (p.f64 > 0) {
+            // f = 0.5 cos(PI + PI count/F64) + 0.5 below F64 (tabulated on the host)
+            const double f = cnt < static_cast<double>(p.f64) ? p.ramp[static_cast<int>(cnt)] : 1.0;
+            wsfout = f * p.f62 + (1.0 - f) * p.f60;
+        }
+    }
+    st[kIoCount] = cnt;
+    st[kIoPhimean] = phimean;
+    st[kIoPhiout] = phiout;
+    st[kIoWsfout] = wsfout;
+    st[kIoFound] = found;
+}
+
+// The imposing half of fsfinflow (step == 1): inflow ghosts of phi =
+// phimean - ZP when a crossing was found and F50 is 2 or 4 (:60-73),
+// outflow ghosts = wsfout - ZP with F62 set and B77 = 2 (:119-130).  Then
+// fsfrkin / fsfrkout (:143-177) on both RK buffers: inflow ghosts copy
+// phi's, outflow ghosts copy phi's or hold F62 - ZP (F62 set, B77 = 2).
+// One thread per (j,k) of the x faces.
+template <typename T>
+__global__ void __launch_bounds__(256) io_ghost_kernel(Layout L, T* __restrict__ phi, T* __restrict__ a1,
+                                                       T* __restrict__ a2, IoParams p, int step) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= L.ny * L.nz) return;
+    const int j = e / L.nz, k = e - j * L.nz;
+    const double zc = p.zp[k + 5];
+    const long long row = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + L.gx;
+    if (p.inflow) {
+        if (step && p.state[kIoFound] != 0.0 && (p.f50 == 2 || p.f50 == 4)) {
+            const T v = static_cast<T>(p.state[kIoPhimean] - zc);
+            for (int q = 1; q <= 3; ++q) phi[row - q] = v;
+        }
+        for (int q = 1; q <= 3; ++q) {
+            const T v = phi[row - q];
+            a1[row - q] = v;
+            a2[row - q] = v;
+        }
+    }
+    if (p.outflow) {
+        const long long c = row + L.nx - 1;
+        const bool fixed = p.f62 > -1.0e20 && p.b77 == 2;
+        if (step && fixed) {
+            const T v = static_cast<T>(p.state[kIoWsfout] - zc);
+            for (int q = 1; q <= 3; ++q) phi[c + q] = v;
+        }
+        for (int q = 1; q <= 3; ++q) {
+            const T v = fixed ? static_cast<T>(p.f62 - zc) : phi[c + q];
+            a1[c + q] = v;
+            a2[c + q] = v;
+        }
+    }
+}
+
+// picard_lsm::correct_ls's target update netvol = netvol + Qi dt - Qo dt
+// (src/picard_lsm.cpp:93), before its iterations.
+__global__ void netvol_kernel(double* pic, const double* dt, double qi, double qo) {
+    pic[2] = pic[2] + qi * *dt - qo * *dt;
+}
+
 }  // namespace
+
+int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, bool step,
+                    cudaStream_t st) {
+    const int rows = L.ny * L.nz;
+    const int blocks = (rows + 255) / 256;
+    int n = 0;
+    if (step) {
+        if (fp32) io_level_kernel<float><<<1, kIoThreads, 0, st>>>(L, static_cast<const float*>(phi), p);
+        else io_level_kernel<double><<<1, kIoThreads, 0, st>>>(L, static_cast<const double*>(phi), p);
+        ++n;
+    }
+    if (fp32)
+        io_ghost_kernel<float><<<blocks, 256, 0, st>>>(L, static_cast<float*>(phi), static_cast<float*>(a1),
+                                                       static_cast<float*>(a2), p, step ? 1 : 0);
+    else
+        io_ghost_kernel<double><<<blocks, 256, 0, st>>>(L, static_cast<double*>(phi), static_cast<double*>(a1),
+                                                        static_cast<double*>(a2), p, step ? 1 : 0);
+    return n + 1;
+}
+
+int launch_netvol(const Scratch& s, double qi, double qo, cudaStream_t st) {
+    netvol_kernel<<<1, 1, 0, st>>>(s.pic, s.dt, qi, qo);
+    return 1;
+}
 
 size_t airy_smem_bytes(const Layout& L) { return (size_t)(2 * (L.nx + 6) + 2 * (L.nz + 6)) * sizeof(double); }
 

@@ -67,8 +67,11 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, Stag
         else if (STAGE == 2) val = 0.75f * fn + 0.25f * (__ldg(a.fs + c) + dtc * Lc);
         else val = (1.0f / 3.0f) * fn + (2.0f / 3.0f) * (__ldg(a.fs + c) + dtc * Lc);
         a.out[c] = val;
-        if (i == 0) { a.out[c - 1] = val; a.out[c - 2] = val; a.out[c - 3] = val; }
-        if (i == g.L.nx - 1) { a.out[c + 1] = val; a.out[c + 2] = val; a.out[c + 3] = val; }
+        // x faces: inflow / outflow faces with ghost label 0 keep their
+        // ghosts; an inflow face also gets the edge ghost (-1, j, nz)
+        if (i == 0 && !(g.L.io & kIoSkipLo)) { a.out[c - 1] = val; a.out[c - 2] = val; a.out[c - 3] = val; }
+        if (i == g.L.nx - 1 && !(g.L.io & kIoSkipHi)) { a.out[c + 1] = val; a.out[c + 2] = val; a.out[c + 3] = val; }
+        if ((g.L.io & kIoEdge) && i == 0 && k == g.L.nz - 1) a.out[c - 1 + g.L.sz] = val;
         if (!TWO_D) {
             const long long sy = g.L.sy;
             if (j == 0) { a.out[c - sy] = val; a.out[c - 2 * sy] = val; a.out[c - 3 * sy] = val; }

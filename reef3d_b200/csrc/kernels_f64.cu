@@ -39,11 +39,15 @@ __device__ __forceinline__ void cell_of_thread(const Layout& L, bool two_d, int&
 }
 
 // Wall ghost copy of the cell value into the three face ghost layers
-// (src/gc_neumann.cpp:29-54; 2D skips y, src/gc_start.cpp:160).
+// (src/gc_neumann.cpp:29-54; 2D skips y, src/gc_start.cpp:160).  Inflow /
+// outflow x faces whose ghost label is 0 keep their ghosts; with an inflow
+// face the top inflow cell also fills the edge ghost (-1, j, nz) as
+// dgcpol4 does (src/gc_dgcpol4.cpp:28-50).
 template <typename T>
 __device__ __forceinline__ void write_ghosts(const Layout& L, T* out, long long c, int i, int j, int k, T val) {
-    if (i == 0) { out[c - 1] = val; out[c - 2] = val; out[c - 3] = val; }
-    if (i == L.nx - 1) { out[c + 1] = val; out[c + 2] = val; out[c + 3] = val; }
+    if (i == 0 && !(L.io & kIoSkipLo)) { out[c - 1] = val; out[c - 2] = val; out[c - 3] = val; }
+    if (i == L.nx - 1 && !(L.io & kIoSkipHi)) { out[c + 1] = val; out[c + 2] = val; out[c + 3] = val; }
+    if ((L.io & kIoEdge) && i == 0 && k == L.nz - 1) out[c - 1 + L.sz] = val;
     if (!L.two_d) {
         if (j == 0) { out[c - L.sy] = val; out[c - 2 * L.sy] = val; out[c - 3 * L.sy] = val; }
         if (j == L.ny - 1) { out[c + L.sy] = val; out[c + 2 * L.sy] = val; out[c + 3 * L.sy] = val; }

@@ -26,7 +26,14 @@ struct Layout {
     long long sy, sz;
     long long ncell;  // px*py*pz
     bool two_d;
+    // inflow / outflow faces (0 for the closed box): kIoSkipLo / kIoSkipHi
+    // leave the x-min / x-max face ghosts of a level-set field untouched
+    // (ghost label 0 of src/gc_epol4.cpp:26-58); kIoEdge also writes the
+    // edge ghost (-1, j, nz) of each inflow column, which the inflow water
+    // level reads (src/ioflow_waterlevel.cpp:55)
+    int io;
 };
+constexpr int kIoSkipLo = 1, kIoSkipHi = 2, kIoEdge = 4;
 
 Layout make_layout(int nx, int ny, int nz);
 
@@ -159,6 +166,26 @@ int launch_volume_direct_clock(const Layout& L, const void* phi, bool fp32, cons
 int launch_cfl(const Layout& L, const void* u, const void* v, const void* w, bool fp32,
                double dxmin, double n47, const Scratch& s, cudaStream_t st);
 int launch_ghost_fill(const Layout& L, void* f, bool fp32, cudaStream_t st);
+
+// ioflow_f level-set hooks (src/ioflow_waterlevel.cpp:29-177) on an
+// inflow x-min face and an outflow x-max face.
+struct IoParams {
+    int inflow, outflow;  // faces present
+    int f50, b77, f64;
+    double f56, f60, f62;
+    const double* zp;     // cell-centre z (ZP), index k + 5
+    const double* dzp;    // centre spacing (DZP), index k + 5
+    const double* ramp;   // outflow level ramp for count = 0 .. f64-1
+    double* state;        // kIo* slots below
+};
+constexpr int kIoPhimean = 0, kIoPhiout = 1, kIoCount = 2, kIoWsfout = 3, kIoFound = 4, kIoStateLen = 8;
+// fsfinflow: advances the step count, measures the water levels, imposes
+// the inflow / outflow ghosts of phi; then fsfrkin/fsfrkout on a1 and a2.
+// step == false: fsfrkin/fsfrkout only (the start of reini_RK3::start).
+int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, bool step,
+                    cudaStream_t st);
+// picard_lsm's netvol = netvol + Qi dt - Qo dt (src/picard_lsm.cpp:93)
+int launch_netvol(const Scratch& s, double qi, double qo, cudaStream_t st);
 // host layout <-> device layout (src is a device staging copy of the host array)
 int launch_import(const Layout& L, const double* staging, int layout, void* dst, bool fp32,
                   cudaStream_t st);

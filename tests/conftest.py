@@ -29,6 +29,14 @@ def golden_flags(g):
                 n47=float(g["n47"]), f46=int(g.get("f46", 0)), f47=int(g.get("f47", 10)))
 
 
+def golden_ioflow(g):
+    """Inflow / outflow flags of an io golden case (None for a closed box)."""
+    if "io_f50" not in g:
+        return None
+    ints = ("inflow", "outflow", "f50", "b77", "f64")
+    return {k[3:]: (int(g[k]) if k[3:] in ints else float(g[k])) for k in g if k.startswith("io_")}
+
+
 @pytest.fixture(scope="session")
 def port_lib():
     """The C restatement oracle, built on demand (test infrastructure)."""

@@ -14,7 +14,10 @@ short trajectory with the time step recomputed before every step) and the
 volume sums after it, with the density and viscosity fields the step's
 fluid update wrote.  The picard cases run with the mass correction on
 (f46 = 1 in the reinitialisation, f46 = 2 around the step, f46 = 3 the
-picard_lsm form that keeps the first step's volume; f47 iterations).
+picard_lsm form that keeps the first step's volume; f47 iterations).  The
+io cases open the x-min face as an inflow and the x-max face as an outflow
+boundary with the reference's ioflow_f (B60 = 1) and record the water
+levels its fsfinflow measured at every step.
 """
 import math
 import multiprocessing as mp
@@ -61,6 +64,30 @@ def random_case(name, nx, ny, nz, f49, stretch, seed, f46=0, f47=10):
                 f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.125, steps=1, vel_scale=None, f46=f46, f47=f47)
 
 
+def tank_case(name, nx, ny, nz, f49, stretch, seed, steps, io, level=0.5, f46=0, f47=10):
+    """A still-water tank with a wavy free surface phi = level + waves - z
+    (not a distance: the reinitialisation moves it) and a random mean flow
+    towards the outflow, for the inflow / outflow hooks."""
+    rng = np.random.default_rng(seed)
+    xn, yn, zn = stretched(nx, stretch), stretched(ny, stretch), stretched(nz, stretch)
+    shape = (nx + 6, ny + 6, nz + 6)
+    ii = 0.5 * (xn[2:-3] + xn[3:-2])
+    jj = 0.5 * (yn[2:-3] + yn[3:-2])
+    kk = 0.5 * (zn[2:-3] + zn[3:-2])
+    X, Y, Z = np.meshgrid(ii, jj, kk, indexing="ij")
+    phi = level + 0.05 * np.cos(2 * np.pi * X) + (0.02 * np.sin(2 * np.pi * Y) if ny > 1 else 0.0) - Z
+    phi = phi + 0.003 * rng.standard_normal(shape)
+    if ny == 1:
+        phi[:, :3, :] = 0.0
+        phi[:, 4:, :] = 0.0
+    u = 0.3 + 0.1 * rng.standard_normal(shape)
+    v = 0.1 * rng.standard_normal(shape)
+    w = 0.05 * np.sin(2 * np.pi * X) + 0.02 * rng.standard_normal(shape)
+    return dict(name=name, nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w,
+                f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.25, steps=steps, vel_scale=None, f46=f46, f47=f47,
+                io=io)
+
+
 def setup_case(name, which, n, steps, f46=0, f47=10):
     from reef3d_b200 import setups
     c = setups.slotted_disk(n) if which == "disk" else setups.vortex3d(n)
@@ -81,6 +108,16 @@ CASES = [
     lambda: setup_case("picard2_vortex3d_n12_3steps", "vortex", 12, 3, f46=2, f47=10),
     lambda: setup_case("picard1_slotted2d_n24_3steps", "disk", 24, 3, f46=1, f47=4),
     lambda: setup_case("picard3_vortex3d_n12_3steps", "vortex", 12, 3, f46=3, f47=10),
+    lambda: tank_case("io_tank3d_f50_2", 20, 6, 16, 1, 0.0, 11, 4, dict(f50=2, b77=1)),
+    lambda: tank_case("io_tank2d_f50_2_b77_2_ramp", 24, 1, 18, 0, 0.0, 12, 4,
+                      dict(f50=2, b77=2, f60=0.5, f62=0.52, f64=3)),
+    lambda: tank_case("io_tank3d_f50_3_lsm_discharge", 18, 5, 14, 1, 0.3, 13, 4,
+                      dict(f50=3, b77=2, f62=0.53, qi=0.01, qo=0.02), f46=3, f47=4),
+    lambda: tank_case("io_tank3d_f50_4_top_edge", 16, 5, 16, 0, 0.0, 14, 3, dict(f50=4), level=0.955),
+    lambda: tank_case("io_tank2d_f50_1_outflow_only", 22, 1, 16, 1, 0.3, 15, 3,
+                      dict(f50=1, inflow=0, b77=2, f62=-0.1)),
+    lambda: tank_case("io_tank3d_inflow_only_picard2", 16, 6, 14, 1, 0.0, 16, 3,
+                      dict(f50=2, outflow=0), f46=2, f47=3),
 ]
 
 
@@ -88,8 +125,9 @@ def run_case(idx):
     from oracle.bindings import RefOracle
     c = CASES[idx]()
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
+    io = c.get("io")
     ref = RefOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                    f49=c["f49"], f46=c["f46"], f47=c["f47"])
+                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io)
     out = {k: c[k] for k in ("nx", "ny", "nz", "xn", "yn", "zn", "phi", "u", "v", "w", "f43", "f44", "f45",
                               "f49", "n47", "steps", "f46", "f47")}
     for a, n in enumerate((nx, ny, nz)):
@@ -97,6 +135,10 @@ def run_case(idx):
         out[f"qf{a}"], out[f"cf{a}"], out[f"isf{a}"] = qf, cf, isf
         for w, name in ((a, "dxn"), (a + 3, "dxp")):
             out[f"{name}{a}"] = ref.metric(w, n + 11)
+    if io is not None:
+        from oracle.bindings import IOFLOW_DEFAULTS
+        for k, val in dict(IOFLOW_DEFAULTS, **io).items():
+            out["io_" + k] = val
     out["psi"] = ref.psi
     out["vel_scale"] = np.array(c["vel_scale"] or "none")
     phi, u, v, w = c["phi"], c["u"], c["v"], c["w"]
@@ -106,7 +148,7 @@ def run_case(idx):
     out["ghost"] = ref.ghost_fill(phi)
     T = 3.0
     t = 0.0
-    traj, dts, vols, ros, viscs = [], [], [], [], []
+    traj, dts, vols, ros, viscs, levels = [], [], [], [], [], []
     for s in range(c["steps"]):
         if c["vel_scale"] == "vortex":
             f = math.cos(math.pi * t / T)
@@ -119,6 +161,7 @@ def run_case(idx):
         ros.append(ref.get_field(6))   # fluid_update_fsf inside the step (W1..W4 defaults)
         viscs.append(ref.get_field(7))
         traj.append(ph)
+        levels.append(ref.io_levels())
         dts.append(dt)
         vols.append(ref.volume())
         t += dt
@@ -127,6 +170,8 @@ def run_case(idx):
     out["step_volume"] = np.array(vols)
     out["step_ro"] = np.array(ros)
     out["step_visc"] = np.array(viscs)
+    if io is not None:
+        out["step_io_levels"] = np.array(levels)
     np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), **out)
     return c["name"]
 

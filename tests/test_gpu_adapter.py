@@ -4,7 +4,9 @@ lexer / fdm / ghostcell objects (oracle/_ref/libreef3d_adapter.so): in one
 process, each reference object (levelset_RK3, weno_hj_df_nug, reinidisc_f /
 reinidisc_fsf, reini_RK3, fluid_update_fsf) and the adapter that replaces it
 start from the same REEF3D fields, and the fields they leave behind are
-compared.  FP64: the level set and the operators bit-identical on every cell
+compared (the tank_io cases with the reference's ioflow_f inflow / outflow
+boundaries, which the adapters hand to r3d_set_ioflow).  FP64: the level
+set and the operators bit-identical on every cell
 (ghost layers included: the adapters finish with REEF3D's own
 ghostcell::start4), volumes, density and viscosity within 1e-12 relative
 (summation order, sin); with the picard correction, whose shift comes from
@@ -40,6 +42,22 @@ def _case(name):
         c = setups.slotted_disk(24)
         return dict(nx=24, ny=1, nz=24, xn=c.xn, yn=c.yn, zn=c.zn, phi=c.phi, u=c.u, v=c.v, w=c.w,
                     f43=c.f43, f44=c.f44, f45=c.f45, f49=1, n47=c.n47, f46=0)
+    if name.startswith("tank_io"):
+        # inflow / outflow faces with ioflow_f (B60 = 1): wavy free surface
+        rng = np.random.default_rng(6)
+        nx, ny, nz = (16, 5, 14) if name == "tank_io3d" else (20, 1, 16)
+        xn, yn, zn = _stretched(nx, 0.0), _stretched(ny, 0.0), _stretched(nz, 0.0)
+        c = lambda a: 0.5 * (a[2:-3] + a[3:-2])
+        X, Y, Z = np.meshgrid(c(xn), c(yn), c(zn), indexing="ij")
+        phi = np.ascontiguousarray(0.5 + 0.05 * np.cos(2 * np.pi * X) - Z + 0.003 * rng.standard_normal(X.shape))
+        if ny == 1:
+            phi[:, :3, :] = 0.0
+            phi[:, 4:, :] = 0.0
+        u = np.ascontiguousarray(0.3 + 0.1 * rng.standard_normal(phi.shape))
+        v, w = (np.ascontiguousarray(0.05 * rng.standard_normal(phi.shape)) for _ in range(2))
+        io = dict(f50=2, b77=2, f60=0.5, f62=0.52, f64=2) if ny > 1 else dict(f50=3, b77=1)
+        return dict(nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w, f43=0.5, f44=2, f45=2.1,
+                    f49=1, n47=0.25, f46=0, io=io)
     # random 3D case on a stretched grid, F49 = 0 (reinidisc_fsf) or picard
     rng = np.random.default_rng(4)
     nx, ny, nz = 11, 9, 10
@@ -70,7 +88,7 @@ def _run(name, precision=0):
     c = _case(name)
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                       f49=c["f49"], f46=c["f46"], f47=6, precision=precision)
+                       f49=c["f49"], f46=c["f46"], f47=6, precision=precision, ioflow=c.get("io"))
     out = {}
     ao.set_state(c["phi"], c["u"], c["v"], c["w"])
     out["weno_L"] = bool(np.array_equal(_interior(ao.weno_L(c["phi"]), nx, ny, nz),
@@ -112,7 +130,8 @@ def _run(name, precision=0):
     return out
 
 
-@pytest.mark.parametrize("name", ["vortex3d", "disk2d", "stretched_f49_0", "stretched_picard"])
+@pytest.mark.parametrize("name", ["vortex3d", "disk2d", "stretched_f49_0", "stretched_picard", "tank_io3d",
+                                  "tank_io2d"])
 def test_adapters_match_reference_objects(name):
     from oracle.bindings import AdapterOracle
     if not AdapterOracle.available():

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import reef3d_b200 as r3d
-from conftest import GOLDEN_CASES, golden_flags, load_golden, velocity_at
+from conftest import GOLDEN_CASES, golden_flags, golden_ioflow, load_golden, velocity_at
 from test_oracle_golden import interior, visible_mask
 
 pytestmark = pytest.mark.gpu
@@ -25,8 +25,16 @@ def relmax(a, b):
 
 
 def make_gpu(g, precision=r3d.FP64):
-    return r3d.LevelSet(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], precision=precision,
-                        **golden_flags(g))
+    ls = r3d.LevelSet(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], precision=precision,
+                      **golden_flags(g))
+    io = golden_ioflow(g)
+    if io is not None:  # inflow / outflow faces with ioflow_f's hooks
+        ls.set_ioflow(**io)
+    return ls
+
+
+def levels_close(got, ref):
+    return all(a == b or abs(a - b) <= RTOL * abs(b) for a, b in zip(got, ref))
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -70,6 +78,8 @@ def test_steps_vs_reference(name):
             v1, v2 = ls.last_volume()
             rv1, rv2 = g["step_volume"][s]
             assert abs(v1 - rv1) <= RTOL * abs(rv1) and abs(v2 - rv2) <= RTOL * abs(rv2)
+            if "step_io_levels" in g:  # water levels measured by fsfinflow
+                assert levels_close(ls.io_levels(), g["step_io_levels"][s]), (s, ls.io_levels())
             t += dt
 
 

@@ -5,7 +5,7 @@ layers; edge and corner ghosts are outside every stencil of the path)."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, golden_flags, load_golden, velocity_at
+from conftest import GOLDEN_CASES, golden_flags, golden_ioflow, load_golden, velocity_at
 
 
 def visible_mask(nx, ny, nz):
@@ -23,7 +23,8 @@ def interior(a, nx, ny, nz):
 @pytest.fixture(params=GOLDEN_CASES)
 def case(request, port_lib):
     g = load_golden(request.param)
-    o = port_lib(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], **golden_flags(g))
+    o = port_lib(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], ioflow=golden_ioflow(g),
+                 **golden_flags(g))
     return g, o
 
 
@@ -63,6 +64,8 @@ def test_steps_dt_volume(case):
         phi = o.step(phi, u, v, w, dt)
         assert np.array_equal(phi[m], g["step_phi"][s][m])
         assert o.volume(phi) == tuple(g["step_volume"][s])
+        if "step_io_levels" in g:
+            assert o.io_levels() == tuple(g["step_io_levels"][s])
         ro, visc = o.fluid(phi)
         assert np.array_equal(ro[m], g["step_ro"][s][m]) and np.array_equal(visc[m], g["step_visc"][s][m])
         t += dt
