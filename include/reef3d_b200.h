@@ -44,6 +44,8 @@ extern "C" {
 #define R3D_WORK2 6      /* RK stage buffer (ark2 / frk2) */
 #define R3D_RO 7         /* a->ro, density (exists once r3d_set_fluid enabled it) */
 #define R3D_VISC 8       /* a->visc, kinematic viscosity (likewise) */
+#define R3D_BODY 9       /* body field of the direct-forcing stencils (exists once
+                            r3d_set_direct_forcing enabled them) */
 
 /* host array layouts for upload/download */
 #define R3D_LAYOUT_REEF3D 0  /* the reference's padded field: (nx+6)(ny+6)(nz+6) doubles,
@@ -185,6 +187,23 @@ int r3d_set_velocity_period(r3d_handle* h, double period);
  * velocity factor set to 1.  wavelength <= 0 turns the generator off.
  * Synchronous.  Not for batch members. */
 int r3d_set_velocity_airy(r3d_handle* h, double amplitude, double wavelength, double depth, double gravity);
+/* Direct-forcing variant of the level-set convection stencils (control
+ * flag X45, src/weno_hj_df_nug.cpp:115-342 selecting :398-987): the five
+ * divided differences of each WENO5 stencil are masked or weighted by a
+ * body field at the two cells of each difference --
+ *   X45 1: zero unless |fb| > 0.6 DXM at both cells        (body = a->fb)
+ *       2: times 0.5 (fbh5 + fbh5) of the two cells         (body = a->fbh5)
+ *       3: zero unless fbh4 < 0.5 at both                   (body = a->fbh4)
+ *       4: times fbh5 of the upwind-most cell of the pair   (body = a->fbh5)
+ *       5: zero unless solid > 0 and topo > 0 at both       (body = min(a->solid, a->topo))
+ *       6: as 3, but 1e20 where masked                      (body = a->fbh4)
+ * The body field is R3D_BODY, allocated (zeroed) by the first call with
+ * x45 != 0 and uploaded like any field (REEF3D layout: its ghost cells are
+ * read too).  The reinitialisation is unchanged (the reference applies X45
+ * to the convection only).  FP64 instances only; 0 turns it off.
+ * Synchronous.  Not for batch members. */
+int r3d_set_direct_forcing(r3d_handle* h, int x45);
+
 /* Inflow and outflow boundaries with the level-set hooks of REEF3D's
  * ioflow_f (B60 >= 1, src/driver_logic_cfd.cpp:509-510), which the
  * closed box's ioflow_v leaves void.  The x-min face becomes an inflow

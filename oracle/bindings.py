@@ -83,6 +83,7 @@ class PortOracle:
                                            + [ctypes.c_double] * 2)
             lib.lso_io_levels.argtypes = [ctypes.c_void_p, _D]
             lib.lso_set_count.argtypes = [ctypes.c_void_p, _I]
+            lib.lso_set_direct_forcing.argtypes = [ctypes.c_void_p, _I, _D, _D]
             cls._lib = lib
         return cls._lib
 
@@ -103,6 +104,13 @@ class PortOracle:
         if ioflow is not None:
             io = dict(IOFLOW_DEFAULTS, **ioflow)
             self._lib.lso_set_ioflow(self.h, *(io[k] for k in IOFLOW_KEYS))
+
+    def set_direct_forcing(self, x45, body1, body2=None):
+        """X45 stencils reading body1 (fb, fbh5, fbh4 or solid) and body2
+        (topo, X45 = 5), padded fields."""
+        self._body = [np.ascontiguousarray(body1, dtype=np.float64),
+                      np.ascontiguousarray(body2 if body2 is not None else body1, dtype=np.float64)]
+        self._lib.lso_set_direct_forcing(self.h, x45, _dp(self._body[0]), _dp(self._body[1]))
 
     def io_levels(self):
         """(phimean, phiout) after the last step's fsfinflow."""
@@ -194,7 +202,7 @@ class RefOracle:
     _loaded = set()
 
     def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10,
-                 path=None, ioflow=None):
+                 path=None, ioflow=None, x45=0):
         """ioflow: None for the closed box, else a dict of IOFLOW_DEFAULTS'
         keys: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags."""
         path = path or (REF_LIB_FAST if fast else REF_LIB)
@@ -204,6 +212,8 @@ class RefOracle:
         lib = ctypes.CDLL(path)
         lib.refls_set_picard.argtypes = [_I, _I]
         lib.refls_set_picard(f46, f47)
+        lib.refls_set_x45.argtypes = [_I]
+        lib.refls_set_x45(x45)
         if ioflow is not None:
             io = dict(IOFLOW_DEFAULTS, **ioflow)
             lib.refls_set_ioflow.argtypes = [_I, _I, _I, _I] + [ctypes.c_double] * 4 + [_I] + [ctypes.c_double] * 2

@@ -221,6 +221,53 @@ static double weno_deriv(const double* f, long c, long s, const double* dp, cons
     return weno_axis(qf, cf, isf, t, plus, q1, q2, q3, q4, q5);
 }
 
+/* Direct-forcing divided difference of the cell pair (a, b = a + s) of the
+ * X45 stencils (src/weno_hj_df_nug.cpp:398-987; the i, j, k variants and
+ * both sides follow one rule per X45): 1 zero unless |fb| > 0.6 DXM at both
+ * cells, 2 weighted by the mean fbh5 of the pair, 3 zero unless fbh4 < 0.5
+ * at both, 4 weighted by fbh5 at the cell `w` (the pair's lower cell on the
+ * minus side, its upper cell on the plus side), 5 zero unless solid > 0 and
+ * topo > 0 at both, 6 like 3 but 1e20 where masked. */
+static double df_q(const lso_grid* g, const double* f, long a, long b, long w, double d) {
+    const double* h = g->body1;
+    switch (g->x45) {
+        case 1:
+            if (fabs(h[b]) > 0.6 * g->dxm_mean && fabs(h[a]) > 0.6 * g->dxm_mean) return (f[b] - f[a]) / d;
+            return 0.0;
+        case 2: return 0.5 * (h[b] + h[a]) * (f[b] - f[a]) / d;
+        case 3:
+            if (h[b] < 0.5 && h[a] < 0.5) return (f[b] - f[a]) / d;
+            return 0.0;
+        case 4: return (h[w]) * (f[b] - f[a]) / d;
+        case 5:
+            if (h[b] > 0.0 && g->body2[b] > 0.0 && h[a] > 0.0 && g->body2[a] > 0.0) return (f[b] - f[a]) / d;
+            return 0.0;
+        case 6:
+            if (h[b] < 0.5 && h[a] < 0.5) return (f[b] - f[a]) / d;
+            return 1.0e20;
+        default: return (f[b] - f[a]) / d;
+    }
+}
+
+/* weno_deriv with the X45 differences: q_m from the pair (m-1, m) of the
+ * six upwind points. */
+static double weno_deriv_df(const lso_grid* g, const double* f, long c, long s, const double* dp, const double* qf,
+                            const double* cf, const double* isf, int t, int plus) {
+    const int o = plus ? -2 : -3;
+    double q[5];
+    for (int m = 1; m <= 5; ++m) {
+        const long a = c + (o + m - 1) * s, b = c + (o + m) * s;
+        q[m - 1] = df_q(g, f, a, b, plus ? b : a, dp[t + o + m - 1]);
+    }
+    return weno_axis(qf, cf, isf, t, plus, q[0], q[1], q[2], q[3], q[4]);
+}
+
+void lso_set_direct_forcing(lso_grid* g, int x45, const double* body1, const double* body2) {
+    g->x45 = x45;
+    g->body1 = body1;
+    g->body2 = body2;
+}
+
 /* ------------------------------------------------------------- convection
  * src/weno_hj_df_nug.cpp:84-111 (ipol 4) with the cell-centre velocities of
  * src/flux_HJ_CDS2.cpp:59-64,90-95,122-127 (2D: src/flux_HJ_CDS2_2D.cpp,
@@ -228,6 +275,7 @@ static double weno_deriv(const double* f, long c, long s, const double* dp, cons
 void lso_weno_L(const lso_grid* g, const double* phi, const double* u, const double* v,
                 const double* w, double* L) {
     const long si = (long)g->jmax * g->kmax, sj = g->kmax, sk = 1;
+#define DERIV(...) (g->x45 ? weno_deriv_df(g, __VA_ARGS__) : weno_deriv(__VA_ARGS__))
     for (int i = 0; i < g->nx; ++i)
         for (int j = 0; j < g->ny; ++j)
             for (int k = 0; k < g->nz; ++k) {
@@ -237,22 +285,23 @@ void lso_weno_L(const lso_grid* g, const double* phi, const double* u, const dou
                 const double kadvec = 0.5 * (w[c] + w[c - sk]);
                 double grad, l;
                 grad = 0.0;
-                if (iadvec > 0.0) grad = weno_deriv(phi, c, si, g->dxp, g->qf[0], g->cf[0], g->isf[0], i + LSO_MARGE, 0);
-                if (iadvec < 0.0) grad = weno_deriv(phi, c, si, g->dxp, g->qf[0], g->cf[0], g->isf[0], i + LSO_MARGE, 1);
+                if (iadvec > 0.0) grad = DERIV(phi, c, si, g->dxp, g->qf[0], g->cf[0], g->isf[0], i + LSO_MARGE, 0);
+                if (iadvec < 0.0) grad = DERIV(phi, c, si, g->dxp, g->qf[0], g->cf[0], g->isf[0], i + LSO_MARGE, 1);
                 l = -iadvec * grad;
                 if (g->jdir == 1) {
                     grad = 0.0;
-                    if (jadvec > 0.0) grad = weno_deriv(phi, c, sj, g->dyp, g->qf[1], g->cf[1], g->isf[1], j + LSO_MARGE, 0);
-                    if (jadvec < 0.0) grad = weno_deriv(phi, c, sj, g->dyp, g->qf[1], g->cf[1], g->isf[1], j + LSO_MARGE, 1);
+                    if (jadvec > 0.0) grad = DERIV(phi, c, sj, g->dyp, g->qf[1], g->cf[1], g->isf[1], j + LSO_MARGE, 0);
+                    if (jadvec < 0.0) grad = DERIV(phi, c, sj, g->dyp, g->qf[1], g->cf[1], g->isf[1], j + LSO_MARGE, 1);
                     l -= jadvec * grad;
                 }
                 grad = 0.0;
-                if (kadvec > 0.0) grad = weno_deriv(phi, c, sk, g->dzp, g->qf[2], g->cf[2], g->isf[2], k + LSO_MARGE, 0);
-                if (kadvec < 0.0) grad = weno_deriv(phi, c, sk, g->dzp, g->qf[2], g->cf[2], g->isf[2], k + LSO_MARGE, 1);
+                if (kadvec > 0.0) grad = DERIV(phi, c, sk, g->dzp, g->qf[2], g->cf[2], g->isf[2], k + LSO_MARGE, 0);
+                if (kadvec < 0.0) grad = DERIV(phi, c, sk, g->dzp, g->qf[2], g->cf[2], g->isf[2], k + LSO_MARGE, 1);
                 l -= kadvec * grad;
                 L[c] = 0.0;
                 L[c] += l;  /* a->L(i,j,k) += aij(...) on a zeroed L */
             }
+#undef DERIV
 }
 
 /* --------------------------------------------------------- reinitialisation

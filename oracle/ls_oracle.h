@@ -52,6 +52,11 @@ typedef struct {
     int io_on, io_in, io_out, f50, b77, f64;
     double f56, f60, f61, f62, qi, qo;
     double phimean, phiout;  /* water levels of the last fsfinflow */
+    /* direct-forcing convection stencils (X45, src/weno_hj_df_nug.cpp:398-987):
+     * body1 = fb (X45 1), fbh5 (2, 4), fbh4 (3, 6) or solid (5), body2 = topo
+     * (5); caller-owned padded fields */
+    int x45;
+    const double *body1, *body2;
 } lso_grid;
 
 /* xn/yn/zn: node coordinates for indices -5..n+5 (n+11 values). */
@@ -99,6 +104,10 @@ void lso_set_ioflow(lso_grid* g, int inflow, int outflow, int f50, int b77, doub
 void lso_io_levels(const lso_grid* g, double* out);
 /* lexer::count the next step runs as minus one (the step increments it) */
 void lso_set_count(lso_grid* g, int count);
+
+/* X45 direct-forcing variant of the convection stencils and the body
+ * fields it reads (kept by pointer). */
+void lso_set_direct_forcing(lso_grid* g, int x45, const double* body1, const double* body2);
 
 /* opaque handle helpers (used through ctypes) */
 lso_grid* lso_new(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,

@@ -57,6 +57,7 @@ heat* HEAT = nullptr;
 concentration* CONC = nullptr;
 field4* TMP = nullptr;
 int G_F46 = 0, G_F47 = 10;  // picard mass correction flags for the next refls_init
+int G_X45 = 0;              // level-set convection stencil at bodies for the next refls_init
 // inflow (x-min) / outflow (x-max) boundaries and ioflow_f flags for the next
 // refls_init; io.on == 0 keeps the closed box and ioflow_v
 struct IoFlags {
@@ -78,6 +79,13 @@ field* field_by_id(int id) {
         case 5: return TMP;
         case 6: return &A->ro;
         case 7: return &A->visc;
+        // body fields the direct-forcing WENO stencils read (X45 1..6,
+        // src/weno_hj_df_nug.cpp:398-987)
+        case 8: return &A->fb;
+        case 9: return &A->fbh4;
+        case 10: return &A->fbh5;
+        case 11: return &A->solid;
+        case 12: return &A->topo;
         default: return nullptr;
     }
 }
@@ -104,6 +112,11 @@ extern "C" {
 // src/levelset_RK3.cpp:110,171) or 3 (picard_lsm there), f47 iterations
 // (src/picard_f.cpp:82-113, src/picard_lsm.cpp:89-116).
 void refls_set_picard(int f46, int f47) { G_F46 = f46; G_F47 = f47; }
+
+// X45 of the next refls_init: the direct-forcing variant of the level-set
+// WENO stencils (0 plain; 1..6 mask or weight the divided differences by
+// the body fields fb, fbh4, fbh5, solid, topo, src/weno_hj_df_nug.cpp:398-987).
+void refls_set_x45(int x45) { G_X45 = x45; }
 
 // Inflow / outflow boundaries of the next refls_init.  inflow: the x-min face
 // is boundary type 1, outflow: the x-max face type 2 (the other faces stay
@@ -139,7 +152,7 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
         p->F50 = G_IO.f50; p->B60 = 1; p->B77 = G_IO.b77;
         p->F56 = G_IO.f56; p->F60 = G_IO.f60; p->F61 = G_IO.f61; p->F62 = G_IO.f62; p->F64 = G_IO.f64;
     }
-    p->X45 = 0; p->X48 = 0; p->M10 = 1; p->P12 = 1000000000;
+    p->X45 = G_X45; p->X48 = 0; p->M10 = 1; p->P12 = 1000000000;
 
     // --- what read_grid() assigns (src/read_grid.cpp:78-300)
     p->knox = nx; p->knoy = ny; p->knoz = nz;

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libreef3d_b200.so")
 
 R3D_OK, R3D_EINVAL, R3D_ENOMEM, R3D_EDEVICE, R3D_ETIMEOUT, R3D_ESTATE = 0, 1, 2, 3, 4, 5
 FP64, FP32 = 0, 1
-PHI, U, V, W, L, WORK1, WORK2, RO, VISC = range(9)
+PHI, U, V, W, L, WORK1, WORK2, RO, VISC, BODY = range(10)
 LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
 STAGE_CONVECTION, STAGE_REINIT = 0, 1
 OPT_TILED, OPT_CHUNK, OPT_BAND64, OPT_WAIT_TEST = 0, 1, 2, 3
@@ -84,6 +84,7 @@ EXPORTS = {
     "r3d_set_fluid": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
+    "r3d_set_direct_forcing": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_io_levels": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_step_count": ([_H, ctypes.c_longlong], ctypes.c_int),
     "r3d_set_velocity_scale": ([_H, ctypes.c_double], ctypes.c_int),
@@ -281,6 +282,11 @@ class LevelSet:
 
     def set_velocity_scale(self, scale):
         _check(_lib.r3d_set_velocity_scale(self.h, scale), self.h)
+
+    def set_direct_forcing(self, x45):
+        """X45 direct-forcing convection stencils reading the BODY field
+        (r3d_set_direct_forcing); 0 turns them off."""
+        _check(_lib.r3d_set_direct_forcing(self.h, x45), self.h)
 
     def set_ioflow(self, **flags):
         """Inflow / outflow faces with ioflow_f's hooks (r3d_set_ioflow):

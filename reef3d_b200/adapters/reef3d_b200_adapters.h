@@ -146,6 +146,29 @@ inline bool ioflow_desc(const lexer* p, int gcv, r3d_ioflow_desc* d) {
     return true;
 }
 
+// Direct-forcing convection stencils (X45 != 0, src/weno_hj_df_nug.cpp:
+// 398-987): enables them on the instance (FP64 only).
+inline void set_direct_forcing(r3d_handle* h, const lexer* p) {
+    if (p->X45 != 0) check(h, r3d_set_direct_forcing(h, p->X45));
+}
+
+// The body field those stencils read, from the fdm: fb (X45 1), fbh5 (2, 4),
+// fbh4 (3, 6), min(solid, topo) (5: both > 0 exactly when the minimum is).
+inline void upload_body(r3d_handle* h, const lexer* p, fdm* a, std::vector<double>& buf) {
+    if (p->X45 == 0) return;
+    const double* src = nullptr;
+    if (p->X45 == 1) src = a->fb.V;
+    if (p->X45 == 2 || p->X45 == 4) src = a->fbh5.V;
+    if (p->X45 == 3 || p->X45 == 6) src = a->fbh4.V;
+    if (p->X45 == 5) {
+        const long n = (long)p->imax * p->jmax * p->kmax;
+        buf.resize((size_t)n);
+        for (long q = 0; q < n; ++q) buf[q] = a->solid.V[q] < a->topo.V[q] ? a->solid.V[q] : a->topo.V[q];
+        src = buf.data();
+    }
+    check(h, r3d_upload(h, R3D_BODY, src, R3D_LAYOUT_REEF3D));
+}
+
 inline bool same_ioflow(const r3d_ioflow_desc& a, const r3d_ioflow_desc& b) {
     return a.inflow == b.inflow && a.outflow == b.outflow && a.f50 == b.f50 && a.b77 == b.b77 && a.f56 == b.f56 &&
            a.f60 == b.f60 && a.f61 == b.f61 && a.f62 == b.f62 && a.f64 == b.f64 && a.qi == b.qi && a.qo == b.qo;
@@ -191,6 +214,7 @@ public:
     levelset_RK3_gpu(lexer* p, fdm*, ghostcell*, int precision = R3D_FP64, bool resident = false)
         : h(r3d_adapter::make_handle(p, precision)), resident(resident) {
         r3d_adapter::check(h, r3d_set_fluid(h, p->W1, p->W2, p->W3, p->W4));
+        r3d_adapter::set_direct_forcing(h, p);
     }
     ~levelset_RK3_gpu() { r3d_destroy(h); }
 
@@ -203,6 +227,7 @@ public:
         check(h, r3d_upload(h, R3D_U, a->u.V, R3D_LAYOUT_REEF3D));
         check(h, r3d_upload(h, R3D_V, a->v.V, R3D_LAYOUT_REEF3D));
         check(h, r3d_upload(h, R3D_W, a->w.V, R3D_LAYOUT_REEF3D));
+        r3d_adapter::upload_body(h, p, a, buf);
         check(h, r3d_ls_step(h, p->dt));
         r3d_adapter::download_owned(h, R3D_PHI, p, ls, true, buf);
         r3d_adapter::download_owned(h, R3D_RO, p, a->ro, true, buf);
@@ -244,7 +269,9 @@ private:
 class weno_hj_gpu final : public convection {
 public:
     explicit weno_hj_gpu(lexer* p, int precision = R3D_FP64)
-        : h(r3d_adapter::make_handle(p, precision)), buf((size_t)p->imax * p->jmax * p->kmax) {}
+        : h(r3d_adapter::make_handle(p, precision)), buf((size_t)p->imax * p->jmax * p->kmax) {
+        r3d_adapter::set_direct_forcing(h, p);
+    }
     ~weno_hj_gpu() { r3d_destroy(h); }
 
     void start(lexer* p, fdm* a, field& f, int ipol, field& u, field& v, field& w) override {
@@ -257,6 +284,7 @@ public:
         check(h, r3d_upload(h, R3D_U, u.V, R3D_LAYOUT_REEF3D));
         check(h, r3d_upload(h, R3D_V, v.V, R3D_LAYOUT_REEF3D));
         check(h, r3d_upload(h, R3D_W, w.V, R3D_LAYOUT_REEF3D));
+        r3d_adapter::upload_body(h, p, a, body);
         check(h, r3d_convection_L(h, R3D_WORK1));
         check(h, r3d_download(h, R3D_L, buf.data(), R3D_LAYOUT_REEF3D));
         for (int i = 0; i < p->knox; ++i)
@@ -269,7 +297,7 @@ public:
 
 private:
     r3d_handle* h;
-    std::vector<double> buf;
+    std::vector<double> buf, body;
 };
 
 // reinidisc: the reinitialisation right-hand side (reinidisc_f, or

@@ -237,8 +237,10 @@ long long volume_block_count(const r3d_handle* h) {
 }
 
 int check_field(r3d_handle* h, int field) {
-    if (field < 0 || field > R3D_VISC) return fail(h, R3D_EINVAL, "bad field id");
-    if (!h->field[field]) return fail(h, R3D_ESTATE, "ro/visc exist once r3d_set_fluid enabled them");
+    if (field < 0 || field > R3D_BODY) return fail(h, R3D_EINVAL, "bad field id");
+    if (!h->field[field])
+        return fail(h, R3D_ESTATE, field == R3D_BODY ? "the body field exists once r3d_set_direct_forcing enabled it"
+                                                     : "ro/visc exist once r3d_set_fluid enabled them");
     return R3D_OK;
 }
 
@@ -762,6 +764,29 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
     if (io->outflow && !(gcv == 51 || gcv == 54 || (gcv == 52 && io->b77 == 1))) mask |= kIoSkipHi;
     if (io->inflow) mask |= kIoEdge;
     set_layout_io(h, mask);
+    return R3D_OK;
+}
+
+int r3d_set_direct_forcing(r3d_handle* h, int x45) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    if (x45 < 0 || x45 > 6) return fail(h, R3D_EINVAL, "x45 must be 0..6");
+    if (x45 != 0 && fp32(h)) return fail(h, R3D_EINVAL, "the direct-forcing stencils run in the FP64 form");
+    DeviceGuard dg(h->device, h->batch_stream);
+    if (x45 != 0 && !h->field[R3D_BODY]) {
+        const size_t bytes = (size_t)h->L.ncell * elem(h);
+        if (cudaMalloc(&h->field[R3D_BODY], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            h->field[R3D_BODY] = nullptr;
+            return fail(h, R3D_ENOMEM, "body field allocation failed");
+        }
+        R3D_CUDA(h, cudaMemsetAsync(h->field[R3D_BODY], 0, bytes, h->stream));
+    }
+    drop_step_graph(h);
+    h->g64.x45 = x45;
+    h->g64.df_thr = 0.6 * h->M.dxm_mean;  // 0.6*p->DXM, src/weno_hj_df_nug.cpp:402
+    h->g64.body = static_cast<const double*>(h->field[R3D_BODY]);
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     return R3D_OK;
 }
 

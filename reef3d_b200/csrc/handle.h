@@ -16,8 +16,9 @@ struct r3d_handle {
     r3d::HostMetrics M;
     int device = 0;
     cudaStream_t stream = nullptr;
-    // fields 0..6 always; 7 (ro) and 8 (visc) once r3d_set_fluid enabled them
-    void* field[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // fields 0..6 always; 7 (ro) and 8 (visc) once r3d_set_fluid enabled
+    // them, 9 (body) once r3d_set_direct_forcing did
+    void* field[10] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     bool fluid = false;
     r3d::FluidConst fc{};
     // Airy wave velocity regenerated at the device clock before every step

@@ -101,7 +101,7 @@ __device__ __forceinline__ void heaviside_volume(const KGrid<double>& g, double 
 //   s=3: out = 1/3 fn + 2/3 fs + 2/3 dt L(fs)
 // Reinit stage s of src/reini_RK3.cpp:113-137: the same with the per-cell
 // pseudo time step.
-template <bool TWO_D, int STAGE, bool REINI, bool VOLUME>
+template <bool TWO_D, int STAGE, bool REINI, bool VOLUME, bool DF = false>
 __global__ void __launch_bounds__(kBX * kBY, R3D_F64_MINB) stage_kernel(KGrid<double> g, StageArgs a) {
     int i, j, k;
     cell_of_thread(g.L, TWO_D, i, j, k);
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kBX * kBY, R3D_F64_MINB) stage_kernel(KGrid<do
                 Lc = 0.0;
             dtc = f64::reini_dt<TWO_D>(g, i, j, k);
         } else {
-            Lc = f64::conv_L<TWO_D>(g, a.fs, a.u, a.v, a.w, c, i, j, k, *a.vscale);
+            Lc = f64::conv_L<TWO_D, DF>(g, a.fs, a.u, a.v, a.w, c, i, j, k, *a.vscale);
             dtc = *a.dt;
         }
         const double fn = a.fn[c];
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kBX * kBY, R3D_F64_MINB) stage_kernel(KGrid<do
 
 // Operator only (drop-ins for convection::start / reinidisc::start): L of
 // `fs` into `out` on interior cells.
-template <bool TWO_D, bool REINI>
+template <bool TWO_D, bool REINI, bool DF = false>
 __global__ void __launch_bounds__(kBX * kBY) operator_kernel(KGrid<double> g, StageArgs a) {
     int i, j, k;
     cell_of_thread(g.L, TWO_D, i, j, k);
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kBX * kBY) operator_kernel(KGrid<double> g, St
         if (g.f49 == 1 || f64::same_sign<TWO_D>(a.fs, c, g.L.sy, g.L.sz)) Lc = f64::reini_L<TWO_D>(g, a.fs, c, i, j, k);
         else Lc = 0.0;
     } else {
-        Lc = f64::conv_L<TWO_D>(g, a.fs, a.u, a.v, a.w, c, i, j, k, *a.vscale);
+        Lc = f64::conv_L<TWO_D, DF>(g, a.fs, a.u, a.v, a.w, c, i, j, k, *a.vscale);
     }
     a.out[c] = Lc;
 }
@@ -158,18 +158,18 @@ dim3 grid_of(const Layout& L) {
     return dim3((L.nx + kBX - 1) / kBX, (L.ny + kBY - 1) / kBY, L.nz);
 }
 
-template <bool TWO_D, bool REINI>
+template <bool TWO_D, bool REINI, bool DF = false>
 void launch_stage_t(const KGrid<double>& g, const StageArgs& a, int stage, bool volume, cudaStream_t st) {
     const dim3 grid = grid_of(g.L), block(kBX, kBY);
     if (stage == 1) {
-        if (volume) stage_kernel<TWO_D, 1, REINI, true><<<grid, block, 0, st>>>(g, a);
-        else stage_kernel<TWO_D, 1, REINI, false><<<grid, block, 0, st>>>(g, a);
+        if (volume) stage_kernel<TWO_D, 1, REINI, true, DF><<<grid, block, 0, st>>>(g, a);
+        else stage_kernel<TWO_D, 1, REINI, false, DF><<<grid, block, 0, st>>>(g, a);
     } else if (stage == 2) {
-        if (volume) stage_kernel<TWO_D, 2, REINI, true><<<grid, block, 0, st>>>(g, a);
-        else stage_kernel<TWO_D, 2, REINI, false><<<grid, block, 0, st>>>(g, a);
+        if (volume) stage_kernel<TWO_D, 2, REINI, true, DF><<<grid, block, 0, st>>>(g, a);
+        else stage_kernel<TWO_D, 2, REINI, false, DF><<<grid, block, 0, st>>>(g, a);
     } else {
-        if (volume) stage_kernel<TWO_D, 3, REINI, true><<<grid, block, 0, st>>>(g, a);
-        else stage_kernel<TWO_D, 3, REINI, false><<<grid, block, 0, st>>>(g, a);
+        if (volume) stage_kernel<TWO_D, 3, REINI, true, DF><<<grid, block, 0, st>>>(g, a);
+        else stage_kernel<TWO_D, 3, REINI, false, DF><<<grid, block, 0, st>>>(g, a);
     }
 }
 
@@ -193,8 +193,13 @@ StageArgs stage_args(const Fields& f, int stage, const Scratch& s) {
 int launch_conv_stage_f64(const KGrid<double>& g, const Fields& f, int stage, const Scratch& s, bool volume,
                           cudaStream_t st) {
     const StageArgs a = stage_args(f, stage, s);
-    if (g.L.two_d) launch_stage_t<true, false>(g, a, stage, volume, st);
-    else launch_stage_t<false, false>(g, a, stage, volume, st);
+    if (g.x45) {  // direct-forcing stencils (X45 1..6)
+        if (g.L.two_d) launch_stage_t<true, false, true>(g, a, stage, volume, st);
+        else launch_stage_t<false, false, true>(g, a, stage, volume, st);
+    } else {
+        if (g.L.two_d) launch_stage_t<true, false>(g, a, stage, volume, st);
+        else launch_stage_t<false, false>(g, a, stage, volume, st);
+    }
     return 1;
 }
 
@@ -215,8 +220,13 @@ int launch_conv_L_f64(const KGrid<double>& g, const void* in, const Fields& f, c
     a.v = static_cast<const double*>(f.v);
     a.w = static_cast<const double*>(f.w);
     const dim3 grid = grid_of(g.L), block(kBX, kBY);
-    if (g.L.two_d) operator_kernel<true, false><<<grid, block, 0, st>>>(g, a);
-    else operator_kernel<false, false><<<grid, block, 0, st>>>(g, a);
+    if (g.x45) {
+        if (g.L.two_d) operator_kernel<true, false, true><<<grid, block, 0, st>>>(g, a);
+        else operator_kernel<false, false, true><<<grid, block, 0, st>>>(g, a);
+    } else {
+        if (g.L.two_d) operator_kernel<true, false><<<grid, block, 0, st>>>(g, a);
+        else operator_kernel<false, false><<<grid, block, 0, st>>>(g, a);
+    }
     return 1;
 }
 

@@ -74,6 +74,11 @@ struct KGrid {
     double f43;
     int f49;
     double psi;
+    // direct-forcing convection stencils (X45 1..6, FP64 only): the body
+    // field they read and 0.6 DXM, the fb threshold of X45 = 1
+    int x45;
+    double df_thr;
+    const T* body;
     // uniform-grid FP32 form
     float h[3], rh[3];
     float eps_u;  // WENO psi (1e-6); rescaled by h^2 per axis for undivided differences

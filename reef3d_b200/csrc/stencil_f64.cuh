@@ -72,12 +72,59 @@ __device__ __forceinline__ double deriv(const double* __restrict__ f, long long 
                  isf + (long long)t * 18 + side * 9, plus, q1, q2, q3, q4, q5);
 }
 
+// Direct-forcing divided difference of the cell pair (a, b = a + s) of the
+// X45 stencils (src/weno_hj_df_nug.cpp:398-987; one rule per X45 for the
+// three axes and both sides), with ha, hb the body field at the two cells:
+//  1 zero unless |fb| > 0.6 DXM at both (body = fb),
+//  2 weighted by 0.5 (fbh5(b) + fbh5(a)),
+//  3 zero unless fbh4 < 0.5 at both,
+//  4 weighted by fbh5 at hw: the pair's lower cell on the minus side, its
+//    upper cell on the plus side,
+//  5 zero unless solid > 0 and topo > 0 at both (body = min(solid, topo),
+//    which is > 0 exactly when both are),
+//  6 like 3 but 1e20 where masked.
+__device__ __forceinline__ double df_q(int x45, double thr, double fa, double fb, double ha, double hb, double hw,
+                                       double d) {
+    switch (x45) {
+        case 1: return (fabs(hb) > thr && fabs(ha) > thr) ? (fb - fa) / d : 0.0;
+        case 2: return 0.5 * (hb + ha) * (fb - fa) / d;
+        case 3: return (hb < 0.5 && ha < 0.5) ? (fb - fa) / d : 0.0;
+        case 4: return hw * (fb - fa) / d;
+        case 5: return (hb > 0.0 && ha > 0.0) ? (fb - fa) / d : 0.0;
+        default: return (hb < 0.5 && ha < 0.5) ? (fb - fa) / d : 1.0e20;
+    }
+}
+
+// deriv with the direct-forcing differences of df_q.
+__device__ __forceinline__ double deriv_df(const double* __restrict__ f, const double* __restrict__ h, long long c,
+                                           long long s, const double* __restrict__ dp,
+                                           const double* __restrict__ qf, const double* __restrict__ cf,
+                                           const double* __restrict__ isf, int t, bool plus, int x45, double thr) {
+    const int o = plus ? -2 : -3;
+    const long long b0 = c + o * s;
+    const double* d = dp + t + o;
+    double fv[6], hv[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        fv[m] = __ldg(f + b0 + m * s);
+        hv[m] = __ldg(h + b0 + m * s);
+    }
+    double q[5];
+#pragma unroll
+    for (int m = 1; m <= 5; ++m)
+        q[m - 1] = df_q(x45, thr, fv[m - 1], fv[m], hv[m - 1], hv[m], plus ? hv[m] : hv[m - 1], __ldg(d + m - 1));
+    const int side = plus ? 1 : 0;
+    return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
+                 isf + (long long)t * 18 + side * 9, plus, q[0], q[1], q[2], q[3], q[4]);
+}
+
 // -u.grad(f) at interior cell (i,j,k): src/weno_hj_df_nug.cpp:93-111 with the
 // cell-centre velocities of src/flux_HJ_CDS2.cpp:59-127 (2D: no y term,
 // src/flux_HJ_CDS2_2D.cpp).  Returned as the reference's a->L value
 // (0.0 + L).
 // The stored face velocities are multiplied by vs (1 leaves them exact).
-template <bool TWO_D>
+// DF: the direct-forcing stencils of g.x45 (g.body) replace the plain ones.
+template <bool TWO_D, bool DF = false>
 __device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* __restrict__ f,
                                          const double* __restrict__ u, const double* __restrict__ v,
                                          const double* __restrict__ w, long long c, int i, int j, int k,
@@ -85,17 +132,21 @@ __device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* _
     const long long sy = g.L.sy, sz = g.L.sz;
     const double iadvec = 0.5 * (vs * __ldg(u + c) + vs * __ldg(u + c - 1));
     const double kadvec = 0.5 * (vs * __ldg(w + c) + vs * __ldg(w + c - sz));
+    auto axis = [&](long long s, int a, int t, bool plus) {
+        if (DF) return deriv_df(f, g.body, c, s, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus, g.x45, g.df_thr);
+        return deriv(f, c, s, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus);
+    };
     // advec > 0: minus side, < 0: plus side, == 0: no contribution (grad 0)
-    double grad = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5, iadvec < 0.0);
+    double grad = axis(1, 0, i + 5, iadvec < 0.0);
     if (iadvec == 0.0) grad = 0.0;
     double l = -iadvec * grad;
     if (!TWO_D) {
         const double jadvec = 0.5 * (vs * __ldg(v + c) + vs * __ldg(v + c - sy));
-        grad = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5, jadvec < 0.0);
+        grad = axis(sy, 1, j + 5, jadvec < 0.0);
         if (jadvec == 0.0) grad = 0.0;
         l -= jadvec * grad;
     }
-    grad = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5, kadvec < 0.0);
+    grad = axis(sz, 2, k + 5, kadvec < 0.0);
     if (kadvec == 0.0) grad = 0.0;
     l -= kadvec * grad;
     double acc = 0.0;

@@ -37,6 +37,20 @@ def golden_ioflow(g):
     return {k[3:]: (int(g[k]) if k[3:] in ints else float(g[k])) for k in g if k.startswith("io_")}
 
 
+def golden_df(g):
+    """(x45, body1, body2) of a direct-forcing golden case, else None."""
+    if "x45" not in g:
+        return None
+    return int(g["x45"]), g["body1"], g["body2"]
+
+
+def body_field(x45, body1, body2):
+    """The one body field the device stencils read: body1, or for X45 = 5
+    min(solid, topo), which is > 0 exactly where both are."""
+    import numpy as np
+    return np.ascontiguousarray(np.minimum(body1, body2) if x45 == 5 else body1)
+
+
 @pytest.fixture(scope="session")
 def port_lib():
     """The C restatement oracle, built on demand (test infrastructure)."""

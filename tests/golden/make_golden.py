@@ -88,6 +88,28 @@ def tank_case(name, nx, ny, nz, f49, stretch, seed, steps, io, level=0.5, f46=0,
                 io=io)
 
 
+def df_case(name, nx, ny, nz, stretch, seed, x45, steps=2):
+    """Direct-forcing convection stencils (X45 1..6) with random body fields:
+    body1 = fb (X45 1), fbh5 (2, 4), fbh4 (3, 6) or solid (5), body2 = topo."""
+    c = random_case(name, nx, ny, nz, 1, stretch, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shape = c["phi"].shape
+    dxm = 1.0 / nx
+    if x45 == 1:
+        b1 = rng.uniform(-3 * dxm, 3 * dxm, shape)
+    elif x45 in (2, 4):
+        b1 = rng.uniform(0.0, 1.0, shape)
+        b1[rng.uniform(size=shape) < 0.3] = 1.0
+    elif x45 in (3, 6):
+        b1 = rng.uniform(0.0, 1.0, shape)
+        b1[rng.uniform(size=shape) < 0.5] = 0.0
+    else:
+        b1 = rng.uniform(-0.3, 1.0, shape)
+    b2 = rng.uniform(-0.3, 1.0, shape) if x45 == 5 else np.zeros(shape)
+    c.update(x45=x45, body1=b1, body2=b2, steps=steps)
+    return c
+
+
 def setup_case(name, which, n, steps, f46=0, f47=10):
     from reef3d_b200 import setups
     c = setups.slotted_disk(n) if which == "disk" else setups.vortex3d(n)
@@ -118,6 +140,12 @@ CASES = [
                       dict(f50=1, inflow=0, b77=2, f62=-0.1)),
     lambda: tank_case("io_tank3d_inflow_only_picard2", 16, 6, 14, 1, 0.0, 16, 3,
                       dict(f50=2, outflow=0), f46=2, f47=3),
+    lambda: df_case("df1_box3d_stretched", 9, 7, 8, 0.3, 21, 1),
+    lambda: df_case("df2_box2d_uniform", 12, 1, 10, 0.0, 22, 2),
+    lambda: df_case("df3_box3d_uniform", 9, 7, 8, 0.0, 23, 3),
+    lambda: df_case("df4_box3d_stretched", 9, 7, 8, 0.3, 24, 4),
+    lambda: df_case("df5_box2d_stretched", 12, 1, 10, 0.3, 25, 5),
+    lambda: df_case("df6_box3d_uniform", 9, 7, 8, 0.0, 26, 6),
 ]
 
 
@@ -126,8 +154,9 @@ def run_case(idx):
     c = CASES[idx]()
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     io = c.get("io")
+    x45 = c.get("x45", 0)
     ref = RefOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io)
+                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io, x45=x45)
     out = {k: c[k] for k in ("nx", "ny", "nz", "xn", "yn", "zn", "phi", "u", "v", "w", "f43", "f44", "f45",
                               "f49", "n47", "steps", "f46", "f47")}
     for a, n in enumerate((nx, ny, nz)):
@@ -143,6 +172,12 @@ def run_case(idx):
     out["vel_scale"] = np.array(c["vel_scale"] or "none")
     phi, u, v, w = c["phi"], c["u"], c["v"], c["w"]
     ref.set_state(phi, u, v, w)
+    if x45:
+        # harness field ids 8..12 = fb, fbh4, fbh5, solid, topo
+        ref.set_field({1: 8, 2: 10, 3: 9, 4: 10, 5: 11, 6: 9}[x45], c["body1"])
+        if x45 == 5:
+            ref.set_field(12, c["body2"])
+        out["x45"], out["body1"], out["body2"] = x45, c["body1"], c["body2"]
     out["weno_L"] = ref.weno_L(phi)
     out["reinidisc_L"] = ref.reinidisc_L(phi)
     out["ghost"] = ref.ghost_fill(phi)

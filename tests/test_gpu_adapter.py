@@ -5,7 +5,9 @@ process, each reference object (levelset_RK3, weno_hj_df_nug, reinidisc_f /
 reinidisc_fsf, reini_RK3, fluid_update_fsf) and the adapter that replaces it
 start from the same REEF3D fields, and the fields they leave behind are
 compared (the tank_io cases with the reference's ioflow_f inflow / outflow
-boundaries, which the adapters hand to r3d_set_ioflow).  FP64: the level
+boundaries, which the adapters hand to r3d_set_ioflow; the stretched_df
+cases with the direct-forcing convection stencils X45 4 and 5 over the
+fdm's body fields).  FP64: the level
 set and the operators bit-identical on every cell
 (ghost layers included: the adapters finish with REEF3D's own
 ghostcell::start4), volumes, density and viscosity within 1e-12 relative
@@ -67,8 +69,21 @@ def _case(name):
     phi = np.sqrt((X - 0.5) ** 2 + (Y - 0.45) ** 2 + (Z - 0.55) ** 2) - 0.23
     phi = np.ascontiguousarray(phi + 0.01 * rng.standard_normal(phi.shape))
     u, v, w = (np.ascontiguousarray(rng.standard_normal(phi.shape)) for _ in range(3))
-    return dict(nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w, f43=0.5, f44=2, f45=2.1,
-                f49=0 if name == "stretched_f49_0" else 1, n47=0.125, f46=2 if name == "stretched_picard" else 0)
+    c = dict(nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w, f43=0.5, f44=2, f45=2.1,
+             f49=0 if name == "stretched_f49_0" else 1, n47=0.125, f46=2 if name == "stretched_picard" else 0)
+    if name.startswith("stretched_df"):
+        # direct-forcing stencils: X45 4 over fbh5 (harness field 10), X45 5
+        # over solid and topo (11, 12)
+        x45 = int(name[-1])
+        shape = phi.shape
+        if x45 == 4:
+            b = rng.uniform(0.0, 1.0, shape)
+            b[rng.uniform(size=shape) < 0.3] = 1.0
+            bodies = {10: b}
+        else:
+            bodies = {11: rng.uniform(-0.3, 1.0, shape), 12: rng.uniform(-0.3, 1.0, shape)}
+        c.update(x45=x45, bodies=bodies)
+    return c
 
 
 def _visible(nx, ny, nz):
@@ -88,9 +103,12 @@ def _run(name, precision=0):
     c = _case(name)
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                       f49=c["f49"], f46=c["f46"], f47=6, precision=precision, ioflow=c.get("io"))
+                       f49=c["f49"], f46=c["f46"], f47=6, precision=precision, ioflow=c.get("io"),
+                       x45=c.get("x45", 0))
     out = {}
     ao.set_state(c["phi"], c["u"], c["v"], c["w"])
+    for fid, arr in c.get("bodies", {}).items():
+        ao.set_field(fid, np.ascontiguousarray(arr))
     out["weno_L"] = bool(np.array_equal(_interior(ao.weno_L(c["phi"]), nx, ny, nz),
                                         _interior(ao.gpu_weno_L(c["phi"]), nx, ny, nz)))
     out["reinidisc_L"] = bool(np.array_equal(_interior(ao.reinidisc_L(c["phi"]), nx, ny, nz),
@@ -131,7 +149,7 @@ def _run(name, precision=0):
 
 
 @pytest.mark.parametrize("name", ["vortex3d", "disk2d", "stretched_f49_0", "stretched_picard", "tank_io3d",
-                                  "tank_io2d"])
+                                  "tank_io2d", "stretched_df4", "stretched_df5"])
 def test_adapters_match_reference_objects(name):
     from oracle.bindings import AdapterOracle
     if not AdapterOracle.available():

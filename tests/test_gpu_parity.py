@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import reef3d_b200 as r3d
-from conftest import GOLDEN_CASES, golden_flags, golden_ioflow, load_golden, velocity_at
+from conftest import GOLDEN_CASES, body_field, golden_df, golden_flags, golden_ioflow, load_golden, velocity_at
 from test_oracle_golden import interior, visible_mask
 
 pytestmark = pytest.mark.gpu
@@ -30,6 +30,10 @@ def make_gpu(g, precision=r3d.FP64):
     io = golden_ioflow(g)
     if io is not None:  # inflow / outflow faces with ioflow_f's hooks
         ls.set_ioflow(**io)
+    df = golden_df(g)
+    if df is not None:  # direct-forcing convection stencils (X45)
+        ls.set_direct_forcing(df[0])
+        ls.upload(r3d.BODY, body_field(*df))
     return ls
 
 

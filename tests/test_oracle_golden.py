@@ -5,7 +5,7 @@ layers; edge and corner ghosts are outside every stencil of the path)."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, golden_flags, golden_ioflow, load_golden, velocity_at
+from conftest import GOLDEN_CASES, golden_df, golden_flags, golden_ioflow, load_golden, velocity_at
 
 
 def visible_mask(nx, ny, nz):
@@ -25,6 +25,9 @@ def case(request, port_lib):
     g = load_golden(request.param)
     o = port_lib(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], ioflow=golden_ioflow(g),
                  **golden_flags(g))
+    df = golden_df(g)
+    if df is not None:  # direct-forcing convection stencils (X45)
+        o.set_direct_forcing(*df)
     return g, o
 
 
