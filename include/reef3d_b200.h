@@ -187,6 +187,48 @@ int r3d_set_velocity_period(r3d_handle* h, double period);
  * velocity factor set to 1.  wavelength <= 0 turns the generator off.
  * Synchronous.  Not for batch members. */
 int r3d_set_velocity_airy(r3d_handle* h, double amplitude, double wavelength, double depth, double gravity);
+/* Subdomain (slab) decomposition along z, the role of the reference's MPI
+ * halo exchange (ghostcell::gcparax, src/gcx_parax.cpp) for a grid split
+ * into slabs of consecutive z cells, one instance per slab (per GPU, or
+ * several on one GPU).  The instance's node coordinates are the slab's own
+ * (zn: node indices -5..nz+5 of the slab, taken from the global grid).
+ *  r3d_set_halo: zlo / zhi = 1 marks the z-min / z-max face as a subdomain
+ *    boundary: no kernel writes wall copies into its three ghost planes
+ *    (a neighbour's halo fills them), and with zhi the faces at nz-1 take
+ *    part in the CFL maximum (wlast = 0 with a neighbour above,
+ *    src/lexer_gridsize.cpp:78-79).  Not with picard (f46 != 0) or
+ *    inflow/outflow faces, whose sums the reference takes globally inside
+ *    the step.
+ *  r3d_halo_copy: dir 0 packs the three interior z planes next to `side`
+ *    (0 z-min, 1 z-max) of `field` into the device buffer buf; dir 1 unpacks
+ *    buf into the three ghost planes on that side.  r3d_halo_bytes gives
+ *    the buffer size (3 padded planes).  Asynchronous on the handle's
+ *    stream.
+ *  r3d_cfl_max: the instance's |u|, |v|, |w| face maxima of the stored
+ *    velocities (the first half of ietimestep, src/ietimestep.cpp:72-88;
+ *    the caller takes the maximum over subdomains, as pgc->globalmax does).
+ *  r3d_cfl_dt_from_max: the time step from given maxima with this
+ *    instance's smallest cell (the second half, :160-188); the minimum of
+ *    it over subdomains is the undivided grid's time step, which the caller
+ *    then sets with r3d_set_dt.
+ * A step over subdomains is then: r3d_stage per RK stage, and after each
+ * stage the stage's output field exchanged (pack on one instance, unpack
+ * into its neighbour); volumes are summed over subdomains (r3d_volume). */
+int r3d_set_halo(r3d_handle* h, int zlo, int zhi);
+/* The grid-wide spacing constants of src/grid.cpp:102-148 (DXM, the mean
+ * cell spacing over the three axes, summed over all subdomains) and of the
+ * DIVEMesh header (DYM, DZM), from which the interface thickness psi
+ * (src/ini_psi.cpp:33-37), the picard epsi and the X45 = 1 threshold derive.
+ * r3d_grid_spacing computes them for a description (out[0..3] = DXM, DYM,
+ * DZM, psi; host only); r3d_set_grid_spacing gives a subdomain instance the
+ * whole grid's values in place of its own. */
+int r3d_grid_spacing(const r3d_grid_desc* desc, double* out);
+int r3d_set_grid_spacing(r3d_handle* h, double dxm, double dym, double dzm);
+int r3d_halo_bytes(const r3d_handle* h, size_t* bytes);
+int r3d_halo_copy(r3d_handle* h, int field, int side, int dir, void* buf);
+int r3d_cfl_max(r3d_handle* h, double* vmax);
+int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt);
+
 /* Direct-forcing variant of the level-set convection stencils (control
  * flag X45, src/weno_hj_df_nug.cpp:115-342 selecting :398-987): the five
  * divided differences of each WENO5 stencil are masked or weighted by a

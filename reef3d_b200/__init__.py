@@ -85,6 +85,13 @@ EXPORTS = {
     "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
     "r3d_set_direct_forcing": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_set_halo": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_grid_spacing": ([ctypes.POINTER(GridDesc), _D], ctypes.c_int),
+    "r3d_set_grid_spacing": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
+    "r3d_halo_bytes": ([_H, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+    "r3d_halo_copy": ([_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "r3d_cfl_max": ([_H, _D], ctypes.c_int),
+    "r3d_cfl_dt_from_max": ([_H, _D, _D], ctypes.c_int),
     "r3d_io_levels": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_step_count": ([_H, ctypes.c_longlong], ctypes.c_int),
     "r3d_set_velocity_scale": ([_H, ctypes.c_double], ctypes.c_int),
@@ -169,6 +176,18 @@ def footprint(nx, ny, nz, precision=FP32):
     out = ctypes.c_size_t()
     _check(_lib.r3d_footprint(ctypes.byref(d), ctypes.byref(out)))
     return out.value
+
+
+def grid_spacing(nx, ny, nz, xn=None, yn=None, zn=None, f45=2.1):
+    """(DXM, DYM, DZM, psi) of a grid (r3d_grid_spacing; host only)."""
+    load_library()
+    xn = uniform_nodes(nx) if xn is None else xn
+    yn = uniform_nodes(ny) if yn is None else yn
+    zn = uniform_nodes(nz) if zn is None else zn
+    d = make_desc(nx, ny, nz, xn, yn, zn, 0.5, 2, f45, 1, 0.3, FP64, 0, 10)
+    out = (ctypes.c_double * 4)()
+    _check(_lib.r3d_grid_spacing(ctypes.byref(d), out))
+    return tuple(out)
 
 
 class LevelSet:
@@ -287,6 +306,38 @@ class LevelSet:
         """X45 direct-forcing convection stencils reading the BODY field
         (r3d_set_direct_forcing); 0 turns them off."""
         _check(_lib.r3d_set_direct_forcing(self.h, x45), self.h)
+
+    def set_halo(self, zlo, zhi):
+        """Mark the z-min / z-max faces as subdomain boundaries (r3d_set_halo)."""
+        _check(_lib.r3d_set_halo(self.h, int(bool(zlo)), int(bool(zhi))), self.h)
+
+    def set_grid_spacing(self, dxm, dym, dzm):
+        """The whole grid's DXM, DYM, DZM for a subdomain instance."""
+        _check(_lib.r3d_set_grid_spacing(self.h, dxm, dym, dzm), self.h)
+
+    def halo_bytes(self):
+        n = ctypes.c_size_t()
+        _check(_lib.r3d_halo_bytes(self.h, ctypes.byref(n)), self.h)
+        return n.value
+
+    def halo_copy(self, field, side, dir, ptr):
+        """dir 0: pack the 3 interior z planes next to side (0 z-min, 1
+        z-max) into the device buffer at ptr; dir 1: unpack ptr into the 3
+        ghost planes.  Asynchronous on the instance's stream."""
+        _check(_lib.r3d_halo_copy(self.h, field, side, dir, ctypes.c_void_p(ptr)), self.h)
+
+    def cfl_max(self):
+        """(|u|max, |v|max, |w|max) over this instance's CFL faces."""
+        out = (ctypes.c_double * 3)()
+        _check(_lib.r3d_cfl_max(self.h, out), self.h)
+        return tuple(out)
+
+    def cfl_dt_from_max(self, vmax):
+        """Time step from given maxima with this instance's smallest cell."""
+        vm = (ctypes.c_double * 3)(*vmax)
+        dt = ctypes.c_double()
+        _check(_lib.r3d_cfl_dt_from_max(self.h, vm, ctypes.byref(dt)), self.h)
+        return dt.value
 
     def set_ioflow(self, **flags):
         """Inflow / outflow faces with ioflow_f's hooks (r3d_set_ioflow):

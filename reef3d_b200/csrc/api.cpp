@@ -396,6 +396,7 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
     std::vector<float> m32;
     fill_kgrid<double>(h, h->g64, h->metrics64, m64);
     fill_kgrid<float>(h, h->g32, h->metrics32, m32);
+    for (int a = 0; a < 3; ++a) h->g64.dxn_d[a] = h->g32.dxn_d[a] = h->g64.dxn[a];
     cudaMemcpy(h->metrics64, m64.data(), m64.size() * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(h->metrics32, m32.data(), m32.size() * sizeof(float), cudaMemcpyHostToDevice);
 
@@ -702,7 +703,7 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
     if (!io) {
         drop_step_graph(h);
         h->io = false;
-        set_layout_io(h, 0);
+        set_layout_io(h, h->L.io & (kHaloZLo | kHaloZHi));
         return R3D_OK;
     }
     if ((io->inflow != 0 && io->inflow != 1) || (io->outflow != 0 && io->outflow != 1))
@@ -710,6 +711,8 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
     if (io->f50 < 1 || io->f50 > 4) return fail(h, R3D_EINVAL, "f50 must be 1..4");
     if (io->b77 != 1 && io->b77 != 2) return fail(h, R3D_EINVAL, "b77 must be 1 or 2");
     if (io->f64 < 0 || io->f64 > (1 << 24)) return fail(h, R3D_EINVAL, "f64 must be 0..2^24");
+    if (h->L.io & (kHaloZLo | kHaloZHi))
+        return fail(h, R3D_EINVAL, "subdomain instances have no inflow/outflow faces");
     drop_step_graph(h);
     // state, ZP (index k + 5), ramp table of the outflow level (F64 > 0)
     const std::vector<double>& zp = h->M.xp[2];
@@ -763,7 +766,108 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
     if (io->inflow && !(gcv == 52 || gcv == 54)) mask |= kIoSkipLo;
     if (io->outflow && !(gcv == 51 || gcv == 54 || (gcv == 52 && io->b77 == 1))) mask |= kIoSkipHi;
     if (io->inflow) mask |= kIoEdge;
+    set_layout_io(h, mask | (h->L.io & (kHaloZLo | kHaloZHi)));
+    return R3D_OK;
+}
+
+// ------------------------------------------------ grid spacing constants
+int r3d_grid_spacing(const r3d_grid_desc* desc, double* out) {
+    std::string why;
+    if (int rc = check_desc(desc, why)) return fail(nullptr, rc, why);
+    if (!out) return fail(nullptr, R3D_EINVAL, "null output");
+    HostMetrics m;
+    build_metrics(desc->nx, desc->ny, desc->nz, desc->xn, desc->yn, desc->zn, desc->f45, m);
+    out[0] = m.dxm_mean;
+    out[1] = m.dym;
+    out[2] = m.dzm;
+    out[3] = m.psi;
+    return R3D_OK;
+}
+
+int r3d_set_grid_spacing(r3d_handle* h, double dxm, double dym, double dzm) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!(dxm > 0.0) || !(dym > 0.0) || !(dzm > 0.0)) return fail(h, R3D_EINVAL, "spacings must be > 0");
+    DeviceGuard dg(h->device, h->batch_stream);
+    drop_step_graph(h);
+    h->M.dxm_mean = dxm;
+    h->M.dym = dym;
+    h->M.dzm = dzm;
+    // src/ini_psi.cpp:33-37, as build_metrics
+    if (h->L.two_d) h->M.psi = h->desc.f45 * (1.0 / 2.0) * (dxm + dzm);
+    else h->M.psi = h->desc.f45 * (1.0 / 3.0) * (dxm + dym + dzm);
+    h->g64.psi = h->M.psi;
+    h->g32.psi = h->M.psi;
+    h->g64.df_thr = 0.6 * dxm;
+    return R3D_OK;
+}
+
+// ------------------------------------------------ subdomain (slab) halos
+int r3d_set_halo(r3d_handle* h, int zlo, int zhi) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    if ((zlo != 0 && zlo != 1) || (zhi != 0 && zhi != 1)) return fail(h, R3D_EINVAL, "zlo and zhi must be 0 or 1");
+    if ((zlo || zhi) && h->desc.f46 != 0)
+        return fail(h, R3D_EINVAL, "subdomain instances run without the picard correction (f46 = 0)");
+    if ((zlo || zhi) && h->io) return fail(h, R3D_EINVAL, "subdomain instances have no inflow/outflow faces");
+    DeviceGuard dg(h->device, h->batch_stream);
+    drop_step_graph(h);
+    const int mask = (h->L.io & ~(kHaloZLo | kHaloZHi)) | (zlo ? kHaloZLo : 0) | (zhi ? kHaloZHi : 0);
     set_layout_io(h, mask);
+    return R3D_OK;
+}
+
+int r3d_halo_bytes(const r3d_handle* h, size_t* bytes) {
+    if (!h || !bytes) return fail(nullptr, R3D_EINVAL, "null argument");
+    *bytes = (size_t)3 * (size_t)h->L.sz * elem(h);
+    return R3D_OK;
+}
+
+int r3d_halo_copy(r3d_handle* h, int field, int side, int dir, void* buf) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (int rc = check_field(h, field)) return rc;
+    if ((side != 0 && side != 1) || (dir != 0 && dir != 1) || !buf)
+        return fail(h, R3D_EINVAL, "side 0 (z-min) or 1 (z-max), dir 0 (pack) or 1 (unpack), device buffer");
+    if (h->L.nz < 3) return fail(h, R3D_EINVAL, "a subdomain needs at least 3 cells in z");
+    DeviceGuard dg(h->device, h->batch_stream);
+    const size_t e = elem(h), plane = (size_t)h->L.sz;
+    // planes k = 0..2 / nz-3..nz-1 (pack) and -3..-1 / nz..nz+2 (unpack);
+    // plane k starts at (k + gz) * sz
+    const long long k0 = dir == 0 ? (side == 0 ? 0 : h->L.nz - 3) : (side == 0 ? -3 : h->L.nz);
+    char* f = static_cast<char*>(h->field[field]) + (size_t)(k0 + h->L.gz) * plane * e;
+    if (dir == 0)
+        R3D_CUDA(h, cudaMemcpyAsync(buf, f, 3 * plane * e, cudaMemcpyDeviceToDevice, h->stream));
+    else
+        R3D_CUDA(h, cudaMemcpyAsync(f, buf, 3 * plane * e, cudaMemcpyDeviceToDevice, h->stream));
+    return R3D_OK;
+}
+
+int r3d_cfl_max(r3d_handle* h, double* vmax) {
+    if (!h || !vmax) return fail(h, R3D_EINVAL, "null argument");
+    DeviceGuard dg(h->device, h->batch_stream);
+    h->launches += refresh_velocity(h);
+    h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h), h->M.dxmin_cfl,
+                              h->desc.n47, h->S, h->stream);
+    unsigned long long bits[3] = {0, 0, 0};
+    R3D_CUDA(h, cudaMemcpyAsync(bits, h->S.vmax, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int a = 0; a < 3; ++a) std::memcpy(&vmax[a], &bits[a], sizeof(double));
+    return R3D_OK;
+}
+
+int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt) {
+    if (!h || !vmax) return fail(h, R3D_EINVAL, "null argument");
+    for (int a = 0; a < 3; ++a)
+        if (!(vmax[a] >= 0.0)) return fail(h, R3D_EINVAL, "velocity maxima must be >= 0");
+    DeviceGuard dg(h->device, h->batch_stream);
+    unsigned long long bits[3];
+    for (int a = 0; a < 3; ++a) std::memcpy(&bits[a], &vmax[a], sizeof(double));
+    R3D_CUDA(h, cudaMemcpyAsync(h->S.vmax, bits, sizeof bits, cudaMemcpyHostToDevice, h->stream));
+    h->launches += launch_dt_from_max(h->M.dxmin_cfl, h->desc.n47, h->S, h->stream);
+    double v = 0.0;
+    R3D_CUDA(h, cudaMemcpyAsync(&v, h->S.dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->dt_host = v;
+    if (dt) *dt = v;
     return R3D_OK;
 }
 

@@ -130,8 +130,8 @@ __global__ void __launch_bounds__(32 * ROWS) batch_stage_kernel(const MemberDesc
                 if (p > psi) H = 1.0;
                 if (p < -psi) H = 0.0;
                 if (fabs(p) <= psi) H = 0.5 * (1.0 + p / psi + (1.0 / PI_REF) * sin((PI_REF * p) / psi));
-                const double vol = (double)__ldg(m.g.dxn[0] + i + 5) * (double)__ldg(m.g.dxn[1] + j + 5) *
-                                   (double)__ldg(m.g.dxn[2] + k + 5);
+                const double vol = __ldg(m.g.dxn_d[0] + i + 5) * __ldg(m.g.dxn_d[1] + j + 5) *
+                                   __ldg(m.g.dxn_d[2] + k + 5);
                 v1 = vol * H;
                 v2 = vol * (1.0 - H);
             }

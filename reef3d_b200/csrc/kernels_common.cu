@@ -75,8 +75,8 @@ __global__ void ghost_kernel(Layout L, T* f) {
         if (i == L.nx - 1 && !(L.io & kIoSkipHi)) f[c + q] = val;
         if (!L.two_d && j == 0) f[c - q * L.sy] = val;
         if (!L.two_d && j == L.ny - 1) f[c + q * L.sy] = val;
-        if (k == 0) f[c - q * L.sz] = val;
-        if (k == L.nz - 1) f[c + q * L.sz] = val;
+        if (k == 0 && !(L.io & kHaloZLo)) f[c - q * L.sz] = val;
+        if (k == L.nz - 1 && !(L.io & kHaloZHi)) f[c + q * L.sz] = val;
     }
 }
 
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256) vmax_kernel(Layout L, const T* __restrict
         for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
             if (i < L.nx - 1) mu = fmax(mu, fabs((double)u[base + i]));
             if (j < L.ny - 1) mv = fmax(mv, fabs((double)v[base + i]));
-            if (k < L.nz - 1) mw = fmax(mw, fabs((double)w[base + i]));
+            if (k < L.nz - 1 || (L.io & kHaloZHi)) mw = fmax(mw, fabs((double)w[base + i]));
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256) vmax_f32_kernel(Layout L, const float* __
             for (int e = 0; e < 4; ++e)
                 if (4 * q + e < L.nx) mv = max(mv, __float_as_uint(bv[e]) & 0x7fffffffu);
         }
-        if (k < L.nz - 1) {
+        if (k < L.nz - 1 || (L.io & kHaloZHi)) {
             const float4 d = __ldg(reinterpret_cast<const float4*>(w + c));
             const float dv[4] = {d.x, d.y, d.z, d.w};
 #pragma unroll
@@ -335,8 +335,8 @@ __global__ void fluid_kernel(Layout L, const T* __restrict__ phi, T* __restrict_
             if (i == L.nx - 1) { ro[c + q] = r; visc[c + q] = m; }
             if (!L.two_d && j == 0) { ro[c - q * L.sy] = r; visc[c - q * L.sy] = m; }
             if (!L.two_d && j == L.ny - 1) { ro[c + q * L.sy] = r; visc[c + q * L.sy] = m; }
-            if (k == 0) { ro[c - q * L.sz] = r; visc[c - q * L.sz] = m; }
-            if (k == L.nz - 1) { ro[c + q * L.sz] = r; visc[c + q * L.sz] = m; }
+            if (k == 0 && !(L.io & kHaloZLo)) { ro[c - q * L.sz] = r; visc[c - q * L.sz] = m; }
+            if (k == L.nz - 1 && !(L.io & kHaloZHi)) { ro[c + q * L.sz] = r; visc[c + q * L.sz] = m; }
         }
         const double vol = dxn[i + 5] * dyn[j + 5] * dzn[k + 5];
         a += vol * (H - (1.0 - 1.0));
@@ -610,6 +610,11 @@ int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, c
         io_ghost_kernel<double><<<blocks, 256, 0, st>>>(L, static_cast<double*>(phi), static_cast<double*>(a1),
                                                         static_cast<double*>(a2), p, step ? 1 : 0);
     return n + 1;
+}
+
+int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st) {
+    dt_kernel<<<1, 1, 0, st>>>(s.vmax, s.vscale, dxmin, n47, s.dt);
+    return 1;
 }
 
 int launch_netvol(const Scratch& s, double qi, double qo, cudaStream_t st) {

@@ -78,8 +78,10 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, Stag
             if (j == g.L.ny - 1) { a.out[c + sy] = val; a.out[c + 2 * sy] = val; a.out[c + 3 * sy] = val; }
         }
         const long long sz = g.L.sz;
-        if (k == 0) { a.out[c - sz] = val; a.out[c - 2 * sz] = val; a.out[c - 3 * sz] = val; }
-        if (k == g.L.nz - 1) { a.out[c + sz] = val; a.out[c + 2 * sz] = val; a.out[c + 3 * sz] = val; }
+        if (k == 0 && !(g.L.io & kHaloZLo)) { a.out[c - sz] = val; a.out[c - 2 * sz] = val; a.out[c - 3 * sz] = val; }
+        if (k == g.L.nz - 1 && !(g.L.io & kHaloZHi)) {
+            a.out[c + sz] = val; a.out[c + 2 * sz] = val; a.out[c + 3 * sz] = val;
+        }
         if (VOLUME) {
             const double PI_REF = 3.14159265359;  // src/definitions.h:37
             const double p = val, psi = g.psi;
@@ -87,8 +89,7 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, Stag
             if (p > psi) H = 1.0;
             if (p < -psi) H = 0.0;
             if (fabs(p) <= psi) H = 0.5 * (1.0 + p / psi + (1.0 / PI_REF) * sin((PI_REF * p) / psi));
-            const double vol = (double)__ldg(g.dxn[0] + i + 5) * (double)__ldg(g.dxn[1] + j + 5) *
-                               (double)__ldg(g.dxn[2] + k + 5);
+            const double vol = __ldg(g.dxn_d[0] + i + 5) * __ldg(g.dxn_d[1] + j + 5) * __ldg(g.dxn_d[2] + k + 5);
             v1 = vol * H;
             v2 = vol * (1.0 - H);
         }

@@ -495,10 +495,10 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                 if (gyhi)
                     for (int q = 1; q <= 3; ++q)
                         for (int e = 0; e < nw; ++e) a.out[c + q * L.sy + e] = e ? val.y : val.x;
-                if (k == 0)
+                if (k == 0 && !(L.io & kHaloZLo))  // a slab face's ghosts come from the neighbour
                     for (int q = 1; q <= 3; ++q)
                         for (int e = 0; e < nw; ++e) a.out[c - q * L.sz + e] = e ? val.y : val.x;
-                if (k == L.nz - 1)
+                if (k == L.nz - 1 && !(L.io & kHaloZHi))
                     for (int q = 1; q <= 3; ++q)
                         for (int e = 0; e < nw; ++e) a.out[c + q * L.sz + e] = e ? val.y : val.x;
             }

@@ -52,8 +52,8 @@ __device__ __forceinline__ void write_ghosts(const Layout& L, T* out, long long 
         if (j == 0) { out[c - L.sy] = val; out[c - 2 * L.sy] = val; out[c - 3 * L.sy] = val; }
         if (j == L.ny - 1) { out[c + L.sy] = val; out[c + 2 * L.sy] = val; out[c + 3 * L.sy] = val; }
     }
-    if (k == 0) { out[c - L.sz] = val; out[c - 2 * L.sz] = val; out[c - 3 * L.sz] = val; }
-    if (k == L.nz - 1) { out[c + L.sz] = val; out[c + 2 * L.sz] = val; out[c + 3 * L.sz] = val; }
+    if (k == 0 && !(L.io & kHaloZLo)) { out[c - L.sz] = val; out[c - 2 * L.sz] = val; out[c - 3 * L.sz] = val; }
+    if (k == L.nz - 1 && !(L.io & kHaloZHi)) { out[c + L.sz] = val; out[c + 2 * L.sz] = val; out[c + 3 * L.sz] = val; }
 }
 
 // Deterministic block sum of two doubles (fixed shuffle tree, fixed warp

@@ -26,14 +26,19 @@ struct Layout {
     long long sy, sz;
     long long ncell;  // px*py*pz
     bool two_d;
-    // inflow / outflow faces (0 for the closed box): kIoSkipLo / kIoSkipHi
-    // leave the x-min / x-max face ghosts of a level-set field untouched
-    // (ghost label 0 of src/gc_epol4.cpp:26-58); kIoEdge also writes the
-    // edge ghost (-1, j, nz) of each inflow column, which the inflow water
-    // level reads (src/ioflow_waterlevel.cpp:55)
+    // faces whose ghosts the stage kernels do not write (0 for the closed
+    // box).  Inflow / outflow: kIoSkipLo / kIoSkipHi leave the x-min / x-max
+    // face ghosts of a level-set field untouched (ghost label 0 of
+    // src/gc_epol4.cpp:26-58); kIoEdge also writes the edge ghost
+    // (-1, j, nz) of each inflow column, which the inflow water level reads
+    // (src/ioflow_waterlevel.cpp:55).  Subdomain (slab) boundaries:
+    // kHaloZLo / kHaloZHi mark z faces whose ghost planes a neighbour's
+    // halo fills (src/gcx_parax.cpp) -- no wall copy there, for any field,
+    // and the z faces at nz-1 belong to the CFL maximum (wlast = 0 with a
+    // neighbour above, src/lexer_gridsize.cpp:78-79).
     int io;
 };
-constexpr int kIoSkipLo = 1, kIoSkipHi = 2, kIoEdge = 4;
+constexpr int kIoSkipLo = 1, kIoSkipHi = 2, kIoEdge = 4, kHaloZLo = 8, kHaloZHi = 16;
 
 Layout make_layout(int nx, int ny, int nz);
 
@@ -74,6 +79,9 @@ struct KGrid {
     double f43;
     int f49;
     double psi;
+    // FP64 cell sizes DXN, DYN, DZN for the volume sums (the FP32 form
+    // sums in FP64 with the exact cell volumes)
+    const double* dxn_d[3];
     // direct-forcing convection stencils (X45 1..6, FP64 only): the body
     // field they read and 0.6 DXM, the fb threshold of X45 = 1
     int x45;
@@ -189,6 +197,8 @@ constexpr int kIoPhimean = 0, kIoPhiout = 1, kIoCount = 2, kIoWsfout = 3, kIoFou
 // step == false: fsfrkin/fsfrkout only (the start of reini_RK3::start).
 int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, bool step,
                     cudaStream_t st);
+// dt from the velocity maxima already in s.vmax (the CFL's second kernel).
+int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st);
 // picard_lsm's netvol = netvol + Qi dt - Qo dt (src/picard_lsm.cpp:93)
 int launch_netvol(const Scratch& s, double qi, double qo, cudaStream_t st);
 // host layout <-> device layout (src is a device staging copy of the host array)
