@@ -141,6 +141,32 @@ int r3d_convection_L(r3d_handle* h, int field_in);
 int r3d_reinidisc_L(r3d_handle* h, int field_in);
 int r3d_ghost_fill(r3d_handle* h, int field);
 
+/* Writes the instance's level set (and, with the fluid update on, its
+ * density and viscosity) as a VTK unstructured-grid file the way the
+ * reference's printer does (printer_CFD::print_vtu, src/printer_CFD.cpp:
+ * 356-727; src/vtu3D.cpp): Float32 point data "phi", "rho", "viscosity" at
+ * the grid nodes with the reference's interpolations (ipol4phi, ipol4_a,
+ * ipol4, src/interpolation_ipol.cpp), node coordinates, hexahedral cells,
+ * appended raw data, and the device clock as TimeValue.  The point data is
+ * formed on the device; the eight triple-corner ghost cells, which the
+ * reference never writes, enter the corner nodes as their corner cell.
+ * Synchronous. */
+int r3d_write_vtu(r3d_handle* h, const char* path);
+
+/* Checkpoint and resume of an instance (the role of the reference's state
+ * files, src/cfd_state_write.cpp / cfd_state_read.cpp, for the fields this
+ * library holds): r3d_save_state writes every device field (level set,
+ * stage buffers, velocities, and ro, visc, body when enabled) in the
+ * instance's own precision, bit for bit, with the device scalars a step
+ * reads (dt, clock, velocity factor, picard and inflow/outflow state);
+ * r3d_load_state restores them into an instance created from the same grid
+ * description and configured the same way (fluid update, direct forcing,
+ * inflow/outflow), so that a resumed run continues exactly as the
+ * uninterrupted one.  Unlike the reference's state files (single precision)
+ * nothing is rounded.  Synchronous. */
+int r3d_save_state(r3d_handle* h, const char* path);
+int r3d_load_state(r3d_handle* h, const char* path);
+
 /* Volume sums of the smoothed Heaviside (fluid_update_fsf::start,
  * src/fluid_update_fsf.cpp:39-74), FP64.  Synchronous. */
 int r3d_volume(r3d_handle* h, double* volume1, double* volume2);

@@ -312,6 +312,15 @@ class RefOracle:
         self._lib.refls_update()
         return self._lib.refls_volume1(), self._lib.refls_volume2()
 
+    def vtu_point_data(self):
+        """The reference printer's phi, rho, viscosity at the grid nodes."""
+        ny = self.ny + 1 if self.ny > 1 else 2
+        n = (self.nx + 1) * ny * (self.nz + 1)
+        out = [np.zeros(n, dtype=np.float32) for _ in range(3)]
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._lib.refls_vtu_point_data(*(a.ctypes.data_as(fp) for a in out))
+        return out
+
     def io_levels(self):
         """(phimean, phiout) after the last step's fsfinflow."""
         out = np.zeros(4)

@@ -384,6 +384,26 @@ double refls_psi() { return P->psi; }
 double refls_dxm() { return P->DXM; }
 double refls_volume1() { return P->volume1; }
 double refls_volume2() { return P->volume2; }
+// Point data of the reference's VTU printer over the TPLOOP nodes (i
+// fastest, src/printer_CFD.cpp:678-727): ipol4phi(a->phi), ipol4_a(a->ro),
+// ipol4(a->visc), each stored as float like the printer.
+int refls_vtu_point_data(float* phi, float* ro, float* visc) {
+    lexer* p = P;
+    long n = 0;
+    for (int k = -1; k < p->knoz; ++k)
+        for (int j = -1; j < p->knoy; ++j)
+            for (int i = -1; i < p->knox; ++i) {
+                increment::i = i;
+                increment::j = j;
+                increment::k = k;
+                phi[n] = float(p->ipol4phi(A, A->phi));
+                ro[n] = float(p->ipol4_a(A->ro));
+                visc[n] = float(p->ipol4(A->visc));
+                ++n;
+            }
+    return 0;
+}
+
 // Water levels of the last ioflow_f::fsfinflow (src/ioflow_waterlevel.cpp:29-141).
 int refls_io_levels(double* out) {
     out[0] = P->phimean; out[1] = P->phiout;

@@ -86,6 +86,9 @@ EXPORTS = {
     "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
     "r3d_set_direct_forcing": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_set_halo": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_write_vtu": ([_H, ctypes.c_char_p], ctypes.c_int),
+    "r3d_save_state": ([_H, ctypes.c_char_p], ctypes.c_int),
+    "r3d_load_state": ([_H, ctypes.c_char_p], ctypes.c_int),
     "r3d_grid_spacing": ([ctypes.POINTER(GridDesc), _D], ctypes.c_int),
     "r3d_set_grid_spacing": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "r3d_halo_bytes": ([_H, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
@@ -306,6 +309,19 @@ class LevelSet:
         """X45 direct-forcing convection stencils reading the BODY field
         (r3d_set_direct_forcing); 0 turns them off."""
         _check(_lib.r3d_set_direct_forcing(self.h, x45), self.h)
+
+    def write_vtu(self, path):
+        """The level set (and rho, viscosity) as a VTU file like the
+        reference's printer (r3d_write_vtu)."""
+        _check(_lib.r3d_write_vtu(self.h, os.fsencode(path)), self.h)
+
+    def save_state(self, path):
+        """Checkpoint every device field and step scalar (r3d_save_state)."""
+        _check(_lib.r3d_save_state(self.h, os.fsencode(path)), self.h)
+
+    def load_state(self, path):
+        """Resume from a checkpoint of the same grid and configuration."""
+        _check(_lib.r3d_load_state(self.h, os.fsencode(path)), self.h)
 
     def set_halo(self, zlo, zhi):
         """Mark the z-min / z-max faces as subdomain boundaries (r3d_set_halo)."""

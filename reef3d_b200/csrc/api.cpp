@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -613,6 +614,218 @@ int r3d_ghost_fill(r3d_handle* h, int field) {
     DeviceGuard dg(h->device, h->batch_stream);
     h->launches += launch_ghost_fill(h->L, h->field[field], fp32(h), h->stream);
     R3D_CUDA(h, cudaGetLastError());
+    return R3D_OK;
+}
+
+int r3d_write_vtu(r3d_handle* h, const char* path) {
+    if (!h || !path) return fail(h, R3D_EINVAL, "null argument");
+    DeviceGuard dg(h->device, h->batch_stream);
+    const Layout& L = h->L;
+    const long long nyp = L.two_d ? 2 : L.ny + 1;
+    const long long np = (long long)(L.nx + 1) * nyp * (L.nz + 1);
+    const long long nc = (long long)L.nx * L.ny * L.nz;
+    if (32 * nc > 0xffffffffLL || 12 * np > 0xffffffffLL)
+        return fail(h, R3D_EINVAL, "grid too large for a VTU file with 32-bit block sizes");
+    const int nf = h->fluid ? 3 : 1;
+    float* dev = nullptr;
+    if (cudaMalloc(&dev, (size_t)nf * np * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, R3D_ENOMEM, "VTU point data buffer");
+    }
+    h->launches += launch_vtu_nodes(L, h->field[R3D_PHI], h->fluid ? h->field[R3D_RO] : nullptr,
+                                    h->fluid ? h->field[R3D_VISC] : nullptr, fp32(h), dev, np, h->stream);
+    std::vector<float> pd((size_t)nf * np);
+    double t = 0.0;
+    cudaMemcpyAsync(pd.data(), dev, pd.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(&t, h->S.t, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(dev);
+    if (e != cudaSuccess) return cuda_fail(h, e, "VTU point data");
+
+    // The reference's printer layout (src/printer_CFD.cpp:356-600,
+    // src/vtu3D.cpp:63-101,125-225): point data at the TPLOOP nodes, then the
+    // node coordinates, hexahedral cells in k, j, i order with the node
+    // numbering of initialize::nodecalc (src/initialize.cpp:118-131),
+    // appended raw blocks each preceded by its byte count.
+    const char* names[3] = {"phi", "rho", "viscosity"};
+    std::ostringstream x;
+    long long off = 0;
+    x << "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"1.0\" byte_order=\"LittleEndian\">\n"
+      << "<UnstructuredGrid>\n<FieldData>\n<DataArray type=\"Float64\" Name=\"TimeValue\" NumberOfTuples=\"1\"> "
+      << t << "\n</DataArray>\n</FieldData>\n<Piece NumberOfPoints=\"" << np << "\" NumberOfCells=\"" << nc
+      << "\">\n<PointData>\n";
+    for (int q = 0; q < nf; ++q) {
+        x << "<DataArray type=\"Float32\" Name=\"" << names[q] << "\" format=\"appended\" offset=\"" << off
+          << "\"/>\n";
+        off += 4 + 4 * np;
+    }
+    x << "</PointData>\n<CellData>\n</CellData>\n<Points>\n<DataArray type=\"Float32\" NumberOfComponents=\"3\" "
+      << "format=\"appended\" offset=\"" << off << "\"/>\n</Points>\n<Cells>\n";
+    off += 4 + 12 * np;
+    x << "<DataArray type=\"Int32\" Name=\"connectivity\" format=\"appended\" offset=\"" << off << "\"/>\n";
+    off += 4 + 32 * nc;
+    x << "<DataArray type=\"Int32\" Name=\"offsets\" format=\"appended\" offset=\"" << off << "\"/>\n";
+    off += 4 + 4 * nc;
+    x << "<DataArray type=\"Int32\" Name=\"types\" format=\"appended\" offset=\"" << off << "\"/>\n"
+      << "</Cells>\n</Piece>\n</UnstructuredGrid>\n<AppendedData encoding=\"raw\">\n_";
+
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(h, R3D_EINVAL, std::string("cannot open ") + path);
+    const std::string head = x.str();
+    bool ok = std::fwrite(head.data(), 1, head.size(), fp) == head.size();
+    auto block = [&](const void* data, long long bytes) {
+        const unsigned n = (unsigned)bytes;
+        ok = ok && std::fwrite(&n, sizeof n, 1, fp) == 1;
+        ok = ok && (bytes == 0 || std::fwrite(data, 1, (size_t)bytes, fp) == (size_t)bytes);
+    };
+    for (int q = 0; q < nf; ++q) block(pd.data() + (size_t)q * np, 4 * np);
+    {
+        std::vector<float> xyz((size_t)3 * np);
+        size_t m = 0;
+        for (long long k = -1; k < L.nz; ++k)
+            for (long long j = -1; j < nyp - 1; ++j)
+                for (long long i = -1; i < L.nx; ++i) {
+                    xyz[m++] = (float)h->M.xn[0][i + 6];
+                    xyz[m++] = (float)h->M.xn[1][j + 6];
+                    xyz[m++] = (float)h->M.xn[2][k + 6];
+                }
+        block(xyz.data(), 12 * np);
+    }
+    {
+        std::vector<int> con((size_t)8 * nc);
+        const long long sx = L.nx + 1, sy = sx * nyp;
+        auto id = [&](long long i, long long j, long long k) { return (int)((k + 1) * sy + (j + 1) * sx + (i + 1)); };
+        size_t m = 0;
+        for (long long k = 0; k < L.nz; ++k)
+            for (long long j = 0; j < L.ny; ++j)
+                for (long long i = 0; i < L.nx; ++i) {
+                    con[m++] = id(i - 1, j - 1, k - 1);
+                    con[m++] = id(i, j - 1, k - 1);
+                    con[m++] = id(i, j, k - 1);
+                    con[m++] = id(i - 1, j, k - 1);
+                    con[m++] = id(i - 1, j - 1, k);
+                    con[m++] = id(i, j - 1, k);
+                    con[m++] = id(i, j, k);
+                    con[m++] = id(i - 1, j, k);
+                }
+        block(con.data(), 32 * nc);
+        for (long long c = 0; c < nc; ++c) con[(size_t)c] = (int)((c + 1) * 8);
+        block(con.data(), 4 * nc);
+        for (long long c = 0; c < nc; ++c) con[(size_t)c] = 12;  // VTK_HEXAHEDRON
+        block(con.data(), 4 * nc);
+    }
+    const char tail[] = "\n</AppendedData>\n</VTKFile>";
+    ok = ok && std::fwrite(tail, 1, sizeof tail - 1, fp) == sizeof tail - 1;
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(h, R3D_EINVAL, std::string("writing ") + path + " failed");
+    return R3D_OK;
+}
+
+// ---------------------------------------------------------- checkpoint
+namespace {
+constexpr char kStateMagic[8] = {'R', '3', 'D', 'S', 'T', 'A', 'T', 'E'};
+constexpr unsigned kStateVersion = 1;
+
+// FNV-1a over the node coordinates: a state loads only into the grid it
+// was written from.
+unsigned long long grid_hash(const r3d_handle* h) {
+    unsigned long long x = 1469598103934665603ULL;
+    for (int a = 0; a < 3; ++a)
+        for (int t = 0; t < h->M.n[a] + 11; ++t) {
+            unsigned long long b;
+            std::memcpy(&b, &h->M.xn[a][t], sizeof b);
+            for (int q = 0; q < 8; ++q) {
+                x ^= (b >> (8 * q)) & 0xffULL;
+                x *= 1099511628211ULL;
+            }
+        }
+    return x;
+}
+
+struct StateHead {
+    char magic[8];
+    unsigned version;
+    int nx, ny, nz, precision;
+    int fluid, x45, io;
+    unsigned long long grid;
+    double scalars[32];  // dt, t, vscale, picard (4), hook state (8), volumes (2)
+};
+}  // namespace
+
+int r3d_save_state(r3d_handle* h, const char* path) {
+    if (!h || !path) return fail(h, R3D_EINVAL, "null argument");
+    DeviceGuard dg(h->device, h->batch_stream);
+    StateHead hd{};
+    std::memcpy(hd.magic, kStateMagic, 8);
+    hd.version = kStateVersion;
+    hd.nx = h->L.nx;
+    hd.ny = h->L.ny;
+    hd.nz = h->L.nz;
+    hd.precision = h->desc.precision;
+    hd.fluid = h->fluid ? 1 : 0;
+    hd.x45 = h->g64.x45;
+    hd.io = h->io ? 1 : 0;
+    hd.grid = grid_hash(h);
+    double* sc = hd.scalars;
+    cudaMemcpyAsync(sc + 0, h->S.dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(sc + 1, h->S.t, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(sc + 2, h->S.vscale, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(sc + 3, h->S.pic, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (h->io) cudaMemcpyAsync(sc + 7, h->io_buf, kIoStateLen * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(sc + 15, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    const size_t bytes = (size_t)h->L.ncell * elem(h);
+    std::vector<char> buf(bytes);
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(h, R3D_EINVAL, std::string("cannot open ") + path);
+    bool ok = true;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    ok = e == cudaSuccess && std::fwrite(&hd, sizeof hd, 1, fp) == 1;
+    for (int id = 0; id <= R3D_BODY && ok; ++id) {
+        if (!h->field[id] || id == R3D_L) continue;
+        e = cudaMemcpy(buf.data(), h->field[id], bytes, cudaMemcpyDeviceToHost);
+        ok = e == cudaSuccess && std::fwrite(&id, sizeof id, 1, fp) == 1 && std::fwrite(buf.data(), 1, bytes, fp) == bytes;
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    if (e != cudaSuccess) return cuda_fail(h, e, "reading the state");
+    if (!ok) return fail(h, R3D_EINVAL, std::string("writing ") + path + " failed");
+    return R3D_OK;
+}
+
+int r3d_load_state(r3d_handle* h, const char* path) {
+    if (!h || !path) return fail(h, R3D_EINVAL, "null argument");
+    DeviceGuard dg(h->device, h->batch_stream);
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return fail(h, R3D_EINVAL, std::string("cannot open ") + path);
+    StateHead hd{};
+    const bool got = std::fread(&hd, sizeof hd, 1, fp) == 1;
+    auto bad = [&](const char* why) {
+        std::fclose(fp);
+        return fail(h, R3D_EINVAL, std::string(path) + ": " + why);
+    };
+    if (!got || std::memcmp(hd.magic, kStateMagic, 8) != 0 || hd.version != kStateVersion)
+        return bad("not a state file of this version");
+    if (hd.nx != h->L.nx || hd.ny != h->L.ny || hd.nz != h->L.nz || hd.precision != h->desc.precision ||
+        hd.grid != grid_hash(h))
+        return bad("written from another grid or precision");
+    if (hd.fluid != (h->fluid ? 1 : 0) || hd.x45 != h->g64.x45 || hd.io != (h->io ? 1 : 0))
+        return bad("written with another fluid / direct-forcing / inflow-outflow configuration");
+    const size_t bytes = (size_t)h->L.ncell * elem(h);
+    std::vector<char> buf(bytes);
+    int id = -1;
+    while (std::fread(&id, sizeof id, 1, fp) == 1) {
+        if (id < 0 || id > R3D_BODY || !h->field[id]) return bad("unexpected field");
+        if (std::fread(buf.data(), 1, bytes, fp) != bytes) return bad("truncated");
+        R3D_CUDA(h, cudaMemcpy(h->field[id], buf.data(), bytes, cudaMemcpyHostToDevice));
+    }
+    std::fclose(fp);
+    const double* sc = hd.scalars;
+    R3D_CUDA(h, cudaMemcpy(h->S.dt, sc + 0, sizeof(double), cudaMemcpyHostToDevice));
+    R3D_CUDA(h, cudaMemcpy(h->S.t, sc + 1, sizeof(double), cudaMemcpyHostToDevice));
+    R3D_CUDA(h, cudaMemcpy(h->S.vscale, sc + 2, sizeof(double), cudaMemcpyHostToDevice));
+    R3D_CUDA(h, cudaMemcpy(h->S.pic, sc + 3, 4 * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->io) R3D_CUDA(h, cudaMemcpy(h->io_buf, sc + 7, kIoStateLen * sizeof(double), cudaMemcpyHostToDevice));
+    R3D_CUDA(h, cudaMemcpy(h->S.vol, sc + 15, 2 * sizeof(double), cudaMemcpyHostToDevice));
+    h->dt_host = sc[0];
     return R3D_OK;
 }
 

@@ -585,6 +585,73 @@ __global__ void __launch_bounds__(256) io_ghost_kernel(Layout L, T* __restrict__
     }
 }
 
+// ------------------------------------------------------ VTU point data
+// Cell value as the reference's fields hold it around the interior: face
+// ghosts as stored (the y face ghosts of a 2D field, which start4 skips, as
+// zero), the first diagonal (edge) ghosts as the copy of the diagonal
+// interior cell that dgcpol4 writes (src/gc_dgcpol4.cpp:28-50, also in 2D);
+// the eight triple-corner ghosts, which nothing in the reference writes, as
+// the corner cell.
+template <typename T>
+__device__ __forceinline__ double vtu_cell(const Layout& L, const T* f, int i, int j, int k) {
+    const int out = (i < 0 || i >= L.nx) + (j < 0 || j >= L.ny) + (k < 0 || k >= L.nz);
+    if (out == 1 && L.two_d && j != 0) return 0.0;
+    if (out >= 2) {
+        i = i < 0 ? 0 : (i >= L.nx ? L.nx - 1 : i);
+        j = j < 0 ? 0 : (j >= L.ny ? L.ny - 1 : j);
+        k = k < 0 ? 0 : (k >= L.nz ? L.nz - 1 : k);
+    }
+    return static_cast<double>(f[(long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx)]);
+}
+
+// Point data of the reference's VTU printer at the grid nodes (TPLOOP:
+// node (i,j,k) for i,j,k = -1..n-1, between cells i and i+1; i fastest),
+// src/printer_CFD.cpp:678-727:
+//   phi: ipol4phi, the mean of the 8 surrounding cells
+//        (src/interpolation_ipol.cpp:480-541);
+//   rho: ipol4_a, 8 cells (2D: the 4 of the j = 0 plane) (:543-559);
+//   viscosity: ipol4, the surrounding interior cells only (flag4 > 0),
+//        divided by 8 (2D: 4) all the same (:326-372).
+// Computed in FP64 in the reference's operation order, stored as float.
+template <typename T>
+__global__ void __launch_bounds__(256) vtu_node_kernel(Layout L, const T* __restrict__ phi, const T* __restrict__ ro,
+                                                       const T* __restrict__ visc, float* __restrict__ out,
+                                                       long long npoints) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= npoints) return;
+    const int nyp = L.two_d ? 2 : L.ny + 1;
+    const int i = (int)(n % (L.nx + 1)) - 1;
+    const int j = (int)((n / (L.nx + 1)) % nyp) - 1;
+    const int k = (int)(n / ((long long)(L.nx + 1) * nyp)) - 1;
+    auto b = [&](const T* f, int di, int dj, int dk) { return vtu_cell(L, f, i + di, j + dj, k + dk); };
+    out[n] = (float)(0.125 * (b(phi, 0, 0, 0) + b(phi, 0, 1, 0) + b(phi, 1, 0, 0) + b(phi, 1, 1, 0) +
+                              b(phi, 0, 0, 1) + b(phi, 0, 1, 1) + b(phi, 1, 0, 1) + b(phi, 1, 1, 1)));
+    if (!ro) return;
+    double r, m;
+    auto in = [&](int di, int dj, int dk) {
+        const int ii = i + di, jj = j + dj, kk = k + dk;
+        return ii >= 0 && ii < L.nx && jj >= 0 && jj < L.ny && kk >= 0 && kk < L.nz;
+    };
+    if (L.two_d) {
+        // ipol4_a and ipol4 evaluate at j = 0 in 2D
+        const int jj = -j;
+        r = 0.25 * (b(ro, 0, jj, 0) + b(ro, 1, jj, 0) + b(ro, 0, jj, 1) + b(ro, 1, jj, 1));
+        const double v1 = in(0, jj, 0) ? b(visc, 0, jj, 0) : 0.0, v2 = in(1, jj, 0) ? b(visc, 1, jj, 0) : 0.0;
+        const double v3 = in(0, jj, 1) ? b(visc, 0, jj, 1) : 0.0, v4 = in(1, jj, 1) ? b(visc, 1, jj, 1) : 0.0;
+        m = 0.25 * (v1 + v2 + v3 + v4);
+    } else {
+        r = 0.125 * (b(ro, 0, 0, 0) + b(ro, 0, 1, 0) + b(ro, 1, 0, 0) + b(ro, 1, 1, 0) + b(ro, 0, 0, 1) +
+                     b(ro, 0, 1, 1) + b(ro, 1, 0, 1) + b(ro, 1, 1, 1));
+        double v[8];
+        const int d[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 0, 0}, {1, 1, 0}, {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = in(d[q][0], d[q][1], d[q][2]) ? b(visc, d[q][0], d[q][1], d[q][2]) : 0.0;
+        m = 0.125 * (v[0] + v[1] + v[2] + v[3] + v[4] + v[5] + v[6] + v[7]);
+    }
+    out[npoints + n] = (float)r;
+    out[2 * npoints + n] = (float)m;
+}
+
 // picard_lsm::correct_ls's target update netvol = netvol + Qi dt - Qo dt
 // (src/picard_lsm.cpp:93), before its iterations.
 __global__ void netvol_kernel(double* pic, const double* dt, double qi, double qo) {
@@ -614,6 +681,19 @@ int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, c
 
 int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st) {
     dt_kernel<<<1, 1, 0, st>>>(s.vmax, s.vscale, dxmin, n47, s.dt);
+    return 1;
+}
+
+int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const void* visc, bool fp32, float* out,
+                     long long npoints, cudaStream_t st) {
+    const unsigned blocks = (unsigned)((npoints + 255) / 256);
+    if (fp32)
+        vtu_node_kernel<float><<<blocks, 256, 0, st>>>(L, static_cast<const float*>(phi), static_cast<const float*>(ro),
+                                                       static_cast<const float*>(visc), out, npoints);
+    else
+        vtu_node_kernel<double><<<blocks, 256, 0, st>>>(L, static_cast<const double*>(phi),
+                                                        static_cast<const double*>(ro),
+                                                        static_cast<const double*>(visc), out, npoints);
     return 1;
 }
 

@@ -197,6 +197,10 @@ constexpr int kIoPhimean = 0, kIoPhiout = 1, kIoCount = 2, kIoWsfout = 3, kIoFou
 // step == false: fsfrkin/fsfrkout only (the start of reini_RK3::start).
 int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, bool step,
                     cudaStream_t st);
+// VTU point data at the grid nodes: out[0..n) phi, then rho and viscosity
+// when ro != nullptr (3 n floats).
+int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const void* visc, bool fp32, float* out,
+                     long long npoints, cudaStream_t st);
 // dt from the velocity maxima already in s.vmax (the CFL's second kernel).
 int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st);
 // picard_lsm's netvol = netvol + Qi dt - Qo dt (src/picard_lsm.cpp:93)
