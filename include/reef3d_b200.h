@@ -267,9 +267,12 @@ int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt);
  *       6: as 3, but 1e20 where masked                      (body = a->fbh4)
  * The body field is R3D_BODY, allocated (zeroed) by the first call with
  * x45 != 0 and uploaded like any field (REEF3D layout: its ghost cells are
- * read too).  The reinitialisation is unchanged (the reference applies X45
- * to the convection only).  FP64 instances only; 0 turns it off.
- * Synchronous.  Not for batch members. */
+ * read too); it is held in FP64 in both arithmetic forms, so the mask
+ * decisions are the reference's.  The reinitialisation is unchanged (the
+ * reference applies X45 to the convection only).  FP32 instances take X45
+ * 1..5 (the 1e20 of X45 6 squares past the FP32 range) and run the
+ * one-cell-per-thread kernels.  0 turns it off.  Synchronous.  Not for
+ * batch members. */
 int r3d_set_direct_forcing(r3d_handle* h, int x45);
 
 /* Inflow and outflow boundaries with the level-set hooks of REEF3D's

@@ -177,9 +177,14 @@ struct DeviceGuard {
     ~DeviceGuard() { int cur = 0; cudaGetDevice(&cur); if (cur != prev) cudaSetDevice(prev); }
 };
 
-// The tiled kernels fill every face as a wall: instances with inflow /
-// outflow faces run the one-cell-per-thread kernels.
-bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile && !h->io; }
+// The tiled kernels fill every face as a wall and know only the plain
+// stencils: instances with inflow / outflow faces or direct forcing run the
+// one-cell-per-thread kernels.
+bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile && !h->io && !h->g64.x45; }
+
+// The body field of the direct-forcing stencils is FP64 in both forms.
+size_t field_elem(const r3d_handle* h, int id) { return id == R3D_BODY ? sizeof(double) : elem(h); }
+bool field_fp32(const r3d_handle* h, int id) { return fp32(h) && id != R3D_BODY; }
 
 }  // namespace
 
@@ -447,7 +452,7 @@ int r3d_upload(r3d_handle* h, int field, const double* host, int layout) {
     if (int rc = ensure_staging(h)) return rc;
     const size_t n = host_count(h, layout);
     R3D_CUDA(h, cudaMemcpyAsync(h->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    h->launches += launch_import(h->L, h->staging, layout, h->field[field], fp32(h), h->stream);
+    h->launches += launch_import(h->L, h->staging, layout, h->field[field], field_fp32(h, field), h->stream);
     R3D_CUDA(h, cudaGetLastError());
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     return R3D_OK;
@@ -462,7 +467,7 @@ int r3d_download(r3d_handle* h, int field, double* host, int layout) {
     if (int rc = ensure_staging(h)) return rc;
     const size_t n = host_count(h, layout);
     if (layout == R3D_LAYOUT_REEF3D) R3D_CUDA(h, cudaMemsetAsync(h->staging, 0, n * sizeof(double), h->stream));
-    h->launches += launch_export(h->L, h->field[field], fp32(h), layout, h->staging, h->stream);
+    h->launches += launch_export(h->L, h->field[field], field_fp32(h, field), layout, h->staging, h->stream);
     R3D_CUDA(h, cudaGetLastError());
     R3D_CUDA(h, cudaMemcpyAsync(host, h->staging, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -773,8 +778,7 @@ int r3d_save_state(r3d_handle* h, const char* path) {
     cudaMemcpyAsync(sc + 3, h->S.pic, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     if (h->io) cudaMemcpyAsync(sc + 7, h->io_buf, kIoStateLen * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     cudaMemcpyAsync(sc + 15, h->S.vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-    const size_t bytes = (size_t)h->L.ncell * elem(h);
-    std::vector<char> buf(bytes);
+    std::vector<char> buf((size_t)h->L.ncell * sizeof(double));
     FILE* fp = std::fopen(path, "wb");
     if (!fp) return fail(h, R3D_EINVAL, std::string("cannot open ") + path);
     bool ok = true;
@@ -782,6 +786,7 @@ int r3d_save_state(r3d_handle* h, const char* path) {
     ok = e == cudaSuccess && std::fwrite(&hd, sizeof hd, 1, fp) == 1;
     for (int id = 0; id <= R3D_BODY && ok; ++id) {
         if (!h->field[id] || id == R3D_L) continue;
+        const size_t bytes = (size_t)h->L.ncell * field_elem(h, id);
         e = cudaMemcpy(buf.data(), h->field[id], bytes, cudaMemcpyDeviceToHost);
         ok = e == cudaSuccess && std::fwrite(&id, sizeof id, 1, fp) == 1 && std::fwrite(buf.data(), 1, bytes, fp) == bytes;
     }
@@ -809,11 +814,11 @@ int r3d_load_state(r3d_handle* h, const char* path) {
         return bad("written from another grid or precision");
     if (hd.fluid != (h->fluid ? 1 : 0) || hd.x45 != h->g64.x45 || hd.io != (h->io ? 1 : 0))
         return bad("written with another fluid / direct-forcing / inflow-outflow configuration");
-    const size_t bytes = (size_t)h->L.ncell * elem(h);
-    std::vector<char> buf(bytes);
+    std::vector<char> buf((size_t)h->L.ncell * sizeof(double));
     int id = -1;
     while (std::fread(&id, sizeof id, 1, fp) == 1) {
         if (id < 0 || id > R3D_BODY || !h->field[id]) return bad("unexpected field");
+        const size_t bytes = (size_t)h->L.ncell * field_elem(h, id);
         if (std::fread(buf.data(), 1, bytes, fp) != bytes) return bad("truncated");
         R3D_CUDA(h, cudaMemcpy(h->field[id], buf.data(), bytes, cudaMemcpyHostToDevice));
     }
@@ -950,7 +955,7 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
         if (cudaMalloc(&h->io_buf, len * sizeof(double)) != cudaSuccess) {
             cudaGetLastError();
             h->io = false;
-            set_layout_io(h, 0);
+            set_layout_io(h, h->L.io & (kHaloZLo | kHaloZHi));
             return fail(h, R3D_ENOMEM, "ioflow state allocation failed");
         }
         h->io_buf_len = len;
@@ -1010,7 +1015,7 @@ int r3d_set_grid_spacing(r3d_handle* h, double dxm, double dym, double dzm) {
     else h->M.psi = h->desc.f45 * (1.0 / 3.0) * (dxm + dym + dzm);
     h->g64.psi = h->M.psi;
     h->g32.psi = h->M.psi;
-    h->g64.df_thr = 0.6 * dxm;
+    h->g64.df_thr = h->g32.df_thr = 0.6 * dxm;
     return R3D_OK;
 }
 
@@ -1042,7 +1047,7 @@ int r3d_halo_copy(r3d_handle* h, int field, int side, int dir, void* buf) {
         return fail(h, R3D_EINVAL, "side 0 (z-min) or 1 (z-max), dir 0 (pack) or 1 (unpack), device buffer");
     if (h->L.nz < 3) return fail(h, R3D_EINVAL, "a subdomain needs at least 3 cells in z");
     DeviceGuard dg(h->device, h->batch_stream);
-    const size_t e = elem(h), plane = (size_t)h->L.sz;
+    const size_t e = field_elem(h, field), plane = (size_t)h->L.sz;
     // planes k = 0..2 / nz-3..nz-1 (pack) and -3..-1 / nz..nz+2 (unpack);
     // plane k starts at (k + gz) * sz
     const long long k0 = dir == 0 ? (side == 0 ? 0 : h->L.nz - 3) : (side == 0 ? -3 : h->L.nz);
@@ -1088,10 +1093,11 @@ int r3d_set_direct_forcing(r3d_handle* h, int x45) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
     if (x45 < 0 || x45 > 6) return fail(h, R3D_EINVAL, "x45 must be 0..6");
-    if (x45 != 0 && fp32(h)) return fail(h, R3D_EINVAL, "the direct-forcing stencils run in the FP64 form");
+    if (x45 == 6 && fp32(h))
+        return fail(h, R3D_EINVAL, "X45 6 (1e20 in masked differences, whose squares overflow FP32) runs in FP64");
     DeviceGuard dg(h->device, h->batch_stream);
     if (x45 != 0 && !h->field[R3D_BODY]) {
-        const size_t bytes = (size_t)h->L.ncell * elem(h);
+        const size_t bytes = (size_t)h->L.ncell * sizeof(double);
         if (cudaMalloc(&h->field[R3D_BODY], bytes) != cudaSuccess) {
             cudaGetLastError();
             h->field[R3D_BODY] = nullptr;
@@ -1100,9 +1106,9 @@ int r3d_set_direct_forcing(r3d_handle* h, int x45) {
         R3D_CUDA(h, cudaMemsetAsync(h->field[R3D_BODY], 0, bytes, h->stream));
     }
     drop_step_graph(h);
-    h->g64.x45 = x45;
-    h->g64.df_thr = 0.6 * h->M.dxm_mean;  // 0.6*p->DXM, src/weno_hj_df_nug.cpp:402
-    h->g64.body = static_cast<const double*>(h->field[R3D_BODY]);
+    h->g64.x45 = h->g32.x45 = x45;
+    h->g64.df_thr = h->g32.df_thr = 0.6 * h->M.dxm_mean;  // 0.6*p->DXM, src/weno_hj_df_nug.cpp:402
+    h->g64.body = h->g32.body = static_cast<const double*>(h->field[R3D_BODY]);
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     return R3D_OK;
 }

@@ -13,7 +13,48 @@ __device__ __forceinline__ void load7(const float* __restrict__ f, long long c, 
     for (int m = 0; m < 7; ++m) o[m] = __ldg(f + c + (m - 3) * s);
 }
 
-template <bool TWO_D, bool UNIFORM>
+// Direct-forcing divided difference of the X45 stencils
+// (src/weno_hj_df_nug.cpp:398-987) in the FP32 form: the mask decisions on
+// the FP64 body field (the reference's), the difference in FP32.  X45 1..5
+// (6 writes 1e20 into masked differences, whose squares overflow FP32).
+__device__ __forceinline__ float df_q32(int x45, double thr, float fa, float fb, double ha, double hb, double hw,
+                                        float d) {
+    switch (x45) {
+        case 1: return (fabs(hb) > thr && fabs(ha) > thr) ? __fdividef(fb - fa, d) : 0.0f;
+        case 2: return __fdividef((float)(0.5 * (hb + ha)) * (fb - fa), d);
+        case 3: return (hb < 0.5 && ha < 0.5) ? __fdividef(fb - fa, d) : 0.0f;
+        case 4: return __fdividef((float)hw * (fb - fa), d);
+        default: return (hb > 0.0 && ha > 0.0) ? __fdividef(fb - fa, d) : 0.0f;
+    }
+}
+
+// deriv_tables with the X45 differences: fv, hv the 7-point windows of the
+// level set and the body field (centre at [3]); q_m from the pair
+// (m-1, m) of the six upwind points, the X45 4 weight at the pair's
+// upwind-most cell.
+__device__ __forceinline__ float deriv_tables_df(const float* fv, const double* hv, bool plus,
+                                                 const float* __restrict__ dp, const float* __restrict__ qf,
+                                                 const float* __restrict__ cf, const float* __restrict__ isf, int t,
+                                                 int x45, double thr) {
+    const int off = plus ? 1 : 0;
+    float q[5];
+#pragma unroll
+    for (int m = 1; m <= 5; ++m) {
+        const int a = m - 1 + off, b = m + off;
+        q[m - 1] = df_q32(x45, thr, fv[a], fv[b], hv[a], hv[b], plus ? hv[b] : hv[a], __ldg(dp + t - 4 + m + off));
+    }
+    const int side = plus ? 1 : 0;
+    return f32::weno5_tables(qf + t * 12 + side * 6, cf + t * 6 + side * 3, isf + t * 18 + side * 9, plus, q[0], q[1],
+                             q[2], q[3], q[4]);
+}
+
+__device__ __forceinline__ void load7d(const double* __restrict__ f, long long c, long long s, double* o) {
+#pragma unroll
+    for (int m = 0; m < 7; ++m) o[m] = __ldg(f + c + (m - 3) * s);
+}
+
+// DF: the direct-forcing stencils of g.x45 over g.body (table form).
+template <bool TWO_D, bool UNIFORM, bool DF = false>
 __device__ __forceinline__ float conv_L(const KGrid<float>& g, const float* __restrict__ f,
                                         const float* __restrict__ u, const float* __restrict__ v,
                                         const float* __restrict__ w, long long c, int i, int j, int k, float vs) {
@@ -21,27 +62,30 @@ __device__ __forceinline__ float conv_L(const KGrid<float>& g, const float* __re
     const float ia = 0.5f * vs * (__ldg(u + c) + __ldg(u + c - 1));
     const float ka = 0.5f * vs * (__ldg(w + c) + __ldg(w + c - sz));
     float fv[7];
+    double hv[7];
+    auto axis = [&](long long s, int a, int t, bool plus) {
+        if (DF) {
+            load7d(g.body, c, s, hv);
+            return deriv_tables_df(fv, hv, plus, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, g.x45, g.df_thr);
+        }
+        return UNIFORM ? f32::deriv_uniform<float>(fv, plus, g.rh[a], g.eps_u * g.h[a] * g.h[a])
+                       : f32::deriv_tables(fv, plus, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t);
+    };
     float l = 0.0f;
     if (ia != 0.0f) {
         load7(f, c, 1, fv);
-        const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ia < 0.0f, g.rh[0], g.eps_u * g.h[0] * g.h[0])
-                                : f32::deriv_tables(fv, ia < 0.0f, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], i + 5);
-        l -= ia * d;
+        l -= ia * axis(1, 0, i + 5, ia < 0.0f);
     }
     if (!TWO_D) {
         const float ja = 0.5f * vs * (__ldg(v + c) + __ldg(v + c - sy));
         if (ja != 0.0f) {
             load7(f, c, sy, fv);
-            const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ja < 0.0f, g.rh[1], g.eps_u * g.h[1] * g.h[1])
-                                    : f32::deriv_tables(fv, ja < 0.0f, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], j + 5);
-            l -= ja * d;
+            l -= ja * axis(sy, 1, j + 5, ja < 0.0f);
         }
     }
     if (ka != 0.0f) {
         load7(f, c, sz, fv);
-        const float d = UNIFORM ? f32::deriv_uniform<float>(fv, ka < 0.0f, g.rh[2], g.eps_u * g.h[2] * g.h[2])
-                                : f32::deriv_tables(fv, ka < 0.0f, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], k + 5);
-        l -= ka * d;
+        l -= ka * axis(sz, 2, k + 5, ka < 0.0f);
     }
     return l;
 }

@@ -44,7 +44,7 @@ __device__ __forceinline__ void block_sum2(double a, double b, double* dst) {
     }
 }
 
-template <bool TWO_D, int STAGE, bool REINI, bool VOLUME, bool UNIFORM>
+template <bool TWO_D, int STAGE, bool REINI, bool VOLUME, bool UNIFORM, bool DF = false>
 __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, StageArgs32 a) {
     const int i = blockIdx.x * kBX + threadIdx.x;
     const int j = TWO_D ? 0 : blockIdx.y * kBY + threadIdx.y;
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, Stag
             Lc = reini_L<TWO_D, UNIFORM>(g, a.fs, c, i, j, k);
             dtc = reini_dt32<TWO_D>(g, i, j, k);
         } else {
-            Lc = conv_L<TWO_D, UNIFORM>(g, a.fs, a.u, a.v, a.w, c, i, j, k, (float)*a.vscale);
+            Lc = conv_L<TWO_D, UNIFORM, DF>(g, a.fs, a.u, a.v, a.w, c, i, j, k, (float)*a.vscale);
             dtc = (float)*a.dt;
         }
         const float fn = a.fn[c];
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kBX * kBY) stage_kernel32(KGrid<float> g, Stag
     }
 }
 
-template <bool TWO_D, bool REINI, bool UNIFORM>
+template <bool TWO_D, bool REINI, bool UNIFORM, bool DF = false>
 __global__ void __launch_bounds__(kBX * kBY) operator_kernel32(KGrid<float> g, StageArgs32 a) {
     const int i = blockIdx.x * kBX + threadIdx.x;
     const int j = TWO_D ? 0 : blockIdx.y * kBY + threadIdx.y;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kBX * kBY) operator_kernel32(KGrid<float> g, S
     if (i >= g.L.nx || j >= g.L.ny || k >= g.L.nz) return;
     const long long c = (long long)(k + g.L.gz) * g.L.sz + (long long)(j + g.L.gy) * g.L.sy + (i + g.L.gx);
     a.out[c] = REINI ? reini_L<TWO_D, UNIFORM>(g, a.fs, c, i, j, k)
-                     : conv_L<TWO_D, UNIFORM>(g, a.fs, a.u, a.v, a.w, c, i, j, k, (float)*a.vscale);
+                     : conv_L<TWO_D, UNIFORM, DF>(g, a.fs, a.u, a.v, a.w, c, i, j, k, (float)*a.vscale);
 }
 
 dim3 grid_of32(const Layout& L) {
@@ -116,10 +116,10 @@ dim3 grid_of32(const Layout& L) {
     return dim3((L.nx + kBX - 1) / kBX, (L.ny + kBY - 1) / kBY, L.nz);
 }
 
-template <bool TWO_D, bool REINI, bool UNIFORM>
+template <bool TWO_D, bool REINI, bool UNIFORM, bool DF = false>
 void launch_t(const KGrid<float>& g, const StageArgs32& a, int stage, bool volume, cudaStream_t st) {
     const dim3 grid = grid_of32(g.L), block(kBX, kBY);
-#define R3D_L32(S, V) stage_kernel32<TWO_D, S, REINI, V, UNIFORM><<<grid, block, 0, st>>>(g, a)
+#define R3D_L32(S, V) stage_kernel32<TWO_D, S, REINI, V, UNIFORM, DF><<<grid, block, 0, st>>>(g, a)
     if (stage == 1) { if (volume) R3D_L32(1, true); else R3D_L32(1, false); }
     else if (stage == 2) { if (volume) R3D_L32(2, true); else R3D_L32(2, false); }
     else { if (volume) R3D_L32(3, true); else R3D_L32(3, false); }
@@ -128,6 +128,11 @@ void launch_t(const KGrid<float>& g, const StageArgs32& a, int stage, bool volum
 
 template <bool REINI>
 void launch_any(const KGrid<float>& g, const StageArgs32& a, int stage, bool volume, bool uniform, cudaStream_t st) {
+    if (!REINI && g.x45) {  // direct-forcing stencils (table form)
+        if (g.L.two_d) launch_t<true, false, false, true>(g, a, stage, volume, st);
+        else launch_t<false, false, false, true>(g, a, stage, volume, st);
+        return;
+    }
     if (g.L.two_d) {
         if (uniform) launch_t<true, REINI, true>(g, a, stage, volume, st);
         else launch_t<true, REINI, false>(g, a, stage, volume, st);
@@ -172,6 +177,11 @@ template <bool REINI>
 static void launch_op(const KGrid<float>& g, const StageArgs32& a, cudaStream_t st) {
     const dim3 grid = grid_of32(g.L), block(kBX, kBY);
     const bool u = is_uniform(g);
+    if (!REINI && g.x45) {
+        if (g.L.two_d) operator_kernel32<true, false, false, true><<<grid, block, 0, st>>>(g, a);
+        else operator_kernel32<false, false, false, true><<<grid, block, 0, st>>>(g, a);
+        return;
+    }
     if (g.L.two_d) {
         if (u) operator_kernel32<true, REINI, true><<<grid, block, 0, st>>>(g, a);
         else operator_kernel32<true, REINI, false><<<grid, block, 0, st>>>(g, a);

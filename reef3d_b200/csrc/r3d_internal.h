@@ -82,11 +82,12 @@ struct KGrid {
     // FP64 cell sizes DXN, DYN, DZN for the volume sums (the FP32 form
     // sums in FP64 with the exact cell volumes)
     const double* dxn_d[3];
-    // direct-forcing convection stencils (X45 1..6, FP64 only): the body
-    // field they read and 0.6 DXM, the fb threshold of X45 = 1
+    // direct-forcing convection stencils (X45 1..6; 1..5 in the FP32 form):
+    // the body field they read (FP64 in both forms, so that every mask
+    // decision is the reference's) and 0.6 DXM, the fb threshold of X45 = 1
     int x45;
     double df_thr;
-    const T* body;
+    const double* body;
     // uniform-grid FP32 form
     float h[3], rh[3];
     float eps_u;  // WENO psi (1e-6); rescaled by h^2 per axis for undivided differences

@@ -4,7 +4,8 @@ differences of every WENO5 stencil masked or weighted by a body field.  The
 golden df* cases against the reference itself run in test_gpu_parity.py;
 here larger cases against the C restatement (pinned bit-exact to the
 reference by test_oracle_golden.py): the operator bit-identical, phi within
-the FP64 tolerance of 1e-12 relative max-norm per step."""
+the FP64 tolerance of 1e-12 relative max-norm per step; the FP32 form
+(X45 1..5) within the FP32 tolerance of the FP64 path."""
 import numpy as np
 import pytest
 
@@ -102,10 +103,42 @@ def test_direct_forcing_graph_replay_equals_direct_steps():
     assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("x45", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("dims", [(40, 33, 27), (64, 1, 48)])
+def test_direct_forcing_fp32_within_tolerance_of_fp64(x45, dims):
+    """The FP32 form of the X45 stencils (one-cell-per-thread table kernels;
+    mask decisions on the FP64 body field) within the FP32 tolerance of the
+    FP64 path, 2e-5 relative max-norm per step."""
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=nx + x45)
+    b1, b2 = bodies(x45, phi.shape, 1.0 / nx, seed=x45)
+    m = visible_mask(nx, ny, nz)
+    out = {}
+    for prec in (r3d.FP64, r3d.FP32):
+        with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=prec, f43=0.5, f44=2, f45=2.1, n47=0.125) as ls:
+            ls.set_direct_forcing(x45)
+            ls.upload(r3d.BODY, body_field(x45, b1, b2))
+            # the body field stays FP64 in both forms
+            assert np.array_equal(interior(ls.download(r3d.BODY), nx, ny, nz),
+                                  interior(body_field(x45, b1, b2), nx, ny, nz))
+            if prec == r3d.FP32:
+                assert ls.get_option(r3d.OPT_TILED) == 0
+            for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+                ls.upload(f, a)
+            res = []
+            for _ in range(2):
+                ls.cfl_dt()
+                ls.step()
+                res.append(ls.download(r3d.PHI))
+            out[prec] = res
+    for a, b in zip(out[r3d.FP32], out[r3d.FP64]):
+        assert relmax(a[m], b[m]) <= 2e-5
+
+
 def test_direct_forcing_refusals():
     with r3d.LevelSet(16, 16, 16, precision=r3d.FP32) as ls:
         with pytest.raises(r3d.R3DError):
-            ls.set_direct_forcing(2)  # the stencils run in the FP64 form
+            ls.set_direct_forcing(6)  # 1e20 differences overflow FP32: FP64 only
     with r3d.LevelSet(16, 16, 16, precision=r3d.FP64) as ls:
         with pytest.raises(r3d.R3DError):
             ls.download(r3d.BODY)  # not enabled yet
