@@ -426,6 +426,58 @@ int r3d_batch_sync(r3d_batch* b);
 int r3d_batch_stream(r3d_batch* b, void** stream);
 int r3d_batch_launch_count(const r3d_batch* b, long long* count);
 
+/* Continuous-batching job server (no counterpart in the reference, which
+ * runs one case per process).  A job is a level set on a uniform grid of the
+ * unit box made of nspheres spheres (spheres[4q..4q+3] = centre x, y, z,
+ * radius) advected by nmodes Taylor-Green modes (modes[2q] = wavenumber,
+ * modes[2q+1] = amplitude; r3d_init_spheres_tg) for `steps` adaptive steps
+ * with f44 reinitialisation pseudo-steps and CFL factor n47 (f43 0.5, f45
+ * 2.1, f49 1).  Submitted jobs wait in arrival order until their device
+ * footprint (r3d_footprint) fits the HBM budget; admitted jobs stay
+ * resident and advance together between polls -- FP32 jobs as members of
+ * one batch (one persistent launch per RK stage over all members, CUDA
+ * graph), FP64 jobs each on its own instance -- and leave when done.  A
+ * job's results do not depend on which jobs shared its steps.
+ *  r3d_serve_poll: admits what fits, then advances every active job by up
+ *    to max_steps steps, stopping at the first job to finish (which is
+ *    retired: volume sums and clock recorded, instance destroyed unless the
+ *    server keeps fields); *nfinished = jobs retired by this call.
+ *  r3d_serve_result: state (0 queued, 1 active, 2 finished, 3 released),
+ *    times on the server's clock (seconds since creation; -1 not yet), and
+ *    with keep_fields the finished job's instance (read its fields, then
+ *    r3d_serve_release). */
+typedef struct r3d_server r3d_server;
+typedef struct {
+    int nx, ny, nz;
+    int steps;
+    int f44;
+    double n47;
+    int nspheres;
+    const double* spheres;
+    int nmodes;
+    const double* modes;
+} r3d_job_desc;
+typedef struct {
+    int state;
+    int steps_done;
+    double volume1, volume2;
+    double sim_time;
+    double t_submit, t_admit, t_done;
+    r3d_handle* instance;
+} r3d_job_result;
+int r3d_serve_create(double budget_bytes, int precision, int keep_fields, r3d_server** out);
+int r3d_serve_destroy(r3d_server* s);
+const char* r3d_serve_last_error(const r3d_server* s);
+int r3d_serve_submit(r3d_server* s, const r3d_job_desc* job, long long* id);
+int r3d_serve_poll(r3d_server* s, int max_steps, int* nfinished);
+int r3d_serve_status(const r3d_server* s, int* queued, int* active, double* used_bytes, double* peak_bytes,
+                     int* max_active);
+int r3d_serve_result(const r3d_server* s, long long id, r3d_job_result* out);
+int r3d_serve_release(r3d_server* s, long long id);
+/* The FP32 server's batch (for r3d_batch_autotune / r3d_batch_set_config);
+ * NULL for an FP64 server. */
+int r3d_serve_batch(r3d_server* s, r3d_batch** batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,25 @@ class IoflowDesc(ctypes.Structure):
     ]
 
 
+class JobDesc(ctypes.Structure):
+    """r3d_job_desc: one transport job of the serving runtime."""
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("steps", ctypes.c_int),
+        ("f44", ctypes.c_int), ("n47", ctypes.c_double),
+        ("nspheres", ctypes.c_int), ("spheres", ctypes.POINTER(ctypes.c_double)),
+        ("nmodes", ctypes.c_int), ("modes", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class JobResult(ctypes.Structure):
+    """r3d_job_result."""
+    _fields_ = [
+        ("state", ctypes.c_int), ("steps_done", ctypes.c_int), ("volume1", ctypes.c_double),
+        ("volume2", ctypes.c_double), ("sim_time", ctypes.c_double), ("t_submit", ctypes.c_double),
+        ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double), ("instance", ctypes.c_void_p),
+    ]
+
+
 # the reference's defaults of those flags (src/ini.cpp:208-441; F50 = 2)
 IOFLOW_DEFAULTS = dict(inflow=1, outflow=1, f50=2, b77=1, f56=1.0e20, f60=-1.0e20, f61=-1.0e20, f62=-1.0e20,
                        f64=0, qi=0.0, qo=0.0)
@@ -126,6 +145,16 @@ EXPORTS = {
     "r3d_batch_sync": ([_H], ctypes.c_int),
     "r3d_batch_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_batch_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "r3d_serve_create": ([ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_H)], ctypes.c_int),
+    "r3d_serve_destroy": ([_H], ctypes.c_int),
+    "r3d_serve_last_error": ([_H], ctypes.c_char_p),
+    "r3d_serve_submit": ([_H, ctypes.POINTER(JobDesc), ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "r3d_serve_poll": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "r3d_serve_status": ([_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _D, _D,
+                          ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "r3d_serve_result": ([_H, ctypes.c_longlong, ctypes.POINTER(JobResult)], ctypes.c_int),
+    "r3d_serve_release": ([_H, ctypes.c_longlong], ctypes.c_int),
+    "r3d_serve_batch": ([_H, ctypes.POINTER(_H)], ctypes.c_int),
 }
 
 

@@ -34,6 +34,7 @@ UNITS = [
     ("grid_metrics.cpp", []),
     ("api.cpp", []),
     ("batch.cpp", []),
+    ("serve.cpp", []),
 ]
 HEADERS = ["r3d_internal.h", "stencil_f64.cuh", "stencil_f32.cuh", "tile_host.h", "cell_f32.cuh", "handle.h", "batch_internal.h"]
 

@@ -1,25 +1,30 @@
 """Continuous-batching server for level-set transport jobs.
 
 Jobs (a sphere-union level set advected by a Taylor-Green velocity for a
-given number of steps) arrive over time.  The server admits waiting jobs in
-arrival order whenever their device footprint fits the HBM budget, keeps
-every admitted job's fields resident on the device, and advances all active
-jobs together one step at a time in a ``Batch`` (one persistent launch per
-RK stage over every member, the step replayed from a CUDA graph).  Jobs join
-and leave between steps, so work of jobs that arrive while others are on
-the GPU overlaps with theirs on the device.  A job's result does not depend
-on which other jobs shared its steps.
+given number of steps) arrive over time.  The native serving runtime
+(r3d_serve_*, reef3d_b200/csrc/serve.cpp) admits waiting jobs in arrival
+order whenever their device footprint fits the HBM budget, keeps every
+admitted job's fields resident on the device, and advances all active jobs
+together in one batch (one persistent launch per RK stage over every
+member, the step replayed from a CUDA graph).  Jobs join and leave between
+steps, so work of jobs that arrive while others are on the GPU overlaps
+with theirs on the device.  A job's result does not depend on which other
+jobs shared its steps.  ``TransportServer`` feeds it a timed job stream.
 
 The FP64 plain path (``precision=FP64``) serves the same stream without
 batching: every active job is stepped on its own instance.
 """
 import collections
+import ctypes
 import math
+import os
 import time
 
 import numpy as np
 
-from . import FP32, FP64, PHI, Batch, LevelSet, footprint, uniform_nodes
+from . import FP32, FP64, LAYOUT_REEF3D, PHI, R3D_OK, JobDesc, JobResult, R3DError, _check, _dp, load_library
+
+_lib = None  # the loaded libreef3d_b200.so (set by TransportServer)
 
 
 class Job:
@@ -73,98 +78,110 @@ def poisson_jobs(seed=1, rate=200.0, njobs=64, edge_lo=32, edge_hi=384, steps_lo
 
 
 class TransportServer:
+    """Python front of the native serving runtime (r3d_serve_*,
+    reef3d_b200/csrc/serve.cpp): admission against the HBM budget in arrival
+    order, continuous batching of the active FP32 jobs (per-instance FP64
+    runs for precision=FP64), retirement with volume sums and clock.  This
+    class feeds it a timed job stream and keeps the per-job record."""
+
     def __init__(self, budget_bytes=150e9, precision=FP32, graph=True, autotune_cache=None, keep_phi=False,
                  clock=time.perf_counter):
+        global _lib
+        _lib = load_library()
         self.budget = float(budget_bytes)
         self.precision = precision
-        self.graph = graph
         self.autotune_cache = autotune_cache
         self.keep_phi = keep_phi
         self.clock = clock
-        self.used = 0.0
-        self.batch = Batch() if precision == FP32 else None
-        if self.batch is not None:
-            self.batch.use_graph(graph)
-        self.active = {}  # job id -> [job, LevelSet, steps done, bytes]
+        s = ctypes.c_void_p()
+        rc = _lib.r3d_serve_create(self.budget, precision, 1 if keep_phi else 0, ctypes.byref(s))
+        if rc != R3D_OK:
+            raise R3DError(rc, "r3d_serve_create failed")
+        self.s = s
         self.done = []
         self.peak_used = 0.0
         self.max_active = 0
+        self.makespan = 0.0
+
+    def _check(self, rc):
+        if rc != R3D_OK:
+            msg = _lib.r3d_serve_last_error(self.s)
+            raise R3DError(rc, msg.decode() if msg else "")
 
     def close(self):
-        for job, ls, _, _ in list(self.active.values()):
-            ls.close()
-        self.active.clear()
-        if self.batch is not None:
-            self.batch.close()
+        if getattr(self, "s", None) is not None and self.s.value:
+            _lib.r3d_serve_destroy(self.s)
+            self.s = ctypes.c_void_p()
 
-    def _footprint(self, job):
-        return float(footprint(job.nx, job.ny, job.nz, self.precision))
+    def _submit(self, job):
+        sph = np.ascontiguousarray(np.asarray(job.spheres, dtype=np.float64).reshape(-1))
+        mod = np.ascontiguousarray(np.asarray(job.modes, dtype=np.float64).reshape(-1))
+        d = JobDesc(job.nx, job.ny, job.nz, job.steps, job.f44, job.n47, len(job.spheres),
+                    sph.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(job.modes),
+                    mod.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        jid = ctypes.c_longlong()
+        self._check(_lib.r3d_serve_submit(self.s, ctypes.byref(d), ctypes.byref(jid)))
+        return jid.value
 
-    def _admit(self, job, now):
-        ls = LevelSet(job.nx, job.ny, job.nz, uniform_nodes(job.nx), uniform_nodes(job.ny), uniform_nodes(job.nz),
-                      f43=0.5, f44=job.f44, f45=2.1, f49=1, n47=job.n47, precision=self.precision)
-        ls.init_spheres_tg(job.spheres, job.modes)
-        ls.set_time(0.0)
-        if self.batch is not None:
-            self.batch.add(ls)
-        fp = self._footprint(job)
-        self.used += fp
-        self.peak_used = max(self.peak_used, self.used)
-        job.t_admit = now
-        self.active[job.id] = [job, ls, 0, fp]
-        self.max_active = max(self.max_active, len(self.active))
+    def _status(self):
+        q, a, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        used, peak = ctypes.c_double(), ctypes.c_double()
+        self._check(_lib.r3d_serve_status(self.s, ctypes.byref(q), ctypes.byref(a), ctypes.byref(used),
+                                          ctypes.byref(peak), ctypes.byref(m)))
+        return q.value, a.value, peak.value, m.value
 
-    def _retire(self, jid, t0):
-        job, ls, _, fp = self.active.pop(jid)
-        if self.batch is not None:
-            self.batch.remove(ls)
-        job.volume = ls.last_volume()
-        job.time = ls.time()
+    def _collect(self, jid, job, offset):
+        r = JobResult()
+        self._check(_lib.r3d_serve_result(self.s, jid, ctypes.byref(r)))
+        if r.state != 2:
+            return False
+        job.volume = (r.volume1, r.volume2)
+        job.time = r.sim_time
+        job.t_admit = r.t_admit + offset
+        job.t_done = r.t_done + offset
         if self.keep_phi:
-            job.phi = ls.download(PHI)
-        job.t_done = self.clock() - t0
-        ls.close()
-        self.used -= fp
+            phi = np.zeros((job.nx + 6, job.ny + 6, job.nz + 6))
+            _check(_lib.r3d_download(ctypes.c_void_p(r.instance), PHI, _dp(phi), LAYOUT_REEF3D))
+            job.phi = phi
+            self._check(_lib.r3d_serve_release(self.s, jid))
         self.done.append(job)
+        return True
 
     def serve(self, jobs, realtime=True):
-        """Runs the stream to completion.  With realtime, a job becomes
-        visible at its arrival time on the wall clock (measured from the
-        start of serve); otherwise all jobs are visible at once.  Returns
-        the finished jobs."""
+        """Runs the stream to completion.  With realtime, a job is submitted
+        at its arrival time on the wall clock (measured from the start of
+        serve) and the runtime advances one step per poll; otherwise all
+        jobs are submitted at once and each poll runs up to the next job
+        completion.  Returns the finished jobs."""
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
-        queue = collections.deque()
+        out = {}  # server job id -> (job, offset of the server clock)
         t0 = self.clock()
-        retuned_for = None
-        while pending or queue or self.active:
+        tuned_for = None
+        while pending or out:
             now = self.clock() - t0
             while pending and (not realtime or pending[0].arrival <= now):
-                queue.append(pending.popleft())
-            changed = False
-            while queue and self.used + self._footprint(queue[0]) <= self.budget:
-                self._admit(queue.popleft(), now)
-                changed = True
-            if queue and not self.active:
-                raise RuntimeError(f"job {queue[0].id} alone exceeds the HBM budget")
-            if not self.active:
+                job = pending.popleft()
+                jid = self._submit(job)
+                r = JobResult()
+                self._check(_lib.r3d_serve_result(self.s, jid, ctypes.byref(r)))
+                out[jid] = (job, (self.clock() - t0) - r.t_submit)
+            queued, active, _, _ = self._status()
+            if active == 0 and queued == 0:
                 if pending:
-                    time.sleep(max(0.0, min(0.01, pending[0].arrival - now)))
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (self.clock() - t0))))
                 continue
-            if self.batch is not None:
-                if changed and self.autotune_cache is not None and retuned_for != len(self.active):
-                    self.batch.autotune(self.autotune_cache)
-                    retuned_for = len(self.active)
-                self.batch.step(1)
-            else:
-                for job, ls, _, _ in self.active.values():
-                    ls.run(1, adaptive=True)
-            finished = []
-            for jid, rec in self.active.items():
-                rec[2] += 1
-                if rec[2] >= rec[0].steps:
-                    finished.append(jid)
-            for jid in finished:
-                self._retire(jid, t0)
+            if self.autotune_cache is not None and self.precision == FP32 and tuned_for != active:
+                b = ctypes.c_void_p()
+                self._check(_lib.r3d_serve_batch(self.s, ctypes.byref(b)))
+                rows, ctas = ctypes.c_int(), ctypes.c_int()
+                _lib.r3d_batch_autotune(b, os.fsencode(self.autotune_cache), ctypes.byref(rows), ctypes.byref(ctas))
+                tuned_for = active
+            nfin = ctypes.c_int()
+            self._check(_lib.r3d_serve_poll(self.s, 1 if realtime else (1 << 30), ctypes.byref(nfin)))
+            if nfin.value:
+                for jid in [j for j in out if self._collect(j, *out[j])]:
+                    del out[jid]
+        _, _, self.peak_used, self.max_active = self._status()
         self.makespan = self.clock() - t0
         return self.done
 

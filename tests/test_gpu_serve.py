@@ -70,3 +70,33 @@ def test_realtime_stream_latency_summary():
     finally:
         s.close()
     assert out["jobs"] == 6 and out["p99_s"] >= out["p50_s"] > 0
+
+
+def test_native_runtime_refusals_and_release():
+    """The C-ABI of the serving runtime: a job larger than the budget is
+    refused at submission, an unfinished job cannot be released, a finished
+    job's instance stays readable until released."""
+    import ctypes
+    from reef3d_b200 import JobDesc, JobResult
+    lib = r3d.load_library()
+    s = ctypes.c_void_p()
+    assert lib.r3d_serve_create(1e9, r3d.FP32, 1, ctypes.byref(s)) == r3d.R3D_OK
+    try:
+        sph = np.array([0.5, 0.5, 0.5, 0.2])
+        mod = np.array([1.0, 0.5])
+        P = ctypes.POINTER(ctypes.c_double)
+        big = JobDesc(512, 512, 512, 5, 2, 0.125, 1, sph.ctypes.data_as(P), 1, mod.ctypes.data_as(P))
+        jid = ctypes.c_longlong()
+        assert lib.r3d_serve_submit(s, ctypes.byref(big), ctypes.byref(jid)) == r3d.R3D_ENOMEM
+        small = JobDesc(24, 24, 24, 4, 2, 0.125, 1, sph.ctypes.data_as(P), 1, mod.ctypes.data_as(P))
+        assert lib.r3d_serve_submit(s, ctypes.byref(small), ctypes.byref(jid)) == r3d.R3D_OK
+        assert lib.r3d_serve_release(s, jid) == r3d.R3D_ESTATE  # still queued
+        nfin = ctypes.c_int()
+        assert lib.r3d_serve_poll(s, 100, ctypes.byref(nfin)) == r3d.R3D_OK and nfin.value == 1
+        r = JobResult()
+        assert lib.r3d_serve_result(s, jid, ctypes.byref(r)) == r3d.R3D_OK
+        assert r.state == 2 and r.steps_done == 4 and r.instance and r.t_done >= r.t_admit >= r.t_submit
+        assert lib.r3d_serve_release(s, jid) == r3d.R3D_OK
+        assert lib.r3d_serve_result(s, jid, ctypes.byref(r)) == r3d.R3D_OK and r.state == 3 and not r.instance
+    finally:
+        lib.r3d_serve_destroy(s)
