@@ -75,7 +75,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
-// plain (non-multicast) tiled TMA load of one box into this CTA's shared memory
+// plain tiled TMA load of one box into this CTA's own shared memory
 __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
