@@ -275,6 +275,17 @@ int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt);
  * batch members. */
 int r3d_set_direct_forcing(r3d_handle* h, int x45);
 
+/* Solid forcing of the level set after each convection stage
+ * (ghostcell::solid_forcing_lsm, src/gc_solid_forcing_lsm.cpp:27-78, called
+ * at src/levelset_RK3.cpp:128,145,160 with X48 = 1): for each of the n
+ * entries (i, j, k, side) of the direct-forcing boundary list gcdf4
+ * (src/gcdf_update.cpp; side 1 -x, 4 +x, 3 -y, 2 +y, 5 -z, 6 +z; entries with
+ * side <= 0 are skipped), in list order, the two cells beyond the side take
+ * the value of cell (i, j, k).  Entries that touch the same cells keep the
+ * list order (the library runs the list in dependency levels).  n = 0 turns
+ * it off.  Synchronous.  Not for batch members. */
+int r3d_set_solid_forcing(r3d_handle* h, int n, const int* cells);
+
 /* Inflow and outflow boundaries with the level-set hooks of REEF3D's
  * ioflow_f (B60 >= 1, src/driver_logic_cfd.cpp:509-510), which the
  * closed box's ioflow_v leaves void.  The x-min face becomes an inflow

@@ -84,6 +84,7 @@ class PortOracle:
             lib.lso_io_levels.argtypes = [ctypes.c_void_p, _D]
             lib.lso_set_count.argtypes = [ctypes.c_void_p, _I]
             lib.lso_set_direct_forcing.argtypes = [ctypes.c_void_p, _I, _D, _D]
+            lib.lso_set_solid_forcing.argtypes = [ctypes.c_void_p, _I, ctypes.POINTER(ctypes.c_int)]
             cls._lib = lib
         return cls._lib
 
@@ -104,6 +105,11 @@ class PortOracle:
         if ioflow is not None:
             io = dict(IOFLOW_DEFAULTS, **ioflow)
             self._lib.lso_set_ioflow(self.h, *(io[k] for k in IOFLOW_KEYS))
+
+    def set_solid_forcing(self, cells):
+        """solid_forcing_lsm entries (i, j, k, side) after each convection stage."""
+        self._sf = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1)
+        self._lib.lso_set_solid_forcing(self.h, self._sf.size // 4, self._sf.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
 
     def set_direct_forcing(self, x45, body1, body2=None):
         """X45 stencils reading body1 (fb, fbh5, fbh4 or solid) and body2
@@ -202,7 +208,7 @@ class RefOracle:
     _loaded = set()
 
     def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10,
-                 path=None, ioflow=None, x45=0):
+                 path=None, ioflow=None, x45=0, solid_forcing=None):
         """ioflow: None for the closed box, else a dict of IOFLOW_DEFAULTS'
         keys: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags."""
         path = path or (REF_LIB_FAST if fast else REF_LIB)
@@ -214,6 +220,10 @@ class RefOracle:
         lib.refls_set_picard(f46, f47)
         lib.refls_set_x45.argtypes = [_I]
         lib.refls_set_x45(x45)
+        if solid_forcing is not None:
+            cells = np.ascontiguousarray(solid_forcing, dtype=np.int32).reshape(-1)
+            lib.refls_set_solid_forcing.argtypes = [_I, ctypes.POINTER(ctypes.c_int)]
+            lib.refls_set_solid_forcing(cells.size // 4, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
         if ioflow is not None:
             io = dict(IOFLOW_DEFAULTS, **ioflow)
             lib.refls_set_ioflow.argtypes = [_I, _I, _I, _I] + [ctypes.c_double] * 4 + [_I] + [ctypes.c_double] * 2

@@ -262,6 +262,29 @@ static double weno_deriv_df(const lso_grid* g, const double* f, long c, long s, 
     return weno_axis(qf, cf, isf, t, plus, q[0], q[1], q[2], q[3], q[4]);
 }
 
+/* ghostcell::solid_forcing_lsm (src/gc_solid_forcing_lsm.cpp:27-78): for
+ * each entry in list order with side > 0, the two cells beyond the side
+ * take the entry cell's value. */
+static void solid_forcing(const lso_grid* g, double* f) {
+    for (int n = 0; n < g->nsf; ++n) {
+        const int* e = g->sf + 4 * n;
+        const int i = e[0], j = e[1], k = e[2], side = e[3];
+        if (side <= 0) continue;
+        const double v = f[lso_index(g, i, j, k)];
+        if (side == 1) { f[lso_index(g, i - 1, j, k)] = v; f[lso_index(g, i - 2, j, k)] = v; }
+        if (side == 4) { f[lso_index(g, i + 1, j, k)] = v; f[lso_index(g, i + 2, j, k)] = v; }
+        if (side == 3) { f[lso_index(g, i, j - 1, k)] = v; f[lso_index(g, i, j - 2, k)] = v; }
+        if (side == 2) { f[lso_index(g, i, j + 1, k)] = v; f[lso_index(g, i, j + 2, k)] = v; }
+        if (side == 5) { f[lso_index(g, i, j, k - 1)] = v; f[lso_index(g, i, j, k - 2)] = v; }
+        if (side == 6) { f[lso_index(g, i, j, k + 1)] = v; f[lso_index(g, i, j, k + 2)] = v; }
+    }
+}
+
+void lso_set_solid_forcing(lso_grid* g, int n, const int* cells) {
+    g->nsf = n;
+    g->sf = cells;
+}
+
 void lso_set_direct_forcing(lso_grid* g, int x45, const double* body1, const double* body2) {
     g->x45 = x45;
     g->body1 = body1;
@@ -631,6 +654,7 @@ void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, con
                 a1[c] = phi[c] + dt * L[c];
             }
     lso_ghost_fill(g, a1);
+    solid_forcing(g, a1);
     lso_weno_L(g, a1, u, v, w, L);
     for (int i = 0; i < g->nx; ++i)
         for (int j = 0; j < g->ny; ++j)
@@ -639,6 +663,7 @@ void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, con
                 a2[c] = 0.75 * phi[c] + 0.25 * a1[c] + 0.25 * dt * L[c];
             }
     lso_ghost_fill(g, a2);
+    solid_forcing(g, a2);
     lso_weno_L(g, a2, u, v, w, L);
     for (int i = 0; i < g->nx; ++i)
         for (int j = 0; j < g->ny; ++j)
@@ -647,6 +672,7 @@ void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, con
                 phi[c] = (1.0 / 3.0) * phi[c] + (2.0 / 3.0) * a2[c] + (2.0 / 3.0) * dt * L[c];
             }
     lso_ghost_fill(g, phi);
+    solid_forcing(g, phi);
     lso_reini(g, phi, a1, a2, L, g->f44);
     if (g->f46 == 2) picard_correct(g, phi, vol1);
     if (g->f46 == 3) picard_correct(g, phi, g->netvol);

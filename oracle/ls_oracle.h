@@ -57,6 +57,10 @@ typedef struct {
      * (5); caller-owned padded fields */
     int x45;
     const double *body1, *body2;
+    /* solid forcing after each convection stage (X48 = 1): nsf entries
+     * (i, j, k, side), caller-owned */
+    int nsf;
+    const int* sf;
 } lso_grid;
 
 /* xn/yn/zn: node coordinates for indices -5..n+5 (n+11 values). */
@@ -108,6 +112,9 @@ void lso_set_count(lso_grid* g, int count);
 /* X45 direct-forcing variant of the convection stencils and the body
  * fields it reads (kept by pointer). */
 void lso_set_direct_forcing(lso_grid* g, int x45, const double* body1, const double* body2);
+
+/* solid_forcing_lsm entries (src/gc_solid_forcing_lsm.cpp:27-78), kept by pointer */
+void lso_set_solid_forcing(lso_grid* g, int n, const int* cells);
 
 /* opaque handle helpers (used through ctypes) */
 lso_grid* lso_new(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,

@@ -58,6 +58,7 @@ concentration* CONC = nullptr;
 field4* TMP = nullptr;
 int G_F46 = 0, G_F47 = 10;  // picard mass correction flags for the next refls_init
 int G_X45 = 0;              // level-set convection stencil at bodies for the next refls_init
+std::vector<int> G_SF;      // gcdf4 entries (i, j, k, side) of the solid forcing (X48 = 1)
 // inflow (x-min) / outflow (x-max) boundaries and ioflow_f flags for the next
 // refls_init; io.on == 0 keeps the closed box and ioflow_v
 struct IoFlags {
@@ -117,6 +118,12 @@ void refls_set_picard(int f46, int f47) { G_F46 = f46; G_F47 = f47; }
 // WENO stencils (0 plain; 1..6 mask or weight the divided differences by
 // the body fields fb, fbh4, fbh5, solid, topo, src/weno_hj_df_nug.cpp:398-987).
 void refls_set_x45(int x45) { G_X45 = x45; }
+
+// The solid forcing of the level set after each convection stage
+// (ghostcell::solid_forcing_lsm, src/gc_solid_forcing_lsm.cpp:27-78, X48 = 1):
+// n entries (i, j, k, side) of the direct-forcing boundary list gcdf4, which
+// a solid geometry would produce (src/gcdf_update.cpp).
+void refls_set_solid_forcing(int n, const int* cells) { G_SF.assign(cells, cells + 4 * n); }
 
 // Inflow / outflow boundaries of the next refls_init.  inflow: the x-min face
 // is boundary type 1, outflow: the x-max face type 2 (the other faces stay
@@ -346,6 +353,14 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     TMP = new field4(p);
     TSTEP = new ietimestep(p);
     TURB = new kepsilon_void(p, A, PGC);
+    if (!G_SF.empty()) {
+        const int n = (int)(G_SF.size() / 4);
+        p->X48 = 1;
+        p->Iarray(p->gcdf4, n, 6);
+        for (int q = 0; q < n; ++q)
+            for (int c = 0; c < 4; ++c) p->gcdf4[q][c] = G_SF[4 * q + c];
+        p->gcdf4_count = n;
+    }
     p->count = 1;
     p->dt = 0.0;
     p->Qi = p->Qo = 0.0;  // closed box: no discharge (read by picard_lsm, src/picard_lsm.cpp:95)

@@ -104,6 +104,7 @@ EXPORTS = {
     "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
     "r3d_set_direct_forcing": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_set_solid_forcing": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_set_halo": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "r3d_write_vtu": ([_H, ctypes.c_char_p], ctypes.c_int),
     "r3d_save_state": ([_H, ctypes.c_char_p], ctypes.c_int),
@@ -333,6 +334,14 @@ class LevelSet:
 
     def set_velocity_scale(self, scale):
         _check(_lib.r3d_set_velocity_scale(self.h, scale), self.h)
+
+    def set_solid_forcing(self, cells):
+        """solid_forcing_lsm after each convection stage: cells = (n, 4)
+        entries (i, j, k, side) of the direct-forcing boundary list; empty
+        turns it off (r3d_set_solid_forcing)."""
+        c = np.ascontiguousarray(np.asarray(cells, dtype=np.int32).reshape(-1))
+        _check(_lib.r3d_set_solid_forcing(self.h, c.size // 4, c.ctypes.data_as(ctypes.POINTER(ctypes.c_int))),
+               self.h)
 
     def set_direct_forcing(self, x45):
         """X45 direct-forcing convection stencils reading the BODY field

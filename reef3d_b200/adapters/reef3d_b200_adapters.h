@@ -169,6 +169,25 @@ inline void upload_body(r3d_handle* h, const lexer* p, fdm* a, std::vector<doubl
     check(h, r3d_upload(h, R3D_BODY, src, R3D_LAYOUT_REEF3D));
 }
 
+// The solid forcing of the level set (X48 = 1): the direct-forcing boundary
+// list gcdf4 (src/gcdf_update.cpp), handed to the device when it changed
+// (moving bodies rebuild it).
+struct SolidForcingState {
+    std::vector<int> last;
+    bool on = false;
+    void sync(r3d_handle* h, const lexer* p) {
+        std::vector<int> cells;
+        if (p->X48 == 1)
+            for (int n = 0; n < p->gcdf4_count; ++n)
+                for (int c = 0; c < 4; ++c) cells.push_back(p->gcdf4[n][c]);
+        if (cells != last || on != (p->X48 == 1)) {
+            check(h, r3d_set_solid_forcing(h, (int)(cells.size() / 4), cells.data()));
+            last = cells;
+            on = p->X48 == 1;
+        }
+    }
+};
+
 inline bool same_ioflow(const r3d_ioflow_desc& a, const r3d_ioflow_desc& b) {
     return a.inflow == b.inflow && a.outflow == b.outflow && a.f50 == b.f50 && a.b77 == b.b77 && a.f56 == b.f56 &&
            a.f60 == b.f60 && a.f61 == b.f61 && a.f62 == b.f62 && a.f64 == b.f64 && a.qi == b.qi && a.qo == b.qo;
@@ -222,6 +241,7 @@ public:
                field& ls) override {
         using r3d_adapter::check;
         io.sync(h, p, r3d_adapter::gcval_phi(p));
+        sf.sync(h, p);
         if (!resident || first) check(h, r3d_upload(h, R3D_PHI, ls.V, R3D_LAYOUT_REEF3D));
         first = false;
         check(h, r3d_upload(h, R3D_U, a->u.V, R3D_LAYOUT_REEF3D));
@@ -260,6 +280,7 @@ private:
     bool resident;
     bool first = true;
     r3d_adapter::IoflowState io;
+    r3d_adapter::SolidForcingState sf;
     std::vector<double> buf;
 };
 

@@ -3,12 +3,14 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <sstream>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "handle.h"
@@ -129,6 +131,7 @@ void release(r3d_handle* h) {
     if (h->staging) cudaFree(h->staging);
     if (h->coord) cudaFree(h->coord);
     if (h->io_buf) cudaFree(h->io_buf);
+    if (h->sf_ops) cudaFree(h->sf_ops);
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaSetDevice(cur);
 }
@@ -224,7 +227,7 @@ TileArgs make_tile_args(r3d_handle* h, int stage) {
 namespace {
 TileArgs tile_args(r3d_handle* h, int stage) { return r3d::make_tile_args(h, stage); }
 
-long long stage_launch(r3d_handle* h, bool reini, int s, bool vol) {
+long long stage_launch_plain(r3d_handle* h, bool reini, int s, bool vol) {
     const Fields f = fields_of(h);
     if (tiled(h)) return launch_tile_stage(h->map[s - 1], tile_args(h, s), reini, s, vol, h->stream);
     if (fp32(h))
@@ -232,6 +235,17 @@ long long stage_launch(r3d_handle* h, bool reini, int s, bool vol) {
                      : launch_conv_stage_f32(h->g32, f, s, h->S, vol, h->stream);
     return reini ? launch_reini_stage_f64(h->g64, f, s, h->S, vol, h->stream)
                  : launch_conv_stage_f64(h->g64, f, s, h->S, vol, h->stream);
+}
+
+// A stage; a convection stage is followed by the solid forcing of its
+// output when enabled (src/levelset_RK3.cpp:128,145,160).
+long long stage_launch(r3d_handle* h, bool reini, int s, bool vol) {
+    long long n = stage_launch_plain(h, reini, s, vol);
+    if (!reini && h->sf_ops) {
+        void* out = h->field[s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI];
+        n += launch_solid_forcing(out, fp32(h), h->sf_ops, h->sf_levels, h->stream);
+    }
+    return n;
 }
 
 long long volume_block_count(const r3d_handle* h) {
@@ -1086,6 +1100,68 @@ int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt) {
     R3D_CUDA(h, cudaStreamSynchronize(h->stream));
     h->dt_host = v;
     if (dt) *dt = v;
+    return R3D_OK;
+}
+
+int r3d_set_solid_forcing(r3d_handle* h, int n, const int* cells) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    if (n < 0 || (n > 0 && !cells)) return fail(h, R3D_EINVAL, "n >= 0 entries of (i, j, k, side)");
+    const Layout& L = h->L;
+    // device index of cell (i,j,k); ops skip sides <= 0 (GCDF4CHECK) and > 6
+    auto idx = [&](long long i, long long j, long long k) { return (k + L.gz) * L.sz + (j + L.gy) * L.sy + (i + L.gx); };
+    struct Op { long long c[3]; };
+    std::vector<Op> ops;
+    std::vector<int> level;
+    std::unordered_map<long long, int> wl, rl;  // last level that wrote / read a cell
+    for (int q = 0; q < n; ++q) {
+        const int i = cells[4 * q], j = cells[4 * q + 1], k = cells[4 * q + 2], side = cells[4 * q + 3];
+        if (side <= 0 || side > 6) continue;
+        if (i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz)
+            return fail(h, R3D_EINVAL, "solid-forcing entry outside the interior");
+        if (L.two_d && (side == 2 || side == 3))
+            return fail(h, R3D_EINVAL, "a 2D instance holds no y ghost planes for y sides");
+        const int di = side == 1 ? -1 : side == 4 ? 1 : 0, dj = side == 3 ? -1 : side == 2 ? 1 : 0;
+        const int dk = side == 5 ? -1 : side == 6 ? 1 : 0;
+        Op o{{idx(i, j, k), idx(i + di, j + dj, k + dk), idx(i + 2 * di, j + 2 * dj, k + 2 * dk)}};
+        // after every earlier entry that wrote a cell this one touches or read a cell it writes
+        int lv = 0;
+        for (int t = 0; t < 3; ++t) {
+            auto w = wl.find(o.c[t]);
+            if (w != wl.end()) lv = std::max(lv, w->second + 1);
+            if (t > 0) {
+                auto r = rl.find(o.c[t]);
+                if (r != rl.end()) lv = std::max(lv, r->second + 1);
+            }
+        }
+        rl[o.c[0]] = std::max(rl.count(o.c[0]) ? rl[o.c[0]] : 0, lv);
+        for (int t = 1; t < 3; ++t) wl[o.c[t]] = std::max(wl.count(o.c[t]) ? wl[o.c[t]] : 0, lv);
+        ops.push_back(o);
+        level.push_back(lv);
+    }
+    DeviceGuard dg(h->device, h->batch_stream);
+    drop_step_graph(h);
+    if (h->sf_ops) cudaFree(h->sf_ops);
+    h->sf_ops = nullptr;
+    h->sf_levels.clear();
+    if (ops.empty()) return R3D_OK;
+    const int nl = *std::max_element(level.begin(), level.end()) + 1;
+    std::vector<int> off(nl + 1, 0);
+    for (int lv : level) ++off[lv + 1];
+    for (int l = 0; l < nl; ++l) off[l + 1] += off[l];
+    std::vector<long long> flat(3 * ops.size());
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (size_t q = 0; q < ops.size(); ++q) {
+        const int at = fill[level[q]]++;
+        for (int t = 0; t < 3; ++t) flat[3 * (size_t)at + t] = ops[q].c[t];
+    }
+    if (cudaMalloc(&h->sf_ops, flat.size() * sizeof(long long)) != cudaSuccess) {
+        cudaGetLastError();
+        h->sf_ops = nullptr;
+        return fail(h, R3D_ENOMEM, "solid-forcing list allocation failed");
+    }
+    R3D_CUDA(h, cudaMemcpy(h->sf_ops, flat.data(), flat.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    h->sf_levels = off;
     return R3D_OK;
 }
 

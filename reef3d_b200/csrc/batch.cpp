@@ -373,7 +373,7 @@ int r3d_batch_add(r3d_batch* b, r3d_handle* h) {
     if (h->fluid) return bfail(b, R3D_EINVAL, "batches hold instances without the fluid update");
     if (h->airy) return bfail(b, R3D_EINVAL, "batches hold instances without the Airy velocity generator");
     if (h->io || h->L.io) return bfail(b, R3D_EINVAL, "batches hold closed-box instances (no inflow/outflow or halo faces)");
-    if (h->g64.x45) return bfail(b, R3D_EINVAL, "batches hold instances without direct forcing");
+    if (h->g64.x45 || h->sf_ops) return bfail(b, R3D_EINVAL, "batches hold instances without direct or solid forcing");
     if (h->device != b->device) return bfail(b, R3D_EINVAL, "instance lives on another device");
     if (h->batch_stream) return bfail(b, R3D_ESTATE, "instance already in a batch");
     // the member's own queued work (uploads, settings) completes first

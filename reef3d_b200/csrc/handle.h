@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "reef3d_b200.h"
 #include "r3d_internal.h"
@@ -32,6 +33,9 @@ struct r3d_handle {
     size_t io_buf_len = 0;
     r3d::IoParams iop{};
     long long next_count = 1;  // lexer::count of the next step, for r3d_set_ioflow's first state
+    // solid forcing after each convection stage (r3d_set_solid_forcing)
+    long long* sf_ops = nullptr;     // device: (entry cell, two target cells) per op, by level
+    std::vector<int> sf_levels;      // op offsets of the dependency levels
     int sms = 148;
     double* metrics64 = nullptr;
     float* metrics32 = nullptr;

@@ -652,6 +652,23 @@ __global__ void __launch_bounds__(256) vtu_node_kernel(Layout L, const T* __rest
     out[2 * npoints + n] = (float)m;
 }
 
+// --------------------------------------------------------- solid forcing
+// One dependency level of ghostcell::solid_forcing_lsm
+// (src/gc_solid_forcing_lsm.cpp:27-78): ops[3q..3q+2] = the entry cell and
+// the two cells beyond its side (device indices); the host puts every entry
+// after the earlier entries whose cells it writes or reads, so the entries
+// of one level touch disjoint cells and the result is the reference's
+// sequential one.
+template <typename T>
+__global__ void __launch_bounds__(256) solid_forcing_kernel(T* __restrict__ f, const long long* __restrict__ ops,
+                                                            int n) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const T v = f[ops[3 * q]];
+    f[ops[3 * q + 1]] = v;
+    f[ops[3 * q + 2]] = v;
+}
+
 // picard_lsm::correct_ls's target update netvol = netvol + Qi dt - Qo dt
 // (src/picard_lsm.cpp:93), before its iterations.
 __global__ void netvol_kernel(double* pic, const double* dt, double qi, double qo) {
@@ -695,6 +712,20 @@ int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const voi
                                                         static_cast<const double*>(ro),
                                                         static_cast<const double*>(visc), out, npoints);
     return 1;
+}
+
+int launch_solid_forcing(void* f, bool fp32, const long long* ops, const std::vector<int>& level_off,
+                         cudaStream_t st) {
+    int n = 0;
+    for (size_t l = 0; l + 1 < level_off.size(); ++l) {
+        const int cnt = level_off[l + 1] - level_off[l];
+        if (cnt <= 0) continue;
+        const long long* o = ops + 3LL * level_off[l];
+        if (fp32) solid_forcing_kernel<float><<<(cnt + 255) / 256, 256, 0, st>>>(static_cast<float*>(f), o, cnt);
+        else solid_forcing_kernel<double><<<(cnt + 255) / 256, 256, 0, st>>>(static_cast<double*>(f), o, cnt);
+        ++n;
+    }
+    return n;
 }
 
 int launch_netvol(const Scratch& s, double qi, double qo, cudaStream_t st) {

@@ -204,6 +204,10 @@ int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const voi
                      long long npoints, cudaStream_t st);
 // dt from the velocity maxima already in s.vmax (the CFL's second kernel).
 int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st);
+// Solid forcing of a field (src/gc_solid_forcing_lsm.cpp): one launch per
+// dependency level [level_off[l], level_off[l+1]) of the device op list.
+int launch_solid_forcing(void* f, bool fp32, const long long* ops, const std::vector<int>& level_off,
+                         cudaStream_t st);
 // picard_lsm's netvol = netvol + Qi dt - Qo dt (src/picard_lsm.cpp:93)
 int launch_netvol(const Scratch& s, double qi, double qo, cudaStream_t st);
 // host layout <-> device layout (src is a device staging copy of the host array)

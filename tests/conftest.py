@@ -44,6 +44,11 @@ def golden_df(g):
     return int(g["x45"]), g["body1"], g["body2"]
 
 
+def golden_sf(g):
+    """The solid-forcing list (n, 4) of an sf golden case, else None."""
+    return g["sf"] if "sf" in g else None
+
+
 def body_field(x45, body1, body2):
     """The one body field the device stencils read: body1, or for X45 = 5
     min(solid, topo), which is > 0 exactly where both are."""

@@ -17,7 +17,10 @@ fluid update wrote.  The picard cases run with the mass correction on
 picard_lsm form that keeps the first step's volume; f47 iterations).  The
 io cases open the x-min face as an inflow and the x-max face as an outflow
 boundary with the reference's ioflow_f (B60 = 1) and record the water
-levels its fsfinflow measured at every step.
+levels its fsfinflow measured at every step.  The df cases turn on the
+direct-forcing convection stencils (X45 1..6) over random body fields; the
+sf cases the solid forcing of the level set after each convection stage
+(X48 = 1) over a random direct-forcing boundary list.
 """
 import math
 import multiprocessing as mp
@@ -110,6 +113,20 @@ def df_case(name, nx, ny, nz, stretch, seed, x45, steps=2):
     return c
 
 
+def sf_case(name, nx, ny, nz, f49, stretch, seed, nsf, steps=2):
+    """Solid forcing after each convection stage (X48 = 1) with a random
+    gcdf4 list: entries on random interior cells with random sides (some 0:
+    skipped), so that entries overwrite each other's targets and read cells
+    other entries wrote."""
+    c = random_case(name, nx, ny, nz, f49, stretch, seed)
+    rng = np.random.default_rng(seed + 2000)
+    sides = [1, 4, 5, 6] if ny == 1 else [0, 1, 2, 3, 4, 5, 6]
+    cells = np.stack([rng.integers(0, nx, nsf), rng.integers(0, ny, nsf), rng.integers(0, nz, nsf),
+                      rng.choice(sides, nsf)], axis=1).astype(np.int32)
+    c.update(sf=cells, steps=steps)
+    return c
+
+
 def setup_case(name, which, n, steps, f46=0, f47=10):
     from reef3d_b200 import setups
     c = setups.slotted_disk(n) if which == "disk" else setups.vortex3d(n)
@@ -146,6 +163,8 @@ CASES = [
     lambda: df_case("df4_box3d_stretched", 9, 7, 8, 0.3, 24, 4),
     lambda: df_case("df5_box2d_stretched", 12, 1, 10, 0.3, 25, 5),
     lambda: df_case("df6_box3d_uniform", 9, 7, 8, 0.0, 26, 6),
+    lambda: sf_case("sf_box3d_stretched_f49_1", 9, 7, 8, 1, 0.3, 31, 60),
+    lambda: sf_case("sf_box2d_uniform_f49_0", 12, 1, 10, 0, 0.0, 32, 40),
 ]
 
 
@@ -156,7 +175,7 @@ def run_case(idx):
     io = c.get("io")
     x45 = c.get("x45", 0)
     ref = RefOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io, x45=x45)
+                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io, x45=x45, solid_forcing=c.get("sf"))
     out = {k: c[k] for k in ("nx", "ny", "nz", "xn", "yn", "zn", "phi", "u", "v", "w", "f43", "f44", "f45",
                               "f49", "n47", "steps", "f46", "f47")}
     for a, n in enumerate((nx, ny, nz)):
@@ -168,6 +187,8 @@ def run_case(idx):
         from oracle.bindings import IOFLOW_DEFAULTS
         for k, val in dict(IOFLOW_DEFAULTS, **io).items():
             out["io_" + k] = val
+    if c.get("sf") is not None:
+        out["sf"] = c["sf"]
     out["psi"] = ref.psi
     out["vel_scale"] = np.array(c["vel_scale"] or "none")
     phi, u, v, w = c["phi"], c["u"], c["v"], c["w"]

@@ -83,6 +83,11 @@ def _case(name):
         else:
             bodies = {11: rng.uniform(-0.3, 1.0, shape), 12: rng.uniform(-0.3, 1.0, shape)}
         c.update(x45=x45, bodies=bodies)
+    if name == "stretched_sf":
+        # solid forcing after each convection stage over a random gcdf4 list
+        sides = rng.choice([1, 2, 3, 4, 5, 6], 80)
+        c["sf"] = np.stack([rng.integers(0, nx, 80), rng.integers(0, ny, 80), rng.integers(0, nz, 80), sides],
+                           axis=1).astype(np.int32)
     return c
 
 
@@ -104,7 +109,7 @@ def _run(name, precision=0):
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
                        f49=c["f49"], f46=c["f46"], f47=6, precision=precision, ioflow=c.get("io"),
-                       x45=c.get("x45", 0))
+                       x45=c.get("x45", 0), solid_forcing=c.get("sf"))
     out = {}
     ao.set_state(c["phi"], c["u"], c["v"], c["w"])
     for fid, arr in c.get("bodies", {}).items():
@@ -149,7 +154,7 @@ def _run(name, precision=0):
 
 
 @pytest.mark.parametrize("name", ["vortex3d", "disk2d", "stretched_f49_0", "stretched_picard", "tank_io3d",
-                                  "tank_io2d", "stretched_df4", "stretched_df5"])
+                                  "tank_io2d", "stretched_df4", "stretched_df5", "stretched_sf"])
 def test_adapters_match_reference_objects(name):
     from oracle.bindings import AdapterOracle
     if not AdapterOracle.available():

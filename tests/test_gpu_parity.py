@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 import reef3d_b200 as r3d
-from conftest import GOLDEN_CASES, body_field, golden_df, golden_flags, golden_ioflow, load_golden, velocity_at
+from conftest import (GOLDEN_CASES, body_field, golden_df, golden_flags, golden_ioflow, golden_sf, load_golden,
+                      velocity_at)
 from test_oracle_golden import interior, visible_mask
 
 pytestmark = pytest.mark.gpu
@@ -34,6 +35,8 @@ def make_gpu(g, precision=r3d.FP64):
     if df is not None:  # direct-forcing convection stencils (X45)
         ls.set_direct_forcing(df[0])
         ls.upload(r3d.BODY, body_field(*df))
+    if golden_sf(g) is not None:  # solid forcing after each convection stage (X48)
+        ls.set_solid_forcing(golden_sf(g))
     return ls
 
 

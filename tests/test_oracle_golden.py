@@ -5,7 +5,7 @@ layers; edge and corner ghosts are outside every stencil of the path)."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, golden_df, golden_flags, golden_ioflow, load_golden, velocity_at
+from conftest import GOLDEN_CASES, golden_df, golden_flags, golden_ioflow, golden_sf, load_golden, velocity_at
 
 
 def visible_mask(nx, ny, nz):
@@ -28,6 +28,8 @@ def case(request, port_lib):
     df = golden_df(g)
     if df is not None:  # direct-forcing convection stencils (X45)
         o.set_direct_forcing(*df)
+    if golden_sf(g) is not None:  # solid forcing after each convection stage (X48)
+        o.set_solid_forcing(golden_sf(g))
     return g, o
 
 
