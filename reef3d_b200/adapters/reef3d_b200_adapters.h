@@ -215,10 +215,12 @@ struct IoflowState {
 // The device writes the interior and the face ghost layers of every field it
 // returns; the adapters then run REEF3D's own ghostcell::start4 on the host
 // copy, which also fills the edge and corner ghosts (dgcpol4) and, in a
-// multi-rank run, exchanges the halo.  (The device step itself knows walls
-// and the inflow / outflow x faces of ioflow_f only: a REEF3D run split over
-// several MPI ranks needs one device instance per rank and a halo exchange
-// per stage, which this library does not do.)
+// multi-rank run, exchanges the halo.  (The device step knows walls, the
+// inflow / outflow x faces of ioflow_f, the X45 stencils and the solid
+// forcing.  A REEF3D run split over several MPI ranks needs a halo exchange
+// in every stage; the library has it for z slabs -- r3d_set_halo,
+// r3d_halo_copy, reef3d_b200/slab.py -- but these adapters drive one
+// single-subdomain instance.)
 
 // freesurface: one level-set step on the device (three WENO5-HJ convection
 // RK stages with the wall ghost fill, F44 reinitialisation pseudo-steps, the
