@@ -204,12 +204,13 @@ def test_bounded_wait_timeout_path_reports_and_recovers():
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("which", ["vortex256", "wave_tank"])
+@pytest.mark.parametrize("which", ["vortex256", "wave_tank", "wave_tank_open"])
 def test_full_size_fp32_step_matches_fp64(which):
     """At the benchmark sizes (256^3 vortex; 1024 x 128 x 256 wave tank with
-    the Airy generator): one step of the FP32 form within the FP32 tolerance
-    of the FP64 path (relative max-norm 2e-5 over the interior), and the FP64
-    volume sums of the two results within 1e-6 of each other."""
+    the Airy generator, closed or with an inflow and an outflow face whose
+    hooks impose the water levels): one step of the FP32 form within the FP32
+    tolerance of the FP64 path (relative max-norm 2e-5 over the interior),
+    and the FP64 volume sums of the two results within 1e-6 of each other."""
     if which == "vortex256":
         c = setups.vortex3d(256)
     else:
@@ -225,6 +226,8 @@ def test_full_size_fp32_step_matches_fp64(which):
             else:
                 ls.set_time(0.0)
                 ls.set_velocity_airy(0.05, 2.0, 0.5)
+            if which == "wave_tank_open":
+                ls.set_ioflow(f50=2, b77=2, f60=0.5, f62=0.5)
             if dt is None:
                 dt = ls.cfl_dt()
             else:
