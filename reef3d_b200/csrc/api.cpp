@@ -1375,3 +1375,286 @@ int r3d_launch_count(const r3d_handle* h, long long* count) {
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------- slab domain
+// One grid split along z into slabs on the current device, stepped as one:
+// every RK stage runs on all slabs (each on its own stream), then the halo
+// planes move between neighbours (the role of ghostcell::gcparax,
+// src/gcx_parax.cpp), then the next stage; the CFL step takes the maxima
+// over all slabs; the whole step is captured in one CUDA graph.
+struct r3d_domain {
+    std::vector<r3d_handle*> slab;
+    std::vector<int> k0, k1;
+    int nx = 0, ny = 0, nz = 0;
+    int f44 = 0;
+    double n47 = 0.0;
+    double dxmin = 0.0;
+    cudaStream_t main = nullptr;
+    std::vector<cudaEvent_t> ev;  // one per slab, reused per stage
+    cudaEvent_t fork = nullptr, xdone = nullptr;
+    unsigned long long** d_vm = nullptr;  // device array of the slabs' s.vmax
+    double** d_dt = nullptr;              // device array of the slabs' s.dt
+    cudaGraphExec_t graph = nullptr;
+    int graph_adaptive = -1;
+    bool ran = false;
+    std::string err;
+};
+
+namespace {
+
+int dfail(r3d_domain* d, int code, const std::string& m) {
+    if (d) d->err = m;
+    return code;
+}
+
+// all slab streams wait for work recorded on `from`
+void domain_fork(r3d_domain* d, cudaStream_t from) {
+    cudaEventRecord(d->fork, from);
+    for (r3d_handle* h : d->slab) cudaStreamWaitEvent(h->stream, d->fork, 0);
+}
+
+// `to` waits for every slab stream
+void domain_join(r3d_domain* d, cudaStream_t to) {
+    for (size_t s = 0; s < d->slab.size(); ++s) {
+        cudaEventRecord(d->ev[s], d->slab[s]->stream);
+        cudaStreamWaitEvent(to, d->ev[s], 0);
+    }
+}
+
+// Halo exchange of `field` on the main stream: slab r's top three interior
+// planes into slab r+1's bottom ghost planes, and back.
+void domain_exchange(r3d_domain* d, int field) {
+    domain_join(d, d->main);
+    for (size_t r = 0; r + 1 < d->slab.size(); ++r) {
+        r3d_handle* lo = d->slab[r];
+        r3d_handle* hi = d->slab[r + 1];
+        const size_t e = field_elem(lo, field), plane = (size_t)lo->L.sz * e;
+        char* flo = static_cast<char*>(lo->field[field]);
+        char* fhi = static_cast<char*>(hi->field[field]);
+        cudaMemcpyAsync(fhi, flo + (size_t)lo->L.nz * plane, 3 * plane, cudaMemcpyDeviceToDevice, d->main);
+        cudaMemcpyAsync(flo + (size_t)(lo->L.nz + 3) * plane, fhi + 3 * plane, 3 * plane, cudaMemcpyDeviceToDevice,
+                        d->main);
+    }
+    domain_fork(d, d->main);
+}
+
+void domain_stage(r3d_domain* d, bool reini, int s, bool vol) {
+    for (r3d_handle* h : d->slab) h->launches += stage_launch(h, reini, s, vol);
+    domain_exchange(d, s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI);
+}
+
+// One step of every slab (levelset_RK3::start without picard, fluid update
+// or inflow/outflow), enqueued from the main stream back to it.
+void domain_enqueue_step(r3d_domain* d, bool adaptive) {
+    domain_fork(d, d->main);
+    if (adaptive) {
+        for (r3d_handle* h : d->slab) {
+            h->launches += refresh_velocity(h);
+            h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h),
+                                      h->M.dxmin_cfl, h->desc.n47, h->S, h->stream);
+        }
+        domain_join(d, d->main);
+        launch_domain_dt(d->d_vm, d->d_dt, (int)d->slab.size(), d->slab[0]->S.vscale, d->dxmin, d->n47, d->main);
+        domain_fork(d, d->main);
+    } else {
+        for (r3d_handle* h : d->slab) h->launches += refresh_velocity(h);
+    }
+    for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, d->f44 == 0 && s == 3);
+    for (int q = 0; q < d->f44; ++q)
+        for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, q == d->f44 - 1 && s == 3);
+    for (r3d_handle* h : d->slab)
+        h->launches += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
+    domain_join(d, d->main);
+}
+
+}  // namespace
+
+extern "C" {
+
+int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, r3d_domain** out) {
+    std::string why;
+    if (!out) return fail(nullptr, R3D_EINVAL, "null output");
+    *out = nullptr;
+    if (int rc = check_desc(desc, why)) return fail(nullptr, rc, why);
+    if (desc->f46 != 0) return fail(nullptr, R3D_EINVAL, "slab domains run without the picard correction");
+    if (nslabs < 1 || desc->nz < 3 * nslabs) return fail(nullptr, R3D_EINVAL, "every slab needs >= 3 z cells");
+    r3d_domain* d = new (std::nothrow) r3d_domain();
+    if (!d) return fail(nullptr, R3D_ENOMEM, "host allocation failed");
+    d->nx = desc->nx;
+    d->ny = desc->ny;
+    d->nz = desc->nz;
+    d->f44 = desc->f44;
+    d->n47 = desc->n47;
+    double out4[4];
+    if (int rc = r3d_grid_spacing(desc, out4)) {
+        delete d;
+        return rc;
+    }
+    const int base = desc->nz / nslabs, extra = desc->nz % nslabs;
+    int k = 0;
+    d->dxmin = 1.0e300;
+    int rc = R3D_OK;
+    for (int r = 0; r < nslabs && !rc; ++r) {
+        const int n = base + (r < extra ? 1 : 0);
+        r3d_grid_desc sd = *desc;
+        sd.nz = n;
+        sd.zn = desc->zn + k;  // node indices -5..n+5 of the slab
+        r3d_handle* h = nullptr;
+        rc = r3d_create(&sd, &h);
+        if (!rc) rc = r3d_set_halo(h, k > 0 ? 1 : 0, k + n < desc->nz ? 1 : 0);
+        if (!rc) rc = r3d_set_grid_spacing(h, out4[0], out4[1], out4[2]);
+        if (h) {
+            d->slab.push_back(h);
+            d->k0.push_back(k);
+            d->k1.push_back(k + n);
+            d->dxmin = std::min(d->dxmin, h->M.dxmin_cfl);
+        }
+        k += n;
+    }
+    auto bail = [&](int code, const std::string& m) {
+        r3d_domain_destroy(d);
+        return fail(nullptr, code, m);
+    };
+    if (rc) return bail(rc, "creating the slabs");
+    if (cudaStreamCreateWithFlags(&d->main, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&d->xdone, cudaEventDisableTiming) != cudaSuccess)
+        return bail(R3D_EDEVICE, "domain stream/events");
+    d->ev.resize(d->slab.size(), nullptr);
+    for (auto& e : d->ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return bail(R3D_EDEVICE, "domain events");
+    std::vector<unsigned long long*> vm;
+    std::vector<double*> dts;
+    for (r3d_handle* h : d->slab) {
+        vm.push_back(h->S.vmax);
+        dts.push_back(h->S.dt);
+    }
+    if (cudaMalloc(&d->d_vm, vm.size() * sizeof(void*)) != cudaSuccess ||
+        cudaMalloc(&d->d_dt, dts.size() * sizeof(void*)) != cudaSuccess)
+        return bail(R3D_ENOMEM, "domain pointer arrays");
+    cudaMemcpy(d->d_vm, vm.data(), vm.size() * sizeof(void*), cudaMemcpyHostToDevice);
+    cudaMemcpy(d->d_dt, dts.data(), dts.size() * sizeof(void*), cudaMemcpyHostToDevice);
+    *out = d;
+    return R3D_OK;
+}
+
+int r3d_domain_destroy(r3d_domain* d) {
+    if (!d) return R3D_EINVAL;
+    if (d->main) cudaStreamSynchronize(d->main);
+    if (d->graph) cudaGraphExecDestroy(d->graph);
+    for (r3d_handle* h : d->slab) r3d_destroy(h);
+    for (auto e : d->ev)
+        if (e) cudaEventDestroy(e);
+    if (d->fork) cudaEventDestroy(d->fork);
+    if (d->xdone) cudaEventDestroy(d->xdone);
+    if (d->d_vm) cudaFree(d->d_vm);
+    if (d->d_dt) cudaFree(d->d_dt);
+    if (d->main) cudaStreamDestroy(d->main);
+    delete d;
+    return R3D_OK;
+}
+
+const char* r3d_domain_last_error(const r3d_domain* d) { return d ? d->err.c_str() : ""; }
+
+int r3d_domain_slab(r3d_domain* d, int s, r3d_handle** h, int* k0, int* k1) {
+    if (!d || s < 0 || s >= (int)d->slab.size()) return dfail(d, R3D_EINVAL, "bad slab index");
+    if (h) *h = d->slab[s];
+    if (k0) *k0 = d->k0[s];
+    if (k1) *k1 = d->k1[s];
+    return R3D_OK;
+}
+
+int r3d_domain_upload(r3d_domain* d, int field, const double* host) {
+    if (!d || !host) return dfail(d, R3D_EINVAL, "null argument");
+    const long long jm = d->ny + 6, km = d->nz + 6;
+    for (size_t s = 0; s < d->slab.size(); ++s) {
+        const int n = d->k1[s] - d->k0[s];
+        std::vector<double> part((size_t)(d->nx + 6) * jm * (n + 6));
+        for (long long i = 0; i < d->nx + 6; ++i)
+            for (long long j = 0; j < jm; ++j)
+                std::memcpy(&part[((size_t)i * jm + j) * (n + 6)], host + (i * jm + j) * km + d->k0[s],
+                            sizeof(double) * (n + 6));
+        if (int rc = r3d_upload(d->slab[s], field, part.data(), R3D_LAYOUT_REEF3D))
+            return dfail(d, rc, r3d_last_error(d->slab[s]));
+    }
+    return R3D_OK;
+}
+
+int r3d_domain_download(r3d_domain* d, int field, double* host) {
+    if (!d || !host) return dfail(d, R3D_EINVAL, "null argument");
+    const long long jm = d->ny + 6, km = d->nz + 6;
+    const size_t ns = d->slab.size();
+    for (size_t s = 0; s < ns; ++s) {
+        const int n = d->k1[s] - d->k0[s];
+        std::vector<double> part((size_t)(d->nx + 6) * jm * (n + 6));
+        if (int rc = r3d_download(d->slab[s], field, part.data(), R3D_LAYOUT_REEF3D))
+            return dfail(d, rc, r3d_last_error(d->slab[s]));
+        // interior planes of the slab; the outer ghost planes from the end slabs
+        const int lo = s == 0 ? 0 : 3, hi = s + 1 == ns ? n + 6 : n + 3;
+        for (long long i = 0; i < d->nx + 6; ++i)
+            for (long long j = 0; j < jm; ++j)
+                std::memcpy(host + (i * jm + j) * km + d->k0[s] + lo, &part[((size_t)i * jm + j) * (n + 6) + lo],
+                            sizeof(double) * (hi - lo));
+    }
+    return R3D_OK;
+}
+
+int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
+    if (!d || nsteps < 0) return dfail(d, R3D_EINVAL, "bad argument");
+    const bool adaptive = !(dt > 0.0);
+    if (!adaptive)
+        for (r3d_handle* h : d->slab)
+            if (int rc = r3d_set_dt(h, dt)) return dfail(d, rc, r3d_last_error(h));
+    for (r3d_handle* h : d->slab) cudaStreamSynchronize(h->stream);
+    if (!d->graph || d->graph_adaptive != (adaptive ? 1 : 0)) {
+        if (d->graph) cudaGraphExecDestroy(d->graph);
+        d->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(d->main, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return dfail(d, R3D_EDEVICE, "domain capture");
+        domain_enqueue_step(d, adaptive);
+        cudaError_t e = cudaStreamEndCapture(d->main, &g);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&d->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            d->graph = nullptr;
+            return dfail(d, R3D_EDEVICE, std::string("domain step graph: ") + cudaGetErrorString(e));
+        }
+        d->graph_adaptive = adaptive ? 1 : 0;
+    }
+    for (int n = 0; n < nsteps; ++n)
+        if (cudaGraphLaunch(d->graph, d->main) != cudaSuccess) return dfail(d, R3D_EDEVICE, "domain step launch");
+    const cudaError_t e = cudaStreamSynchronize(d->main);
+    if (e != cudaSuccess) return dfail(d, R3D_EDEVICE, cudaGetErrorString(e));
+    for (r3d_handle* h : d->slab) {
+        h->have_last_volume = true;
+        if (int rc = check_device_flag(h)) return dfail(d, rc, r3d_last_error(h));
+    }
+    d->ran = d->ran || nsteps > 0;
+    return R3D_OK;
+}
+
+int r3d_domain_last_volume(r3d_domain* d, double* volume1, double* volume2) {
+    if (!d) return R3D_EINVAL;
+    if (!d->ran) return dfail(d, R3D_ESTATE, "no step has run yet");
+    double a = 0.0, b = 0.0;
+    for (r3d_handle* h : d->slab) {
+        double v1 = 0.0, v2 = 0.0;
+        if (int rc = r3d_last_volume(h, &v1, &v2)) return dfail(d, rc, r3d_last_error(h));
+        a += v1;
+        b += v2;
+    }
+    if (volume1) *volume1 = a;
+    if (volume2) *volume2 = b;
+    return R3D_OK;
+}
+
+int r3d_domain_get_dt(r3d_domain* d, double* dt) {
+    if (!d || !dt) return R3D_EINVAL;
+    if (cudaMemcpy(dt, d->slab[0]->S.dt, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return dfail(d, R3D_EDEVICE, "reading dt");
+    return R3D_OK;
+}
+
+}  // extern "C"

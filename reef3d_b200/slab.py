@@ -12,6 +12,9 @@ Two ways to hold the slabs:
 * ``DistSlab``: one slab per rank of ``torch.distributed`` (one process per
   GPU, NCCL over NVLink); halos move by point-to-point send/recv, maxima,
   minima and sums by all-reduce.
+* ``Domain``: the native runner (r3d_domain_*): all slabs on the current
+  GPU, each on its own stream, the whole decomposed step -- stages, halo
+  copies, the global CFL step -- captured in one CUDA graph.
 
 A step is the step of ``r3d_ls_step`` taken stage by stage (three
 convection stages, f44 reinitialisation pseudo-steps of three stages, the
@@ -22,7 +25,10 @@ middle of a step.
 """
 import numpy as np
 
-from . import PHI, R3DError, RO, VISC, WORK1, WORK2, LevelSet, STAGE_CONVECTION, STAGE_REINIT, grid_spacing
+import ctypes
+
+from . import (FP64, PHI, R3D_OK, R3DError, RO, VISC, WORK1, WORK2, LevelSet, STAGE_CONVECTION, STAGE_REINIT,
+               grid_spacing, load_library, make_desc, uniform_nodes)
 
 # stage s writes phi -> WORK1 -> WORK2 -> phi (convection and reinitialisation)
 STAGE_OUT = {1: WORK1, 2: WORK2, 3: PHI}
@@ -256,3 +262,63 @@ class DistSlab(_Stepper):
 
     def close(self):
         self.ls.close()
+
+
+class Domain:
+    """One grid split along z into `nslabs` slabs on the current GPU and
+    stepped as one by the native runner (r3d_domain_*): fields in the
+    reference's layout of the whole grid."""
+
+    def __init__(self, nx, ny, nz, xn=None, yn=None, zn=None, nslabs=2, f43=0.55, f44=3, f45=2.1, f49=1,
+                 n47=0.3, precision=FP64):
+        self._lib = load_library()
+        xn = uniform_nodes(nx) if xn is None else xn
+        yn = uniform_nodes(ny) if yn is None else yn
+        zn = uniform_nodes(nz) if zn is None else zn
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision, 0, 10)
+        d = ctypes.c_void_p()
+        rc = self._lib.r3d_domain_create(ctypes.byref(self.desc), nslabs, ctypes.byref(d))
+        if rc != R3D_OK:
+            msg = self._lib.r3d_last_error(None)
+            raise R3DError(rc, msg.decode() if msg else "")
+        self.d = d
+
+    def _check(self, rc):
+        if rc != R3D_OK:
+            msg = self._lib.r3d_domain_last_error(self.d)
+            raise R3DError(rc, msg.decode() if msg else "")
+
+    def upload(self, field, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self._check(self._lib.r3d_domain_upload(self.d, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def download(self, field):
+        a = np.zeros((self.nx + 6, self.ny + 6, self.nz + 6))
+        self._check(self._lib.r3d_domain_download(self.d, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return a
+
+    def run(self, nsteps, dt=0.0):
+        """nsteps steps; dt <= 0: adaptive (CFL over all slabs)."""
+        self._check(self._lib.r3d_domain_run(self.d, nsteps, dt))
+
+    def last_volume(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.r3d_domain_last_volume(self.d, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def dt(self):
+        v = ctypes.c_double()
+        self._check(self._lib.r3d_domain_get_dt(self.d, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "d", None) is not None and self.d.value:
+            self._lib.r3d_domain_destroy(self.d)
+            self.d = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
