@@ -202,6 +202,7 @@ def run_configs(ctx):
     out["ensemble_accuracy"] = workloads.ensemble_accuracy(200)
     out["serving_fp32"] = workloads.serving(njobs=16)
     out["serving_fp64"] = workloads.serving(njobs=16, precision=FP64)
+    out["slab_domain"] = workloads.slab_domain()
     return out
 
 

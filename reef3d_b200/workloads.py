@@ -300,3 +300,43 @@ def serving(njobs=48, rate=200.0, seed=1, budget=150e9, precision=FP32, autotune
     finally:
         srv.close()
     return out
+
+
+def slab_domain(n=256, nslabs=4, steps=20, warmup=3, precision=FP32):
+    """The 256^3 vortex split into z slabs on this GPU and stepped by the
+    native runner (r3d_domain_*, one CUDA graph per step with the halo
+    copies), beside the undivided instance on the same steps: the cost of
+    the decomposition.  Fixed-velocity adaptive steps from t = 0."""
+    import time
+    from . import PHI, U, V, W, LevelSet
+    from .slab import Domain
+    c = setups.vortex3d(n)
+    res = {}
+    d = Domain(n, n, n, c.xn, c.yn, c.zn, nslabs=nslabs, precision=precision, **c.flags())
+    try:
+        for f, a in ((PHI, c.phi), (U, c.u), (V, c.v), (W, c.w)):
+            d.upload(f, a)
+        d.run(warmup)
+        t0 = time.perf_counter()
+        d.run(steps)
+        res["domain_ms_per_step"] = 1e3 * (time.perf_counter() - t0) / steps
+        phi_d = d.download(PHI)
+    finally:
+        d.close()
+    with LevelSet(n, n, n, c.xn, c.yn, c.zn, precision=precision, **c.flags()) as ls:
+        for f, a in ((PHI, c.phi), (U, c.u), (V, c.v), (W, c.w)):
+            ls.upload(f, a)
+        ls.run(warmup, adaptive=True)
+        ls.sync()
+        t0 = time.perf_counter()
+        ls.run(steps, adaptive=True)
+        ls.sync()
+        res["single_ms_per_step"] = 1e3 * (time.perf_counter() - t0) / steps
+        phi_s = ls.download(PHI)
+    cells = n ** 3
+    res.update({"workload": f"vortex {n}^3 in {nslabs} z slabs on one GPU (r3d_domain), {steps} adaptive steps",
+                "cell_updates_per_s": cells / (res["domain_ms_per_step"] * 1e-3),
+                "overhead": res["domain_ms_per_step"] / res["single_ms_per_step"] - 1.0,
+                "phi_identical_to_undivided": bool(np.array_equal(phi_d[3:-3, 3:-3, 3:-3], phi_s[3:-3, 3:-3, 3:-3])),
+                "precision": "fp32 form" if precision == FP32 else "fp64"})
+    return res
