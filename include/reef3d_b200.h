@@ -450,7 +450,9 @@ int r3d_batch_launch_count(const r3d_batch* b, long long* count);
  * r3d_domain_upload / download take the whole grid in the reference's
  * layout.  r3d_domain_run: nsteps steps with time step dt, or adaptive ones
  * when dt <= 0; synchronous.  Not with the picard correction (its sums are
- * global inside the step).  Across GPUs the same decomposition runs one
+ * global inside the step), the fluid update or inflow/outflow faces; the
+ * slabs' own settings (velocity generator, X45 stencils, solid forcing)
+ * apply, set through r3d_domain_slab.  Across GPUs the same decomposition runs one
  * slab per process (reef3d_b200.slab.DistSlab, NCCL). */
 typedef struct r3d_domain r3d_domain;
 int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, r3d_domain** out);

@@ -1395,7 +1395,7 @@ struct r3d_domain {
     unsigned long long** d_vm = nullptr;  // device array of the slabs' s.vmax
     double** d_dt = nullptr;              // device array of the slabs' s.dt
     cudaGraphExec_t graph = nullptr;
-    int graph_adaptive = -1;
+    long long graph_adaptive = -1;  // configuration key of the captured step
     bool ran = false;
     std::string err;
 };
@@ -1603,11 +1603,20 @@ int r3d_domain_download(r3d_domain* d, int field, double* host) {
 int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
     if (!d || nsteps < 0) return dfail(d, R3D_EINVAL, "bad argument");
     const bool adaptive = !(dt > 0.0);
+    for (r3d_handle* h : d->slab)
+        if (h->fluid || h->io)
+            return dfail(d, R3D_EINVAL, "the domain step has no fluid update and no inflow/outflow faces");
     if (!adaptive)
         for (r3d_handle* h : d->slab)
             if (int rc = r3d_set_dt(h, dt)) return dfail(d, rc, r3d_last_error(h));
     for (r3d_handle* h : d->slab) cudaStreamSynchronize(h->stream);
-    if (!d->graph || d->graph_adaptive != (adaptive ? 1 : 0)) {
+    // the captured step depends on the slabs' configuration (velocity
+    // generator, forcing, precision path): recapture when it changed
+    long long key = adaptive ? 1 : 0;
+    for (r3d_handle* h : d->slab)
+        key = key * 64 + (h->airy ? 1 : 0) + (h->sf_ops ? 2 : 0) + (h->g64.x45 ? 4 : 0) + (tiled(h) ? 8 : 0) +
+              (h->band64 ? 16 : 0) + (h->fluid ? 32 : 0);
+    if (!d->graph || d->graph_adaptive != key) {
         if (d->graph) cudaGraphExecDestroy(d->graph);
         d->graph = nullptr;
         cudaGraph_t g = nullptr;
@@ -1621,7 +1630,7 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
             d->graph = nullptr;
             return dfail(d, R3D_EDEVICE, std::string("domain step graph: ") + cudaGetErrorString(e));
         }
-        d->graph_adaptive = adaptive ? 1 : 0;
+        d->graph_adaptive = key;
     }
     for (int n = 0; n < nsteps; ++n)
         if (cudaGraphLaunch(d->graph, d->main) != cudaSuccess) return dfail(d, R3D_EDEVICE, "domain step launch");
