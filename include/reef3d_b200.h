@@ -437,25 +437,27 @@ int r3d_batch_sync(r3d_batch* b);
 int r3d_batch_stream(r3d_batch* b, void** stream);
 int r3d_batch_launch_count(const r3d_batch* b, long long* count);
 
-/* One grid split along z into nslabs slabs on the current device and
- * stepped as one (the role of the reference's MPI decomposition with
+/* One grid split along z into nslabs slabs -- on the current device, or
+ * slab r on devices[r] -- and stepped as one (the role of the reference's
+ * MPI decomposition with
  * ghostcell::gcparax, src/gcx_parax.cpp, for z splits): each slab is an
  * instance with halo faces towards its neighbours (r3d_set_halo) and the
  * whole grid's spacing constants; a step runs every RK stage on all slabs,
  * each on its own stream, then moves the three halo planes between
- * neighbours, then the next stage; the adaptive time step takes the maxima
- * over all slabs (pgc->globalmax) at the grid's smallest cell.  The step is
- * captured in one CUDA graph.  The level set, dt and clock equal the
+ * neighbours by peer copies (over NVLink between GPUs), then the next
+ * stage; the adaptive time step takes the maxima over all slabs
+ * (pgc->globalmax) at the grid's smallest cell.  The step is captured in one
+ * CUDA graph.  The level set, dt and clock equal the
  * undivided grid's; the volume sums are taken per slab and added.
  * r3d_domain_upload / download take the whole grid in the reference's
  * layout.  r3d_domain_run: nsteps steps with time step dt, or adaptive ones
  * when dt <= 0; synchronous.  Not with the picard correction (its sums are
  * global inside the step), the fluid update or inflow/outflow faces; the
  * slabs' own settings (velocity generator, X45 stencils, solid forcing)
- * apply, set through r3d_domain_slab.  Across GPUs the same decomposition runs one
- * slab per process (reef3d_b200.slab.DistSlab, NCCL). */
+ * apply, set through r3d_domain_slab.  One process per GPU runs the same
+ * decomposition with reef3d_b200.slab.DistSlab (NCCL). */
 typedef struct r3d_domain r3d_domain;
-int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, r3d_domain** out);
+int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices, r3d_domain** out);
 int r3d_domain_destroy(r3d_domain* d);
 const char* r3d_domain_last_error(const r3d_domain* d);
 int r3d_domain_slab(r3d_domain* d, int s, r3d_handle** h, int* k0, int* k1);

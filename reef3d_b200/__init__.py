@@ -146,7 +146,8 @@ EXPORTS = {
     "r3d_batch_sync": ([_H], ctypes.c_int),
     "r3d_batch_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_batch_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
-    "r3d_domain_create": ([ctypes.POINTER(GridDesc), ctypes.c_int, ctypes.POINTER(_H)], ctypes.c_int),
+    "r3d_domain_create": ([ctypes.POINTER(GridDesc), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_H)],
+                          ctypes.c_int),
     "r3d_domain_destroy": ([_H], ctypes.c_int),
     "r3d_domain_last_error": ([_H], ctypes.c_char_p),
     "r3d_domain_slab": ([_H, ctypes.c_int, ctypes.POINTER(_H), ctypes.POINTER(ctypes.c_int),

@@ -1377,11 +1377,12 @@ int r3d_launch_count(const r3d_handle* h, long long* count) {
 }  // extern "C"
 
 // ----------------------------------------------------------- slab domain
-// One grid split along z into slabs on the current device, stepped as one:
-// every RK stage runs on all slabs (each on its own stream), then the halo
-// planes move between neighbours (the role of ghostcell::gcparax,
-// src/gcx_parax.cpp), then the next stage; the CFL step takes the maxima
-// over all slabs; the whole step is captured in one CUDA graph.
+// One grid split along z into slabs, on one device or several, stepped as
+// one: every RK stage runs on all slabs (each on its own stream), then the
+// halo planes move between neighbours by peer copies (the role of
+// ghostcell::gcparax, src/gcx_parax.cpp), then the next stage; the CFL step
+// takes the maxima over all slabs; the whole step is captured in one CUDA
+// graph.
 struct r3d_domain {
     std::vector<r3d_handle*> slab;
     std::vector<int> k0, k1;
@@ -1392,8 +1393,9 @@ struct r3d_domain {
     cudaStream_t main = nullptr;
     std::vector<cudaEvent_t> ev;  // one per slab, reused per stage
     cudaEvent_t fork = nullptr, xdone = nullptr;
-    unsigned long long** d_vm = nullptr;  // device array of the slabs' s.vmax
-    double** d_dt = nullptr;              // device array of the slabs' s.dt
+    int dev0 = 0;                          // device of slab 0: main stream, gather buffers
+    unsigned long long* gather = nullptr;  // the slabs' CFL maxima, 3 per slab (on dev0)
+    double* dtbuf = nullptr;               // the grid's time step (on dev0)
     cudaGraphExec_t graph = nullptr;
     long long graph_adaptive = -1;  // configuration key of the captured step
     bool ran = false;
@@ -1407,71 +1409,92 @@ int dfail(r3d_domain* d, int code, const std::string& m) {
     return code;
 }
 
-// all slab streams wait for work recorded on `from`
-void domain_fork(r3d_domain* d, cudaStream_t from) {
-    cudaEventRecord(d->fork, from);
-    for (r3d_handle* h : d->slab) cudaStreamWaitEvent(h->stream, d->fork, 0);
+// all slab streams wait for work recorded on the main stream
+void domain_fork(r3d_domain* d) {
+    cudaSetDevice(d->dev0);
+    cudaEventRecord(d->fork, d->main);
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
+        cudaStreamWaitEvent(h->stream, d->fork, 0);
+    }
+    cudaSetDevice(d->dev0);
 }
 
-// `to` waits for every slab stream
-void domain_join(r3d_domain* d, cudaStream_t to) {
+// the main stream waits for every slab stream
+void domain_join(r3d_domain* d) {
     for (size_t s = 0; s < d->slab.size(); ++s) {
+        cudaSetDevice(d->slab[s]->device);
         cudaEventRecord(d->ev[s], d->slab[s]->stream);
-        cudaStreamWaitEvent(to, d->ev[s], 0);
     }
+    cudaSetDevice(d->dev0);
+    for (size_t s = 0; s < d->slab.size(); ++s) cudaStreamWaitEvent(d->main, d->ev[s], 0);
 }
 
 // Halo exchange of `field` on the main stream: slab r's top three interior
 // planes into slab r+1's bottom ghost planes, and back.
 void domain_exchange(r3d_domain* d, int field) {
-    domain_join(d, d->main);
+    domain_join(d);
     for (size_t r = 0; r + 1 < d->slab.size(); ++r) {
         r3d_handle* lo = d->slab[r];
         r3d_handle* hi = d->slab[r + 1];
         const size_t e = field_elem(lo, field), plane = (size_t)lo->L.sz * e;
         char* flo = static_cast<char*>(lo->field[field]);
         char* fhi = static_cast<char*>(hi->field[field]);
-        cudaMemcpyAsync(fhi, flo + (size_t)lo->L.nz * plane, 3 * plane, cudaMemcpyDeviceToDevice, d->main);
-        cudaMemcpyAsync(flo + (size_t)(lo->L.nz + 3) * plane, fhi + 3 * plane, 3 * plane, cudaMemcpyDeviceToDevice,
+        // unified addressing: the copy engine moves the planes between the
+        // slabs' devices (peer copies over NVLink) or within one
+        cudaMemcpyAsync(fhi, flo + (size_t)lo->L.nz * plane, 3 * plane, cudaMemcpyDefault, d->main);
+        cudaMemcpyAsync(flo + (size_t)(lo->L.nz + 3) * plane, fhi + 3 * plane, 3 * plane, cudaMemcpyDefault,
                         d->main);
     }
-    domain_fork(d, d->main);
+    domain_fork(d);
 }
 
 void domain_stage(r3d_domain* d, bool reini, int s, bool vol) {
-    for (r3d_handle* h : d->slab) h->launches += stage_launch(h, reini, s, vol);
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
+        h->launches += stage_launch(h, reini, s, vol);
+    }
     domain_exchange(d, s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI);
 }
 
 // One step of every slab (levelset_RK3::start without picard, fluid update
 // or inflow/outflow), enqueued from the main stream back to it.
 void domain_enqueue_step(r3d_domain* d, bool adaptive) {
-    domain_fork(d, d->main);
-    if (adaptive) {
-        for (r3d_handle* h : d->slab) {
-            h->launches += refresh_velocity(h);
+    domain_fork(d);
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
+        h->launches += refresh_velocity(h);
+        if (adaptive)
             h->launches += launch_cfl(h->L, h->field[R3D_U], h->field[R3D_V], h->field[R3D_W], fp32(h),
                                       h->M.dxmin_cfl, h->desc.n47, h->S, h->stream);
-        }
-        domain_join(d, d->main);
-        launch_domain_dt(d->d_vm, d->d_dt, (int)d->slab.size(), d->slab[0]->S.vscale, d->dxmin, d->n47, d->main);
-        domain_fork(d, d->main);
-    } else {
-        for (r3d_handle* h : d->slab) h->launches += refresh_velocity(h);
+    }
+    if (adaptive) {
+        // gather the maxima on slab 0's device, one dt, back to every slab
+        domain_join(d);
+        const int n = (int)d->slab.size();
+        for (int s = 0; s < n; ++s)
+            cudaMemcpyAsync(d->gather + 3 * s, d->slab[s]->S.vmax, 3 * sizeof(unsigned long long), cudaMemcpyDefault,
+                            d->main);
+        launch_domain_dt(d->gather, n, d->slab[0]->S.vscale, d->dxmin, d->n47, d->dtbuf, d->main);
+        for (int s = 0; s < n; ++s)
+            cudaMemcpyAsync(d->slab[s]->S.dt, d->dtbuf, sizeof(double), cudaMemcpyDefault, d->main);
+        domain_fork(d);
     }
     for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, d->f44 == 0 && s == 3);
     for (int q = 0; q < d->f44; ++q)
         for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, q == d->f44 - 1 && s == 3);
-    for (r3d_handle* h : d->slab)
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
         h->launches += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
-    domain_join(d, d->main);
+    }
+    domain_join(d);
 }
 
 }  // namespace
 
 extern "C" {
 
-int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, r3d_domain** out) {
+int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices, r3d_domain** out) {
     std::string why;
     if (!out) return fail(nullptr, R3D_EINVAL, "null output");
     *out = nullptr;
@@ -1494,12 +1517,19 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, r3d_domain** out) {
     int k = 0;
     d->dxmin = 1.0e300;
     int rc = R3D_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    d->dev0 = devices ? devices[0] : cur;
     for (int r = 0; r < nslabs && !rc; ++r) {
         const int n = base + (r < extra ? 1 : 0);
         r3d_grid_desc sd = *desc;
         sd.nz = n;
         sd.zn = desc->zn + k;  // node indices -5..n+5 of the slab
         r3d_handle* h = nullptr;
+        if (cudaSetDevice(devices ? devices[r] : cur) != cudaSuccess) {
+            rc = R3D_EINVAL;
+            break;
+        }
         rc = r3d_create(&sd, &h);
         if (!rc) rc = r3d_set_halo(h, k > 0 ? 1 : 0, k + n < desc->nz ? 1 : 0);
         if (!rc) rc = r3d_set_grid_spacing(h, out4[0], out4[1], out4[2]);
@@ -1515,26 +1545,26 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, r3d_domain** out) {
         r3d_domain_destroy(d);
         return fail(nullptr, code, m);
     };
-    if (rc) return bail(rc, "creating the slabs");
-    if (cudaStreamCreateWithFlags(&d->main, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&d->xdone, cudaEventDisableTiming) != cudaSuccess)
-        return bail(R3D_EDEVICE, "domain stream/events");
-    d->ev.resize(d->slab.size(), nullptr);
-    for (auto& e : d->ev)
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
-            return bail(R3D_EDEVICE, "domain events");
-    std::vector<unsigned long long*> vm;
-    std::vector<double*> dts;
-    for (r3d_handle* h : d->slab) {
-        vm.push_back(h->S.vmax);
-        dts.push_back(h->S.dt);
+    if (rc) {
+        cudaSetDevice(cur);
+        return bail(rc, "creating the slabs");
     }
-    if (cudaMalloc(&d->d_vm, vm.size() * sizeof(void*)) != cudaSuccess ||
-        cudaMalloc(&d->d_dt, dts.size() * sizeof(void*)) != cudaSuccess)
-        return bail(R3D_ENOMEM, "domain pointer arrays");
-    cudaMemcpy(d->d_vm, vm.data(), vm.size() * sizeof(void*), cudaMemcpyHostToDevice);
-    cudaMemcpy(d->d_dt, dts.data(), dts.size() * sizeof(void*), cudaMemcpyHostToDevice);
+    d->ev.resize(d->slab.size(), nullptr);
+    for (size_t r = 0; r < d->slab.size(); ++r) {  // each event on its slab's device
+        cudaSetDevice(d->slab[r]->device);
+        if (cudaEventCreateWithFlags(&d->ev[r], cudaEventDisableTiming) != cudaSuccess) {
+            cudaSetDevice(cur);
+            return bail(R3D_EDEVICE, "domain events");
+        }
+    }
+    cudaSetDevice(d->dev0);
+    const bool ok = cudaStreamCreateWithFlags(&d->main, cudaStreamNonBlocking) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) == cudaSuccess &&
+                    cudaEventCreateWithFlags(&d->xdone, cudaEventDisableTiming) == cudaSuccess &&
+                    cudaMalloc(&d->gather, 3 * d->slab.size() * sizeof(unsigned long long)) == cudaSuccess &&
+                    cudaMalloc(&d->dtbuf, sizeof(double)) == cudaSuccess;
+    cudaSetDevice(cur);
+    if (!ok) return bail(R3D_EDEVICE, "domain stream, events and buffers");
     *out = d;
     return R3D_OK;
 }
@@ -1548,8 +1578,8 @@ int r3d_domain_destroy(r3d_domain* d) {
         if (e) cudaEventDestroy(e);
     if (d->fork) cudaEventDestroy(d->fork);
     if (d->xdone) cudaEventDestroy(d->xdone);
-    if (d->d_vm) cudaFree(d->d_vm);
-    if (d->d_dt) cudaFree(d->d_dt);
+    if (d->gather) cudaFree(d->gather);
+    if (d->dtbuf) cudaFree(d->dtbuf);
     if (d->main) cudaStreamDestroy(d->main);
     delete d;
     return R3D_OK;
@@ -1602,6 +1632,7 @@ int r3d_domain_download(r3d_domain* d, int field, double* host) {
 
 int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
     if (!d || nsteps < 0) return dfail(d, R3D_EINVAL, "bad argument");
+    DeviceGuard dg(d->dev0);  // restores the caller's device
     const bool adaptive = !(dt > 0.0);
     for (r3d_handle* h : d->slab)
         if (h->fluid || h->io)
@@ -1620,6 +1651,7 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
         if (d->graph) cudaGraphExecDestroy(d->graph);
         d->graph = nullptr;
         cudaGraph_t g = nullptr;
+        cudaSetDevice(d->dev0);
         if (cudaStreamBeginCapture(d->main, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return dfail(d, R3D_EDEVICE, "domain capture");
         domain_enqueue_step(d, adaptive);
@@ -1628,10 +1660,12 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
         if (g) cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             d->graph = nullptr;
+            cudaGetLastError();  // leave no capture error behind for later calls
             return dfail(d, R3D_EDEVICE, std::string("domain step graph: ") + cudaGetErrorString(e));
         }
         d->graph_adaptive = key;
     }
+    cudaSetDevice(d->dev0);
     for (int n = 0; n < nsteps; ++n)
         if (cudaGraphLaunch(d->graph, d->main) != cudaSuccess) return dfail(d, R3D_EDEVICE, "domain step launch");
     const cudaError_t e = cudaStreamSynchronize(d->main);

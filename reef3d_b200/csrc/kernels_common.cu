@@ -729,13 +729,14 @@ int launch_solid_forcing(void* f, bool fp32, const long long* ops, const std::ve
 }
 
 // One time step for every slab of a decomposed grid: the maxima over the
-// slabs' CFL maxima (pgc->globalmax, src/ietimestep.cpp) and the expression
-// of dt_kernel at the smallest cell of the whole grid, written to each slab.
-__global__ void domain_dt_kernel(const unsigned long long* const* vm, double* const* dts, int n,
-                                 const double* vscale, double dxmin, double n47) {
+// slabs' CFL maxima (gathered into vm[3 n], pgc->globalmax,
+// src/ietimestep.cpp) and the expression of dt_kernel at the smallest cell
+// of the whole grid.
+__global__ void domain_dt_kernel(const unsigned long long* vm, int n, const double* vscale, double dxmin, double n47,
+                                 double* dt) {
     unsigned long long m[3] = {0, 0, 0};
     for (int s = 0; s < n; ++s)
-        for (int a = 0; a < 3; ++a) m[a] = vm[s][a] > m[a] ? vm[s][a] : m[a];
+        for (int a = 0; a < 3; ++a) m[a] = vm[3 * s + a] > m[a] ? vm[3 * s + a] : m[a];
     const double sc = fabs(*vscale);
     const double umax = sc * __longlong_as_double((long long)m[0]);
     const double vmax = sc * __longlong_as_double((long long)m[1]);
@@ -743,12 +744,12 @@ __global__ void domain_dt_kernel(const unsigned long long* const* vm, double* co
     double cu = 1.0e10;
     const double cand = 2.0 / ((sqrt(umax * umax + vmax * vmax + wmax * wmax)) / dxmin + sqrt((4.0 * fabs(0.0)) / dxmin));
     cu = cu < cand ? cu : cand;
-    for (int s = 0; s < n; ++s) *dts[s] = n47 * cu;
+    *dt = n47 * cu;
 }
 
-int launch_domain_dt(const unsigned long long* const* vm, double* const* dts, int n, const double* vscale,
-                     double dxmin, double n47, cudaStream_t st) {
-    domain_dt_kernel<<<1, 1, 0, st>>>(vm, dts, n, vscale, dxmin, n47);
+int launch_domain_dt(const unsigned long long* vm, int n, const double* vscale, double dxmin, double n47, double* dt,
+                     cudaStream_t st) {
+    domain_dt_kernel<<<1, 1, 0, st>>>(vm, n, vscale, dxmin, n47, dt);
     return 1;
 }
 

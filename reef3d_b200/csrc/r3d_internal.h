@@ -202,10 +202,10 @@ int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, c
 // when ro != nullptr (3 n floats).
 int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const void* visc, bool fp32, float* out,
                      long long npoints, cudaStream_t st);
-// dt of a decomposed grid from every slab's maxima (vm[s] = slab s's
-// s.vmax), at the grid's smallest cell, written to every slab's dt.
-int launch_domain_dt(const unsigned long long* const* vm, double* const* dts, int n, const double* vscale,
-                     double dxmin, double n47, cudaStream_t st);
+// dt of a decomposed grid from the slabs' maxima gathered into vm[3 n], at
+// the grid's smallest cell.
+int launch_domain_dt(const unsigned long long* vm, int n, const double* vscale, double dxmin, double n47, double* dt,
+                     cudaStream_t st);
 // dt from the velocity maxima already in s.vmax (the CFL's second kernel).
 int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st);
 // Solid forcing of a field (src/gc_solid_forcing_lsm.cpp): one launch per

@@ -12,9 +12,9 @@ Two ways to hold the slabs:
 * ``DistSlab``: one slab per rank of ``torch.distributed`` (one process per
   GPU, NCCL over NVLink); halos move by point-to-point send/recv, maxima,
   minima and sums by all-reduce.
-* ``Domain``: the native runner (r3d_domain_*): all slabs on the current
-  GPU, each on its own stream, the whole decomposed step -- stages, halo
-  copies, the global CFL step -- captured in one CUDA graph.
+* ``Domain``: the native runner (r3d_domain_*): slabs on one GPU or on
+  several, each on its own stream, the whole decomposed step -- stages, halo
+  peer copies, the global CFL step -- captured in one CUDA graph.
 
 A step is the step of ``r3d_ls_step`` taken stage by stage (three
 convection stages, f44 reinitialisation pseudo-steps of three stages, the
@@ -265,12 +265,12 @@ class DistSlab(_Stepper):
 
 
 class Domain:
-    """One grid split along z into `nslabs` slabs on the current GPU and
-    stepped as one by the native runner (r3d_domain_*): fields in the
-    reference's layout of the whole grid."""
+    """One grid split along z into `nslabs` slabs (on the current GPU, or
+    slab r on devices[r]) and stepped as one by the native runner
+    (r3d_domain_*): fields in the reference's layout of the whole grid."""
 
     def __init__(self, nx, ny, nz, xn=None, yn=None, zn=None, nslabs=2, f43=0.55, f44=3, f45=2.1, f49=1,
-                 n47=0.3, precision=FP64):
+                 n47=0.3, precision=FP64, devices=None):
         self._lib = load_library()
         xn = uniform_nodes(nx) if xn is None else xn
         yn = uniform_nodes(ny) if yn is None else yn
@@ -278,7 +278,10 @@ class Domain:
         self.nx, self.ny, self.nz = nx, ny, nz
         self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision, 0, 10)
         d = ctypes.c_void_p()
-        rc = self._lib.r3d_domain_create(ctypes.byref(self.desc), nslabs, ctypes.byref(d))
+        devs = None
+        if devices is not None:
+            devs = (ctypes.c_int * nslabs)(*devices)
+        rc = self._lib.r3d_domain_create(ctypes.byref(self.desc), nslabs, devs, ctypes.byref(d))
         if rc != R3D_OK:
             msg = self._lib.r3d_last_error(None)
             raise R3DError(rc, msg.decode() if msg else "")

@@ -112,7 +112,9 @@ def test_native_domain_equals_undivided_grid(dims, nslabs, precision):
     nx, ny, nz = dims
     xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=nz)
     whole, dts, vols = run_whole(dims, precision, 3, FLAGS)
-    with Domain(nx, ny, nz, xn, yn, zn, nslabs=nslabs, precision=precision, **FLAGS) as d:
+    # explicit device list: the peer-copy path of the multi-GPU layout, here
+    # with every slab on device 0
+    with Domain(nx, ny, nz, xn, yn, zn, nslabs=nslabs, precision=precision, devices=[0] * nslabs, **FLAGS) as d:
         for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
             d.upload(f, a)
         for s in range(3):
