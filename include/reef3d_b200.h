@@ -452,9 +452,10 @@ int r3d_batch_launch_count(const r3d_batch* b, long long* count);
  * r3d_domain_upload / download take the whole grid in the reference's
  * layout.  r3d_domain_run: nsteps steps with time step dt, or adaptive ones
  * when dt <= 0; synchronous.  Not with the picard correction (its sums are
- * global inside the step), the fluid update or inflow/outflow faces; the
- * slabs' own settings (velocity generator, X45 stencils, solid forcing)
- * apply, set through r3d_domain_slab.  One process per GPU runs the same
+ * global inside the step) or inflow/outflow faces; r3d_domain_set_fluid
+ * turns on the density/viscosity update on every slab (its ro, visc halos
+ * exchanged too); the slabs' own settings (velocity generator, X45
+ * stencils, solid forcing) apply, set through r3d_domain_slab.  One process per GPU runs the same
  * decomposition with reef3d_b200.slab.DistSlab (NCCL). */
 typedef struct r3d_domain r3d_domain;
 int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices, r3d_domain** out);
@@ -466,6 +467,10 @@ int r3d_domain_download(r3d_domain* d, int field, double* host);
 int r3d_domain_run(r3d_domain* d, int nsteps, double dt);
 int r3d_domain_last_volume(r3d_domain* d, double* volume1, double* volume2);
 int r3d_domain_get_dt(r3d_domain* d, double* dt);
+int r3d_domain_set_fluid(r3d_domain* d, double ro_water, double visc_water, double ro_air, double visc_air);
+/* The density/viscosity update alone on the current level set of every slab
+ * (fluid_update_fsf::start), with the ro, visc halos; volume sums added. */
+int r3d_domain_fluid_update(r3d_domain* d, double* volume1, double* volume2);
 
 /* Continuous-batching job server (no counterpart in the reference, which
  * runs one case per process).  A job is a level set on a uniform grid of the

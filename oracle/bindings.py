@@ -356,8 +356,21 @@ class AdapterOracle(RefOracle):
         lib.refad_weno_L.argtypes = [_D, _D]
         lib.refad_reinidisc_L.argtypes = [_D, _D]
         lib.refad_create.argtypes = [_I, _I]
+        self._precision = precision
         if lib.refad_create(precision, 1 if resident else 0) != 0:
             raise RuntimeError("refad_create failed")
+
+    def make_domain(self, nslabs):
+        """Also build the slab-domain free-surface adapter (levelset_RK3_domain)."""
+        self._lib.refad_create_domain.argtypes = [_I, _I]
+        if self._lib.refad_create_domain(self._precision, nslabs) != 0:
+            raise RuntimeError("refad_create_domain failed")
+
+    def gpu_step_domain(self, dt):
+        """freesurface::start of levelset_RK3_domain on a->phi."""
+        self._lib.refls_set_dt(dt)
+        self._lib.refad_step_domain()
+        return self.get_field(0)
 
     def gpu_step(self, dt):
         """freesurface::start of levelset_RK3_gpu on a->phi."""

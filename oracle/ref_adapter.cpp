@@ -20,6 +20,7 @@ field4* tmp();
 
 namespace {
 levelset_RK3_gpu* G_LS = nullptr;
+levelset_RK3_domain* G_LSD = nullptr;
 weno_hj_gpu* G_CONV = nullptr;
 reinidisc_gpu* G_DISC = nullptr;
 reini_RK3_gpu* G_REINI = nullptr;
@@ -44,7 +45,20 @@ int refad_create(int precision, int resident) {
     return 0;
 }
 
+// The slab-domain free-surface adapter with nslabs slabs on the current GPU.
+int refad_create_domain(int precision, int nslabs) {
+    G_LSD = new levelset_RK3_domain(refh::lex(), refh::fd(), refh::gc(), nslabs, nullptr, precision);
+    return 0;
+}
+// freesurface::start of levelset_RK3_domain on a->phi.
+int refad_step_domain() {
+    G_LSD->start(refh::fd(), refh::lex(), nullptr, nullptr, refh::gc(), refh::flow(), nullptr, nullptr,
+                 refh::fd()->phi);
+    return 0;
+}
 void refad_destroy() {
+    delete G_LSD;
+    G_LSD = nullptr;
     delete G_LS;
     delete G_CONV;
     delete G_DISC;

@@ -157,6 +157,8 @@ EXPORTS = {
     "r3d_domain_run": ([_H, ctypes.c_int, ctypes.c_double], ctypes.c_int),
     "r3d_domain_last_volume": ([_H, _D, _D], ctypes.c_int),
     "r3d_domain_get_dt": ([_H, _D], ctypes.c_int),
+    "r3d_domain_set_fluid": ([_H] + [ctypes.c_double] * 4, ctypes.c_int),
+    "r3d_domain_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_serve_create": ([ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_H)], ctypes.c_int),
     "r3d_serve_destroy": ([_H], ctypes.c_int),
     "r3d_serve_last_error": ([_H], ctypes.c_char_p),

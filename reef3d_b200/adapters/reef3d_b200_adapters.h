@@ -7,6 +7,7 @@
 // REEF3D's headers) and links against libreef3d_b200.so:
 //
 //   levelset_RK3_gpu : freesurface   replaces levelset_RK3 (src/levelset_RK3.h)
+//   levelset_RK3_domain : freesurface  the same over z slabs on several GPUs
 //   weno_hj_gpu      : convection    replaces weno_hj_df_nug (src/weno_hj_df_nug.h)
 //   reinidisc_gpu    : reinidisc     replaces reinidisc_f / reinidisc_fsf
 //   reini_RK3_gpu    : reini         replaces reini_RK3 (src/reini_RK3.h)
@@ -44,7 +45,7 @@ inline void check(r3d_handle* h, int rc) {
 // node coordinates DIVEMesh wrote (p->XN etc., node indices -5..n+5) and the
 // level-set flags of the control file.  precision: R3D_FP64 (the reference's
 // arithmetic) or R3D_FP32 (the FP32 form).
-inline r3d_handle* make_handle(lexer* p, int precision) {
+inline r3d_grid_desc grid_desc(const lexer* p, int precision) {
     r3d_grid_desc d{};
     d.nx = p->knox;
     d.ny = p->knoy;
@@ -60,9 +61,21 @@ inline r3d_handle* make_handle(lexer* p, int precision) {
     d.precision = precision;
     d.f46 = p->F46;
     d.f47 = p->F47;
+    return d;
+}
+
+inline r3d_handle* make_handle(lexer* p, int precision) {
+    const r3d_grid_desc d = grid_desc(p, precision);
     r3d_handle* h = nullptr;
     check(nullptr, r3d_create(&d, &h));
     return h;
+}
+
+inline void check_domain(r3d_domain* d, int rc) {
+    if (rc != R3D_OK) {
+        std::cout << "reef3d_b200: " << (d ? r3d_domain_last_error(d) : r3d_last_error(nullptr)) << std::endl;
+        std::exit(1);
+    }
 }
 
 // Interior cell (i,j,k) of a REEF3D field array (src/field_base.h:47).
@@ -283,6 +296,63 @@ private:
     bool first = true;
     r3d_adapter::IoflowState io;
     r3d_adapter::SolidForcingState sf;
+    std::vector<double> buf;
+};
+
+// freesurface over several slabs of the grid: the grid split along z into
+// nslabs slabs (r3d_domain_*; slab r on devices[r], or all on the current
+// GPU), stepped as one with the halo exchange between stages -- one
+// REEF3D process spreading its level set over the GPUs of a node.  The same
+// contract as levelset_RK3_gpu, for runs without picard correction,
+// inflow/outflow, X45 stencils or solid forcing (the run stops on them).
+class levelset_RK3_domain final : public freesurface {
+public:
+    levelset_RK3_domain(lexer* p, fdm*, ghostcell*, int nslabs, const int* devices = nullptr,
+                        int precision = R3D_FP64) {
+        if (p->F46 != 0 || p->X45 != 0 || p->X48 == 1 || p->B60 >= 1 || p->B90 >= 1) {
+            std::cout << "reef3d_b200: the slab domain runs without picard, ioflow, X45 or X48" << std::endl;
+            std::exit(1);
+        }
+        const r3d_grid_desc g = r3d_adapter::grid_desc(p, precision);
+        r3d_adapter::check_domain(nullptr, r3d_domain_create(&g, nslabs, devices, &d));
+        r3d_adapter::check_domain(d, r3d_domain_set_fluid(d, p->W1, p->W2, p->W3, p->W4));
+    }
+    ~levelset_RK3_domain() { r3d_domain_destroy(d); }
+
+    void start(fdm* a, lexer* p, convection*, solver*, ghostcell* pgc, ioflow*, reini*, particle_corr*,
+               field& ls) override {
+        using r3d_adapter::check_domain;
+        check_domain(d, r3d_domain_upload(d, R3D_PHI, ls.V));
+        check_domain(d, r3d_domain_upload(d, R3D_U, a->u.V));
+        check_domain(d, r3d_domain_upload(d, R3D_V, a->v.V));
+        check_domain(d, r3d_domain_upload(d, R3D_W, a->w.V));
+        check_domain(d, r3d_domain_run(d, 1, p->dt));
+        download(p, R3D_PHI, ls);
+        download(p, R3D_RO, a->ro);
+        download(p, R3D_VISC, a->visc);
+        check_domain(d, r3d_domain_last_volume(d, &p->volume1, &p->volume2));
+        pgc->start4(p, ls, r3d_adapter::gcval_phi(p));
+        pgc->start4(p, a->ro, 1);
+        pgc->start4(p, a->visc, 1);
+    }
+
+    void update(lexer* p, fdm* a, ghostcell* pgc, field&) override {
+        using r3d_adapter::check_domain;
+        check_domain(d, r3d_domain_upload(d, R3D_PHI, a->phi.V));
+        check_domain(d, r3d_domain_fluid_update(d, &p->volume1, &p->volume2));
+        download(p, R3D_RO, a->ro);
+        download(p, R3D_VISC, a->visc);
+        pgc->start4(p, a->ro, 1);
+        pgc->start4(p, a->visc, 1);
+    }
+
+private:
+    void download(const lexer* p, int id, field& f) {
+        buf.resize((size_t)p->imax * p->jmax * p->kmax);
+        r3d_adapter::check_domain(d, r3d_domain_download(d, id, buf.data()));
+        r3d_adapter::copy_owned(p, buf, f, true);
+    }
+    r3d_domain* d = nullptr;
     std::vector<double> buf;
 };
 

@@ -1480,12 +1480,20 @@ void domain_enqueue_step(r3d_domain* d, bool adaptive) {
             cudaMemcpyAsync(d->slab[s]->S.dt, d->dtbuf, sizeof(double), cudaMemcpyDefault, d->main);
         domain_fork(d);
     }
-    for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, d->f44 == 0 && s == 3);
+    const bool fluid = d->slab[0]->fluid;
+    for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, !fluid && d->f44 == 0 && s == 3);
     for (int q = 0; q < d->f44; ++q)
-        for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, q == d->f44 - 1 && s == 3);
+        for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, !fluid && q == d->f44 - 1 && s == 3);
     for (r3d_handle* h : d->slab) {
         cudaSetDevice(h->device);
-        h->launches += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
+        if (fluid)  // fluid_update_fsf: ro, visc and the volume sums (src/levelset_RK3.cpp:174)
+            h->launches += fluid_update(h, true);
+        else
+            h->launches += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
+    }
+    if (fluid) {
+        domain_exchange(d, R3D_RO);
+        domain_exchange(d, R3D_VISC);
     }
     domain_join(d);
 }
@@ -1635,8 +1643,8 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
     DeviceGuard dg(d->dev0);  // restores the caller's device
     const bool adaptive = !(dt > 0.0);
     for (r3d_handle* h : d->slab)
-        if (h->fluid || h->io)
-            return dfail(d, R3D_EINVAL, "the domain step has no fluid update and no inflow/outflow faces");
+        if (h->io || h->fluid != d->slab[0]->fluid)
+            return dfail(d, R3D_EINVAL, "domain slabs have no inflow/outflow faces and all or none the fluid update");
     if (!adaptive)
         for (r3d_handle* h : d->slab)
             if (int rc = r3d_set_dt(h, dt)) return dfail(d, rc, r3d_last_error(h));
@@ -1687,6 +1695,34 @@ int r3d_domain_last_volume(r3d_domain* d, double* volume1, double* volume2) {
         if (int rc = r3d_last_volume(h, &v1, &v2)) return dfail(d, rc, r3d_last_error(h));
         a += v1;
         b += v2;
+    }
+    if (volume1) *volume1 = a;
+    if (volume2) *volume2 = b;
+    return R3D_OK;
+}
+
+int r3d_domain_set_fluid(r3d_domain* d, double ro_water, double visc_water, double ro_air, double visc_air) {
+    if (!d) return R3D_EINVAL;
+    for (r3d_handle* h : d->slab)
+        if (int rc = r3d_set_fluid(h, ro_water, visc_water, ro_air, visc_air)) return dfail(d, rc, r3d_last_error(h));
+    return R3D_OK;
+}
+
+int r3d_domain_fluid_update(r3d_domain* d, double* volume1, double* volume2) {
+    if (!d) return R3D_EINVAL;
+    double a = 0.0, b = 0.0;
+    for (r3d_handle* h : d->slab) {
+        double v1 = 0.0, v2 = 0.0;
+        if (int rc = r3d_fluid_update(h, &v1, &v2)) return dfail(d, rc, r3d_last_error(h));
+        a += v1;
+        b += v2;
+    }
+    {
+        DeviceGuard dg(d->dev0);
+        domain_exchange(d, R3D_RO);
+        domain_exchange(d, R3D_VISC);
+        domain_join(d);
+        if (cudaStreamSynchronize(d->main) != cudaSuccess) return dfail(d, R3D_EDEVICE, "domain halo copies");
     }
     if (volume1) *volume1 = a;
     if (volume2) *volume2 = b;

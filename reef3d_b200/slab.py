@@ -310,6 +310,10 @@ class Domain:
         self._check(self._lib.r3d_domain_last_volume(self.d, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def set_fluid(self, ro_water=998.2, visc_water=1.004e-6, ro_air=1.205, visc_air=1.41e-5):
+        """Density/viscosity update on every slab (r3d_domain_set_fluid)."""
+        self._check(self._lib.r3d_domain_set_fluid(self.d, ro_water, visc_water, ro_air, visc_air))
+
     def dt(self):
         v = ctypes.c_double()
         self._check(self._lib.r3d_domain_get_dt(self.d, ctypes.byref(v)))
