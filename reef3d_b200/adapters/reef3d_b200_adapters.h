@@ -303,14 +303,15 @@ private:
 // nslabs slabs (r3d_domain_*; slab r on devices[r], or all on the current
 // GPU), stepped as one with the halo exchange between stages -- one
 // REEF3D process spreading its level set over the GPUs of a node.  The same
-// contract as levelset_RK3_gpu, for runs without picard correction,
-// inflow/outflow, X45 stencils or solid forcing (the run stops on them).
+// contract as levelset_RK3_gpu (the picard correction F46 selects included,
+// over the whole grid), for runs without inflow/outflow, X45 stencils or
+// solid forcing (the run stops on them).
 class levelset_RK3_domain final : public freesurface {
 public:
     levelset_RK3_domain(lexer* p, fdm*, ghostcell*, int nslabs, const int* devices = nullptr,
                         int precision = R3D_FP64) {
-        if (p->F46 != 0 || p->X45 != 0 || p->X48 == 1 || p->B60 >= 1 || p->B90 >= 1) {
-            std::cout << "reef3d_b200: the slab domain runs without picard, ioflow, X45 or X48" << std::endl;
+        if (p->X45 != 0 || p->X48 == 1 || p->B60 >= 1 || p->B90 >= 1) {
+            std::cout << "reef3d_b200: the slab domain runs without ioflow, X45 or X48" << std::endl;
             std::exit(1);
         }
         const r3d_grid_desc g = r3d_adapter::grid_desc(p, precision);
@@ -331,7 +332,7 @@ public:
         download(p, R3D_RO, a->ro);
         download(p, R3D_VISC, a->visc);
         check_domain(d, r3d_domain_last_volume(d, &p->volume1, &p->volume2));
-        pgc->start4(p, ls, r3d_adapter::gcval_phi(p));
+        if (p->F46 == 0) pgc->start4(p, ls, r3d_adapter::gcval_phi(p));  // picard moves the interior only
         pgc->start4(p, a->ro, 1);
         pgc->start4(p, a->visc, 1);
     }

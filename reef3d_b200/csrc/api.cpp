@@ -1388,6 +1388,7 @@ struct r3d_domain {
     std::vector<int> k0, k1;
     int nx = 0, ny = 0, nz = 0;
     int f44 = 0;
+    int f46 = 0, f47 = 0;  // picard correction of the whole grid (the slabs run with f46 = 0)
     double n47 = 0.0;
     double dxmin = 0.0;
     cudaStream_t main = nullptr;
@@ -1396,6 +1397,7 @@ struct r3d_domain {
     int dev0 = 0;                          // device of slab 0: main stream, gather buffers
     unsigned long long* gather = nullptr;  // the slabs' CFL maxima, 3 per slab (on dev0)
     double* dtbuf = nullptr;               // the grid's time step (on dev0)
+    double* pgather = nullptr;             // the slabs' picard slots, 5 per slab (on dev0)
     cudaGraphExec_t graph = nullptr;
     long long graph_adaptive = -1;  // configuration key of the captured step
     bool ran = false;
@@ -1449,6 +1451,46 @@ void domain_exchange(r3d_domain* d, int field) {
     domain_fork(d);
 }
 
+// One picard volume of the whole grid: every slab's row pass and ordered
+// reduce (mode 0: volcalc; 2: an iteration's vol2 share, after the shift by
+// the current w when `shift`), then on slab 0's device the sum over the
+// slabs in slab order (the role of ghostcell::globalsum,
+// src/picard_f.cpp:53, :75) and the grid's w, written back into every
+// slab's picard slots.
+void domain_picard_sum(r3d_domain* d, bool shift, int mode) {
+    const bool lsm = d->f46 == 3;
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
+        h->launches += launch_picard_local(h->L, h->field[R3D_PHI], fp32(h), picard_epsi(h), picard_cellvol(h), shift,
+                                           true, mode, lsm, h->S, h->stream);
+    }
+    domain_join(d);
+    const int n = (int)d->slab.size();
+    for (int s = 0; s < n; ++s)
+        cudaMemcpyAsync(d->pgather + 5 * s, d->slab[s]->S.pic, 5 * sizeof(double), cudaMemcpyDefault, d->main);
+    launch_domain_picard(d->pgather, n, mode == 0 ? 0 : 1, lsm, d->main);
+    for (int s = 0; s < n; ++s)
+        cudaMemcpyAsync(d->slab[s]->S.pic, d->pgather + 5 * s, 5 * sizeof(double), cudaMemcpyDefault, d->main);
+    domain_fork(d);
+}
+
+// picard_f / picard_lsm correct_ls over the slabs (src/picard_f.cpp:79-113,
+// src/picard_lsm.cpp:88-115): F47 iterations of grid volume, w and shift,
+// the last shift alone.  The phi halo planes then follow the shifted
+// interiors, so that the next stage reads what the undivided grid reads
+// (the reference's decomposed run calls no ghostcell::start4 there and
+// keeps the neighbours' pre-shift values in its halos).
+void domain_picard_correct(r3d_domain* d) {
+    if (d->f47 <= 0) return;
+    for (int n = 0; n < d->f47; ++n) domain_picard_sum(d, n > 0, 2);
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
+        h->launches += launch_picard_local(h->L, h->field[R3D_PHI], fp32(h), picard_epsi(h), picard_cellvol(h), true,
+                                           false, 0, d->f46 == 3, h->S, h->stream);
+    }
+    domain_exchange(d, R3D_PHI);
+}
+
 void domain_stage(r3d_domain* d, bool reini, int s, bool vol) {
     for (r3d_handle* h : d->slab) {
         cudaSetDevice(h->device);
@@ -1457,8 +1499,10 @@ void domain_stage(r3d_domain* d, bool reini, int s, bool vol) {
     domain_exchange(d, s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI);
 }
 
-// One step of every slab (levelset_RK3::start without picard, fluid update
-// or inflow/outflow), enqueued from the main stream back to it.
+// One step of every slab (levelset_RK3::start without inflow/outflow, with
+// the picard correction F46 selects: 2 or 3 around the step, 1 around the
+// reinitialisation, src/reini_RK3.cpp:92, :140), enqueued from the main
+// stream back to it.
 void domain_enqueue_step(r3d_domain* d, bool adaptive) {
     domain_fork(d);
     for (r3d_handle* h : d->slab) {
@@ -1481,13 +1525,20 @@ void domain_enqueue_step(r3d_domain* d, bool adaptive) {
         domain_fork(d);
     }
     const bool fluid = d->slab[0]->fluid;
-    for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, !fluid && d->f44 == 0 && s == 3);
+    const bool fused = !fluid && d->f46 == 0;  // volume partials from the last stage
+    if (d->f46 >= 2) domain_picard_sum(d, false, 0);
+    for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, fused && d->f44 == 0 && s == 3);
+    if (d->f46 == 1) domain_picard_sum(d, false, 0);
     for (int q = 0; q < d->f44; ++q)
-        for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, !fluid && q == d->f44 - 1 && s == 3);
+        for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, fused && q == d->f44 - 1 && s == 3);
+    if (d->f46 != 0) domain_picard_correct(d);
     for (r3d_handle* h : d->slab) {
         cudaSetDevice(h->device);
         if (fluid)  // fluid_update_fsf: ro, visc and the volume sums (src/levelset_RK3.cpp:174)
             h->launches += fluid_update(h, true);
+        else if (!fused)
+            h->launches += launch_volume_direct_clock(h->L, h->field[R3D_PHI], fp32(h), h->g64.dxn[0], h->g64.dxn[1],
+                                                      h->g64.dxn[2], h->M.psi, h->period, h->S, h->stream);
         else
             h->launches += launch_volume_reduce(h->L, h->S, volume_block_count(h), h->period, h->stream);
     }
@@ -1507,7 +1558,6 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices,
     if (!out) return fail(nullptr, R3D_EINVAL, "null output");
     *out = nullptr;
     if (int rc = check_desc(desc, why)) return fail(nullptr, rc, why);
-    if (desc->f46 != 0) return fail(nullptr, R3D_EINVAL, "slab domains run without the picard correction");
     if (nslabs < 1 || desc->nz < 3 * nslabs) return fail(nullptr, R3D_EINVAL, "every slab needs >= 3 z cells");
     r3d_domain* d = new (std::nothrow) r3d_domain();
     if (!d) return fail(nullptr, R3D_ENOMEM, "host allocation failed");
@@ -1515,6 +1565,8 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices,
     d->ny = desc->ny;
     d->nz = desc->nz;
     d->f44 = desc->f44;
+    d->f46 = desc->f46;
+    d->f47 = desc->f47;
     d->n47 = desc->n47;
     double out4[4];
     if (int rc = r3d_grid_spacing(desc, out4)) {
@@ -1532,6 +1584,7 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices,
         const int n = base + (r < extra ? 1 : 0);
         r3d_grid_desc sd = *desc;
         sd.nz = n;
+        sd.f46 = 0;  // the grid's picard runs over all slabs at once
         sd.zn = desc->zn + k;  // node indices -5..n+5 of the slab
         r3d_handle* h = nullptr;
         if (cudaSetDevice(devices ? devices[r] : cur) != cudaSuccess) {
@@ -1570,7 +1623,8 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices,
                     cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) == cudaSuccess &&
                     cudaEventCreateWithFlags(&d->xdone, cudaEventDisableTiming) == cudaSuccess &&
                     cudaMalloc(&d->gather, 3 * d->slab.size() * sizeof(unsigned long long)) == cudaSuccess &&
-                    cudaMalloc(&d->dtbuf, sizeof(double)) == cudaSuccess;
+                    cudaMalloc(&d->dtbuf, sizeof(double)) == cudaSuccess &&
+                    cudaMalloc(&d->pgather, 5 * d->slab.size() * sizeof(double)) == cudaSuccess;
     cudaSetDevice(cur);
     if (!ok) return bail(R3D_EDEVICE, "domain stream, events and buffers");
     *out = d;
@@ -1588,6 +1642,7 @@ int r3d_domain_destroy(r3d_domain* d) {
     if (d->xdone) cudaEventDestroy(d->xdone);
     if (d->gather) cudaFree(d->gather);
     if (d->dtbuf) cudaFree(d->dtbuf);
+    if (d->pgather) cudaFree(d->pgather);
     if (d->main) cudaStreamDestroy(d->main);
     delete d;
     return R3D_OK;

@@ -428,11 +428,34 @@ __global__ void picard_reduce_kernel(const double* __restrict__ partial, long lo
                 pic[3] += 1.0;
                 if (pic[3] == 1.0) pic[2] = sa[0];
             }
-        } else {
+        } else if (mode == 1) {
             const double r1 = pow((0.75 / PI_REF) * (lsm ? pic[2] : pic[0]), 1.0 / 3.0);
             const double r2 = pow((0.75 / PI_REF) * sa[0], 1.0 / 3.0);
             pic[1] = r1 - r2;
+        } else {
+            pic[4] = sa[0];  // mode 2: this subdomain's share only (the grid's sum follows)
         }
+    }
+}
+
+// Picard over the slabs of a decomposed grid (the globalsum of
+// src/picard_f.cpp:53 and :75): p holds each slab's pic[0..4], gathered.
+// mode 0 (after volcalc): every slab's step-start volume becomes the grid's,
+// and picard_lsm's first-step target too; mode 1 (after an iteration's
+// volume): w = r(target) - r(grid's vol2) for every slab.
+__global__ void domain_picard_kernel(double* p, int n, int mode, int lsm) {
+    const double PI_REF = 3.14159265359;
+    double v = 0.0;
+    for (int s = 0; s < n; ++s) v += p[5 * s + (mode == 0 ? 0 : 4)];
+    if (mode == 0) {
+        for (int s = 0; s < n; ++s) {
+            p[5 * s] = v;
+            if (lsm && p[5 * s + 3] == 1.0) p[5 * s + 2] = v;
+        }
+    } else {
+        const double r1 = pow((0.75 / PI_REF) * (lsm ? p[2] : p[0]), 1.0 / 3.0);
+        const double r2 = pow((0.75 / PI_REF) * v, 1.0 / 3.0);
+        for (int s = 0; s < n; ++s) p[5 * s + 1] = r1 - r2;
     }
 }
 
@@ -750,6 +773,21 @@ __global__ void domain_dt_kernel(const unsigned long long* vm, int n, const doub
 int launch_domain_dt(const unsigned long long* vm, int n, const double* vscale, double dxmin, double n47, double* dt,
                      cudaStream_t st) {
     domain_dt_kernel<<<1, 1, 0, st>>>(vm, n, vscale, dxmin, n47, dt);
+    return 1;
+}
+
+int launch_picard_local(const Layout& L, void* phi, bool fp32, double epsi, double cellvol, bool shift, bool sum,
+                        int mode, bool lsm, const Scratch& s, cudaStream_t st) {
+    if (shift && sum) picard_pass<true, true>(L, phi, fp32, epsi, cellvol, s, st);
+    else if (shift) picard_pass<true, false>(L, phi, fp32, epsi, cellvol, s, st);
+    else picard_pass<false, true>(L, phi, fp32, epsi, cellvol, s, st);
+    if (!sum) return 1;
+    picard_reduce_kernel<<<1, 1024, 0, st>>>(s.partial, (long long)L.ny * L.nz, s.pic, mode, lsm ? 1 : 0);
+    return 2;
+}
+
+int launch_domain_picard(double* gathered, int n, int mode, bool lsm, cudaStream_t st) {
+    domain_picard_kernel<<<1, 1, 0, st>>>(gathered, n, mode, lsm ? 1 : 0);
     return 1;
 }
 

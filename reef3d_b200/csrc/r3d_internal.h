@@ -202,6 +202,12 @@ int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, c
 // when ro != nullptr (3 n floats).
 int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const void* visc, bool fp32, float* out,
                      long long npoints, cudaStream_t st);
+// One picard pass of one subdomain (row pass with the shift and/or the
+// volume; with sum, the reduce in `mode`: 0 volcalc, 2 this slab's vol2 into
+// s.pic[4]); and the grid-wide step over the gathered pic[0..4] of n slabs.
+int launch_picard_local(const Layout& L, void* phi, bool fp32, double epsi, double cellvol, bool shift, bool sum,
+                        int mode, bool lsm, const Scratch& s, cudaStream_t st);
+int launch_domain_picard(double* gathered, int n, int mode, bool lsm, cudaStream_t st);
 // dt of a decomposed grid from the slabs' maxima gathered into vm[3 n], at
 // the grid's smallest cell.
 int launch_domain_dt(const unsigned long long* vm, int n, const double* vscale, double dxmin, double n47, double* dt,

@@ -19,9 +19,11 @@ Two ways to hold the slabs:
 A step is the step of ``r3d_ls_step`` taken stage by stage (three
 convection stages, f44 reinitialisation pseudo-steps of three stages, the
 volume sums or the fluid update), each stage followed by the exchange of
-the field it wrote.  Slab instances run without the picard correction and
-without inflow/outflow faces, whose sums the reference takes globally in the
-middle of a step.
+the field it wrote.  Host-driven slabs (LocalSlabs, DistSlab) run without
+the picard correction and without inflow/outflow faces, whose sums the
+reference takes globally in the middle of a step; the native Domain runs the
+picard correction over the whole grid (per-slab volume sums added on the
+device between the slabs' passes).
 """
 import numpy as np
 
@@ -267,16 +269,17 @@ class DistSlab(_Stepper):
 class Domain:
     """One grid split along z into `nslabs` slabs (on the current GPU, or
     slab r on devices[r]) and stepped as one by the native runner
-    (r3d_domain_*): fields in the reference's layout of the whole grid."""
+    (r3d_domain_*): fields in the reference's layout of the whole grid.
+    f46/f47: the picard correction of the whole grid (as LevelSet's)."""
 
     def __init__(self, nx, ny, nz, xn=None, yn=None, zn=None, nslabs=2, f43=0.55, f44=3, f45=2.1, f49=1,
-                 n47=0.3, precision=FP64, devices=None):
+                 n47=0.3, precision=FP64, devices=None, f46=0, f47=10):
         self._lib = load_library()
         xn = uniform_nodes(nx) if xn is None else xn
         yn = uniform_nodes(ny) if yn is None else yn
         zn = uniform_nodes(nz) if zn is None else zn
         self.nx, self.ny, self.nz = nx, ny, nz
-        self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision, 0, 10)
+        self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision, f46, f47)
         d = ctypes.c_void_p()
         devs = None
         if devices is not None:

@@ -125,3 +125,39 @@ def test_native_domain_equals_undivided_grid(dims, nslabs, precision):
         got = d.download(r3d.PHI)
     m = visible_mask(*dims)
     assert np.array_equal(got[m], whole[r3d.PHI][m])
+
+
+@pytest.mark.parametrize("f46,nslabs,precision", [(1, 3, r3d.FP64), (2, 3, r3d.FP64), (3, 4, r3d.FP64),
+                                                  (2, 1, r3d.FP64), (3, 3, r3d.FP32)])
+def test_native_domain_picard_equals_undivided_grid(f46, nslabs, precision):
+    """The picard correction over the slabs (picard_f with F46 = 1 around the
+    reinitialisation and 2 around the step, picard_lsm with 3): each
+    iteration's volume summed per slab, then over the slabs, w taken from the
+    grid's volume and the phi halos refreshed after the shift.  The step then
+    equals the undivided grid's up to the volume sums' order (phi within
+    1e-12 of its largest value in FP64, and bit-identical with one slab; a
+    few single-precision roundings of the shifted values in FP32)."""
+    from reef3d_b200.slab import Domain
+    dims = (40, 33, 27)
+    nx, ny, nz = dims
+    flags = dict(FLAGS, f46=f46, f47=3)
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=nz)
+    whole, dts, vols = run_whole(dims, precision, 3, flags)
+    with Domain(nx, ny, nz, xn, yn, zn, nslabs=nslabs, precision=precision, devices=[0] * nslabs, **flags) as d:
+        for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+            d.upload(f, a)
+        for s in range(3):
+            d.run(1)
+            assert d.dt() == dts[s]
+            a, b = d.last_volume()
+            assert abs(a - vols[s][0]) <= RTOL * abs(vols[s][0]) and abs(b - vols[s][1]) <= RTOL * abs(vols[s][1])
+        got = d.download(r3d.PHI)
+    m = visible_mask(*dims)
+    ref = whole[r3d.PHI][m]
+    if nslabs == 1:
+        assert np.array_equal(got[m], ref)
+    tol = (1e-12 if precision == r3d.FP64 else 1e-5) * np.abs(ref).max()
+    assert np.abs(got[m] - ref).max() <= tol
+    # the correction moved the level set: the run without it ends elsewhere
+    plain, _, _ = run_whole(dims, precision, 3, FLAGS)
+    assert np.abs(plain[r3d.PHI][m] - ref).max() > 10 * tol
