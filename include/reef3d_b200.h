@@ -451,8 +451,15 @@ int r3d_batch_launch_count(const r3d_batch* b, long long* count);
  * undivided grid's; the volume sums are taken per slab and added.
  * r3d_domain_upload / download take the whole grid in the reference's
  * layout.  r3d_domain_run: nsteps steps with time step dt, or adaptive ones
- * when dt <= 0; synchronous.  Not with the picard correction (its sums are
- * global inside the step) or inflow/outflow faces; r3d_domain_set_fluid
+ * when dt <= 0; synchronous.  The picard correction the descriptor selects
+ * (f46, f47) runs over the whole grid: each volume summed per slab, the
+ * slabs' shares added on slab 0's device (pgc->globalsum), w written back to
+ * every slab, the phi halos exchanged after the last shift.
+ * r3d_domain_set_ioflow opens inflow/outflow faces on every slab
+ * (r3d_set_ioflow's faces; nullptr closes them): the water levels come from
+ * the crossing heights of all slabs gathered in the whole grid's order, so
+ * they equal the undivided grid's; the step count is slab 0's
+ * (r3d_set_step_count through r3d_domain_slab).  r3d_domain_set_fluid
  * turns on the density/viscosity update on every slab (its ro, visc halos
  * exchanged too); the slabs' own settings (velocity generator, X45
  * stencils, solid forcing) apply, set through r3d_domain_slab.  One process per GPU runs the same
@@ -467,6 +474,7 @@ int r3d_domain_download(r3d_domain* d, int field, double* host);
 int r3d_domain_run(r3d_domain* d, int nsteps, double dt);
 int r3d_domain_last_volume(r3d_domain* d, double* volume1, double* volume2);
 int r3d_domain_get_dt(r3d_domain* d, double* dt);
+int r3d_domain_set_ioflow(r3d_domain* d, const r3d_ioflow_desc* io);
 int r3d_domain_set_fluid(r3d_domain* d, double ro_water, double visc_water, double ro_air, double visc_air);
 /* The density/viscosity update alone on the current level set of every slab
  * (fluid_update_fsf::start), with the ro, visc halos; volume sums added. */

@@ -158,6 +158,7 @@ EXPORTS = {
     "r3d_domain_last_volume": ([_H, _D, _D], ctypes.c_int),
     "r3d_domain_get_dt": ([_H, _D], ctypes.c_int),
     "r3d_domain_set_fluid": ([_H] + [ctypes.c_double] * 4, ctypes.c_int),
+    "r3d_domain_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
     "r3d_domain_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_serve_create": ([ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_H)], ctypes.c_int),
     "r3d_serve_destroy": ([_H], ctypes.c_int),

@@ -943,7 +943,7 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
     if (io->f50 < 1 || io->f50 > 4) return fail(h, R3D_EINVAL, "f50 must be 1..4");
     if (io->b77 != 1 && io->b77 != 2) return fail(h, R3D_EINVAL, "b77 must be 1 or 2");
     if (io->f64 < 0 || io->f64 > (1 << 24)) return fail(h, R3D_EINVAL, "f64 must be 0..2^24");
-    if (h->L.io & (kHaloZLo | kHaloZHi))
+    if ((h->L.io & (kHaloZLo | kHaloZHi)) && !h->domain_slab)
         return fail(h, R3D_EINVAL, "subdomain instances have no inflow/outflow faces");
     drop_step_graph(h);
     // state, ZP (index k + 5), ramp table of the outflow level (F64 > 0)
@@ -1398,6 +1398,9 @@ struct r3d_domain {
     unsigned long long* gather = nullptr;  // the slabs' CFL maxima, 3 per slab (on dev0)
     double* dtbuf = nullptr;               // the grid's time step (on dev0)
     double* pgather = nullptr;             // the slabs' picard slots, 5 per slab (on dev0)
+    bool io = false;                       // inflow/outflow faces (r3d_domain_set_ioflow)
+    std::vector<double*> iol;              // each slab's crossing heights, 2 ny n (on its device)
+    double* iog = nullptr;                 // the grid's heights, 2 ny nz, and state (on dev0)
     cudaGraphExec_t graph = nullptr;
     long long graph_adaptive = -1;  // configuration key of the captured step
     bool ran = false;
@@ -1491,6 +1494,41 @@ void domain_picard_correct(r3d_domain* d) {
     domain_exchange(d, R3D_PHI);
 }
 
+// fsfinflow + fsfrkin/fsfrkout of a decomposed grid (src/ioflow_waterlevel.cpp
+// :29-177): the slabs' crossing heights gathered on slab 0's device into the
+// whole grid's order (a strided copy per slab and face), one fold into the
+// grid's levels and step count (from slab 0's state), the state copied back
+// to every slab, then each slab's ghosts.
+void domain_io_step(r3d_domain* d) {
+    const int n = (int)d->slab.size();
+    const size_t plane = (size_t)d->ny * d->nz;
+    double* state = d->iog + 2 * plane;
+    for (int s = 0; s < n; ++s) {
+        r3d_handle* h = d->slab[s];
+        cudaSetDevice(h->device);
+        h->launches += launch_io_heights(h->L, h->field[R3D_PHI], fp32(h), h->iop, d->iol[s], h->stream);
+    }
+    domain_join(d);
+    cudaMemcpyAsync(state, d->slab[0]->iop.state, kIoStateLen * sizeof(double), cudaMemcpyDefault, d->main);
+    for (int s = 0; s < n; ++s) {
+        const size_t ns = (size_t)(d->k1[s] - d->k0[s]);
+        for (int f = 0; f < 2; ++f)
+            cudaMemcpy2DAsync(d->iog + f * plane + d->k0[s], d->nz * sizeof(double), d->iol[s] + f * d->ny * ns,
+                              ns * sizeof(double), ns * sizeof(double), d->ny, cudaMemcpyDefault, d->main);
+    }
+    IoParams p = d->slab[0]->iop;
+    p.state = state;
+    launch_io_fold(d->iog, (int)plane, p, d->main);
+    for (int s = 0; s < n; ++s)
+        cudaMemcpyAsync(d->slab[s]->iop.state, state, kIoStateLen * sizeof(double), cudaMemcpyDefault, d->main);
+    domain_fork(d);
+    for (r3d_handle* h : d->slab) {
+        cudaSetDevice(h->device);
+        h->launches += launch_io_ghosts(h->L, h->field[R3D_PHI], h->field[R3D_WORK1], h->field[R3D_WORK2], fp32(h),
+                                        h->iop, h->stream);
+    }
+}
+
 void domain_stage(r3d_domain* d, bool reini, int s, bool vol) {
     for (r3d_handle* h : d->slab) {
         cudaSetDevice(h->device);
@@ -1499,9 +1537,9 @@ void domain_stage(r3d_domain* d, bool reini, int s, bool vol) {
     domain_exchange(d, s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI);
 }
 
-// One step of every slab (levelset_RK3::start without inflow/outflow, with
-// the picard correction F46 selects: 2 or 3 around the step, 1 around the
-// reinitialisation, src/reini_RK3.cpp:92, :140), enqueued from the main
+// One step of every slab (levelset_RK3::start with the inflow/outflow hooks
+// and the picard correction F46 selects: 2 or 3 around the step, 1 around
+// the reinitialisation, src/reini_RK3.cpp:92, :140), enqueued from the main
 // stream back to it.
 void domain_enqueue_step(r3d_domain* d, bool adaptive) {
     domain_fork(d);
@@ -1526,11 +1564,21 @@ void domain_enqueue_step(r3d_domain* d, bool adaptive) {
     }
     const bool fluid = d->slab[0]->fluid;
     const bool fused = !fluid && d->f46 == 0;  // volume partials from the last stage
+    if (d->io) domain_io_step(d);
     if (d->f46 >= 2) domain_picard_sum(d, false, 0);
     for (int s = 1; s <= 3; ++s) domain_stage(d, false, s, fused && d->f44 == 0 && s == 3);
     if (d->f46 == 1) domain_picard_sum(d, false, 0);
+    for (r3d_handle* h : d->slab) {  // fsfrkin/fsfrkout at the start of reini_RK3::start
+        cudaSetDevice(h->device);
+        h->launches += io_hooks(h, false);
+    }
     for (int q = 0; q < d->f44; ++q)
         for (int s = 1; s <= 3; ++s) domain_stage(d, true, s, fused && q == d->f44 - 1 && s == 3);
+    if (d->f46 == 3 && d->io)
+        for (r3d_handle* h : d->slab) {  // picard_lsm's netvol += (Qi - Qo) dt
+            cudaSetDevice(h->device);
+            h->launches += launch_netvol(h->S, h->iod.qi, h->iod.qo, h->stream);
+        }
     if (d->f46 != 0) domain_picard_correct(d);
     for (r3d_handle* h : d->slab) {
         cudaSetDevice(h->device);
@@ -1592,6 +1640,7 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices,
             break;
         }
         rc = r3d_create(&sd, &h);
+        if (h) h->domain_slab = true;
         if (!rc) rc = r3d_set_halo(h, k > 0 ? 1 : 0, k + n < desc->nz ? 1 : 0);
         if (!rc) rc = r3d_set_grid_spacing(h, out4[0], out4[1], out4[2]);
         if (h) {
@@ -1643,6 +1692,9 @@ int r3d_domain_destroy(r3d_domain* d) {
     if (d->gather) cudaFree(d->gather);
     if (d->dtbuf) cudaFree(d->dtbuf);
     if (d->pgather) cudaFree(d->pgather);
+    for (size_t s = 0; s < d->iol.size(); ++s)
+        if (d->iol[s]) cudaFree(d->iol[s]);
+    if (d->iog) cudaFree(d->iog);
     if (d->main) cudaStreamDestroy(d->main);
     delete d;
     return R3D_OK;
@@ -1698,15 +1750,16 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
     DeviceGuard dg(d->dev0);  // restores the caller's device
     const bool adaptive = !(dt > 0.0);
     for (r3d_handle* h : d->slab)
-        if (h->io || h->fluid != d->slab[0]->fluid)
-            return dfail(d, R3D_EINVAL, "domain slabs have no inflow/outflow faces and all or none the fluid update");
+        if (h->io != d->io || h->fluid != d->slab[0]->fluid)
+            return dfail(d, R3D_EINVAL, "inflow/outflow faces only through r3d_domain_set_ioflow; fluid update on all "
+                                        "slabs or none");
     if (!adaptive)
         for (r3d_handle* h : d->slab)
             if (int rc = r3d_set_dt(h, dt)) return dfail(d, rc, r3d_last_error(h));
     for (r3d_handle* h : d->slab) cudaStreamSynchronize(h->stream);
     // the captured step depends on the slabs' configuration (velocity
     // generator, forcing, precision path): recapture when it changed
-    long long key = adaptive ? 1 : 0;
+    long long key = (adaptive ? 1 : 0) + (d->io ? 2 : 0);
     for (r3d_handle* h : d->slab)
         key = key * 64 + (h->airy ? 1 : 0) + (h->sf_ops ? 2 : 0) + (h->g64.x45 ? 4 : 0) + (tiled(h) ? 8 : 0) +
               (h->band64 ? 16 : 0) + (h->fluid ? 32 : 0);
@@ -1753,6 +1806,44 @@ int r3d_domain_last_volume(r3d_domain* d, double* volume1, double* volume2) {
     }
     if (volume1) *volume1 = a;
     if (volume2) *volume2 = b;
+    return R3D_OK;
+}
+
+int r3d_domain_set_ioflow(r3d_domain* d, const r3d_ioflow_desc* io) {
+    if (!d) return R3D_EINVAL;
+    if (d->graph) {  // the captured step holds the faces' parameters
+        cudaGraphExecDestroy(d->graph);
+        d->graph = nullptr;
+    }
+    for (r3d_handle* h : d->slab)
+        if (int rc = r3d_set_ioflow(h, io)) {
+            for (r3d_handle* g : d->slab) r3d_set_ioflow(g, nullptr);
+            d->io = false;
+            return dfail(d, rc, r3d_last_error(h));
+        }
+    d->io = io != nullptr;
+    if (!d->io || d->iog) return R3D_OK;
+    // crossing heights: per slab on its device, the grid's on slab 0's
+    DeviceGuard dg(d->dev0);
+    d->iol.assign(d->slab.size(), nullptr);
+    bool ok = true;
+    for (size_t s = 0; s < d->slab.size() && ok; ++s) {
+        cudaSetDevice(d->slab[s]->device);
+        ok = cudaMalloc(&d->iol[s], 2 * (size_t)d->ny * (d->k1[s] - d->k0[s]) * sizeof(double)) == cudaSuccess;
+    }
+    cudaSetDevice(d->dev0);
+    ok = ok && cudaMalloc(&d->iog, (2 * (size_t)d->ny * d->nz + kIoStateLen) * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        for (size_t s = 0; s < d->iol.size(); ++s)
+            if (d->iol[s]) cudaFree(d->iol[s]);
+        d->iol.clear();
+        if (d->iog) cudaFree(d->iog);
+        d->iog = nullptr;
+        for (r3d_handle* g : d->slab) r3d_set_ioflow(g, nullptr);
+        d->io = false;
+        return dfail(d, R3D_ENOMEM, "inflow/outflow buffers");
+    }
     return R3D_OK;
 }
 

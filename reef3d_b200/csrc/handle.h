@@ -28,6 +28,7 @@ struct r3d_handle {
     double* coord = nullptr;  // x centres, x faces, z centres, z faces
     // inflow / outflow faces with ioflow_f's hooks (r3d_set_ioflow)
     bool io = false;
+    bool domain_slab = false;  // a slab of an r3d_domain (its io levels are the grid's)
     r3d_ioflow_desc iod{};
     double* io_buf = nullptr;  // hook state, ZP, ramp table (r3d::IoParams)
     size_t io_buf_len = 0;

@@ -485,11 +485,46 @@ constexpr int kIoThreads = 1024;
 // so the FP64 sum rounds exactly as the reference's loop does.  zval is
 // valid in thread 0, count in every thread.
 template <typename T>
-__device__ void crossing_sum(const Layout& L, const T* __restrict__ phi, int i, const IoParams& p, double& zval,
-                             int& count) {
+__device__ __forceinline__ bool crossing_height(const Layout& L, const T* __restrict__ phi, int i, const IoParams& p,
+                                                int j, int k, double& h) {
+    const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+    const double a = static_cast<double>(phi[c]), b = static_cast<double>(phi[c + L.sz]);
+    if (!(a >= 0.0 && b < 0.0)) return false;
+    h = -(a * p.dzp[k + 5]) / (b - a) + p.zp[k + 5];
+    return true;
+}
+
+// The face's cells of one grid (the crossing heights formed on the spot).
+template <typename T>
+struct CellHeights {
+    Layout L;
+    const T* phi;
+    IoParams p;
+    int i;
+    __device__ int size() const { return L.ny * L.nz; }
+    __device__ bool at(int e, double& h) const {
+        const int j = e / L.nz, k = e - j * L.nz;
+        return crossing_height(L, phi, i, p, j, k, h);
+    }
+};
+
+// Heights gathered from the slabs of a decomposed grid, in the order
+// j * nz + k of the whole grid (NaN: no crossing in that cell).
+struct GatheredHeights {
+    const double* h;
+    int n;
+    __device__ int size() const { return n; }
+    __device__ bool at(int e, double& v) const {
+        v = h[e];
+        return !isnan(v);
+    }
+};
+
+template <typename Src>
+__device__ void crossing_sum(const Src& src, double& zval, int& count) {
     __shared__ double vals[kIoThreads];
     __shared__ int wc[kIoThreads / 32];
-    const int n = L.ny * L.nz;
+    const int n = src.size();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     zval = 0.0;
     count = 0;
@@ -497,15 +532,7 @@ __device__ void crossing_sum(const Layout& L, const T* __restrict__ phi, int i, 
         const int e = base + threadIdx.x;
         bool hit = false;
         double h = 0.0;
-        if (e < n) {
-            const int j = e / L.nz, k = e - j * L.nz;
-            const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
-            const double a = static_cast<double>(phi[c]), b = static_cast<double>(phi[c + L.sz]);
-            if (a >= 0.0 && b < 0.0) {
-                hit = true;
-                h = -(a * p.dzp[k + 5]) / (b - a) + p.zp[k + 5];
-            }
-        }
+        if (e < n) hit = src.at(e, h);
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (lane == 0) wc[warp] = __popc(m);
         __syncthreads();
@@ -528,8 +555,8 @@ __device__ void crossing_sum(const Layout& L, const T* __restrict__ phi, int i, 
 // F56/F60 or the inflow crossings, phiout from F60/F62 or the outflow
 // crossings, and the outflow level wsfout (F62, or its ramp from F60 over
 // F64 steps).  One block.
-template <typename T>
-__global__ void __launch_bounds__(kIoThreads) io_level_kernel(Layout L, const T* __restrict__ phi, IoParams p) {
+template <typename In, typename Out>
+__device__ void io_levels(const In& in, const Out& out, const IoParams& p) {
     double* st = p.state;
     double phimean = p.f56, phiout = st[kIoPhiout];
     if (p.f60 > -1.0e20) {
@@ -540,14 +567,14 @@ __global__ void __launch_bounds__(kIoThreads) io_level_kernel(Layout L, const T*
     double zval = 0.0;
     int count = 0, found = 0;
     if (p.inflow) {
-        crossing_sum(L, phi, -1, p, zval, count);
+        crossing_sum(in, zval, count);
         if (count > 0) {
             phimean = zval / static_cast<double>(count);
             found = 1;
         }
     }
     if (p.outflow) {
-        crossing_sum(L, phi, L.nx - 1, p, zval, count);
+        crossing_sum(out, zval, count);
         if (count > 0) phiout = zval / static_cast<double>(count);
     }
     if (threadIdx.x != 0) return;
@@ -566,6 +593,33 @@ __global__ void __launch_bounds__(kIoThreads) io_level_kernel(Layout L, const T*
     st[kIoPhiout] = phiout;
     st[kIoWsfout] = wsfout;
     st[kIoFound] = found;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kIoThreads) io_level_kernel(Layout L, const T* __restrict__ phi, IoParams p) {
+    io_levels(CellHeights<T>{L, phi, p, -1}, CellHeights<T>{L, phi, p, L.nx - 1}, p);
+}
+
+// One slab's crossing heights (NaN where none) of the inflow column (out[0,
+// ny nz)) and the outflow column (out[ny nz, 2 ny nz)), j-major over its own
+// cells, for the gather into the whole grid's order.
+template <typename T>
+__global__ void __launch_bounds__(256) io_heights_kernel(Layout L, const T* __restrict__ phi, IoParams p,
+                                                         double* __restrict__ out) {
+    const int n = L.ny * L.nz;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 2 * n) return;
+    const int f = e / n, r = e - f * n, j = r / L.nz, k = r - j * L.nz;
+    double h = 0.0;
+    const bool on = f == 0 ? p.inflow : p.outflow;
+    out[e] = on && crossing_height(L, phi, f == 0 ? -1 : L.nx - 1, p, j, k, h) ? h : nan("");
+}
+
+// The measuring half of fsfinflow for a decomposed grid: the gathered
+// heights folded in the undivided grid's order, so the levels are the
+// undivided grid's bit for bit.  p.state: the grid's state (one copy).
+__global__ void __launch_bounds__(kIoThreads) io_fold_kernel(const double* __restrict__ heights, int n, IoParams p) {
+    io_levels(GatheredHeights{heights, n}, GatheredHeights{heights + n, n}, p);
 }
 
 // The imposing half of fsfinflow (step == 1): inflow ghosts of phi =
@@ -717,6 +771,29 @@ int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, c
         io_ghost_kernel<double><<<blocks, 256, 0, st>>>(L, static_cast<double*>(phi), static_cast<double*>(a1),
                                                         static_cast<double*>(a2), p, step ? 1 : 0);
     return n + 1;
+}
+
+int launch_io_heights(const Layout& L, const void* phi, bool fp32, const IoParams& p, double* out, cudaStream_t st) {
+    const int blocks = (2 * L.ny * L.nz + 255) / 256;
+    if (fp32) io_heights_kernel<float><<<blocks, 256, 0, st>>>(L, static_cast<const float*>(phi), p, out);
+    else io_heights_kernel<double><<<blocks, 256, 0, st>>>(L, static_cast<const double*>(phi), p, out);
+    return 1;
+}
+
+int launch_io_fold(const double* heights, int n, const IoParams& p, cudaStream_t st) {
+    io_fold_kernel<<<1, kIoThreads, 0, st>>>(heights, n, p);
+    return 1;
+}
+
+int launch_io_ghosts(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, cudaStream_t st) {
+    const int blocks = (L.ny * L.nz + 255) / 256;
+    if (fp32)
+        io_ghost_kernel<float><<<blocks, 256, 0, st>>>(L, static_cast<float*>(phi), static_cast<float*>(a1),
+                                                       static_cast<float*>(a2), p, 1);
+    else
+        io_ghost_kernel<double><<<blocks, 256, 0, st>>>(L, static_cast<double*>(phi), static_cast<double*>(a1),
+                                                        static_cast<double*>(a2), p, 1);
+    return 1;
 }
 
 int launch_dt_from_max(double dxmin, double n47, const Scratch& s, cudaStream_t st) {

@@ -198,6 +198,13 @@ constexpr int kIoPhimean = 0, kIoPhiout = 1, kIoCount = 2, kIoWsfout = 3, kIoFou
 // step == false: fsfrkin/fsfrkout only (the start of reini_RK3::start).
 int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, bool step,
                     cudaStream_t st);
+// The same split for a decomposed grid: every slab's crossing heights
+// (2 ny nz doubles, NaN where none), the fold of the gathered heights of the
+// whole grid (n = ny nz per face) into p.state, then every slab's imposing
+// half of fsfinflow with fsfrkin/fsfrkout.
+int launch_io_heights(const Layout& L, const void* phi, bool fp32, const IoParams& p, double* out, cudaStream_t st);
+int launch_io_fold(const double* heights, int n, const IoParams& p, cudaStream_t st);
+int launch_io_ghosts(const Layout& L, void* phi, void* a1, void* a2, bool fp32, const IoParams& p, cudaStream_t st);
 // VTU point data at the grid nodes: out[0..n) phi, then rho and viscosity
 // when ro != nullptr (3 n floats).
 int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const void* visc, bool fp32, float* out,

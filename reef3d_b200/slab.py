@@ -278,7 +278,7 @@ class Domain:
         xn = uniform_nodes(nx) if xn is None else xn
         yn = uniform_nodes(ny) if yn is None else yn
         zn = uniform_nodes(nz) if zn is None else zn
-        self.nx, self.ny, self.nz = nx, ny, nz
+        self.nx, self.ny, self.nz, self.nslabs = nx, ny, nz, nslabs
         self.desc = make_desc(nx, ny, nz, xn, yn, zn, f43, f44, f45, f49, n47, precision, f46, f47)
         d = ctypes.c_void_p()
         devs = None
@@ -321,6 +321,39 @@ class Domain:
         v = ctypes.c_double()
         self._check(self._lib.r3d_domain_get_dt(self.d, ctypes.byref(v)))
         return v.value
+
+    def _slab(self, s):
+        h = ctypes.c_void_p()
+        self._check(self._lib.r3d_domain_slab(self.d, s, ctypes.byref(h), None, None))
+        return h
+
+    def set_ioflow(self, **flags):
+        """Inflow / outflow faces on every slab (r3d_domain_set_ioflow), the
+        keys of LevelSet.set_ioflow; off=True closes them."""
+        from . import IOFLOW_DEFAULTS, IoflowDesc
+        if flags.pop("off", False):
+            self._check(self._lib.r3d_domain_set_ioflow(self.d, None))
+            return
+        unknown = set(flags) - set(IOFLOW_DEFAULTS)
+        if unknown:
+            raise TypeError(f"unknown ioflow flags {sorted(unknown)}")
+        desc = IoflowDesc(**dict(IOFLOW_DEFAULTS, **flags))
+        self._check(self._lib.r3d_domain_set_ioflow(self.d, ctypes.byref(desc)))
+
+    def io_levels(self):
+        """(phimean, phiout) of the grid, measured by the last step."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        h = self._slab(0)
+        if self._lib.r3d_io_levels(h, ctypes.byref(a), ctypes.byref(b)) != R3D_OK:
+            raise R3DError(1, self._lib.r3d_last_error(h).decode())
+        return a.value, b.value
+
+    def set_step_count(self, count):
+        """lexer::count of the next step (every slab's)."""
+        for s in range(self.nslabs):
+            h = self._slab(s)
+            if self._lib.r3d_set_step_count(h, count) != R3D_OK:
+                raise R3DError(1, self._lib.r3d_last_error(h).decode())
 
     def close(self):
         if getattr(self, "d", None) is not None and self.d.value:

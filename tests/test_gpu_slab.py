@@ -161,3 +161,50 @@ def test_native_domain_picard_equals_undivided_grid(f46, nslabs, precision):
     # the correction moved the level set: the run without it ends elsewhere
     plain, _, _ = run_whole(dims, precision, 3, FLAGS)
     assert np.abs(plain[r3d.PHI][m] - ref).max() > 10 * tol
+
+
+@pytest.mark.parametrize("case,nslabs,precision", [(0, 3, r3d.FP64), (1, 4, r3d.FP64), (2, 3, r3d.FP64),
+                                                   (3, 3, r3d.FP64), (1, 3, r3d.FP32), (5, 2, r3d.FP64)])
+def test_native_domain_ioflow_equals_undivided_grid(case, nslabs, precision):
+    """Inflow/outflow faces over the slabs (r3d_domain_set_ioflow): the
+    crossing heights of every slab gathered into the whole grid's order and
+    folded once, so the water levels and the step count are the undivided
+    grid's bit for bit and so is phi (within 1e-12 of its largest value with
+    the picard correction, whose volumes are summed per slab)."""
+    from reef3d_b200.slab import Domain
+    from test_gpu_ioflow import IO_CASES, tank
+    dims, io, f49, f46 = IO_CASES[case]
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = tank(nx, ny, nz, seed=nx + f46, stretch=0.2 if f46 == 3 else 0.0)
+    flags = dict(f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.25, f46=f46, f47=3)
+    count = 1 if f46 == 3 else 2  # picard_lsm takes its target volume at count 1
+    with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=precision, **flags) as ls:
+        ls.set_ioflow(**io)
+        ls.set_step_count(count)
+        for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+            ls.upload(f, a)
+        dts, levels = [], []
+        for _ in range(3):
+            dts.append(ls.cfl_dt())
+            ls.step()
+            levels.append(ls.io_levels())
+        ref = ls.download(r3d.PHI)
+    with Domain(nx, ny, nz, xn, yn, zn, nslabs=nslabs, precision=precision, devices=[0] * nslabs, **flags) as d:
+        d.set_ioflow(**io)
+        d.set_step_count(count)
+        for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+            d.upload(f, a)
+        for s in range(3):
+            d.run(1)
+            assert d.dt() == dts[s]
+            if f46 == 0:
+                assert d.io_levels() == levels[s]
+            else:
+                assert np.allclose(d.io_levels(), levels[s], rtol=1e-12, atol=0)
+        got = d.download(r3d.PHI)
+    m = visible_mask(*dims)
+    assert np.isfinite(ref[m]).all()
+    if f46 == 0:
+        assert np.array_equal(got[m], ref[m])
+    else:
+        assert np.abs(got[m] - ref[m]).max() <= 1e-12 * np.abs(ref[m]).max()
