@@ -221,6 +221,20 @@ struct IoflowState {
         }
         check(h, r3d_set_step_count(h, p->count));
     }
+    // the same for a slab domain: the faces on every slab, the step count
+    // on every slab (the grid's levels are taken from slab 0's)
+    void sync(r3d_domain* dm, const lexer* p, int gcv) {
+        r3d_ioflow_desc d{};
+        const bool now = ioflow_desc(p, gcv, &d);
+        if (now != on || (now && !same_ioflow(d, last))) {
+            check_domain(dm, r3d_domain_set_ioflow(dm, now ? &d : nullptr));
+            on = now;
+            last = d;
+        }
+        r3d_handle* h = nullptr;
+        for (int s = 0; r3d_domain_slab(dm, s, &h, nullptr, nullptr) == R3D_OK; ++s)
+            check(h, r3d_set_step_count(h, p->count));
+    }
 };
 
 }  // namespace r3d_adapter
@@ -303,15 +317,15 @@ private:
 // nslabs slabs (r3d_domain_*; slab r on devices[r], or all on the current
 // GPU), stepped as one with the halo exchange between stages -- one
 // REEF3D process spreading its level set over the GPUs of a node.  The same
-// contract as levelset_RK3_gpu (the picard correction F46 selects included,
-// over the whole grid), for runs without inflow/outflow, X45 stencils or
-// solid forcing (the run stops on them).
+// contract as levelset_RK3_gpu (the picard correction F46 selects and the
+// ioflow_f inflow/outflow faces included, over the whole grid), for runs
+// without X45 stencils or solid forcing (the run stops on them).
 class levelset_RK3_domain final : public freesurface {
 public:
     levelset_RK3_domain(lexer* p, fdm*, ghostcell*, int nslabs, const int* devices = nullptr,
                         int precision = R3D_FP64) {
-        if (p->X45 != 0 || p->X48 == 1 || p->B60 >= 1 || p->B90 >= 1) {
-            std::cout << "reef3d_b200: the slab domain runs without ioflow, X45 or X48" << std::endl;
+        if (p->X45 != 0 || p->X48 == 1) {
+            std::cout << "reef3d_b200: the slab domain runs without X45 or X48" << std::endl;
             std::exit(1);
         }
         const r3d_grid_desc g = r3d_adapter::grid_desc(p, precision);
@@ -323,6 +337,7 @@ public:
     void start(fdm* a, lexer* p, convection*, solver*, ghostcell* pgc, ioflow*, reini*, particle_corr*,
                field& ls) override {
         using r3d_adapter::check_domain;
+        io.sync(d, p, r3d_adapter::gcval_phi(p));
         check_domain(d, r3d_domain_upload(d, R3D_PHI, ls.V));
         check_domain(d, r3d_domain_upload(d, R3D_U, a->u.V));
         check_domain(d, r3d_domain_upload(d, R3D_V, a->v.V));
@@ -354,6 +369,7 @@ private:
         r3d_adapter::copy_owned(p, buf, f, true);
     }
     r3d_domain* d = nullptr;
+    r3d_adapter::IoflowState io;
     std::vector<double> buf;
 };
 

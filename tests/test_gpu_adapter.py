@@ -207,7 +207,7 @@ def _run_domain(name, nslabs):
     c = _case(name)
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                       f49=c["f49"], f46=c["f46"], f47=6, precision=0)
+                       f49=c["f49"], f46=c["f46"], f47=6, precision=0, ioflow=c.get("io"))
     ao.make_domain(nslabs)
     ao.set_state(c["phi"], c["u"], c["v"], c["w"])
     phi, same, rel = c["phi"], [], []
@@ -233,14 +233,15 @@ def _run_domain(name, nslabs):
 
 
 @pytest.mark.parametrize("name,nslabs", [("vortex3d", 3), ("stretched_f49_0", 3), ("disk2d", 4),
-                                         ("stretched_picard", 3)])
+                                         ("stretched_picard", 3), ("tank_io3d", 3), ("tank_io2d", 4)])
 def test_domain_adapter_matches_reference_objects(name, nslabs):
     """The free-surface adapter over z slabs (one REEF3D process spreading its
     level set over several GPUs; here the slabs share one): the level set
     bit-identical to the reference's on every cell, ghosts included, the
     density within 1e-12 relative (the device's sin), for three steps; with
     the picard correction (F46 = 2) phi (interior and faces) and density
-    within 1e-12."""
+    within 1e-12; with ioflow_f's inflow/outflow faces (tank cases) bit for
+    bit as without."""
     with mp.get_context("spawn").Pool(1) as pool:
         same = pool.apply(_run_domain, (name, nslabs))
     assert all(same), same
