@@ -104,18 +104,35 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- CPU side
-def _ref_worker(args):
-    edge, steps, fast = args
+# resident size of one reference process per padded cell of its grid (the
+# reference's fdm/lexer fields, measured: 1.55 GB at 128^3, 12.4 GB at 256^3)
+REF_BYTES_PER_CELL = 700.0
+
+
+def _ref_proc(edge, warm, steps, fast, barrier, queue):
+    """One reference process: its own vortex grid at `edge`^3, `warm`
+    untimed steps, then (after every process is ready) `steps` timed ones."""
     from oracle.bindings import RefOracle
     from reef3d_b200 import setups
-    c = setups.vortex3d(edge)
-    o = RefOracle(edge, edge, edge, c.xn, c.yn, c.zn, f43=c.f43, f44=c.f44, f45=c.f45, f49=c.f49, fast=fast)
-    o.set_state(c.phi, c.u, c.v, c.w)
-    dt = o.cfl_dt(c.n47)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        o.step(dt)
-    return time.perf_counter() - t0, edge ** 3 * steps
+    try:
+        c = setups.vortex3d(edge)
+        o = RefOracle(edge, edge, edge, c.xn, c.yn, c.zn, f43=c.f43, f44=c.f44, f45=c.f45, f49=c.f49, fast=fast)
+        o.set_state(c.phi, c.u, c.v, c.w)
+        del c
+        dt = o.cfl_dt(0.125)
+        o.set_count(1)
+        for _ in range(warm):
+            o.step(dt)
+        barrier.wait()
+        per = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            o.step(dt)
+            per.append(time.perf_counter() - t0)
+        queue.put((per, None))
+    except Exception as e:  # reported by the parent
+        barrier.abort()
+        queue.put(([], repr(e)))
 
 
 def host_cpu():
@@ -139,25 +156,71 @@ def host_has_avx2_fma():
         return False
 
 
-def reference_cpu(procs, edge, steps):
-    """The reference's own level-set step (oracle/_ref) on the host cores:
-    one single-threaded process per core (the reference's only parallel mode
-    is MPI), each advancing its own grid.  Returns (cell-updates/s, info)."""
+def mem_available():
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
+
+
+def reference_procs(edge, steps):
+    """Processes for the reference CPU arm: one per host core, no more than
+    80 % of the available memory holds (each process owns a whole grid), and
+    a divisor of `steps` so every process runs the same number of steps."""
+    cap = os.cpu_count() or 1
+    avail = mem_available()
+    if avail is not None:
+        per = REF_BYTES_PER_CELL * (edge + 6) ** 3 + 2e8
+        cap = min(cap, max(1, int(0.8 * avail // per)))
+    cap = max(1, min(cap, steps))
+    return max(p for p in range(1, cap + 1) if steps % p == 0)
+
+
+def reference_cpu(edge, steps, warmup, procs):
+    """The reference's own level-set step (oracle/_ref) on the host cores at
+    the benchmark's grid: `procs` single-threaded processes (the reference's
+    only parallel mode is MPI, absent here), each advancing its own
+    `edge`^3 vortex grid; `steps` timed steps and `warmup` untimed ones in
+    all, shared equally.  The timed region starts when every process has
+    built its grid and run its warm-up (a barrier) and ends when the last
+    process finishes.  Returns (cell-updates/s, info)."""
     from oracle.bindings import REF_LIB, REF_LIB_FAST
     fast = host_has_avx2_fma() and os.path.exists(REF_LIB_FAST)
     if not os.path.exists(REF_LIB) and not fast:
         return None, {"unavailable": "oracle/_ref was not built (needs the reference sources)"}
     ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs + 1)
+    queue = ctx.Queue()
+    share = [steps // procs + (1 if r < steps % procs else 0) for r in range(procs)]
+    warm = [warmup // procs + (1 if r < warmup % procs else 0) for r in range(procs)]
+    ps = [ctx.Process(target=_ref_proc, args=(edge, warm[r], share[r], fast, barrier, queue)) for r in range(procs)]
+    t_start = time.perf_counter()
+    for p in ps:
+        p.start()
+    try:
+        barrier.wait(timeout=3600)
+    except Exception:  # a process failed before its timed steps (it aborted the barrier)
+        pass
     t0 = time.perf_counter()
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(edge, steps, fast)] * procs)
+    res = [queue.get(timeout=3600) for _ in ps]
     wall = time.perf_counter() - t0
-    slowest = max(r[0] for r in res)
-    cells = sum(r[1] for r in res)
-    return cells / slowest, {"cores": procs, "kind": "reference", "host": host_cpu(),
-                             "build": "-O3 -mavx2 -mfma" if fast else "-O2 -ffp-contract=off",
-                             "sample": f"{procs} processes x vortex {edge}^3 x {steps} steps (same per-cell work as "
-                                       f"256^3), slowest process timed; wall {wall:.1f}s"}
+    for p in ps:
+        p.join()
+    errs = [e for _, e in res if e]
+    if errs:
+        return None, {"unavailable": "reference process failed: " + errs[0]}
+    per = [t for r, _ in res for t in r]
+    cells = edge ** 3 * steps
+    return cells / wall, {"cores": procs, "kind": "reference", "host": host_cpu(),
+                          "build": "-O3 -mavx2 -mfma" if fast else "-O2 -ffp-contract=off",
+                          "steps": steps, "warmup": warmup,
+                          "s_per_step_one_core": statistics.mean(per),
+                          "sample": f"{procs} processes x vortex {edge}^3 (the benchmark grid itself), {steps} timed "
+                                    f"steps in all ({steps // procs} per process), {warmup} untimed; timed region "
+                                    f"{wall:.1f}s, set-up {t0 - t_start:.1f}s"}
 
 
 def _ref_disk_worker(args):
@@ -209,21 +272,18 @@ def run_configs(ctx):
 def run_reference_arm(args, rank):
     if rank != 0:
         return
-    procs = os.cpu_count() or 1
-    edge = 96
-    steps_per = max(1, min(args.steps, 3))
-    rate, info = reference_cpu(procs, edge, steps_per)
-    base = {"metric": METRIC, "impl": "reference", "n_gpus": args.gpus, "steps": steps_per,
-            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD, "edge": args.edge}}
+    procs = reference_procs(args.edge, args.steps)
+    rate, info = reference_cpu(args.edge, args.steps, args.warmup, procs)
     if rate is None:
         print(json.dumps({"impl": "reference", "unavailable": info["unavailable"]}))
         return
-    base.update({"value": rate, "unit": "cell-updates/s",
-                 "ms_per_step": 1e3 * (N_CELLS_EDGE ** 3) / rate,
-                 "cpu_baseline": dict(value=rate, unit="cell-updates/s", **info),
-                 "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
-                         "d2h_bytes_per_step": 0}})
+    base = {"metric": METRIC, "impl": "reference", "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.edge ** 3 / rate,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "edge": args.edge, "cells_per_step": args.edge ** 3,
+                       "form": "the reference's FP64 code on the host cores"},
+            "cpu_baseline": dict(value=rate, unit="cell-updates/s", **info),
+            "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(base))
 
 
@@ -320,7 +380,7 @@ def tile_variants(ls, reps=10):
 
 def e2e_steps(case, precision, steps, warmup):
     """Through the C-ABI with host buffers in the reference's layout, the
-    way the levelset_RK3 adapter of INTEGRATION.md drives it: the level set
+    way the levelset_RK3 adapter drives it: the level set
     stays on the device between steps; every step uploads the velocities
     u, v, w the host's momentum solver owns (pinned host memory), runs the
     step (CFL + RK3 convection + reinitialisation + volume) and downloads
@@ -417,7 +477,9 @@ def run_ours(args):
                        "pinned host buffers in the reference layout, FP32 form"}
     cpu = None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu:
-        rate, info = reference_cpu(min(os.cpu_count() or 1, 8), 96, 2)
+        # the same processes (cores) as the reference arm, one step each
+        procs = reference_procs(args.edge, args.steps)
+        rate, info = reference_cpu(args.edge, procs, 0, procs)
         if rate is not None:
             cpu = dict(value=rate, unit="cell-updates/s", **info)
         else:

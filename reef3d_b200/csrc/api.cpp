@@ -549,6 +549,7 @@ void drop_step_graph(r3d_handle* h) {
     if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
     h->step_graph = nullptr;
     h->graph_key = -1;
+    ++h->config_gen;
 }
 
 // Captures one step into a CUDA graph (the step reads dt, the clock and the
@@ -1340,12 +1341,19 @@ int r3d_sync(r3d_handle* h) {
 int r3d_set_option(r3d_handle* h, int option, int value) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     switch (option) {
-        case R3D_OPT_TILED: h->use_tile = value ? 1 : 0; return R3D_OK;
+        case R3D_OPT_TILED:
+            if (h->use_tile != (value ? 1 : 0)) drop_step_graph(h);
+            h->use_tile = value ? 1 : 0;
+            return R3D_OK;
         case R3D_OPT_CHUNK:
             if (value < 1 || value > 4096) return fail(h, R3D_EINVAL, "chunk must be 1..4096 planes");
+            if (h->kc != value) drop_step_graph(h);
             h->kc = value;
             return R3D_OK;
-        case R3D_OPT_BAND64: h->band64 = value ? 1 : 0; return R3D_OK;
+        case R3D_OPT_BAND64:
+            if (h->band64 != (value ? 1 : 0)) drop_step_graph(h);
+            h->band64 = value ? 1 : 0;
+            return R3D_OK;
         case R3D_OPT_WAIT_TEST: h->wait_test = value ? 1 : 0; return R3D_OK;
         default: return fail(h, R3D_EINVAL, "unknown option");
     }
@@ -1402,7 +1410,11 @@ struct r3d_domain {
     std::vector<double*> iol;              // each slab's crossing heights, 2 ny n (on its device)
     double* iog = nullptr;                 // the grid's heights, 2 ny nz, and state (on dev0)
     cudaGraphExec_t graph = nullptr;
-    long long graph_adaptive = -1;  // configuration key of the captured step
+    // what the captured step was built from: adaptive time step, the faces,
+    // and each slab's configuration generation (r3d_handle::config_gen)
+    int graph_adaptive = -1;
+    bool graph_io = false;
+    std::vector<unsigned long long> graph_gen;
     bool ran = false;
     std::string err;
 };
@@ -1659,6 +1671,31 @@ int r3d_domain_create(const r3d_grid_desc* desc, int nslabs, const int* devices,
         cudaSetDevice(cur);
         return bail(rc, "creating the slabs");
     }
+    // halo, CFL and picard copies go between neighbouring slabs and to slab
+    // 0's device: let those devices address each other's memory directly
+    // (without it a copy between two GPUs is staged through the host)
+    for (size_t r = 0; r < d->slab.size(); ++r) {
+        const int a = d->slab[r]->device;
+        std::vector<int> peers = {d->dev0};
+        if (r + 1 < d->slab.size()) peers.push_back(d->slab[r + 1]->device);
+        for (int b : peers) {
+            if (a == b) continue;
+            for (int pass = 0; pass < 2; ++pass) {
+                const int from = pass ? b : a, to = pass ? a : b;
+                int can = 0;
+                if (cudaDeviceCanAccessPeer(&can, from, to) != cudaSuccess || !can) continue;
+                cudaSetDevice(from);
+                const cudaError_t e = cudaDeviceEnablePeerAccess(to, 0);
+                if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) {
+                    cudaGetLastError();
+                    cudaSetDevice(cur);
+                    return bail(R3D_EDEVICE, std::string("peer access: ") + cudaGetErrorString(e));
+                }
+                cudaGetLastError();  // clear cudaErrorPeerAccessAlreadyEnabled
+            }
+        }
+    }
+    cudaSetDevice(cur);
     d->ev.resize(d->slab.size(), nullptr);
     for (size_t r = 0; r < d->slab.size(); ++r) {  // each event on its slab's device
         cudaSetDevice(d->slab[r]->device);
@@ -1757,13 +1794,12 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
         for (r3d_handle* h : d->slab)
             if (int rc = r3d_set_dt(h, dt)) return dfail(d, rc, r3d_last_error(h));
     for (r3d_handle* h : d->slab) cudaStreamSynchronize(h->stream);
-    // the captured step depends on the slabs' configuration (velocity
-    // generator, forcing, precision path): recapture when it changed
-    long long key = (adaptive ? 1 : 0) + (d->io ? 2 : 0);
-    for (r3d_handle* h : d->slab)
-        key = key * 64 + (h->airy ? 1 : 0) + (h->sf_ops ? 2 : 0) + (h->g64.x45 ? 4 : 0) + (tiled(h) ? 8 : 0) +
-              (h->band64 ? 16 : 0) + (h->fluid ? 32 : 0);
-    if (!d->graph || d->graph_adaptive != key) {
+    // the captured step bakes in the slabs' configuration (velocity
+    // generator and its parameters, forcing lists, fluid constants, options):
+    // recapture when any slab's configuration generation moved
+    std::vector<unsigned long long> gen;
+    for (r3d_handle* h : d->slab) gen.push_back(h->config_gen);
+    if (!d->graph || d->graph_adaptive != (adaptive ? 1 : 0) || d->graph_io != d->io || d->graph_gen != gen) {
         if (d->graph) cudaGraphExecDestroy(d->graph);
         d->graph = nullptr;
         cudaGraph_t g = nullptr;
@@ -1779,7 +1815,9 @@ int r3d_domain_run(r3d_domain* d, int nsteps, double dt) {
             cudaGetLastError();  // leave no capture error behind for later calls
             return dfail(d, R3D_EDEVICE, std::string("domain step graph: ") + cudaGetErrorString(e));
         }
-        d->graph_adaptive = key;
+        d->graph_adaptive = adaptive ? 1 : 0;
+        d->graph_io = d->io;
+        d->graph_gen = gen;
     }
     cudaSetDevice(d->dev0);
     for (int n = 0; n < nsteps; ++n)
@@ -1849,6 +1887,10 @@ int r3d_domain_set_ioflow(r3d_domain* d, const r3d_ioflow_desc* io) {
 
 int r3d_domain_set_fluid(r3d_domain* d, double ro_water, double visc_water, double ro_air, double visc_air) {
     if (!d) return R3D_EINVAL;
+    if (d->graph) {  // the captured step holds the fluid constants
+        cudaGraphExecDestroy(d->graph);
+        d->graph = nullptr;
+    }
     for (r3d_handle* h : d->slab)
         if (int rc = r3d_set_fluid(h, ro_water, visc_water, ro_air, visc_air)) return dfail(d, rc, r3d_last_error(h));
     return R3D_OK;

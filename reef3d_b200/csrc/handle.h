@@ -63,6 +63,10 @@ struct r3d_handle {
     // rebuilt when anything baked into it changes
     cudaGraphExec_t step_graph = nullptr;
     long long graph_key = -1;
+    // bumped whenever something a captured step bakes in changes (kernel
+    // arguments by value, device pointers, options): graphs that hold this
+    // instance's work (its own step graph, a slab domain's) compare it
+    unsigned long long config_gen = 0;
     long long graph_launches = 0;
     std::string err;
 };

@@ -348,6 +348,14 @@ class Domain:
             raise R3DError(1, self._lib.r3d_last_error(h).decode())
         return a.value, b.value
 
+    def set_direct_forcing(self, x45):
+        """X45 direct-forcing convection stencils on every slab (each slab's
+        r3d_set_direct_forcing); the BODY field goes up by upload()."""
+        for s in range(self.nslabs):
+            h = self._slab(s)
+            if self._lib.r3d_set_direct_forcing(h, x45) != R3D_OK:
+                raise R3DError(1, self._lib.r3d_last_error(h).decode())
+
     def set_step_count(self, count):
         """lexer::count of the next step (every slab's)."""
         for s in range(self.nslabs):

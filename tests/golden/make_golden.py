@@ -3,7 +3,7 @@ level-set code (oracle/_ref, built by oracle/Makefile.ref from the reference
 sources) on small seeded cases.  One process per case: the reference keeps
 its grid tables in static members.
 
-    make -f oracle/Makefile.ref REF=/root/reference -j8
+    make -f oracle/Makefile.ref REF=$REEF3D_SRC -j8   (REEF3D_SRC: the reference sources)
     python tests/golden/make_golden.py [case name ...]   # default: every case
 
 Each case file holds the inputs (node coordinates, control flags, phi, u, v,

@@ -127,6 +127,48 @@ def test_native_domain_equals_undivided_grid(dims, nslabs, precision):
     assert np.array_equal(got[m], whole[r3d.PHI][m])
 
 
+@pytest.mark.parametrize("precision", [r3d.FP64, r3d.FP32])
+def test_native_domain_reconfigured_between_runs(precision):
+    """Settings changed on the slabs after the domain's step graph was
+    captured (new fluid densities, direct-forcing stencils switched on and
+    then changed to another X45) reach the next run: the domain keeps stepping as the undivided grid given the same
+    settings at the same points."""
+    from reef3d_b200.slab import Domain
+    dims = (36, 20, 30)
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=31)
+    df2 = (2,) + bodies(2, (nx + 6, ny + 6, nz + 6), 1.0 / nx, seed=8)
+    df3 = (3,) + bodies(3, (nx + 6, ny + 6, nz + 6), 1.0 / nx, seed=9)
+    dens = [(998.2, 1.004e-6, 1.205, 1.41e-5), (1025.0, 1.2e-6, 1.0, 1.5e-5)]
+
+    def script(obj, run, set_df):
+        obj.set_fluid(*dens[0])
+        for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+            obj.upload(f, a)
+        run(2)
+        obj.set_fluid(*dens[1])
+        run(1)
+        set_df(df2)
+        run(2)
+        set_df(df3)
+        run(1)
+        return {f: obj.download(f) for f in (r3d.PHI, r3d.RO, r3d.VISC)}
+
+    with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=precision, **FLAGS) as ls:
+        def whole_df(df):
+            ls.set_direct_forcing(df[0])
+            ls.upload(r3d.BODY, body_field(*df))
+        whole = script(ls, lambda n: ls.run(n, adaptive=True), whole_df)
+    with Domain(nx, ny, nz, xn, yn, zn, nslabs=3, precision=precision, devices=[0] * 3, **FLAGS) as d:
+        def dom_df(df):
+            d.set_direct_forcing(df[0])
+            d.upload(r3d.BODY, body_field(*df))
+        parts = script(d, lambda n: d.run(n), dom_df)
+    m = visible_mask(*dims)
+    for f in (r3d.PHI, r3d.RO, r3d.VISC):
+        assert np.array_equal(whole[f][m], parts[f][m]), f
+
+
 @pytest.mark.parametrize("f46,nslabs,precision", [(1, 3, r3d.FP64), (2, 3, r3d.FP64), (3, 4, r3d.FP64),
                                                   (2, 1, r3d.FP64), (3, 3, r3d.FP32)])
 def test_native_domain_picard_equals_undivided_grid(f46, nslabs, precision):
