@@ -64,8 +64,14 @@ def run_vortex(n, precision, period=3.0):
     return c, phi, v0, v1, steps
 
 
-def test_vortex_period_fp32_matches_fp64_accuracy():
-    n = 32
+@pytest.mark.parametrize("n", [64, 256])
+def test_vortex_period_fp32_matches_fp64_accuracy(n):
+    """The 3D vortex over a full period, FP32 form against the FP64 path: L1
+    shape error and relative volume change within 1 % of the FP64 run's own,
+    at 64^3 and at the benchmark's 256^3 (~85 s of GPU time).  At 128^3 the
+    filament is thinner than the grid resolves at t = T/2 and the two metrics
+    move by ~6 % under a 1e-12 relative perturbation of the FP64 start, so no
+    form of the arithmetic can meet a 1 % bar there."""
     c, p64, a64, b64, s64 = run_vortex(n, r3d.FP64)
     _, p32, a32, b32, s32 = run_vortex(n, r3d.FP32)
     assert abs(s64 - s32) <= 1
