@@ -267,6 +267,7 @@ def run_configs(ctx):
     out["ensemble"] = workloads.ensemble(steps=200)
     out["ensemble_accuracy"] = workloads.ensemble_accuracy(200)
     out["serving_fp32"] = workloads.serving(njobs=16)
+    out["serving_fp32_loads"] = workloads.serving_loads(out["serving_fp32"])
     out["serving_fp64"] = workloads.serving(njobs=16, precision=FP64)
     out["slab_domain"] = workloads.slab_domain()
     return out
@@ -363,18 +364,20 @@ def stage_roofline(ls, cells, elem, peak_gbs, reps=20):
 
 
 def tile_variants(ls, reps=10):
-    """Stage times of the tiled FP32 kernels under other chunkings and with
-    the FP64 interface band off (information for the tuning of R3D_OPT_*)."""
+    """Stage times of the tiled FP32 kernels under other chunkings (both
+    stage kinds on the convection stages' tile configuration) and with the
+    FP64 interface band off (information for the tuning of R3D_OPT_*)."""
     import reef3d_b200 as r3d
     if not ls.get_option(r3d.OPT_TILED):
         return None
     out = {}
-    base_kc = ls.get_option(r3d.OPT_CHUNK)
+    base = [ls.get_option(o) for o in (r3d.OPT_CHUNK, r3d.OPT_CHUNK_REINIT)]
     for kc in (8, 16, 32, 64):
         ls.set_option(r3d.OPT_CHUNK, kc)
         out[f"kc{kc}"] = {"conv_ms": device_time(ls, lambda: ls.stage(r3d.STAGE_CONVECTION, 2), reps),
                           "reinit_ms": device_time(ls, lambda: ls.stage(r3d.STAGE_REINIT, 2), reps)}
-    ls.set_option(r3d.OPT_CHUNK, base_kc)
+    ls.set_option(r3d.OPT_CHUNK, base[0])
+    ls.set_option(r3d.OPT_CHUNK_REINIT, base[1])
     ls.set_option(r3d.OPT_BAND64, 0)
     out["band64_off_reinit_ms"] = device_time(ls, lambda: ls.stage(r3d.STAGE_REINIT, 2), reps)
     ls.set_option(r3d.OPT_BAND64, 1)
@@ -455,6 +458,14 @@ def run_ours(args):
 
     # FP32 form (headline) -------------------------------------------------
     ls32 = make_instance(case, r3d.FP32)
+    # tile configuration and z chunk per stage kind, picked by timing
+    # (r3d_autotune; untimed, before the warm-up)
+    cfg, kc = ls32.autotune()
+    tile_cfg = {"convection": {"cfg": cfg, "chunk": kc, "tile": r3d.tile_configs()[cfg]},
+                "reinit": {"cfg": ls32.get_option(r3d.OPT_TILE_CFG_REINIT),
+                           "chunk": ls32.get_option(r3d.OPT_CHUNK_REINIT),
+                           "tile": r3d.tile_configs()[ls32.get_option(r3d.OPT_TILE_CFG_REINIT)]},
+                "tile_fields": "(tx, ty, rows per thread, ring slots, threads)"}
     with ClockSampler(ctx.local) as clk:
         total32, per32, launches32 = timed_steps(ls32, args.steps, args.warmup, ctx)
     total32 = ctx.max(total32)
@@ -509,6 +520,7 @@ def run_ours(args):
         "fp32_over_fp64": value32 / value64,
         "roofline": dict(roof32, traffic=NCU_TRAFFIC.get((args.edge, roof32["kernel"])), peak_source=peak_src),
         "tile_variants": variants,
+        "tile_config": tile_cfg,
         "gpu_launches": launches32,
         "clocks": clk.summary(),
         "e2e": e2e,

@@ -275,6 +275,27 @@ int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt);
  * batch members. */
 int r3d_set_direct_forcing(r3d_handle* h, int x45);
 
+/* Relaxation zones of REEF3D's wave generator and numerical beach on the
+ * level set (iowave::phi_relax, src/iowave_relax.cpp:346-378, called by
+ * levelset_RK3::start after every convection stage,
+ * src/levelset_RK3.cpp:125,142,158).  w_gen[i*ny + j] is the generation
+ * zone's weight relax4_wg(i,j) of column (i,j), w_beach the beach zone's
+ * relax4_nb(i,j); a negative weight marks a column outside that zone
+ * (iowave's distgen / distbeach >= 1e20); NULL: no such zone (B98 != 2, or
+ * B99 != 2).  After each convection stage, on the columns of the zones:
+ *   generation: f = (1 - w_gen) ramp lsval + w_gen f
+ *   beach:      f = (1 - w_beach) (phimean - z) + w_beach f
+ * with z the cell-centre height, and the relaxed values go into the wall
+ * ghost layers.  Both NULL turns the zones off.  Synchronous.  Not for
+ * batch members or slabs of a domain. */
+int r3d_set_relaxation(r3d_handle* h, const double* w_gen, const double* w_beach, double phimean);
+/* The generation zone's target level set of the coming step (iowave's
+ * lsval, filled by wavegen_precalc, src/iowave_precalc_relax.cpp) in the
+ * reference's LOOP order over the zone (columns i-major, j, then k), n =
+ * nz x the zone's columns, and the wave generation ramp of the step
+ * (iowave::ramp).  Synchronous. */
+int r3d_set_relaxation_target(r3d_handle* h, const double* lsval, long long n, double ramp);
+
 /* Solid forcing of the level set after each convection stage
  * (ghostcell::solid_forcing_lsm, src/gc_solid_forcing_lsm.cpp:27-78, called
  * at src/levelset_RK3.cpp:128,145,160 with X48 = 1): for each of the n
@@ -359,7 +380,10 @@ int r3d_init_spheres_tg(r3d_handle* h, int nspheres, const double* spheres, int 
  *  R3D_OPT_TILED  1 = TMA-tiled FP32x2 stage kernels on 3D uniform FP32
  *                 grids (default), 0 = one-cell-per-thread kernels;
  *                 reading it returns whether the tiled path is in use.
- *  R3D_OPT_CHUNK  z-planes per CTA of the tiled kernels (default 16).
+ *  R3D_OPT_CHUNK  z-planes per CTA of the tiled kernels (default 16); sets
+ *                 both stage kinds, R3D_OPT_CHUNK_REINIT then sets the
+ *                 reinitialisation stages' alone (reading CHUNK returns the
+ *                 convection stages' value).
  *  R3D_OPT_BAND64 1 = FP64 re-anchoring of interface-band cells in the FP32
  *                 reinitialisation (default), 0 = FP32 everywhere.
  *  R3D_OPT_WAIT_TEST  diagnostic for the bounded waits of the tiled kernels:
@@ -368,13 +392,37 @@ int r3d_init_spheres_tg(r3d_handle* h, int nspheres, const double* spheres, int 
  *                 kernels take their timeout path -- raise the error flag,
  *                 wait for their own copies, return -- and the next
  *                 r3d_sync reports R3D_ETIMEOUT; the instance stays usable.
- *                 Cleared by that step.  No effect off the tiled path. */
+ *                 Cleared by that step.  No effect off the tiled path.
+ *  R3D_OPT_TILE_CFG  tile configuration of the tiled kernels, 0 ..
+ *                 r3d_tile_config_count()-1 (r3d_tile_config_describe: tile
+ *                 shape, rows per thread, ring depth); the level set is the
+ *                 same under every configuration.  Sets both stage kinds;
+ *                 R3D_OPT_TILE_CFG_REINIT then sets the reinitialisation
+ *                 stages' alone.  r3d_autotune picks both with the chunks. */
 #define R3D_OPT_TILED 0
 #define R3D_OPT_CHUNK 1
 #define R3D_OPT_BAND64 2
 #define R3D_OPT_WAIT_TEST 3
+#define R3D_OPT_TILE_CFG 4
+#define R3D_OPT_TILE_CFG_REINIT 6
+#define R3D_OPT_CHUNK_REINIT 7
 int r3d_set_option(r3d_handle* h, int option, int value);
 int r3d_get_option(r3d_handle* h, int option, int* value);
+
+/* Tile configurations of the tiled kernels: how many there are, and for
+ * id cfg the tile (tx x ty cells per CTA), rows per thread, plane slots of
+ * the shared-memory ring and threads per CTA (R3D_EINVAL for a bad id). */
+int r3d_tile_config_count(void);
+int r3d_tile_config_describe(int cfg, int* tx, int* ty, int* rows_per_thread, int* ring, int* threads);
+/* Picks the instance's tile configuration and z chunk, for the convection
+ * and the reinitialisation stages separately, by timing a stage of each
+ * kind under every candidate (the level set is untouched: the timed stages
+ * write only a stage buffer), and caches the choice per grid size, in
+ * memory and in cache_path (may be NULL; the file r3d_batch_autotune
+ * uses).  cfg/chunk receive the convection stages' choice (the
+ * reinitialisation stages': R3D_OPT_TILE_CFG_REINIT, R3D_OPT_CHUNK_REINIT).
+ * No effect (and no timing) off the tiled path.  Synchronous. */
+int r3d_autotune(r3d_handle* h, const char* cache_path, int* cfg, int* chunk);
 
 /* Wait for the handle's stream; R3D_ETIMEOUT if a bounded device wait of a
  * kernel gave up since the last check. */
@@ -422,13 +470,19 @@ const char* r3d_batch_last_error(const r3d_batch* b);
 int r3d_batch_add(r3d_batch* b, r3d_handle* h);
 int r3d_batch_remove(r3d_batch* b, r3d_handle* h);
 int r3d_batch_size(const r3d_batch* b, int* n);
-/* Tile rows (2, 4, 8: tiles of 32 x rows cells, 32*rows threads) and
- * persistent CTAs per SM. */
+/* Members on the one-cell-per-thread kernels (2D, stretched): tile rows
+ * (2, 4, 8: tiles of 32 x rows cells, 32*rows threads) and persistent CTAs
+ * per SM. */
 int r3d_batch_set_config(r3d_batch* b, int rows, int ctas_per_sm);
 int r3d_batch_get_config(const r3d_batch* b, int* rows, int* ctas_per_sm);
-/* Times the candidate configurations on the batch (state-preserving) and
- * caches the best per size class, in memory and in cache_path (may be
- * NULL); a cached class is reused without timing. */
+/* Members on the tiled kernels (3D uniform FP32): tile configuration (as
+ * R3D_OPT_TILE_CFG) and z chunk of the batch's persistent launches. */
+int r3d_batch_set_tile_config(r3d_batch* b, int cfg, int chunk);
+int r3d_batch_get_tile_config(const r3d_batch* b, int* cfg, int* chunk);
+/* Times the candidate configurations on the batch (state-preserving): tile
+ * configuration x z chunk of the tiled members, then rows x CTAs per SM of
+ * the others; caches the best per size class, in memory and in cache_path
+ * (may be NULL); a cached class is reused without timing. */
 int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows, int* ctas_per_sm);
 int r3d_batch_use_graph(r3d_batch* b, int on);
 /* nsteps adaptive steps of every member; asynchronous on the batch stream. */

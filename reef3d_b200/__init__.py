@@ -23,7 +23,8 @@ FP64, FP32 = 0, 1
 PHI, U, V, W, L, WORK1, WORK2, RO, VISC, BODY = range(10)
 LAYOUT_REEF3D, LAYOUT_DENSE = 0, 1
 STAGE_CONVECTION, STAGE_REINIT = 0, 1
-OPT_TILED, OPT_CHUNK, OPT_BAND64, OPT_WAIT_TEST = 0, 1, 2, 3
+OPT_TILED, OPT_CHUNK, OPT_BAND64, OPT_WAIT_TEST, OPT_TILE_CFG = 0, 1, 2, 3, 4
+OPT_TILE_CFG_REINIT, OPT_CHUNK_REINIT = 6, 7
 
 _ERRNAMES = {1: "EINVAL", 2: "ENOMEM", 3: "EDEVICE", 4: "ETIMEOUT", 5: "ESTATE"}
 
@@ -104,6 +105,8 @@ EXPORTS = {
     "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
     "r3d_set_direct_forcing": ([_H, ctypes.c_int], ctypes.c_int),
+    "r3d_set_relaxation": ([_H, _D, _D, ctypes.c_double], ctypes.c_int),
+    "r3d_set_relaxation_target": ([_H, _D, ctypes.c_longlong, ctypes.c_double], ctypes.c_int),
     "r3d_set_solid_forcing": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_set_halo": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "r3d_write_vtu": ([_H, ctypes.c_char_p], ctypes.c_int),
@@ -125,6 +128,9 @@ EXPORTS = {
     "r3d_init_spheres_tg": ([_H, ctypes.c_int, _D, ctypes.c_int, _D], ctypes.c_int),
     "r3d_set_option": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "r3d_get_option": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "r3d_tile_config_count": ([], ctypes.c_int),
+    "r3d_tile_config_describe": ([ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 5, ctypes.c_int),
+    "r3d_autotune": ([_H, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_sync": ([_H], ctypes.c_int),
     "r3d_stream": ([_H, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "r3d_launch_count": ([_H, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
@@ -141,6 +147,8 @@ EXPORTS = {
     "r3d_batch_get_config": ([_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_batch_autotune": ([_H, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
                            ctypes.c_int),
+    "r3d_batch_set_tile_config": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "r3d_batch_get_tile_config": ([_H, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_batch_use_graph": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_batch_step": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_batch_sync": ([_H], ctypes.c_int),
@@ -171,6 +179,19 @@ EXPORTS = {
     "r3d_serve_release": ([_H, ctypes.c_longlong], ctypes.c_int),
     "r3d_serve_batch": ([_H, ctypes.POINTER(_H)], ctypes.c_int),
 }
+
+
+def tile_configs():
+    """[(tx, ty, rows_per_thread, ring, threads)] of the tiled kernels'
+    configurations, by id."""
+    lib = load_library()
+    out = []
+    for c in range(lib.r3d_tile_config_count()):
+        v = [ctypes.c_int() for _ in range(5)]
+        if lib.r3d_tile_config_describe(c, *(ctypes.byref(x) for x in v)) != R3D_OK:
+            raise R3DError(R3D_EINVAL, f"tile configuration {c}")
+        out.append(tuple(x.value for x in v))
+    return out
 
 
 def load_library(path=LIB_PATH):
@@ -362,6 +383,24 @@ class LevelSet:
         (r3d_set_direct_forcing); 0 turns them off."""
         _check(_lib.r3d_set_direct_forcing(self.h, x45), self.h)
 
+    def set_relaxation(self, w_gen=None, w_beach=None, phimean=0.0):
+        """Wave-generation / numerical-beach relaxation zones after every
+        convection stage (r3d_set_relaxation): weights per column as arrays
+        of shape (nx, ny), negative outside the zone; None: no such zone."""
+        def arr(a):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+            return a, a.ctypes.data_as(_D)
+        g, gp = arr(w_gen)
+        b, bp = arr(w_beach)
+        _check(_lib.r3d_set_relaxation(self.h, gp, bp, phimean), self.h)
+
+    def set_relaxation_target(self, lsval, ramp):
+        """The generation zone's targets of the coming step and the ramp."""
+        a = np.ascontiguousarray(lsval, dtype=np.float64).reshape(-1)
+        _check(_lib.r3d_set_relaxation_target(self.h, a.ctypes.data_as(_D), a.size, ramp), self.h)
+
     def write_vtu(self, path):
         """The level set (and rho, viscosity) as a VTU file like the
         reference's printer (r3d_write_vtu)."""
@@ -458,6 +497,14 @@ class LevelSet:
     def set_option(self, option, value):
         _check(_lib.r3d_set_option(self.h, option, int(value)), self.h)
 
+    def autotune(self, cache_path=None):
+        """Tile configuration and z chunk picked by timing (r3d_autotune);
+        returns (cfg, chunk)."""
+        c, k = ctypes.c_int(), ctypes.c_int()
+        p = os.fsencode(cache_path) if cache_path else None
+        _check(_lib.r3d_autotune(self.h, p, ctypes.byref(c), ctypes.byref(k)), self.h)
+        return c.value, k.value
+
     def get_option(self, option):
         v = ctypes.c_int()
         _check(_lib.r3d_get_option(self.h, option, ctypes.byref(v)), self.h)
@@ -531,10 +578,21 @@ class Batch:
         return r.value, c.value
 
     def autotune(self, cache_path=None):
+        """(rows, ctas_per_sm) of the cell members; the tiled members' choice
+        is tile_config()."""
         r, c = ctypes.c_int(), ctypes.c_int()
         p = cache_path.encode() if cache_path else None
         _bcheck(_lib.r3d_batch_autotune(self.b, p, ctypes.byref(r), ctypes.byref(c)), self.b)
         return r.value, c.value
+
+    def set_tile_config(self, cfg, chunk):
+        _bcheck(_lib.r3d_batch_set_tile_config(self.b, cfg, chunk), self.b)
+
+    def tile_config(self):
+        """(tile configuration id, z chunk) of the tiled members' launches."""
+        c, k = ctypes.c_int(), ctypes.c_int()
+        _bcheck(_lib.r3d_batch_get_tile_config(self.b, ctypes.byref(c), ctypes.byref(k)), self.b)
+        return c.value, k.value
 
     def use_graph(self, on):
         _bcheck(_lib.r3d_batch_use_graph(self.b, 1 if on else 0), self.b)

@@ -132,6 +132,8 @@ void release(r3d_handle* h) {
     if (h->coord) cudaFree(h->coord);
     if (h->io_buf) cudaFree(h->io_buf);
     if (h->sf_ops) cudaFree(h->sf_ops);
+    if (h->rz_col) cudaFree(h->rz_col);
+    if (h->rz_buf) cudaFree(h->rz_buf);
     if (h->stream) cudaStreamDestroy(h->stream);
     cudaSetDevice(cur);
 }
@@ -183,7 +185,13 @@ struct DeviceGuard {
 // The tiled kernels fill every face as a wall and know only the plain
 // stencils: instances with inflow / outflow faces or direct forcing run the
 // one-cell-per-thread kernels.
-bool tiled(const r3d_handle* h) { return h->tile_ok && h->use_tile && !h->io && !h->g64.x45; }
+// the volume partials of a tiled stage (one pair per CTA) must fit the
+// scratch buffer sized at creation for the cell kernels
+bool tile_fits(const r3d_handle* h, int kc, int cfg) { return tile_items_of(h->L, kc, cfg) <= h->S.npartial; }
+bool tiled(const r3d_handle* h) {
+    return h->tile_ok && h->use_tile && !h->io && !h->g64.x45 && tile_fits(h, h->kc, h->tile_cfg) &&
+           tile_fits(h, h->kc_r, h->tile_cfg_r);
+}
 
 // The body field of the direct-forcing stencils is FP64 in both forms.
 size_t field_elem(const r3d_handle* h, int id) { return id == R3D_BODY ? sizeof(double) : elem(h); }
@@ -229,7 +237,12 @@ TileArgs tile_args(r3d_handle* h, int stage) { return r3d::make_tile_args(h, sta
 
 long long stage_launch_plain(r3d_handle* h, bool reini, int s, bool vol) {
     const Fields f = fields_of(h);
-    if (tiled(h)) return launch_tile_stage(h->map[s - 1], tile_args(h, s), reini, s, vol, h->stream);
+    if (tiled(h)) {
+        TileArgs a = tile_args(h, s);
+        a.kc = reini ? h->kc_r : h->kc;
+        return launch_tile_stage(reini ? h->map_r[s - 1] : h->map[s - 1], a, reini ? h->tile_cfg_r : h->tile_cfg,
+                                 reini, s, vol, h->stream);
+    }
     if (fp32(h))
         return reini ? launch_reini_stage_f32(h->g32, f, s, h->S, vol, h->stream)
                      : launch_conv_stage_f32(h->g32, f, s, h->S, vol, h->stream);
@@ -237,20 +250,36 @@ long long stage_launch_plain(r3d_handle* h, bool reini, int s, bool vol) {
                  : launch_conv_stage_f64(h->g64, f, s, h->S, vol, h->stream);
 }
 
-// A stage; a convection stage is followed by the solid forcing of its
-// output when enabled (src/levelset_RK3.cpp:128,145,160).
+RelaxZones relax_zones(const r3d_handle* h) {
+    RelaxZones z{};
+    z.col = h->rz_col;
+    z.ncol = h->rz_ncol;
+    z.w = h->rz_buf;
+    z.zc = h->rz_buf + 2 * (size_t)h->rz_ncol;
+    z.ramp = z.zc + h->L.nz;
+    z.lsval = z.ramp + 1;
+    z.phimean = h->rz_phimean;
+    return z;
+}
+
+// A stage; a convection stage is followed by the relaxation zones
+// (src/levelset_RK3.cpp:125,142,158) and the solid forcing of its output
+// (:128,145,160) when enabled.
 long long stage_launch(r3d_handle* h, bool reini, int s, bool vol) {
     long long n = stage_launch_plain(h, reini, s, vol);
-    if (!reini && h->sf_ops) {
-        void* out = h->field[s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI];
-        n += launch_solid_forcing(out, fp32(h), h->sf_ops, h->sf_levels, h->stream);
-    }
+    if (reini) return n;
+    void* out = h->field[s == 1 ? R3D_WORK1 : s == 2 ? R3D_WORK2 : R3D_PHI];
+    if (h->relax) n += launch_relax(h->L, out, fp32(h), relax_zones(h), h->stream);
+    if (h->sf_ops) n += launch_solid_forcing(out, fp32(h), h->sf_ops, h->sf_levels, h->stream);
     return n;
 }
 
 long long volume_block_count(const r3d_handle* h) {
     if (tiled(h)) {
-        const dim3 g = tile_grid(h->L, h->kc);
+        // the step's last stage writes the partials: reinitialisation stage
+        // 3, or convection stage 3 without reinitialisation
+        const bool r = h->desc.f44 > 0;
+        const dim3 g = tile_grid(h->L, r ? h->kc_r : h->kc, r ? h->tile_cfg_r : h->tile_cfg);
         return (long long)g.x * g.y * g.z;
     }
     return volume_blocks(h->L);
@@ -443,7 +472,8 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
         const int ids[3] = {R3D_PHI, R3D_WORK1, R3D_WORK2};
         bool ok = true;
         for (int q = 0; q < 3 && ok; ++q)
-            ok = encode_plane_map(h->L, static_cast<const float*>(h->field[ids[q]]), &h->map[q], &why) == 0;
+            ok = encode_plane_map(h->L, static_cast<const float*>(h->field[ids[q]]), h->tile_cfg, &h->map[q], &why) == 0 &&
+                 encode_plane_map(h->L, static_cast<const float*>(h->field[ids[q]]), h->tile_cfg_r, &h->map_r[q], &why) == 0;
         h->tile_ok = ok && tile_prepare();
     }
     *out = h;
@@ -542,6 +572,7 @@ long long run_graph_key(const r3d_handle* h, int adaptive) {
     k = k * 2 + (tiled(h) ? 1 : 0);
     k = k * 2 + (h->band64 ? 1 : 0);
     k = k * 8192 + h->kc;
+    k = k * 8192 + h->kc_r;
     return k;
 }
 
@@ -1166,6 +1197,80 @@ int r3d_set_solid_forcing(r3d_handle* h, int n, const int* cells) {
     return R3D_OK;
 }
 
+int r3d_set_relaxation(r3d_handle* h, const double* w_gen, const double* w_beach, double phimean) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
+    if (h->domain_slab) return fail(h, R3D_ESTATE, "relaxation zones are not supported on slabs of a domain");
+    DeviceGuard dg(h->device, h->batch_stream);
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_step_graph(h);
+    if (h->rz_col) cudaFree(h->rz_col);
+    if (h->rz_buf) cudaFree(h->rz_buf);
+    h->rz_col = nullptr;
+    h->rz_buf = nullptr;
+    h->relax = false;
+    h->rz_ncol = 0;
+    h->rz_ntarget = 0;
+    if (!w_gen && !w_beach) return R3D_OK;
+    if (!std::isfinite(phimean)) return fail(h, R3D_EINVAL, "phimean must be finite");
+    const int nx = h->L.nx, ny = h->L.ny, nz = h->L.nz;
+    // zone columns in the reference's LOOP order (i outer, j inner), the
+    // generation targets of a column at nz consecutive offsets
+    std::vector<int> col;
+    std::vector<double> w;
+    int ngen = 0;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const double wg = w_gen ? w_gen[(size_t)i * ny + j] : -1.0;
+            const double wb = w_beach ? w_beach[(size_t)i * ny + j] : -1.0;
+            const bool g = wg >= 0.0, b = wb >= 0.0;
+            if ((g && !(wg <= 1.0)) || (b && !(wb <= 1.0)))
+                return fail(h, R3D_EINVAL, "relaxation weights must lie in [0, 1] (negative: outside the zone)");
+            if (!g && !b) continue;
+            col.insert(col.end(), {i, j, (g ? 1 : 0) | (b ? 2 : 0), g ? ngen * nz : 0});
+            w.push_back(g ? wg : 0.0);
+            w.push_back(b ? wb : 0.0);
+            if (g) ++ngen;
+        }
+    if (col.empty()) return R3D_OK;
+    const int ncol = (int)(col.size() / 4);
+    const long long ntarget = (long long)ngen * nz;
+    std::vector<double> buf(w);
+    for (int k = 0; k < nz; ++k) buf.push_back(h->M.xp[2][k + 5]);  // cell-centre z
+    buf.push_back(0.0);                                             // ramp
+    buf.resize(buf.size() + (size_t)ntarget, 0.0);                  // targets
+    if (cudaMalloc(&h->rz_col, col.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h->rz_buf, buf.size() * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        if (h->rz_col) cudaFree(h->rz_col);
+        h->rz_col = nullptr;
+        return fail(h, R3D_ENOMEM, "relaxation zone allocation failed");
+    }
+    R3D_CUDA(h, cudaMemcpy(h->rz_col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
+    R3D_CUDA(h, cudaMemcpy(h->rz_buf, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->rz_ncol = ncol;
+    h->rz_ntarget = ntarget;
+    h->rz_phimean = phimean;
+    h->relax = true;
+    return R3D_OK;
+}
+
+int r3d_set_relaxation_target(r3d_handle* h, const double* lsval, long long n, double ramp) {
+    if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
+    if (!h->relax) return fail(h, R3D_ESTATE, "no relaxation zones (r3d_set_relaxation)");
+    if (n != h->rz_ntarget) return fail(h, R3D_EINVAL, "target count must be nz x the generation zone's columns");
+    if (n > 0 && !lsval) return fail(h, R3D_EINVAL, "null targets");
+    if (!std::isfinite(ramp)) return fail(h, R3D_EINVAL, "ramp must be finite");
+    DeviceGuard dg(h->device, h->batch_stream);
+    const RelaxZones z = relax_zones(h);
+    h->launches += launch_set_scalar(const_cast<double*>(z.ramp), ramp, h->stream);
+    if (n > 0)
+        R3D_CUDA(h, cudaMemcpyAsync(const_cast<double*>(z.lsval), lsval, (size_t)n * sizeof(double),
+                                    cudaMemcpyHostToDevice, h->stream));
+    R3D_CUDA(h, cudaStreamSynchronize(h->stream));
+    return R3D_OK;
+}
+
 int r3d_set_direct_forcing(r3d_handle* h, int x45) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
@@ -1346,15 +1451,38 @@ int r3d_set_option(r3d_handle* h, int option, int value) {
             h->use_tile = value ? 1 : 0;
             return R3D_OK;
         case R3D_OPT_CHUNK:
+        case R3D_OPT_CHUNK_REINIT:
             if (value < 1 || value > 4096) return fail(h, R3D_EINVAL, "chunk must be 1..4096 planes");
-            if (h->kc != value) drop_step_graph(h);
-            h->kc = value;
+            drop_step_graph(h);
+            if (option == R3D_OPT_CHUNK) h->kc = value;
+            h->kc_r = value;
             return R3D_OK;
         case R3D_OPT_BAND64:
             if (h->band64 != (value ? 1 : 0)) drop_step_graph(h);
             h->band64 = value ? 1 : 0;
             return R3D_OK;
         case R3D_OPT_WAIT_TEST: h->wait_test = value ? 1 : 0; return R3D_OK;
+        case R3D_OPT_TILE_CFG:
+        case R3D_OPT_TILE_CFG_REINIT: {
+            if (value < 0 || value >= tile_cfg_count()) return fail(h, R3D_EINVAL, "unknown tile configuration");
+            CUtensorMap m[3];
+            if (h->tile_ok) {
+                // the stage inputs' tensor maps carry the configuration's box
+                const int ids[3] = {R3D_PHI, R3D_WORK1, R3D_WORK2};
+                std::string why;
+                for (int q = 0; q < 3; ++q)
+                    if (encode_plane_map(h->L, static_cast<const float*>(h->field[ids[q]]), value, &m[q], &why))
+                        return fail(h, R3D_EDEVICE, why);
+            }
+            drop_step_graph(h);
+            for (int q = 0; q < 3 && h->tile_ok; ++q) {
+                if (option == R3D_OPT_TILE_CFG) h->map[q] = m[q];
+                h->map_r[q] = m[q];
+            }
+            if (option == R3D_OPT_TILE_CFG) h->tile_cfg = value;
+            h->tile_cfg_r = value;
+            return R3D_OK;
+        }
         default: return fail(h, R3D_EINVAL, "unknown option");
     }
 }
@@ -1366,8 +1494,17 @@ int r3d_get_option(r3d_handle* h, int option, int* value) {
         case R3D_OPT_CHUNK: *value = h->kc; return R3D_OK;
         case R3D_OPT_BAND64: *value = h->band64; return R3D_OK;
         case R3D_OPT_WAIT_TEST: *value = h->wait_test; return R3D_OK;
+        case R3D_OPT_TILE_CFG: *value = h->tile_cfg; return R3D_OK;
+        case R3D_OPT_TILE_CFG_REINIT: *value = h->tile_cfg_r; return R3D_OK;
+        case R3D_OPT_CHUNK_REINIT: *value = h->kc_r; return R3D_OK;
         default: return fail(h, R3D_EINVAL, "unknown option");
     }
+}
+
+int r3d_tile_config_count(void) { return tile_cfg_count(); }
+
+int r3d_tile_config_describe(int cfg, int* tx, int* ty, int* rows_per_thread, int* ring, int* threads) {
+    return tile_cfg_describe(cfg, tx, ty, rows_per_thread, ring, threads) ? R3D_EINVAL : R3D_OK;
 }
 
 int r3d_stream(r3d_handle* h, void** stream) {

@@ -44,6 +44,10 @@ struct r3d_batch {
     int max_f44 = 0;
     int rows = 4;
     int ctas_per_sm = 8;
+    // tile configuration and z chunk of the tiled members' launches (the
+    // batch encodes its own tensor maps of their fields for it)
+    int tile_cfg = 0;
+    int tile_kc = 16;
     bool tuned = false;  // rows/ctas set explicitly or by the autotuner
     bool dirty = true;
     bool use_graph = true;
@@ -115,16 +119,21 @@ int rebuild(r3d_batch* b) {
         r3d_handle* h = order[q];
         desc[q] = describe(h);
         const bool t = (int)q < b->n_tiled;
-        tile0[q + 1] = tile0[q] + (t ? tile_items_of(h->L, h->kc) : batch_tiles_of(h->L, b->rows));
+        tile0[q + 1] = tile0[q] + (t ? tile_items_of(h->L, b->tile_kc, b->tile_cfg) : batch_tiles_of(h->L, b->rows));
         b->max_f44 = std::max(b->max_f44, h->desc.f44);
         if (t) {
             TiledMember& m = tiled[q];
             m.args = make_tile_args(h, 1);
+            m.args.kc = b->tile_kc;
             m.phi = static_cast<float*>(h->field[R3D_PHI]);
             m.a1 = static_cast<float*>(h->field[R3D_WORK1]);
             m.a2 = static_cast<float*>(h->field[R3D_WORK2]);
             m.f44 = h->desc.f44;
-            for (int s = 0; s < 3; ++s) maps[3 * q + s] = h->map[s];
+            const float* src[3] = {m.phi, m.a1, m.a2};
+            std::string why;
+            for (int s = 0; s < 3; ++s)
+                if (encode_plane_map(h->L, src[s], b->tile_cfg, &maps[3 * q + s], &why))
+                    return bfail(b, R3D_EDEVICE, why);
         }
     }
     b->t_tiled = tile0[b->n_tiled];
@@ -212,7 +221,7 @@ BatchLaunch cell_launch_of(const r3d_batch* b) {
 }
 
 unsigned tiled_grid(const r3d_batch* b) {
-    const long long want = (long long)batch_tile_ctas_per_sm() * b->sms;  // the co-resident CTAs
+    const long long want = (long long)tile_ctas_per_sm(b->tile_cfg) * b->sms;  // the co-resident CTAs
     return (unsigned)std::max<long long>(1, std::min<long long>(want, b->t_tiled));
 }
 
@@ -238,8 +247,8 @@ long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
     return fork_join(
         b,
         [&](cudaStream_t st) {
-            return (long long)launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, reini, s, q,
-                                                      b->d_vol, b->d_work, tiled_grid(b), st);
+            return (long long)launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, b->tile_cfg,
+                                                      reini, s, q, b->d_vol, b->d_work, tiled_grid(b), st);
         },
         [&](cudaStream_t st) { return (long long)launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, st); });
 }
@@ -248,7 +257,7 @@ long long enqueue_vmax(r3d_batch* b) {
     return fork_join(
         b,
         [&](cudaStream_t st) {
-            return (long long)launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->d_vmax,
+            return (long long)launch_batch_tile_vmax(b->d_tiled, b->d_tile0, b->n_tiled, b->tile_cfg, b->d_vmax,
                                                      tiled_grid(b), st);
         },
         [&](cudaStream_t st) { return (long long)launch_batch_vmax(cell_launch_of(b), st); });
@@ -284,7 +293,10 @@ int capture(r3d_batch* b) {
 
 // ---------------------------------------------------------------- autotuner
 std::mutex g_tune_mu;
-std::map<std::string, std::pair<int, int>> g_tune_cache;
+// size class -> (rows, CTAs per SM, tile configuration, z chunk) of a
+// batch, or (convection tile configuration, chunk, reinitialisation tile
+// configuration, chunk) of an instance ("inst-" keys)
+std::map<std::string, std::vector<int>> g_tune_cache;
 
 std::string size_class(const r3d_batch* b) {
     double c3 = 0, c2 = 0;
@@ -299,18 +311,35 @@ std::string size_class(const r3d_batch* b) {
     return os.str();
 }
 
+// One line per size class: the key and four integers.
 void load_cache(const char* path) {
     if (!path || !*path) return;
     std::ifstream f(path);
-    std::string key;
-    int r, c;
-    while (f >> key >> r >> c) g_tune_cache[key] = {r, c};
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream is(line);
+        std::string key;
+        std::vector<int> v(4, 0);
+        if (is >> key >> v[0] >> v[1] >> v[2] >> v[3]) g_tune_cache[key] = v;
+    }
 }
 
 void save_cache(const char* path) {
     if (!path || !*path) return;
     std::ofstream f(path, std::ios::trunc);
-    for (auto& kv : g_tune_cache) f << kv.first << " " << kv.second.first << " " << kv.second.second << "\n";
+    for (auto& kv : g_tune_cache) {
+        f << kv.first;
+        for (int x : kv.second) f << " " << x;
+        f << "\n";
+    }
+}
+
+// The (tile configuration, z chunk) candidates of the autotuners.
+std::vector<std::pair<int, int>> tile_candidates() {
+    std::vector<std::pair<int, int>> out;
+    for (int c = 0; c < tile_cfg_count(); ++c)
+        for (int kc : {8, 16, 32}) out.push_back({c, kc});
+    return out;
 }
 
 }  // namespace
@@ -426,68 +455,200 @@ int r3d_batch_use_graph(r3d_batch* b, int on) {
     return R3D_OK;
 }
 
-// Picks (rows, CTAs per SM) for the batch's size class by timing the first
-// convection and reinitialisation stages (they write only the stage buffer
-// WORK1, so the members' state is untouched), and caches the choice per
+int r3d_batch_set_tile_config(r3d_batch* b, int cfg, int kc) {
+    if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
+    if (cfg < 0 || cfg >= tile_cfg_count()) return bfail(b, R3D_EINVAL, "unknown tile configuration");
+    if (kc < 1 || kc > 4096) return bfail(b, R3D_EINVAL, "chunk must be 1..4096 planes");
+    b->tile_cfg = cfg;
+    b->tile_kc = kc;
+    b->dirty = true;
+    drop_graph(b);
+    return R3D_OK;
+}
+
+int r3d_batch_get_tile_config(const r3d_batch* b, int* cfg, int* kc) {
+    if (!b || !cfg || !kc) return bfail(nullptr, R3D_EINVAL, "null argument");
+    *cfg = b->tile_cfg;
+    *kc = b->tile_kc;
+    return R3D_OK;
+}
+
+// Picks the tiled members' (tile configuration, z chunk) and the cell
+// members' (rows, CTAs per SM) for the batch's size class by timing the
+// first convection and reinitialisation stages (they write only the stage
+// buffer WORK1, so the members' state is untouched): first the tile
+// configurations with the cell members at their current choice, then the
+// cell choices with the best tile configuration.  The choice is cached per
 // size class in memory and in `cache_path` (a text file; may be NULL).
 int r3d_batch_autotune(r3d_batch* b, const char* cache_path, int* rows_out, int* ctas_out) {
     if (!b) return bfail(nullptr, R3D_EINVAL, "null batch");
     if (b->members.empty()) return bfail(b, R3D_ESTATE, "empty batch");
     const std::string key = size_class(b);
+    auto finish = [&](int r, int c, int cfg, int kc) {
+        int rc = r3d_batch_set_config(b, r, c);
+        if (!rc) rc = r3d_batch_set_tile_config(b, cfg, kc);
+        if (rows_out) *rows_out = b->rows;
+        if (ctas_out) *ctas_out = b->ctas_per_sm;
+        return rc;
+    };
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         if (g_tune_cache.empty()) load_cache(cache_path);
         auto it = g_tune_cache.find(key);
-        if (it != g_tune_cache.end()) {
-            int rc = r3d_batch_set_config(b, it->second.first, it->second.second);
-            if (rows_out) *rows_out = b->rows;
-            if (ctas_out) *ctas_out = b->ctas_per_sm;
-            return rc;
-        }
+        if (it != g_tune_cache.end() && it->second.size() == 4 && it->second[2] < tile_cfg_count() &&
+            it->second[3] > 0)
+            return finish(it->second[0], it->second[1], it->second[2], it->second[3]);
     }
-    const int cand_rows[3] = {2, 4, 8};
-    const int cand_ctas[4] = {4, 8, 16, 32};
-    float best = 1e30f;
-    int br = 4, bc = 8;
     cudaEvent_t e0, e1;
     B_CUDA(b, cudaEventCreate(&e0));
     B_CUDA(b, cudaEventCreate(&e1));
     // the stages read dt: give every member a valid one first
     b->rows = 4;
     b->ctas_per_sm = 8;
+    b->tile_cfg = 0;
+    b->tile_kc = 16;
     if (int rc = rebuild(b)) return rc;
     enqueue_vmax(b);
     launch_batch_dt(launch_of(b), b->stream);
-    for (int r : cand_rows)
-        for (int c : cand_ctas) {
-            if (c * 32 * r > 2048) continue;
-            b->rows = r;
-            b->ctas_per_sm = c;
-            if (int rc = rebuild(b)) return rc;
-            enqueue_stage(b, false, 1, 0);  // warm
-            cudaEventRecord(e0, b->stream);
-            for (int rep = 0; rep < 3; ++rep) {
-                enqueue_stage(b, false, 1, 0);
-                enqueue_stage(b, true, 1, 0);
-            }
-            cudaEventRecord(e1, b->stream);
-            B_CUDA(b, cudaEventSynchronize(e1));
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) { best = ms; br = r; bc = c; }
+    int err = R3D_OK;
+    auto time_now = [&]() -> float {
+        if (int rc = rebuild(b)) {
+            err = rc;
+            return 1e30f;
         }
+        enqueue_stage(b, false, 1, 0);  // warm
+        cudaEventRecord(e0, b->stream);
+        for (int rep = 0; rep < 3; ++rep) {
+            enqueue_stage(b, false, 1, 0);
+            enqueue_stage(b, true, 1, 0);
+        }
+        cudaEventRecord(e1, b->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            err = bfail(b, R3D_EDEVICE, "autotune timing");
+            return 1e30f;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
+    float best = 1e30f;
+    int bcfg = 0, bkc = 16;
+    if (b->n_tiled > 0)
+        for (auto [cfg, kc] : tile_candidates()) {
+            b->tile_cfg = cfg;
+            b->tile_kc = kc;
+            const float ms = time_now();
+            if (err) break;
+            if (ms < best) { best = ms; bcfg = cfg; bkc = kc; }
+        }
+    b->tile_cfg = bcfg;
+    b->tile_kc = bkc;
+    best = 1e30f;
+    int br = 4, bc = 8;
+    const int cand_rows[3] = {2, 4, 8};
+    const int cand_ctas[4] = {4, 8, 16, 32};
+    if (!err && (size_t)b->n_tiled < b->members.size())
+        for (int r : cand_rows)
+            for (int c : cand_ctas) {
+                if (c * 32 * r > 2048) continue;
+                b->rows = r;
+                b->ctas_per_sm = c;
+                const float ms = time_now();
+                if (err) break;
+                if (ms < best) { best = ms; br = r; bc = c; }
+            }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (err) return err;
     B_CUDA(b, cudaGetLastError());
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tune_cache[key] = {br, bc};
+        g_tune_cache[key] = {br, bc, bcfg, bkc};
         save_cache(cache_path);
     }
-    int rc = r3d_batch_set_config(b, br, bc);
-    if (rows_out) *rows_out = br;
-    if (ctas_out) *ctas_out = bc;
-    return rc;
+    return finish(br, bc, bcfg, bkc);
+}
+
+// Picks the tile configuration and z chunk of one instance on the tiled
+// path for its grid size, for the convection and the reinitialisation
+// stages separately, by timing stage 2 of each kind under every candidate
+// (stage 2 reads phi and WORK1 and writes only WORK2, so the level set is
+// untouched), and caches the choice per grid size like r3d_batch_autotune
+// (cache line: key, convection configuration and chunk, reinitialisation
+// configuration and chunk).
+int r3d_autotune(r3d_handle* h, const char* cache_path, int* cfg_out, int* kc_out) {
+    if (!h) return R3D_EINVAL;
+    int on = 0;
+    if (int rc = r3d_get_option(h, R3D_OPT_TILED, &on)) return rc;
+    auto report = [&]() {
+        if (cfg_out) *cfg_out = h->tile_cfg;
+        if (kc_out) *kc_out = h->kc;
+    };
+    if (!on) {  // not on the tiled kernels: nothing to choose
+        report();
+        return R3D_OK;
+    }
+    std::ostringstream os;
+    os << "inst-" << h->L.nx << "x" << h->L.ny << "x" << h->L.nz;
+    const std::string key = os.str();
+    auto finish = [&](int c, int k, int cr, int kr) {
+        int rc = r3d_set_option(h, R3D_OPT_TILE_CFG, c);
+        if (!rc) rc = r3d_set_option(h, R3D_OPT_CHUNK, k);
+        if (!rc) rc = r3d_set_option(h, R3D_OPT_TILE_CFG_REINIT, cr);
+        if (!rc) rc = r3d_set_option(h, R3D_OPT_CHUNK_REINIT, kr);
+        report();
+        return rc;
+    };
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        if (g_tune_cache.empty()) load_cache(cache_path);
+        auto it = g_tune_cache.find(key);
+        const int n = tile_cfg_count();
+        if (it != g_tune_cache.end() && it->second.size() == 4 && it->second[0] < n && it->second[2] < n &&
+            it->second[1] > 0 && it->second[3] > 0)
+            return finish(it->second[0], it->second[1], it->second[2], it->second[3]);
+    }
+    double dt = 0.0;
+    if (int rc = r3d_cfl_dt(h, &dt)) return rc;
+    if (int rc = r3d_set_dt(h, dt)) return rc;
+    const int c0 = h->tile_cfg, k0 = h->kc, cr0 = h->tile_cfg_r, kr0 = h->kc_r;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return R3D_EDEVICE;
+    float best[2] = {1e30f, 1e30f};
+    int bc[2] = {c0, cr0}, bk[2] = {k0, kr0};
+    int rc = R3D_OK;
+    for (auto [cfg, kc] : tile_candidates()) {
+        if ((rc = r3d_set_option(h, R3D_OPT_TILE_CFG, cfg)) || (rc = r3d_set_option(h, R3D_OPT_CHUNK, kc))) break;
+        if ((rc = r3d_get_option(h, R3D_OPT_TILED, &on))) break;
+        if (!on) continue;  // e.g. more items than the volume scratch holds
+        for (int kind = 0; kind < 2 && !rc; ++kind) {
+            const int st = kind ? R3D_STAGE_REINIT : R3D_STAGE_CONVECTION;
+            if ((rc = r3d_stage(h, st, 2))) break;  // warm
+            cudaEventRecord(e0, h->stream);
+            for (int rep = 0; rep < 5 && !rc; ++rep) rc = r3d_stage(h, st, 2);
+            cudaEventRecord(e1, h->stream);
+            if (rc || cudaEventSynchronize(e1) != cudaSuccess) {
+                if (!rc) rc = R3D_EDEVICE;
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best[kind]) { best[kind] = ms; bc[kind] = cfg; bk[kind] = kc; }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) {
+        finish(c0, k0, cr0, kr0);
+        return rc;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = {bc[0], bk[0], bc[1], bk[1]};
+        save_cache(cache_path);
+    }
+    return finish(bc[0], bk[0], bc[1], bk[1]);
 }
 
 // nsteps physical steps of every member: per member the CFL time step from

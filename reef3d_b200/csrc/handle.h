@@ -34,6 +34,13 @@ struct r3d_handle {
     size_t io_buf_len = 0;
     r3d::IoParams iop{};
     long long next_count = 1;  // lexer::count of the next step, for r3d_set_ioflow's first state
+    // relaxation zones after each convection stage (r3d_set_relaxation)
+    bool relax = false;
+    int* rz_col = nullptr;       // 4 ints per zone column
+    double* rz_buf = nullptr;    // weights (2 per column), z centres (nz), ramp (1), targets
+    int rz_ncol = 0;
+    long long rz_ntarget = 0;    // generation targets: nz x generation columns
+    double rz_phimean = 0.0;
     // solid forcing after each convection stage (r3d_set_solid_forcing)
     long long* sf_ops = nullptr;     // device: (entry cell, two target cells) per op, by level
     std::vector<int> sf_levels;      // op offsets of the dependency levels
@@ -52,10 +59,16 @@ struct r3d_handle {
     // TMA-tiled FP32 path (3D uniform grids)
     bool tile_ok = false;
     int use_tile = 1;
+    // tile configuration (shape, rows per thread, ring depth) and z chunk of
+    // the convection stages; *_r: of the reinitialisation stages
     int kc = 16;
+    int tile_cfg = 0;
+    int kc_r = 16;
+    int tile_cfg_r = 0;
     int band64 = 1;
     int wait_test = 0;  // R3D_OPT_WAIT_TEST: armed for the next r3d_ls_step
-    CUtensorMap map[3];  // stage inputs: phi, WORK1, WORK2
+    CUtensorMap map[3];    // stage inputs phi, WORK1, WORK2 for tile_cfg
+    CUtensorMap map_r[3];  // the same for tile_cfg_r
     // set while the instance is a member of a batch: calls on the handle
     // first wait for the batch's stream
     cudaStream_t batch_stream = nullptr;

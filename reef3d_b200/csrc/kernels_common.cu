@@ -814,6 +814,52 @@ int launch_vtu_nodes(const Layout& L, const void* phi, const void* ro, const voi
     return 1;
 }
 
+// Relaxation zones (iowave::phi_relax, src/iowave_relax.cpp:346-378), one
+// thread per (zone column, k).  In the generation zone
+//   f = (1 - relax4_wg) ramp lsval + relax4_wg f,
+// then in the beach zone
+//   f = (1 - relax4_nb) (phimean - z) + relax4_nb f,
+// in the reference's operation order (FP64; the FP32 form rounds the
+// result), and the relaxed value goes into the cell's wall ghost layers as
+// ghostcell::start4 afterwards does (src/levelset_RK3.cpp:125-127).
+template <typename T>
+__global__ void relax_kernel(Layout L, T* f, RelaxZones z) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)z.ncol * L.nz) return;
+    const int q = (int)(t / L.nz), k = (int)(t % L.nz);
+    const int i = z.col[4 * q], j = z.col[4 * q + 1], zone = z.col[4 * q + 2], off = z.col[4 * q + 3];
+    const long long c = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + (i + L.gx);
+    double v = (double)f[c];
+    if (zone & 1) {
+        const double w = z.w[2 * q];
+        v = (1.0 - w) * (*z.ramp) * z.lsval[off + k] + w * v;
+    }
+    if (zone & 2) {
+        const double w = z.w[2 * q + 1];
+        v = (1.0 - w) * (z.phimean - z.zc[k]) + w * v;
+    }
+    const T val = (T)v;
+    f[c] = val;
+    if ((L.io & kIoEdge) && i == 0 && k == L.nz - 1) f[c - 1 + L.sz] = val;
+    for (int r = 1; r <= 3; ++r) {
+        if (i == 0 && !(L.io & kIoSkipLo)) f[c - r] = val;
+        if (i == L.nx - 1 && !(L.io & kIoSkipHi)) f[c + r] = val;
+        if (!L.two_d && j == 0) f[c - r * L.sy] = val;
+        if (!L.two_d && j == L.ny - 1) f[c + r * L.sy] = val;
+        if (k == 0 && !(L.io & kHaloZLo)) f[c - r * L.sz] = val;
+        if (k == L.nz - 1 && !(L.io & kHaloZHi)) f[c + r * L.sz] = val;
+    }
+}
+
+int launch_relax(const Layout& L, void* f, bool fp32, const RelaxZones& z, cudaStream_t st) {
+    const long long n = (long long)z.ncol * L.nz;
+    if (n <= 0) return 0;
+    const unsigned g = (unsigned)((n + 255) / 256);
+    if (fp32) relax_kernel<float><<<g, 256, 0, st>>>(L, static_cast<float*>(f), z);
+    else relax_kernel<double><<<g, 256, 0, st>>>(L, static_cast<double*>(f), z);
+    return 1;
+}
+
 int launch_solid_forcing(void* f, bool fp32, const long long* ops, const std::vector<int>& level_off,
                          cudaStream_t st) {
     int n = 0;

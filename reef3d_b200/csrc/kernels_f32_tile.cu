@@ -1,15 +1,20 @@
 // FP32 form, 3D uniform grids: TMA-tiled fused stage kernels.
 //
-// A CTA owns a 64 x 8 (x, y) column of cells and marches a chunk of kc
+// A CTA owns a TX x TY (x, y) column of cells and marches a chunk of kc
 // z-planes.  Each plane of the stage input is staged once into shared memory
-// by one TMA box copy (72 x 14 floats: the tile plus its 3-cell x/y halo,
-// x rounded down to a 16-byte boundary) into a 16-slot ring guarded by
-// mbarriers; the ring holds the seven planes of the z stencil as well as the
-// planes being prefetched.  Every thread computes two x-adjacent cells with packed FP32x2
-// arithmetic (Blackwell FFMA2/FADD2/FMUL2).  The WENO5-HJ upwind side and
-// the Godunov branch of the reinitialisation are chosen with selects: the
-// plus-side derivative is the minus-side formula on the mirrored difference
-// sequence, so one evaluation per axis serves both sides.
+// by one TMA box copy ((TX+8) x (TY+6) floats: the tile plus its 3-cell x/y
+// halo, x rounded down to a 16-byte boundary) into a ring of RING slots
+// guarded by mbarriers; the ring holds the seven planes of the z stencil as
+// well as the planes being prefetched.  Every thread computes two
+// x-adjacent cells in each of RY consecutive rows with packed FP32x2
+// arithmetic (Blackwell FFMA2/FADD2/FMUL2); the rows of a thread are
+// independent chains of arithmetic and share their y-stencil loads.  The
+// WENO5-HJ upwind side and the Godunov branch of the reinitialisation are
+// chosen with selects: the plus-side derivative is the minus-side formula on
+// the mirrored difference sequence, so one evaluation per axis serves both
+// sides.  The tile shape, the rows per thread and the ring depth form a
+// configuration (TileCfg, kTileCfgs); the autotuner picks one per size
+// class, with the z chunk.
 //
 // Waits on the mbarriers are bounded: on a timeout the kernel raises the
 // instance's error flag, waits (bounded) for its copies in flight and
@@ -25,24 +30,7 @@ namespace r3d {
 
 namespace {
 
-constexpr int kTX = 64, kTY = 8, kThreads = 256;
-constexpr int kBoxX = kTX + 8, kBoxY = kTY + 6;
-constexpr int kRing = 16;          // plane boxes in shared memory (a power of two)
-constexpr int kSlotFloats = 1024;  // 72*14 = 1008 floats, padded to 4 KB
-constexpr unsigned kBoxBytes = kBoxX * kBoxY * 4;
 constexpr long long kSpin = 1ll << 22;
-// CTAs per SM the stage kernels are register-limited for (the ring takes
-// 64 KB of shared memory per CTA, so three fit an SM)
-#ifndef R3D_TILE_MINB_CONV
-#define R3D_TILE_MINB_CONV 3
-#endif
-#ifndef R3D_TILE_MINB_REINI
-#define R3D_TILE_MINB_REINI 3
-#endif
-// the batched persistent form (its per-item arguments sit in shared memory)
-#ifndef R3D_TILE_MINB_BATCH
-#define R3D_TILE_MINB_BATCH 3
-#endif
 
 // ------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -208,63 +196,117 @@ __device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, co
     return (float)(S - S * dn);  // -(S |grad| - S)
 }
 
-// One work item: the 64 x 8 column (bx, by) over planes [bz*kc, bz*kc+kc)
+// 3-input minimum / maximum (one instruction on sm_100)
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// One tile configuration: TX x TY cells per CTA (TX/2 threads per row
+// group, RY rows per thread), RING plane slots in shared memory, MINB CTAs
+// per SM the registers are limited for.
+template <int TX_, int TY_, int RY_, int RING_, int MINB_>
+struct TileCfg {
+    static constexpr int TX = TX_, TY = TY_, RY = RY_, RING = RING_, MINB = MINB_;
+    static constexpr int TPR = TX / 2;           // threads per row group
+    static constexpr int NT = TPR * (TY / RY);   // threads per CTA
+    static constexpr int NW = NT / 32;
+    static constexpr int BX = TX + 8, BY = TY + 6;
+    static constexpr int SLOT = (BX * BY + 31) / 32 * 32;  // floats per slot (128-byte aligned)
+    static constexpr unsigned BOX_BYTES = BX * BY * 4;
+    static_assert(NT % 32 == 0 && TY % RY == 0, "whole warps, whole row groups");
+    static_assert(RING >= 8, "the ring holds the 7-plane stencil and one plane in flight");
+    static_assert(BX <= 256 && BY <= 256 && (BX * 4) % 16 == 0, "TMA box limits");
+    static constexpr size_t smem() { return (size_t)RING * SLOT * 4 + RING * sizeof(uint64_t) + (RING + 2) * sizeof(int); }
+};
+
+// The configurations the library is built with (id = position).
+#define R3D_TILE_CFGS(X)        \
+    X(0, 64, 8, 1, 16, 3)       \
+    X(1, 64, 8, 2, 12, 4)       \
+    X(2, 64, 16, 2, 10, 2)      \
+    X(3, 32, 16, 2, 12, 4)      \
+    X(4, 128, 8, 2, 8, 2)       \
+    X(5, 64, 8, 1, 10, 4)
+
+#define R3D_CFG_TYPE(id, tx, ty, ry, ring, minb) using Cfg##id = TileCfg<tx, ty, ry, ring, minb>;
+R3D_TILE_CFGS(R3D_CFG_TYPE)
+#undef R3D_CFG_TYPE
+
+// One work item: the TX x TY column (bx, by) over planes [bz*kc, bz*kc+kc)
 // of one instance.  Returns false when a bounded wait gave up (the error
 // flag is raised and the copies in flight have been waited for).  The
 // item's volume partials (when `volume`) go to partial_out[0..1].  The
 // mbarriers are initialised at the start of the item and invalidated at its
 // end, so a persistent CTA can run items back to back.
 //
-// Shared memory is a ring of kRing plane boxes: the x and y stencils of
+// Shared memory is a ring of RING plane boxes: the x and y stencils of
 // plane k come from its box, the z stencil from the thread's own column in
 // the seven boxes k-3..k+3.  Each box has a "full" mbarrier (the TMA copy
-// landed).  After plane k the box of plane k-3 is refilled with plane k+13:
-// in the convection stages after a CTA barrier, in the reinitialisation
-// stages by the last warp to count itself out of the box (a per-box release
-// counter), so that warps there drift apart where their work differs
-// (interface-band cells in FP64) instead of meeting at a barrier every plane.
-template <bool REINI, int STAGE>
+// landed).  After plane k the box of plane k-3 is refilled with plane
+// k-3+RING by the last warp to count itself out of the box (a per-box
+// release counter), so that warps drift apart where their work differs
+// (interface-band cells in FP64, wall ghosts) instead of meeting at a CTA
+// barrier every plane.
+template <class C, bool REINI, int STAGE>
 __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArgs& a, int bx, int by, int bz,
                                           bool volume, unsigned char* smem_raw, double* red_a, double* red_b,
                                           double* partial_out) {
+    constexpr int RY = C::RY, BX = C::BX, RING = C::RING, SLOT = C::SLOT;
     float* ring = reinterpret_cast<float*>(smem_raw);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(ring + kRing * kSlotFloats);  // full
-    int* rel = reinterpret_cast<int*>(bar + kRing);                           // release counters
-    volatile int* s_abort = rel + kRing;
-    int* s_issued = rel + kRing + 1;                                          // last plane issued
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ring + RING * SLOT);  // full
+    int* rel = reinterpret_cast<int*>(bar + RING);                    // release counters
+    volatile int* s_abort = rel + RING;
+    int* s_issued = rel + RING + 1;  // last plane issued
 
     const Layout& L = a.L;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int i0 = bx * kTX + 2 * tx;
-    const int j = by * kTY + ty;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int tx = tid % C::TPR, tg = tid / C::TPR;
+    const int i0 = bx * C::TX + 2 * tx;
+    const int jb = by * C::TY + tg * RY;  // the thread's first row
     const int k0 = bz * a.kc;
     const int k1 = min(k0 + a.kc, L.nz);
-    const int xbox = bx * kTX + L.gx - 4;  // 16-byte aligned x start
-    const int ybox = by * kTY + L.gy - 3;
+    const int xbox = bx * C::TX + L.gx - 4;  // 16-byte aligned x start
+    const int ybox = by * C::TY + L.gy - 3;
     const int pfirst = k0 - 3;  // first plane staged (ring position 0)
     const int plast = k1 + 2;   // last plane staged
-    const bool act0 = i0 < L.nx && j < L.ny;
-    const bool act1 = i0 + 1 < L.nx && j < L.ny;
-    const long long col = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
-    const int own = (ty + 3) * kBoxX + 2 * tx + 4;  // the thread's two cells in a box
-    // wall ghost layers this thread writes on every plane (x, y faces)
-    const bool gxlo = act0 && i0 == 0;
-    const bool gxhi2 = act1 && i0 + 1 == L.nx - 1;  // second cell is the last one
-    const bool gxhi1 = act0 && !act1;                // first cell is the last one
-    const bool gylo = act0 && j == 0, gyhi = act0 && j == L.ny - 1;
-    const bool gside = gxlo || gxhi2 || gxhi1 || gylo || gyhi;
+    const int rowb = tg * RY;   // box row of the first y-stencil point of the thread's first row
+    bool act0[RY], act1[RY], gside[RY], gxlo[RY], gxhi1[RY], gxhi2[RY], gylo[RY], gyhi[RY];
+    long long col[RY];
+    int own[RY];  // the thread's two cells of row r in a box
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        const int j = jb + r;
+        act0[r] = i0 < L.nx && j < L.ny;
+        act1[r] = i0 + 1 < L.nx && j < L.ny;
+        col[r] = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
+        own[r] = (rowb + r + 3) * BX + 2 * tx + 4;
+        // wall ghost layers this thread writes on every plane (x, y faces)
+        gxlo[r] = act0[r] && i0 == 0;
+        gxhi2[r] = act1[r] && i0 + 1 == L.nx - 1;  // second cell is the last one
+        gxhi1[r] = act0[r] && !act1[r];             // first cell is the last one
+        gylo[r] = act0[r] && j == 0;
+        gyhi[r] = act0[r] && j == L.ny - 1;
+        gside[r] = gxlo[r] || gxhi2[r] || gxhi1[r] || gylo[r] || gyhi[r];
+    }
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kRing; ++s) {
+    if (tid == 0) {
+        for (int s = 0; s < RING; ++s) {
             mbar_init(bar + s, 1);
             rel[s] = 0;
         }
         *s_abort = 0;
         mbar_fence_init();
-        for (int p = pfirst; p <= min(pfirst + kRing - 1, plast); ++p) {
+        for (int p = pfirst; p <= min(pfirst + RING - 1, plast); ++p) {
             const int s = p - pfirst;
-            mbar_expect_tx(bar + s, kBoxBytes);
-            tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, p + L.gz);
+            mbar_expect_tx(bar + s, C::BOX_BYTES);
+            tma_load_3d(ring + s * SLOT, tmap, bar + s, xbox, ybox, p + L.gz);
             *s_issued = p;
         }
     }
@@ -283,216 +325,264 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
 
     const float vs = (float)*a.vscale;
     const float dtc = REINI ? a.dtr : (float)*a.dt;
-    long long c = (long long)(k0 + L.gz) * L.sz + col;
-    float2 wprev = make_float2(0.f, 0.f);
-    if (!REINI && act0)
-        wprev = act1 ? __ldg(reinterpret_cast<const float2*>(a.w + c - L.sz)) : make_float2(__ldg(a.w + c - L.sz), 0.f);
+    const long long c0 = (long long)(k0 + L.gz) * L.sz;
+    float2 wprev[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        wprev[r] = make_float2(0.f, 0.f);
+        if (!REINI && act0[r]) {
+            const float* wp = a.w + c0 + col[r] - L.sz;
+            wprev[r] = act1[r] ? __ldg(reinterpret_cast<const float2*>(wp)) : make_float2(__ldg(wp), 0.f);
+        }
+    }
     double vol_a = 0.0, vol_b = 0.0;
 
     // cell-local global operands of a plane (velocities, step start value),
-    // fetched one plane ahead so their latency overlaps the current plane
-    float2 nu = make_float2(0.f, 0.f), nv = nu, nvm = nu, nw = nu, nfn = nu;
-    float num = 0.f;
-    auto fetch = [&](long long cc) {
-        if (!act0) return;
-        if (!REINI) {
-            if (act1) {
-                nu = __ldg(reinterpret_cast<const float2*>(a.u + cc));
-                nv = __ldg(reinterpret_cast<const float2*>(a.v + cc));
-                nvm = __ldg(reinterpret_cast<const float2*>(a.v + cc - L.sy));
-                nw = __ldg(reinterpret_cast<const float2*>(a.w + cc));
-            } else {
-                nu.x = __ldg(a.u + cc);
-                nv.x = __ldg(a.v + cc);
-                nvm.x = __ldg(a.v + cc - L.sy);
-                nw.x = __ldg(a.w + cc);
+    // fetched one plane ahead so their latency overlaps the current plane;
+    // v on the face below row r is v of row r-1 for r > 0
+    float2 nu[RY], nv[RY], nw[RY], nfn[RY], nvm0;
+    float num[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        nu[r] = nv[r] = nw[r] = nfn[r] = make_float2(0.f, 0.f);
+        num[r] = 0.f;
+    }
+    nvm0 = make_float2(0.f, 0.f);
+    auto fetch = [&](long long cz) {
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            if (!act0[r]) continue;
+            const long long cc = cz + col[r];
+            if (!REINI) {
+                if (act1[r]) {
+                    nu[r] = __ldg(reinterpret_cast<const float2*>(a.u + cc));
+                    nv[r] = __ldg(reinterpret_cast<const float2*>(a.v + cc));
+                    nw[r] = __ldg(reinterpret_cast<const float2*>(a.w + cc));
+                    if (r == 0) nvm0 = __ldg(reinterpret_cast<const float2*>(a.v + cc - L.sy));
+                } else {
+                    nu[r].x = __ldg(a.u + cc);
+                    nv[r].x = __ldg(a.v + cc);
+                    nw[r].x = __ldg(a.w + cc);
+                    if (r == 0) nvm0.x = __ldg(a.v + cc - L.sy);
+                }
+                num[r] = __ldg(a.u + cc - 1);
             }
-            num = __ldg(a.u + cc - 1);
+            // the step start value may be this stage's output (stage 3): plain loads
+            if (STAGE != 1) nfn[r] = act1[r] ? *reinterpret_cast<const float2*>(a.fn + cc) : make_float2(a.fn[cc], 0.f);
         }
-        // the step start value may be this stage's output (stage 3): plain loads
-        if (STAGE != 1) nfn = act1 ? *reinterpret_cast<const float2*>(a.fn + cc) : make_float2(a.fn[cc], 0.f);
     };
-    fetch(c);
+    fetch(c0);
 
-    for (int k = k0; k < k1; ++k, c += L.sz) {
-        const int n = k - k0;  // ring position of plane k-3
-        {
-            const int nt = n + 6;  // plane k+3
-            ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + (nt & (kRing - 1)), (nt / kRing) & 1, spin));
+    int sb = 0;          // ring slot of position n = k - k0 (plane k-3)
+    int ws = 6, wp = 0;  // ring slot and phase parity of position n + 6 (plane k+3)
+    long long cz = c0;
+    for (int k = k0; k < k1; ++k, cz += L.sz) {
+        ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + ws, (uint32_t)wp, spin));
+        if (!ok) *s_abort = 1;
+        if (__any_sync(0xffffffffu, *s_abort != 0)) break;
+        const float* slot[7];
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+            int s = sb + m;
+            if (RING < 16 || (RING & (RING - 1))) s -= s >= RING ? RING : 0;
+            else s &= RING - 1;
+            slot[m] = ring + s * SLOT;
         }
-        if (REINI) {
-            if (!ok) *s_abort = 1;
-            if (__any_sync(0xffffffffu, *s_abort != 0)) break;
-        }
-        const float* sl = ring + ((n + 3) & (kRing - 1)) * kSlotFloats;  // plane k
+        const float* sl = slot[3];  // plane k
 
-        // x stencil: the row's columns 2tx .. 2tx+9 (the cells at 2tx+4, 2tx+5)
-        float xv[10];
+        // y stencil values of all RY rows (rows rowb .. rowb+RY+5 of the box)
+        float2 DY[RY + 5];
+        float2 fy2[RY], fy4[RY];
         {
-            const float* r = sl + (ty + 3) * kBoxX + 2 * tx;
+            float2 fy[RY + 6];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                const float2 t = *reinterpret_cast<const float2*>(r + 2 * q);
-                xv[2 * q] = t.x;
-                xv[2 * q + 1] = t.y;
-            }
+            for (int m = 0; m < RY + 6; ++m) fy[m] = *reinterpret_cast<const float2*>(sl + (rowb + m) * BX + 2 * tx + 4);
+#pragma unroll
+            for (int m = 0; m < RY + 5; ++m) DY[m] = sub2(fy[m + 1], fy[m]);
+#pragma unroll
+            for (int r = 0; r < RY; ++r) { fy2[r] = fy[r + 2]; fy4[r] = fy[r + 4]; }
         }
-        float2 Dx[6], Dy[6], Dz[6];
-#pragma unroll
-        for (int m = 0; m < 6; ++m) Dx[m] = make_float2(xv[m + 2] - xv[m + 1], xv[m + 3] - xv[m + 2]);
-        float2 fy2, fy4, fz2, fz4;
-        {
-            float2 fy[7], fz[7];
-#pragma unroll
-            for (int m = 0; m < 7; ++m) {
-                fy[m] = *reinterpret_cast<const float2*>(sl + (ty + m) * kBoxX + 2 * tx + 4);
-                fz[m] = *reinterpret_cast<const float2*>(ring + ((n + m) & (kRing - 1)) * kSlotFloats + own);
-            }
-            diffs2(fy, Dy);
-            diffs2(fz, Dz);
-            fy2 = fy[2]; fy4 = fy[4]; fz2 = fz[2]; fz4 = fz[4];
-        }
-        const float2 f0 = make_float2(xv[4], xv[5]);
-
-        float2 Lc;
         // this plane's operands, then the next plane's loads in flight
         // through the whole computation of this one
-        const float2 fn = nfn;
-        const float2 uc = nu, vc = nv, vm = nvm, wc = nw;
-        const float um = num;
-        if (k + 1 < k1) fetch(c + L.sz);
-        if (!REINI) {
-            const float2 h2 = f2(0.5f * vs);
-            const float2 ia = mul2(h2, add2(make_float2(um, uc.x), uc));
-            const float2 ja = mul2(h2, add2(vc, vm));
-            const float2 ka = mul2(h2, add2(wc, wprev));
-            wprev = wc;
-            const float2 gx = mul2(f2(a.rh[0]), deriv2(Dx, ia.x < 0.f, ia.y < 0.f, a.eps[0]));
-            const float2 gy = mul2(f2(a.rh[1]), deriv2(Dy, ja.x < 0.f, ja.y < 0.f, a.eps[1]));
-            const float2 gz = mul2(f2(a.rh[2]), deriv2(Dz, ka.x < 0.f, ka.y < 0.f, a.eps[2]));
-            Lc = mul2(f2(-1.f), fma2(ka, gz, fma2(ja, gy, mul2(ia, gx))));
-        } else {
-            // Godunov selection per axis (src/reinidisc_f.cpp:70-109) on the
-            // backward and forward differences D[2], D[3] times the sign s
-            // (the grid factor 1/h > 0 leaves every test unchanged):
-            //   upwind minus side: m > 0 && p > -m, i.e. m > 0 && m + p > 0
-            //   upwind plus side:  p < 0 && m < -p, i.e. p < 0 && m + p < 0
-            // (the sign of a rounded sum is the sign of the exact sum)
-            const float2 sg = make_float2(fabsf(f0.x) < 1.0e-8f ? 1.f : (f0.x > 0.f ? 1.f : -1.f),
-                                          fabsf(f0.y) < 1.0e-8f ? 1.f : (f0.y > 0.f ? 1.f : -1.f));
-            const float2* ax[3] = {Dx, Dy, Dz};
-            float2 g2 = make_float2(0.f, 0.f);
+        float2 fnr[RY], ucr[RY], vcr[RY], wcr[RY], vm0;
+        float umr[RY];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const float2* D = ax[d];
-                const float2 ms = mul2(D[2], sg), ps = mul2(D[3], sg);
-                const float2 sum = add2(ms, ps);
-                const bool c1x = ms.x > 0.f && sum.x > 0.f, c2x = ps.x < 0.f && sum.x < 0.f;
-                const bool c1y = ms.y > 0.f && sum.y > 0.f, c2y = ps.y < 0.f && sum.y < 0.f;
-                float2 g = mul2(f2(a.rh[d]), deriv2(D, c2x, c2y, a.eps[d]));
-                g.x = (c1x || c2x) ? g.x : 0.f;
-                g.y = (c1y || c2y) ? g.y : 0.f;
-                g2 = fma2(g, g, g2);
+        for (int r = 0; r < RY; ++r) { fnr[r] = nfn[r]; ucr[r] = nu[r]; vcr[r] = nv[r]; wcr[r] = nw[r]; umr[r] = num[r]; }
+        vm0 = nvm0;
+        if (k + 1 < k1) fetch(cz + L.sz);
+
+        float2 f0[RY], Lc[RY];
+        bool bandx[RY], bandy[RY];
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            // x stencil: the row's columns 2tx .. 2tx+9 (the cells at 2tx+4, 2tx+5)
+            float xv[10];
+            {
+                const float* rp = sl + (rowb + r + 3) * BX + 2 * tx;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const float2 t = *reinterpret_cast<const float2*>(rp + 2 * q);
+                    xv[2 * q] = t.x;
+                    xv[2 * q + 1] = t.y;
+                }
             }
-            const float2 dn = make_float2(sqrt_approx(g2.x), sqrt_approx(g2.y));
-            const float2 dl = f2(a.deltax);
-            const float2 den = fma2(mul2(mul2(dn, dn), dl), dl, mul2(f0, f0));
-            float2 S = mul2(f0, make_float2(rsqrtf(den.x), rsqrtf(den.y)));
-            if (S.x != S.x) S.x = 1.f;
-            if (S.y != S.y) S.y = 1.f;
-            Lc = sub2(S, mul2(S, dn));  // -(S |grad| - S)
-            // interface band: the 7-point stencil changes sign, i.e. neither
-            // all values >= 0 (min >= 0) nor all < 0 (max < 0)
-            const float lox = fminf(fminf(fminf(f0.x, xv[3]), fminf(xv[5], fy2.x)), fminf(fminf(fy4.x, fz2.x), fz4.x));
-            const float hix = fmaxf(fmaxf(fmaxf(f0.x, xv[3]), fmaxf(xv[5], fy2.x)), fmaxf(fmaxf(fy4.x, fz2.x), fz4.x));
-            const float loy = fminf(fminf(fminf(f0.y, xv[4]), fminf(xv[6], fy2.y)), fminf(fminf(fy4.y, fz2.y), fz4.y));
-            const float hiy = fmaxf(fmaxf(fmaxf(f0.y, xv[4]), fmaxf(xv[6], fy2.y)), fmaxf(fmaxf(fy4.y, fz2.y), fz4.y));
-            const bool bandx = lox < 0.f && hix >= 0.f, bandy = loy < 0.f && hiy >= 0.f;
-            if (a.f49 == 0) {
-                if (bandx) Lc.x = 0.f;  // src/reinidisc_fsf.cpp:70-72
-                if (bandy) Lc.y = 0.f;
-            } else if (a.band64) {
-                // The warp's band cells (at most 64) are dealt out to its
-                // lanes, one FP64 evaluation each, stencils from shared
-                // memory; results go back to the owning lanes by shuffles.
-                const unsigned mx = __ballot_sync(0xffffffffu, act0 && bandx);
-                const unsigned my = __ballot_sync(0xffffffffu, act1 && bandy);
+            float2 Dx[6], Dz[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) Dx[m] = make_float2(xv[m + 2] - xv[m + 1], xv[m + 3] - xv[m + 2]);
+            float2 fz2, fz4;
+            {
+                float2 fz[7];
+#pragma unroll
+                for (int m = 0; m < 7; ++m) fz[m] = *reinterpret_cast<const float2*>(slot[m] + own[r]);
+                diffs2(fz, Dz);
+                fz2 = fz[2];
+                fz4 = fz[4];
+            }
+            const float2* Dy = DY + r;
+            f0[r] = make_float2(xv[4], xv[5]);
+            bandx[r] = bandy[r] = false;
+            if (!REINI) {
+                const float2 h2 = f2(0.5f * vs);
+                const float2 vm = r == 0 ? vm0 : vcr[r - 1];
+                const float2 ia = mul2(h2, add2(make_float2(umr[r], ucr[r].x), ucr[r]));
+                const float2 ja = mul2(h2, add2(vcr[r], vm));
+                const float2 ka = mul2(h2, add2(wcr[r], wprev[r]));
+                wprev[r] = wcr[r];
+                const float2 gx = mul2(f2(a.rh[0]), deriv2(Dx, ia.x < 0.f, ia.y < 0.f, a.eps[0]));
+                const float2 gy = mul2(f2(a.rh[1]), deriv2(Dy, ja.x < 0.f, ja.y < 0.f, a.eps[1]));
+                const float2 gz = mul2(f2(a.rh[2]), deriv2(Dz, ka.x < 0.f, ka.y < 0.f, a.eps[2]));
+                Lc[r] = mul2(f2(-1.f), fma2(ka, gz, fma2(ja, gy, mul2(ia, gx))));
+            } else {
+                // Godunov selection per axis (src/reinidisc_f.cpp:70-109) on the
+                // backward and forward differences D[2], D[3] times the sign s
+                // (the grid factor 1/h > 0 leaves every test unchanged):
+                //   upwind minus side: m > 0 && p > -m, i.e. m > 0 && m + p > 0
+                //   upwind plus side:  p < 0 && m < -p, i.e. p < 0 && m + p < 0
+                // (the sign of a rounded sum is the sign of the exact sum)
+                const float2 fc = f0[r];
+                const float2 sg = make_float2(fabsf(fc.x) < 1.0e-8f ? 1.f : (fc.x > 0.f ? 1.f : -1.f),
+                                              fabsf(fc.y) < 1.0e-8f ? 1.f : (fc.y > 0.f ? 1.f : -1.f));
+                const float2* ax[3] = {Dx, Dy, Dz};
+                float2 g2 = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const float2* D = ax[d];
+                    const float2 ms = mul2(D[2], sg), ps = mul2(D[3], sg);
+                    const float2 sum = add2(ms, ps);
+                    const bool c1x = ms.x > 0.f && sum.x > 0.f, c2x = ps.x < 0.f && sum.x < 0.f;
+                    const bool c1y = ms.y > 0.f && sum.y > 0.f, c2y = ps.y < 0.f && sum.y < 0.f;
+                    float2 g = mul2(f2(a.rh[d]), deriv2(D, c2x, c2y, a.eps[d]));
+                    g.x = (c1x || c2x) ? g.x : 0.f;
+                    g.y = (c1y || c2y) ? g.y : 0.f;
+                    g2 = fma2(g, g, g2);
+                }
+                const float2 dn = make_float2(sqrt_approx(g2.x), sqrt_approx(g2.y));
+                const float2 dl = f2(a.deltax);
+                const float2 den = fma2(mul2(mul2(dn, dn), dl), dl, mul2(fc, fc));
+                float2 S = mul2(fc, make_float2(rsqrtf(den.x), rsqrtf(den.y)));
+                if (S.x != S.x) S.x = 1.f;
+                if (S.y != S.y) S.y = 1.f;
+                Lc[r] = sub2(S, mul2(S, dn));  // -(S |grad| - S)
+                // interface band: the 7-point stencil changes sign, i.e. neither
+                // all values >= 0 (min >= 0) nor all < 0 (max < 0)
+                const float lox = min3f(min3f(fc.x, xv[3], xv[5]), min3f(fy2[r].x, fy4[r].x, fz2.x), fz4.x);
+                const float hix = max3f(max3f(fc.x, xv[3], xv[5]), max3f(fy2[r].x, fy4[r].x, fz2.x), fz4.x);
+                const float loy = min3f(min3f(fc.y, xv[4], xv[6]), min3f(fy2[r].y, fy4[r].y, fz2.y), fz4.y);
+                const float hiy = max3f(max3f(fc.y, xv[4], xv[6]), max3f(fy2[r].y, fy4[r].y, fz2.y), fz4.y);
+                bandx[r] = lox < 0.f && hix >= 0.f;
+                bandy[r] = loy < 0.f && hiy >= 0.f;
+                if (a.f49 == 0) {
+                    if (bandx[r]) Lc[r].x = 0.f;  // src/reinidisc_fsf.cpp:70-72
+                    if (bandy[r]) Lc[r].y = 0.f;
+                }
+            }
+        }
+        if (REINI && a.f49 != 0 && a.band64) {
+            // The warp's band cells of row r (at most 64) are dealt out to
+            // its lanes, one FP64 evaluation each, stencils from shared
+            // memory; results go back to the owning lanes by shuffles.
+#pragma unroll
+            for (int r = 0; r < RY; ++r) {
+                const unsigned mx = __ballot_sync(0xffffffffu, act0[r] && bandx[r]);
+                const unsigned my = __ballot_sync(0xffffffffu, act1[r] && bandy[r]);
                 if (mx | my) {
                     const int cx = __popc(mx), total = cx + __popc(my);
-                    const unsigned below = (1u << tx) - 1u;
+                    const unsigned below = (1u << lane) - 1u;
                     const int bxi = __popc(mx & below), byi = cx + __popc(my & below);
                     for (int base = 0; base < total; base += 32) {
                         float res = 0.f;
-                        const int b = base + tx;
+                        const int b = base + lane;
                         if (b < total) {
                             const bool isy = b >= cx;
                             // the lane holding the (b or b-cx)-th set bit of the mask
                             unsigned msk = isy ? my : mx;
                             for (int q = isy ? b - cx : b; q > 0; --q) msk &= msk - 1u;
                             const int src = __ffs(msk) - 1;
-                            const int e = isy ? 1 : 0;
-                            const float* r = sl + (ty + 3) * kBoxX + 2 * src + e;
-                            const int o = (ty + 3) * kBoxX + 2 * src + 4 + e;
+                            const int st = (tid & ~31) + src;  // the source lane's thread
+                            const int sx = 2 * (st % C::TPR) + (isy ? 1 : 0);
+                            const int srow = (st / C::TPR) * RY + r;  // its y-stencil base row
                             float X[7], Y[7], Z[7];
 #pragma unroll
                             for (int m = 0; m < 7; ++m) {
-                                X[m] = r[m + 1];
-                                Y[m] = sl[(ty + m) * kBoxX + 2 * src + 4 + e];
-                                Z[m] = ring[((n + m) & (kRing - 1)) * kSlotFloats + o];
+                                X[m] = sl[(srow + 3) * BX + sx + 1 + m];
+                                Y[m] = sl[(srow + m) * BX + sx + 4];
+                                Z[m] = slot[m][(srow + 3) * BX + sx + 4];
                             }
                             res = reini_cell_fp64(X, Y, Z, a.rh[0], a.rh[1], a.rh[2], a.deltax);
                         }
                         const float rx = __shfl_sync(0xffffffffu, res, (bxi - base) & 31);
                         const float ry = __shfl_sync(0xffffffffu, res, (byi - base) & 31);
-                        if (act0 && bandx && bxi >= base && bxi < base + 32) Lc.x = rx;
-                        if (act1 && bandy && byi >= base && byi < base + 32) Lc.y = ry;
+                        if (act0[r] && bandx[r] && bxi >= base && bxi < base + 32) Lc[r].x = rx;
+                        if (act1[r] && bandy[r] && byi >= base && byi < base + 32) Lc[r].y = ry;
                     }
                 }
             }
         }
 
-        // reinitialisation: the warp's shared-memory reads of this plane are
-        // done, so it counts itself out of the box of plane k-3 (before its
-        // global stores and loads, so the fence waits on nothing in flight),
-        // and the last warp out refills the box with plane k+13
-        if (REINI) __syncwarp();
-        if (REINI && tx == 0) {
-            const int s = n & (kRing - 1);
+        // the warp's shared-memory reads of this plane are done, so it counts
+        // itself out of the box of plane k-3 (before its global stores and
+        // loads, so the fence waits on nothing in flight), and the last warp
+        // out refills the box with plane k-3+RING
+        __syncwarp();
+        if (lane == 0) {
             __threadfence_block();
-            if (atomicAdd(rel + s, 1) == kThreads / 32 - 1) {
+            if (atomicAdd(rel + sb, 1) == C::NW - 1) {
                 __threadfence_block();
-                rel[s] = 0;
-                if (k + kRing - 3 <= plast) {
+                rel[sb] = 0;
+                if (k - 3 + RING <= plast) {
                     fence_proxy_async();
-                    mbar_expect_tx(bar + s, kBoxBytes);
-                    tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, k + kRing - 3 + L.gz);
-                    atomicMax(s_issued, k + kRing - 3);
+                    mbar_expect_tx(bar + sb, C::BOX_BYTES);
+                    tma_load_3d(ring + sb * SLOT, tmap, bar + sb, xbox, ybox, k - 3 + RING + L.gz);
+                    atomicMax(s_issued, k - 3 + RING);
                 }
             }
         }
 
-        // RK combine (src/levelset_RK3.cpp:121-156, src/reini_RK3.cpp:118-135)
-        float2 val;
-        const float2 sdl = fma2(f2(dtc), Lc, f0);  // stage input + dt L
-        if (STAGE == 1) {
-            val = sdl;
-        } else {
-            if (STAGE == 2) val = fma2(f2(0.75f), fn, mul2(f2(0.25f), sdl));
-            else val = fma2(f2(1.0f / 3.0f), fn, mul2(f2(2.0f / 3.0f), sdl));
-        }
-        if (act0) {
-            if (act1) *reinterpret_cast<float2*>(a.out + c) = val;
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            if (!act0[r]) continue;
+            // RK combine (src/levelset_RK3.cpp:121-156, src/reini_RK3.cpp:118-135)
+            float2 val;
+            const float2 sdl = fma2(f2(dtc), Lc[r], f0[r]);  // stage input + dt L
+            if (STAGE == 1) {
+                val = sdl;
+            } else {
+                if (STAGE == 2) val = fma2(f2(0.75f), fnr[r], mul2(f2(0.25f), sdl));
+                else val = fma2(f2(1.0f / 3.0f), fnr[r], mul2(f2(2.0f / 3.0f), sdl));
+            }
+            const long long c = cz + col[r];
+            if (act1[r]) *reinterpret_cast<float2*>(a.out + c) = val;
             else a.out[c] = val.x;
             // wall ghost copies (src/gc_neumann.cpp:29-54)
-            if (gside || k == 0 || k == L.nz - 1) {
-                if (gxlo) { a.out[c - 1] = val.x; a.out[c - 2] = val.x; a.out[c - 3] = val.x; }
-                if (gxhi2) { a.out[c + 2] = val.y; a.out[c + 3] = val.y; a.out[c + 4] = val.y; }
-                if (gxhi1) { a.out[c + 1] = val.x; a.out[c + 2] = val.x; a.out[c + 3] = val.x; }
-                const int nw = act1 ? 2 : 1;
-                if (gylo)
+            if (gside[r] || k == 0 || k == L.nz - 1) {
+                if (gxlo[r]) { a.out[c - 1] = val.x; a.out[c - 2] = val.x; a.out[c - 3] = val.x; }
+                if (gxhi2[r]) { a.out[c + 2] = val.y; a.out[c + 3] = val.y; a.out[c + 4] = val.y; }
+                if (gxhi1[r]) { a.out[c + 1] = val.x; a.out[c + 2] = val.x; a.out[c + 3] = val.x; }
+                const int nw = act1[r] ? 2 : 1;
+                if (gylo[r])
                     for (int q = 1; q <= 3; ++q)
                         for (int e = 0; e < nw; ++e) a.out[c - q * L.sy + e] = e ? val.y : val.x;
-                if (gyhi)
+                if (gyhi[r])
                     for (int q = 1; q <= 3; ++q)
                         for (int e = 0; e < nw; ++e) a.out[c + q * L.sy + e] = e ? val.y : val.x;
                 if (k == 0 && !(L.io & kHaloZLo))  // a slab face's ghosts come from the neighbour
@@ -505,7 +595,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             if (volume) {
                 // smoothed Heaviside in FP64 (src/fluid_update_fsf.cpp:50-71)
                 const double PI_REF = 3.14159265359;
-                const int nw = act1 ? 2 : 1;
+                const int nw = act1[r] ? 2 : 1;
                 for (int e = 0; e < nw; ++e) {
                     const double ph = e ? val.y : val.x;
                     double H = 0.0;
@@ -518,32 +608,22 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             }
         }
 
-        if (!REINI) {
-            // convection (the same work in every warp): one CTA barrier per
-            // plane, after which thread 0 refills the box of plane k-3
-            if (__syncthreads_or(!ok || *s_abort != 0)) {
-                if (threadIdx.x == 0) *s_abort = 1;
-                break;
-            }
-            if (threadIdx.x == 0 && k + kRing - 3 <= plast) {
-                const int s = n & (kRing - 1);
-                fence_proxy_async();
-                mbar_expect_tx(bar + s, kBoxBytes);
-                tma_load_3d(ring + s * kSlotFloats, tmap, bar + s, xbox, ybox, k + kRing - 3 + L.gz);
-                *s_issued = k + kRing - 3;
-            }
+        sb = sb + 1 == RING ? 0 : sb + 1;
+        if (++ws == RING) {
+            ws = 0;
+            wp ^= 1;
         }
     }
     __syncthreads();
     const bool aborted = *s_abort != 0;
 
     if (aborted) {
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             atomicExch(a.err, 1);
             // wait (bounded) for every copy still in flight before leaving
             for (int p = pfirst; p <= *s_issued; ++p) {
                 const int q = p - pfirst;
-                mbar_wait_bounded(bar + (q & (kRing - 1)), (q / kRing) & 1);
+                mbar_wait_bounded(bar + (q % RING), (uint32_t)((q / RING) & 1));
             }
         }
         return false;
@@ -553,30 +633,30 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
             vol_a += __shfl_down_sync(0xffffffffu, vol_a, o);
             vol_b += __shfl_down_sync(0xffffffffu, vol_b, o);
         }
-        if (tx == 0) { red_a[ty] = vol_a; red_b[ty] = vol_b; }
+        if (lane == 0) { red_a[tid >> 5] = vol_a; red_b[tid >> 5] = vol_b; }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            double sa = 0.0, sb = 0.0;
-            for (int q = 0; q < kThreads / 32; ++q) { sa += red_a[q]; sb += red_b[q]; }
+        if (tid == 0) {
+            double sa = 0.0, sb2 = 0.0;
+            for (int q = 0; q < C::NW; ++q) { sa += red_a[q]; sb2 += red_b[q]; }
             partial_out[0] = sa;
-            partial_out[1] = sb;
+            partial_out[1] = sb2;
         }
     }
     // every wait of the item has completed: retire the barriers
     __syncthreads();
-    if (threadIdx.x == 0)
-        for (int s = 0; s < kRing; ++s) mbar_inval(bar + s);
+    if (tid == 0)
+        for (int s = 0; s < RING; ++s) mbar_inval(bar + s);
     __syncthreads();
     return true;
 }
 
-template <bool REINI, int STAGE, bool VOLUME>
-__global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
+template <class C, bool REINI, int STAGE, bool VOLUME>
+__global__ void __launch_bounds__(C::NT, C::MINB) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
+    __shared__ double red_a[C::NW], red_b[C::NW];
     const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    tile_item<REINI, STAGE>(&tmap, a, blockIdx.x, blockIdx.y, blockIdx.z, VOLUME, smem_raw, red_a, red_b,
-                            a.partial + 2 * b);
+    tile_item<C, REINI, STAGE>(&tmap, a, blockIdx.x, blockIdx.y, blockIdx.z, VOLUME, smem_raw, red_a, red_b,
+                               a.partial + 2 * b);
 }
 
 // Persistent batched form: CTAs take the work items of all tiled members
@@ -586,14 +666,14 @@ __global__ void __launch_bounds__(kThreads, REINI ? R3D_TILE_MINB_REINI : R3D_TI
 // last CTA to leave resets the counter pair work[0..1] for the next launch
 // on the stream.  Reinitialisation pseudo-step q is skipped by members with
 // f44 <= q; the last stage of a member's step adds its volume partials.
-template <bool REINI, int STAGE>
-__global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kernel(const TiledMember* __restrict__ members,
-                                                                 const CUtensorMap* __restrict__ maps,
-                                                                 const long long* __restrict__ tile0, int nm,
-                                                                 int q, double* __restrict__ vol_part,
-                                                                 unsigned* __restrict__ work) {
+template <class C, bool REINI, int STAGE>
+__global__ void __launch_bounds__(C::NT, C::MINB) batch_tile_kernel(const TiledMember* __restrict__ members,
+                                                                    const CUtensorMap* __restrict__ maps,
+                                                                    const long long* __restrict__ tile0, int nm,
+                                                                    int q, double* __restrict__ vol_part,
+                                                                    unsigned* __restrict__ work) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ double red_a[kThreads / 32], red_b[kThreads / 32];
+    __shared__ double red_a[C::NW], red_b[C::NW];
     __shared__ TileArgs sa;
     __shared__ int s_member;
     __shared__ long long s_t;
@@ -625,15 +705,15 @@ __global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kern
         }
         const bool volume = STAGE == 3 && (REINI ? q == f44 - 1 : f44 == 0);
         const long long lt = t - tile0[m];
-        const int ntx = (sa.L.nx + kTX - 1) / kTX, nty = (sa.L.ny + kTY - 1) / kTY;
+        const int ntx = (sa.L.nx + C::TX - 1) / C::TX, nty = (sa.L.ny + C::TY - 1) / C::TY;
         const int bx = (int)(lt % ntx);
         const int by = (int)((lt / ntx) % nty);
         const int bz = (int)(lt / ((long long)ntx * nty));
         // the item's arguments in a thread-local copy: the plane loop reads
         // them across CTA barriers, after which shared memory would be reread
         const TileArgs a = sa;
-        if (!tile_item<REINI, STAGE>(maps + 3 * m + (STAGE - 1), a, bx, by, bz, volume, smem_raw, red_a, red_b,
-                                     vol_part + 2 * t))
+        if (!tile_item<C, REINI, STAGE>(maps + 3 * m + (STAGE - 1), a, bx, by, bz, volume, smem_raw, red_a, red_b,
+                                        vol_part + 2 * t))
             break;
     }
     if (threadIdx.x == 0) {
@@ -648,10 +728,11 @@ __global__ void __launch_bounds__(kThreads, R3D_TILE_MINB_BATCH) batch_tile_kern
 
 // Face maxima over the cells of one item (x faces 0..nx-2, y 0..ny-2, z
 // 0..nz-2, src/ietimestep.cpp:72-88) for every tiled member's item.
-__global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMember* __restrict__ members,
-                                                                   const long long* __restrict__ tile0, int nm,
-                                                                   double* __restrict__ vmax_part) {
-    __shared__ unsigned s[3][kThreads / 32];
+template <class C>
+__global__ void __launch_bounds__(C::NT) batch_tile_vmax_kernel(const TiledMember* __restrict__ members,
+                                                                const long long* __restrict__ tile0, int nm,
+                                                                double* __restrict__ vmax_part) {
+    __shared__ unsigned s[3][C::NW];
     const long long nt = tile0[nm];
     for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
         int lo = 0, hi = nm - 1;
@@ -663,15 +744,16 @@ __global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMe
         const TileArgs& a = members[lo].args;
         const Layout& L = a.L;
         const long long lt = t - tile0[lo];
-        const int ntx = (L.nx + kTX - 1) / kTX, nty = (L.ny + kTY - 1) / kTY;
+        const int ntx = (L.nx + C::TX - 1) / C::TX, nty = (L.ny + C::TY - 1) / C::TY;
         const int bx = (int)(lt % ntx), by = (int)((lt / ntx) % nty), bz = (int)(lt / ((long long)ntx * nty));
-        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-        const int j = by * kTY + ty;
-        const int i0 = bx * kTX + 2 * tx;
+        const int tx = threadIdx.x % C::TPR, tg = threadIdx.x / C::TPR;
+        const int i0 = bx * C::TX + 2 * tx;
         const int k0 = bz * a.kc, k1 = min(k0 + a.kc, L.nz);
         // |x| compared as the float's bit pattern with the sign cleared (exact)
         unsigned mu = 0u, mv = 0u, mw = 0u;
-        if (j < L.ny && i0 < L.nx) {
+        for (int r = 0; r < C::RY; ++r) {
+            const int j = by * C::TY + tg * C::RY + r;
+            if (j >= L.ny || i0 >= L.nx) continue;
             const bool two = i0 + 1 < L.nx;
             const long long col = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
             for (int k = k0; k < k1; ++k) {
@@ -695,10 +777,11 @@ __global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMe
         mu = __reduce_max_sync(0xffffffffu, mu);
         mv = __reduce_max_sync(0xffffffffu, mv);
         mw = __reduce_max_sync(0xffffffffu, mw);
-        if (tx == 0) { s[0][ty] = mu; s[1][ty] = mv; s[2][ty] = mw; }
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) { s[0][w] = mu; s[1][w] = mv; s[2][w] = mw; }
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int q = 1; q < kThreads / 32; ++q) { mu = max(mu, s[0][q]); mv = max(mv, s[1][q]); mw = max(mw, s[2][q]); }
+            for (int q = 1; q < C::NW; ++q) { mu = max(mu, s[0][q]); mv = max(mv, s[1][q]); mw = max(mw, s[2][q]); }
             vmax_part[3 * t] = (double)__uint_as_float(mu);
             vmax_part[3 * t + 1] = (double)__uint_as_float(mv);
             vmax_part[3 * t + 2] = (double)__uint_as_float(mw);
@@ -710,53 +793,51 @@ __global__ void __launch_bounds__(kThreads) batch_tile_vmax_kernel(const TiledMe
 // The ring needs more than the default 48 KB of dynamic shared memory, and a
 // full shared-memory carveout lets several CTAs share an SM.
 template <typename K>
-bool tile_attr(K kernel, int bytes) {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess &&
+bool tile_attr(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess &&
            cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
 }
 
-}  // namespace
+template <class C>
+bool cfg_prepare() {
+    const size_t b = C::smem();
+    return tile_attr(tile_kernel<C, false, 1, false>, b) && tile_attr(tile_kernel<C, false, 2, false>, b) &&
+           tile_attr(tile_kernel<C, false, 3, false>, b) && tile_attr(tile_kernel<C, false, 1, true>, b) &&
+           tile_attr(tile_kernel<C, false, 2, true>, b) && tile_attr(tile_kernel<C, false, 3, true>, b) &&
+           tile_attr(tile_kernel<C, true, 1, false>, b) && tile_attr(tile_kernel<C, true, 2, false>, b) &&
+           tile_attr(tile_kernel<C, true, 3, false>, b) && tile_attr(tile_kernel<C, true, 1, true>, b) &&
+           tile_attr(tile_kernel<C, true, 2, true>, b) && tile_attr(tile_kernel<C, true, 3, true>, b) &&
+           tile_attr(batch_tile_kernel<C, false, 1>, b) && tile_attr(batch_tile_kernel<C, false, 2>, b) &&
+           tile_attr(batch_tile_kernel<C, false, 3>, b) && tile_attr(batch_tile_kernel<C, true, 1>, b) &&
+           tile_attr(batch_tile_kernel<C, true, 2>, b) && tile_attr(batch_tile_kernel<C, true, 3>, b);
+}
 
-int tile_ctas_per_sm(bool reini) { return reini ? R3D_TILE_MINB_REINI : R3D_TILE_MINB_CONV; }
-int batch_tile_ctas_per_sm() { return R3D_TILE_MINB_BATCH; }
-
-// Sets the attributes of every instantiation once per device.
-bool tile_prepare() {
-    static bool done[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return false;
-    if (dev >= 0 && dev < 64 && done[dev]) return true;
-    const int b = (int)tile_smem_bytes();
-    const bool ok =
-        tile_attr(tile_kernel<false, 1, false>, b) && tile_attr(tile_kernel<false, 2, false>, b) &&
-        tile_attr(tile_kernel<false, 3, false>, b) && tile_attr(tile_kernel<false, 1, true>, b) &&
-        tile_attr(tile_kernel<false, 2, true>, b) && tile_attr(tile_kernel<false, 3, true>, b) &&
-        tile_attr(tile_kernel<true, 1, false>, b) && tile_attr(tile_kernel<true, 2, false>, b) &&
-        tile_attr(tile_kernel<true, 3, false>, b) && tile_attr(tile_kernel<true, 1, true>, b) &&
-        tile_attr(tile_kernel<true, 2, true>, b) && tile_attr(tile_kernel<true, 3, true>, b) &&
-        tile_attr(batch_tile_kernel<false, 1>, b) && tile_attr(batch_tile_kernel<false, 2>, b) &&
-        tile_attr(batch_tile_kernel<false, 3>, b) && tile_attr(batch_tile_kernel<true, 1>, b) &&
-        tile_attr(batch_tile_kernel<true, 2>, b) && tile_attr(batch_tile_kernel<true, 3>, b);
-    if (!ok) {
-        cudaGetLastError();
-        return false;
+template <class C>
+void launch_stage_cfg(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume,
+                      cudaStream_t st) {
+    const dim3 grid((a.L.nx + C::TX - 1) / C::TX, (a.L.ny + C::TY - 1) / C::TY, (a.L.nz + a.kc - 1) / a.kc);
+    const dim3 block(C::NT);
+    const size_t sm = C::smem();
+#define R3D_TL(R, S, V) tile_kernel<C, R, S, V><<<grid, block, sm, st>>>(map, a)
+    if (reini) {
+        if (stage == 1) { if (volume) R3D_TL(true, 1, true); else R3D_TL(true, 1, false); }
+        else if (stage == 2) { if (volume) R3D_TL(true, 2, true); else R3D_TL(true, 2, false); }
+        else { if (volume) R3D_TL(true, 3, true); else R3D_TL(true, 3, false); }
+    } else {
+        if (stage == 1) { if (volume) R3D_TL(false, 1, true); else R3D_TL(false, 1, false); }
+        else if (stage == 2) { if (volume) R3D_TL(false, 2, true); else R3D_TL(false, 2, false); }
+        else { if (volume) R3D_TL(false, 3, true); else R3D_TL(false, 3, false); }
     }
-    if (dev >= 0 && dev < 64) done[dev] = true;
-    return true;
+#undef R3D_TL
 }
 
-long long tile_items_of(const Layout& L, int kc) {
-    const dim3 g = tile_grid(L, kc);
-    return (long long)g.x * g.y * g.z;
-}
-
-int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
-                            bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
-                            cudaStream_t st) {
-    tile_prepare();  // a failure here makes the launch below fail, which the caller reports
-    const size_t sm = tile_smem_bytes();
-    const dim3 g(grid), block(kThreads);
-#define R3D_BT(R, S) batch_tile_kernel<R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part, work)
+template <class C>
+void launch_batch_cfg(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
+                      bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
+                      cudaStream_t st) {
+    const size_t sm = C::smem();
+    const dim3 g(grid), block(C::NT);
+#define R3D_BT(R, S) batch_tile_kernel<C, R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part, work)
     if (reini) {
         if (stage == 1) R3D_BT(true, 1);
         else if (stage == 2) R3D_BT(true, 2);
@@ -767,16 +848,89 @@ int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps,
         else R3D_BT(false, 3);
     }
 #undef R3D_BT
+}
+
+struct CfgInfo {
+    int tx, ty, ry, ring, minb, threads;
+    size_t smem;
+};
+
+const CfgInfo kCfgInfo[] = {
+#define R3D_CFG_INFO(id, tx, ty, ry, ring, minb) {tx, ty, ry, ring, minb, Cfg##id::NT, Cfg##id::smem()},
+    R3D_TILE_CFGS(R3D_CFG_INFO)
+#undef R3D_CFG_INFO
+};
+constexpr int kNumCfg = sizeof(kCfgInfo) / sizeof(kCfgInfo[0]);
+
+const CfgInfo& info(int cfg) { return kCfgInfo[(cfg >= 0 && cfg < kNumCfg) ? cfg : 0]; }
+
+}  // namespace
+
+int tile_cfg_count() { return kNumCfg; }
+
+int tile_cfg_describe(int cfg, int* tx, int* ty, int* ry, int* ring, int* threads) {
+    if (cfg < 0 || cfg >= kNumCfg) return 1;
+    const CfgInfo& c = kCfgInfo[cfg];
+    if (tx) *tx = c.tx;
+    if (ty) *ty = c.ty;
+    if (ry) *ry = c.ry;
+    if (ring) *ring = c.ring;
+    if (threads) *threads = c.threads;
+    return 0;
+}
+
+int tile_ctas_per_sm(int cfg) { return info(cfg).minb; }
+
+// Sets the attributes of every instantiation once per device.
+bool tile_prepare() {
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (dev >= 0 && dev < 64 && done[dev]) return true;
+    bool ok = true;
+#define R3D_CFG_PREP(id, tx, ty, ry, ring, minb) ok = ok && cfg_prepare<Cfg##id>();
+    R3D_TILE_CFGS(R3D_CFG_PREP)
+#undef R3D_CFG_PREP
+    if (!ok) {
+        cudaGetLastError();
+        return false;
+    }
+    if (dev >= 0 && dev < 64) done[dev] = true;
+    return true;
+}
+
+long long tile_items_of(const Layout& L, int kc, int cfg) {
+    const dim3 g = tile_grid(L, kc, cfg);
+    return (long long)g.x * g.y * g.z;
+}
+
+int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
+                            int cfg, bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
+                            cudaStream_t st) {
+    tile_prepare();  // a failure here makes the launch below fail, which the caller reports
+    switch (cfg) {
+#define R3D_CFG_CASE(id, tx, ty, ry, ring, minb) \
+    case id: launch_batch_cfg<Cfg##id>(members, maps, tile0, nm, reini, stage, q, vol_part, work, grid, st); break;
+        R3D_TILE_CFGS(R3D_CFG_CASE)
+#undef R3D_CFG_CASE
+        default: launch_batch_cfg<Cfg0>(members, maps, tile0, nm, reini, stage, q, vol_part, work, grid, st);
+    }
     return 1;
 }
 
-int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, double* vmax_part,
+int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, int cfg, double* vmax_part,
                            unsigned grid, cudaStream_t st) {
-    batch_tile_vmax_kernel<<<grid, kThreads, 0, st>>>(members, tile0, nm, vmax_part);
+    switch (cfg) {
+#define R3D_CFG_CASE(id, tx, ty, ry, ring, minb) \
+    case id: batch_tile_vmax_kernel<Cfg##id><<<grid, Cfg##id::NT, 0, st>>>(members, tile0, nm, vmax_part); break;
+        R3D_TILE_CFGS(R3D_CFG_CASE)
+#undef R3D_CFG_CASE
+        default: batch_tile_vmax_kernel<Cfg0><<<grid, Cfg0::NT, 0, st>>>(members, tile0, nm, vmax_part);
+    }
     return 1;
 }
 
-int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::string* why) {
+int encode_plane_map(const Layout& L, const float* base, int cfg, CUtensorMap* out, std::string* why) {
     using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -797,9 +951,10 @@ int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::
         if (why) *why = "field not 16-byte aligned for TMA";
         return 1;
     }
+    const CfgInfo& c = info(cfg);
     const cuuint64_t dims[3] = {(cuuint64_t)L.px, (cuuint64_t)L.py, (cuuint64_t)L.pz};
     const cuuint64_t strides[2] = {(cuuint64_t)L.px * 4, (cuuint64_t)L.px * L.py * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)kBoxX, (cuuint32_t)kBoxY, 1};
+    const cuuint32_t box[3] = {(cuuint32_t)(c.tx + 8), (cuuint32_t)(c.ty + 6), 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -811,29 +966,23 @@ int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::
     return 0;
 }
 
-size_t tile_smem_bytes() {
-    return (size_t)kRing * kSlotFloats * 4 + kRing * sizeof(uint64_t) + (kRing + 2) * sizeof(int);
+size_t tile_smem_bytes(int cfg) { return info(cfg).smem; }
+
+dim3 tile_grid(const Layout& L, int kc, int cfg) {
+    const CfgInfo& c = info(cfg);
+    return dim3((L.nx + c.tx - 1) / c.tx, (L.ny + c.ty - 1) / c.ty, (L.nz + kc - 1) / kc);
 }
 
-dim3 tile_grid(const Layout& L, int kc) {
-    return dim3((L.nx + kTX - 1) / kTX, (L.ny + kTY - 1) / kTY, (L.nz + kc - 1) / kc);
-}
-
-int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume, cudaStream_t st) {
+int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, int cfg, bool reini, int stage, bool volume,
+                      cudaStream_t st) {
     tile_prepare();  // a failure here makes the launch below fail, which the caller reports
-    const dim3 grid = tile_grid(a.L, a.kc), block(kThreads);
-    const size_t sm = tile_smem_bytes();
-#define R3D_TL(R, S, V) tile_kernel<R, S, V><<<grid, block, sm, st>>>(map, a)
-    if (reini) {
-        if (stage == 1) { if (volume) R3D_TL(true, 1, true); else R3D_TL(true, 1, false); }
-        else if (stage == 2) { if (volume) R3D_TL(true, 2, true); else R3D_TL(true, 2, false); }
-        else { if (volume) R3D_TL(true, 3, true); else R3D_TL(true, 3, false); }
-    } else {
-        if (stage == 1) { if (volume) R3D_TL(false, 1, true); else R3D_TL(false, 1, false); }
-        else if (stage == 2) { if (volume) R3D_TL(false, 2, true); else R3D_TL(false, 2, false); }
-        else { if (volume) R3D_TL(false, 3, true); else R3D_TL(false, 3, false); }
+    switch (cfg) {
+#define R3D_CFG_CASE(id, tx, ty, ry, ring, minb) \
+    case id: launch_stage_cfg<Cfg##id>(map, a, reini, stage, volume, st); break;
+        R3D_TILE_CFGS(R3D_CFG_CASE)
+#undef R3D_CFG_CASE
+        default: launch_stage_cfg<Cfg0>(map, a, reini, stage, volume, st);
     }
-#undef R3D_TL
     return 1;
 }
 

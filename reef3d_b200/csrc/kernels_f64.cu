@@ -245,4 +245,6 @@ long long volume_blocks(const Layout& L) {
     return (long long)g.x * g.y * g.z;
 }
 
+
+
 }  // namespace r3d

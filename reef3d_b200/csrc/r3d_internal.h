@@ -133,12 +133,32 @@ int launch_conv_L_f32(const KGrid<float>& g, const void* in, const Fields& f, co
 int launch_reini_L_f32(const KGrid<float>& g, const void* in, const Fields& f, cudaStream_t st);
 
 long long volume_blocks(const Layout& L);
+
 // also advances the device clock by dt and, with period > 0, sets the
 // velocity factor cos(pi t / period)
 int launch_volume_reduce(const Layout& L, const Scratch& s, long long nblocks, double period, cudaStream_t st);
 int launch_volume_direct(const Layout& L, const void* phi, bool fp32, const double* dxn,
                          const double* dyn, const double* dzn, double psi, const Scratch& s,
                          cudaStream_t st);
+// Relaxation zones of the wave generator and the numerical beach on the
+// level set (iowave::phi_relax, src/iowave_relax.cpp:346-378), device side:
+// col[4 q .. 4 q + 3] = (i, j, zone bits: 1 generation, 2 beach, offset of
+// the column's first generation target) for each zone column q; w[2 q],
+// w[2 q + 1] = its generation and beach weights relax4_wg(i,j),
+// relax4_nb(i,j); zc the cell-centre z of k = 0..nz-1; lsval the
+// generation zone's targets (the wave theory's level set, LOOP order);
+// *ramp the wave generation ramp of the step.
+struct RelaxZones {
+    const int* col;
+    const double* w;
+    const double* zc;
+    const double* lsval;
+    const double* ramp;
+    int ncol;
+    double phimean;
+};
+int launch_relax(const Layout& L, void* f, bool fp32, const RelaxZones& z, cudaStream_t st);
+
 // Airy wave velocity generator: a = amp om / sinh(kw depth), kw = 2 pi /
 // wavelength, om = sqrt(g kw tanh(kw depth)).
 struct AiryParams {
@@ -236,8 +256,8 @@ int launch_zero(void* p, size_t bytes, cudaStream_t st);
 
 // TMA-tiled FP32 stage kernels (kernels_f32_tile.cu), 3D uniform grids
 struct TileArgs;
-size_t tile_smem_bytes();
-dim3 tile_grid(const Layout& L, int kc);
+size_t tile_smem_bytes(int cfg);
+dim3 tile_grid(const Layout& L, int kc, int cfg);
 int launch_set_scalar(double* dst, double value, cudaStream_t st);
 int launch_init_fields(const Layout& L, const double* xc, const double* xf, int ns, const double* sph, int nm,
                        const double* modes, bool fp32, void* phi, void* u, void* v, void* w, cudaStream_t st);

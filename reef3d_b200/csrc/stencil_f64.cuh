@@ -72,6 +72,21 @@ __device__ __forceinline__ double deriv(const double* __restrict__ f, long long 
                  isf + (long long)t * 18 + side * 9, plus, q1, q2, q3, q4, q5);
 }
 
+// deriv from precomputed face differences: Q[m] = (f_{c+m-2} - f_{c+m-3}) /
+// DXP[t+m-3], m = 0..5, i.e. the divided differences of the six faces
+// around the cell (face m lies between cells c+m-3 and c+m-2).  The minus
+// stencil reads faces 0..4, the plus stencil faces 1..5, in the order deriv
+// forms them; each face value is the same IEEE operation whichever cell
+// computes it, so the result is deriv's bit for bit.
+__device__ __forceinline__ double deriv_q(const double* Q, const double* __restrict__ qf,
+                                          const double* __restrict__ cf, const double* __restrict__ isf, int t,
+                                          bool plus) {
+    const int side = plus ? 1 : 0;
+    return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
+                 isf + (long long)t * 18 + side * 9, plus, plus ? Q[1] : Q[0], plus ? Q[2] : Q[1],
+                 plus ? Q[3] : Q[2], plus ? Q[4] : Q[3], plus ? Q[5] : Q[4]);
+}
+
 // Direct-forcing divided difference of the cell pair (a, b = a + s) of the
 // X45 stencils (src/weno_hj_df_nug.cpp:398-987; one rule per X45 for the
 // three axes and both sides), with ha, hb the body field at the two cells:
@@ -166,8 +181,41 @@ __device__ __forceinline__ bool same_sign(const double* __restrict__ f, long lon
            (f0 < 0.0 && xp < 0.0 && xm < 0.0 && yp < 0.0 && ym < 0.0 && zp < 0.0 && zm < 0.0);
 }
 
+// The six face divided differences around the cell along one axis (stride
+// s, cell index t = idx + 5): Q[m] = (f[c+(m-2)s] - f[c+(m-3)s]) /
+// DXP[t+m-3], the layout deriv_q reads.  Each is the division deriv forms
+// for that face, and faces 2 and 3 are the backward and forward differences
+// of the reinitialisation's Godunov test.
+__device__ __forceinline__ void faces6(const double* __restrict__ f, long long c, long long s,
+                                       const double* __restrict__ dp, int t, double* Q) {
+    double fv[7];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) fv[m] = __ldg(f + c + (m - 3) * s);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) Q[m] = (fv[m + 1] - fv[m]) / __ldg(dp + t + m - 3);
+}
+
+// One axis of the reinitialisation right-hand side: the Godunov selection
+// of src/reinidisc_f.cpp:70-109 on the backward / forward differences (faces
+// 2, 3), then the one-sided WENO derivative of the selected side from the
+// same faces (src/ddweno_nug_sf.cpp), or 0.
+__device__ __forceinline__ double reini_axis(const double* Q, double lsSig, const double* __restrict__ qf,
+                                             const double* __restrict__ cf, const double* __restrict__ isf, int t) {
+    const double xmin = Q[2], xplus = Q[3];
+    // minus side if c1, plus side if c2 (the later test wins, as there), else 0
+    const bool c1 = xmin * lsSig > 0.0 && xplus * lsSig > -xmin * lsSig;
+    const bool c2 = xplus * lsSig < 0.0 && xmin * lsSig < -xplus * lsSig;
+    double d = deriv_q(Q, qf, cf, isf, t, c2);
+    if (!(c1 || c2)) d = 0.0;
+    if (xplus * lsSig > 0.0 && xmin * lsSig < 0.0) d = 0.0;
+    return d;
+}
+
 // Reinitialisation right-hand side at (i,j,k): src/reinidisc_f.cpp:58-127
-// (and the body of src/reinidisc_fsf.cpp:74-139).
+// (and the body of src/reinidisc_fsf.cpp:74-139).  Each axis's six face
+// differences are formed once and serve the Godunov test and the WENO
+// stencil (the reference divides the two Godunov faces a second time; the
+// quotients are the same).
 template <bool TWO_D>
 __device__ __forceinline__ double reini_L(const KGrid<double>& g, const double* __restrict__ f, long long c,
                                           int i, int j, int k) {
@@ -177,41 +225,15 @@ __device__ __forceinline__ double reini_L(const KGrid<double>& g, const double* 
     const double lsv = __ldg(f + c);
     double lsSig = lsv / sqrt(lsv * lsv);
     if (fabs(lsv) < 1.0e-8) lsSig = 1.0;
-
-    const double xmin = (lsv - __ldg(f + c - 1)) / __ldg(g.dxp[0] + ti - 1);
-    const double xplus = (__ldg(f + c + 1) - lsv) / __ldg(g.dxp[0] + ti);
-    {
-        // minus side if c1, plus side if c2 (the later test wins, as there), else 0
-        const bool c1 = xmin * lsSig > 0.0 && xplus * lsSig > -xmin * lsSig;
-        const bool c2 = xplus * lsSig < 0.0 && xmin * lsSig < -xplus * lsSig;
-        dx = deriv(f, c, 1, g.dxp[0], g.qf[0], g.cf[0], g.isf[0], ti, c2);
-        if (!(c1 || c2)) dx = 0.0;
-        if (xplus * lsSig > 0.0 && xmin * lsSig < 0.0) dx = 0.0;
-    }
-
+    double Q[6];
+    faces6(f, c, 1, g.dxp[0], ti, Q);
+    dx = reini_axis(Q, lsSig, g.qf[0], g.cf[0], g.isf[0], ti);
     if (!TWO_D) {
-        const double ymin = (lsv - __ldg(f + c - sy)) / __ldg(g.dxp[1] + tj - 1);
-        const double yplus = (__ldg(f + c + sy) - lsv) / __ldg(g.dxp[1] + tj);
-        {
-            // minus side if c1, plus side if c2 (the later test wins, as there), else 0
-            const bool c1 = ymin * lsSig > 0.0 && yplus * lsSig > -ymin * lsSig;
-            const bool c2 = yplus * lsSig < 0.0 && ymin * lsSig < -yplus * lsSig;
-            dy = deriv(f, c, sy, g.dxp[1], g.qf[1], g.cf[1], g.isf[1], tj, c2);
-            if (!(c1 || c2)) dy = 0.0;
-            if (yplus * lsSig > 0.0 && ymin * lsSig < 0.0) dy = 0.0;
-        }
+        faces6(f, c, sy, g.dxp[1], tj, Q);
+        dy = reini_axis(Q, lsSig, g.qf[1], g.cf[1], g.isf[1], tj);
     }
-
-    const double zmin = (lsv - __ldg(f + c - sz)) / __ldg(g.dxp[2] + tk - 1);
-    const double zplus = (__ldg(f + c + sz) - lsv) / __ldg(g.dxp[2] + tk);
-    {
-        // minus side if c1, plus side if c2 (the later test wins, as there), else 0
-        const bool c1 = zmin * lsSig > 0.0 && zplus * lsSig > -zmin * lsSig;
-        const bool c2 = zplus * lsSig < 0.0 && zmin * lsSig < -zplus * lsSig;
-        dz = deriv(f, c, sz, g.dxp[2], g.qf[2], g.cf[2], g.isf[2], tk, c2);
-        if (!(c1 || c2)) dz = 0.0;
-        if (zplus * lsSig > 0.0 && zmin * lsSig < 0.0) dz = 0.0;
-    }
+    faces6(f, c, sz, g.dxp[2], tk, Q);
+    dz = reini_axis(Q, lsSig, g.qf[2], g.cf[2], g.isf[2], tk);
 
     const double dnorm = sqrt(dx * dx + dy * dy + dz * dz);
     double deltax;

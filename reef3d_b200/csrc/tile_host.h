@@ -40,25 +40,30 @@ struct TiledMember {
     int f44;
 };
 
-// Encodes the 3D tensor map of a padded FP32 field for the 72 x 14 x 1
-// plane boxes the tile kernels load.  Returns 0 on success.
-int encode_plane_map(const Layout& L, const float* base, CUtensorMap* out, std::string* why);
-int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume, cudaStream_t st);
+// Tile configurations of the tiled kernels (tile shape, rows per thread,
+// ring depth); id 0 .. tile_cfg_count()-1.  describe: returns 0 for a valid id.
+int tile_cfg_count();
+int tile_cfg_describe(int cfg, int* tx, int* ty, int* ry, int* ring, int* threads);
+// Encodes the 3D tensor map of a padded FP32 field for the (TX+8) x (TY+6) x 1
+// plane boxes configuration `cfg` loads.  Returns 0 on success.
+int encode_plane_map(const Layout& L, const float* base, int cfg, CUtensorMap* out, std::string* why);
+int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, int cfg, bool reini, int stage, bool volume,
+                      cudaStream_t st);
 // Sets the tiled kernels' shared-memory attributes on the current device
 // (once per device); false when the device refuses them.
 bool tile_prepare();
-// CTAs per SM the stage kernels are built to co-reside (persistent grids)
-int tile_ctas_per_sm(bool reini);
-int batch_tile_ctas_per_sm();
-long long tile_items_of(const Layout& L, int kc);
-// Batched persistent tiled stage over the items of nm tiled members.
+// CTAs per SM configuration `cfg` is built to co-reside (persistent grids)
+int tile_ctas_per_sm(int cfg);
+long long tile_items_of(const Layout& L, int kc, int cfg);
+// Batched persistent tiled stage over the items of nm tiled members, whose
+// maps were encoded for configuration `cfg`.
 // work: two zero-initialised counters the launch takes items from (it leaves
 // them at zero for the next launch on the same stream).
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
-                            bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
+                            int cfg, bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
                             cudaStream_t st);
 // Per-item face maxima of the tiled members (3 doubles per item).
-int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, double* vmax_part,
+int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, int cfg, double* vmax_part,
                            unsigned grid, cudaStream_t st);
 
 }  // namespace r3d

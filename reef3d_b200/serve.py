@@ -187,8 +187,24 @@ class TransportServer:
 
 
 def summarize(jobs, makespan):
+    """Latency (arrival to completion) split into queueing delay (arrival to
+    admission) and service time (admission to completion), p50 / p99 / mean
+    of each, and the throughput over the whole run."""
     lat = np.array([j.latency for j in jobs])
+    queue = np.array([j.t_admit - j.arrival for j in jobs])
+    service = np.array([j.t_done - j.t_admit for j in jobs])
     cells = sum(j.cells * j.steps for j in jobs)
-    return {"jobs": len(jobs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "mean_s": float(lat.mean()), "makespan_s": makespan, "cell_updates": cells,
-            "cell_updates_per_s": cells / makespan}
+    out = {"jobs": len(jobs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+           "mean_s": float(lat.mean()), "makespan_s": makespan, "cell_updates": cells,
+           "cell_updates_per_s": cells / makespan}
+    for name, a in (("queue", queue), ("service", service)):
+        out[name] = {"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99)),
+                     "mean_s": float(a.mean())}
+    return out
+
+
+def mean_job_cell_updates(edge_lo=32, edge_hi=384, steps_lo=50, steps_hi=500):
+    """Expected cell-updates of one job of the serving mix: E[edge^3] of the
+    log-uniform edge times the mean step count."""
+    e3 = (edge_hi ** 3 - edge_lo ** 3) / (3.0 * math.log(edge_hi / edge_lo))
+    return e3 * 0.5 * (steps_lo + steps_hi)

@@ -310,6 +310,24 @@ def serving(njobs=48, rate=200.0, seed=1, budget=150e9, precision=FP32, autotune
     return out
 
 
+def serving_loads(burst, fractions=(0.5, 0.9), njobs=200, seed=1, budget=150e9, autotune_cache=None):
+    """The serving mix at loads the server can carry: its capacity in jobs/s
+    is the cell-updates/s of the saturating burst run (`burst`, the output
+    of serving() at 200 jobs/s) over the expected cell-updates of one job;
+    `njobs` Poisson arrivals at each fraction of that capacity, with p50/p99
+    latency split into queueing delay and service time."""
+    from .serve import mean_job_cell_updates
+    per_job = mean_job_cell_updates()
+    cap = burst["cell_updates_per_s"] / per_job
+    out = {"capacity_jobs_per_s": cap, "mean_job_cell_updates": per_job,
+           "capacity_from": "cell-updates/s of the 200 jobs/s burst / expected cell-updates per job"}
+    for f in fractions:
+        r = serving(njobs=njobs, rate=f * cap, seed=seed, budget=budget, autotune_cache=autotune_cache)
+        r["load_fraction"] = f
+        out[f"load_{f:g}"] = r
+    return out
+
+
 def slab_domain(n=256, nslabs=4, steps=20, warmup=3, precision=FP32):
     """The 256^3 vortex split into z slabs on this GPU and stepped by the
     native runner (r3d_domain_*, one CUDA graph per step with the halo

@@ -97,9 +97,14 @@ def test_autotune_cache(tmp_path):
         for x, y in zip(before, after):
             assert np.array_equal(x, y)  # tuning leaves the state untouched
         assert cfg in [(r, c) for r in (2, 4, 8) for c in (4, 8, 16, 32) if r * c * 32 <= 2048]
+        tcfg = b.tile_config()
+        assert 0 <= tcfg[0] < len(r3d.tile_configs()) and tcfg[1] in (8, 16, 32)
+        # one line per size class (the process-wide cache may hold others):
+        # key, rows, CTAs per SM, tile configuration, z chunk
         with open(path) as f:
-            assert len(f.read().split()) == 3
-        assert b.autotune(path) == cfg
+            lines = [ln.split() for ln in f if not ln.startswith("inst-")]
+        assert len(lines) == 1 and [int(x) for x in lines[0][1:]] == [cfg[0], cfg[1], tcfg[0], tcfg[1]]
+        assert b.autotune(path) == cfg and b.tile_config() == tcfg
         b.step(2)
         b.sync()
     for m in ms:

@@ -242,3 +242,60 @@ def test_full_size_fp32_step_matches_fp64(which):
             out.append((interior(ls.download(r3d.PHI), nx, ny, nz), ls.last_volume()))
     assert relmax(out[1][0], out[0][0]) <= 2e-5
     assert abs(out[1][1][0] - out[0][1][0]) <= 1e-6 * abs(out[0][1][0])
+
+
+@pytest.mark.parametrize("cfg", list(range(1, len(r3d.tile_configs()))))
+@pytest.mark.parametrize("dims,kc,f49", [((70, 21, 19), 16, 1), ((130, 9, 33), 7, 0), ((65, 37, 40), 3, 1),
+                                         ((64, 64, 64), 32, 1)])
+def test_tile_configs_bit_identical(port_lib, cfg, dims, kc, f49):
+    """Every tile configuration (tile shape, rows per thread, ring depth) of
+    the tiled kernels computes each cell with the same operations: two steps
+    give the level set of configuration 0 bit for bit (ghost layers
+    included), within 1e-4 of the FP64 oracle; the volume sums (summed over
+    other tiles) within 1e-12."""
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=nx + kc)
+    flags = dict(f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.125)
+    o = port_lib(nx, ny, nz, xn, yn, zn, **flags)
+    dt = o.cfl_dt(u, v, w)
+    ref = o.step(o.step(phi, u, v, w, dt), u, v, w, dt)
+    m = visible_mask(nx, ny, nz)
+    out, vols = {}, {}
+    for c in (0, cfg):
+        with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=r3d.FP32, **flags) as ls:
+            ls.set_option(r3d.OPT_TILE_CFG, c)
+            ls.set_option(r3d.OPT_CHUNK, kc)
+            assert ls.get_option(r3d.OPT_TILED) == 1 and ls.get_option(r3d.OPT_TILE_CFG) == c
+            for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+                ls.upload(f, a)
+            ls.step(dt)
+            ls.step(dt)
+            out[c] = ls.download(r3d.PHI)
+            vols[c] = ls.last_volume()
+    assert np.array_equal(out[cfg][m], out[0][m])
+    assert relmax(out[cfg][m], ref[m]) <= 1e-4
+    for a, b in zip(vols[cfg], vols[0]):
+        assert abs(a - b) <= 1e-12 * abs(b)
+
+
+def test_instance_autotune_keeps_state_and_caches(tmp_path):
+    """r3d_autotune times the configurations without touching the level set,
+    leaves the instance on the chosen one and reuses the cached choice."""
+    c = setups.vortex3d(96)
+    cache = str(tmp_path / "tune.txt")
+    res = []
+    for tune in (True, False):
+        with r3d.LevelSet(96, 96, 96, c.xn, c.yn, c.zn, precision=r3d.FP32, **c.flags()) as ls:
+            for f, a in ((r3d.PHI, c.phi), (r3d.U, c.u), (r3d.V, c.v), (r3d.W, c.w)):
+                ls.upload(f, a)
+            if tune:
+                cfg, kc = ls.autotune(cache)
+                assert ls.get_option(r3d.OPT_TILE_CFG) == cfg and ls.get_option(r3d.OPT_CHUNK) == kc
+                assert ls.autotune(cache) == (cfg, kc)  # cached
+            ls.run(3, adaptive=True)
+            res.append(ls.download(r3d.PHI))
+    assert np.array_equal(res[0], res[1])
+    # the process-wide cache may hold other size classes: one line for this grid,
+    # key + convection (configuration, chunk) + reinitialisation (configuration, chunk)
+    line = [ln.split() for ln in open(cache) if ln.startswith("inst-96x96x96 ")]
+    assert len(line) == 1 and len(line[0]) == 5 and int(line[0][1]) == cfg and int(line[0][2]) == kc

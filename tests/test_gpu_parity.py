@@ -199,3 +199,4 @@ def test_graph_replayed_run_equals_direct_steps(precision, extras):
     if extras:
         assert np.array_equal(out[0][3], out[1][3])
     assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+
