@@ -343,6 +343,14 @@ typedef struct {
     double qi, qo;
 } r3d_ioflow_desc;
 int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io);
+/* The same faces owned by REEF3D's wave generator iowave (B90 >= 1) instead
+ * of ioflow_f: the ghost labels of gcval 50+F50 as above, while
+ * iowave::fsfinflow imposes no ghosts (src/iowave_waterlevel.cpp:29-35,
+ * without flow-file input or patch boundaries) and fsfrkin / fsfrkout copy
+ * the level set's ghost layers at the faces into both stage buffers
+ * (:37-63).  F56 .. F64, qi, qo are not read; r3d_io_levels reports
+ * nothing measured.  Pair with r3d_set_relaxation. */
+int r3d_set_ioflow_waves(r3d_handle* h, const r3d_ioflow_desc* io);
 /* Water levels phimean and phiout of the last step's fsfinflow (both may be
  * NULL).  Synchronous. */
 int r3d_io_levels(r3d_handle* h, double* phimean, double* phiout);

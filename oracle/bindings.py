@@ -38,6 +38,12 @@ def _dp(a):
 IOFLOW_KEYS = ("inflow", "outflow", "f50", "b77", "f56", "f60", "f61", "f62", "f64", "qi", "qo")
 IOFLOW_DEFAULTS = dict(inflow=1, outflow=1, f50=2, b77=1, f56=1.0e20, f60=-1.0e20, f61=-1.0e20, f62=-1.0e20,
                        f64=0, qi=0.0, qo=0.0)
+# iowave flags in refls_set_iowave's argument order: wave theory B92, wave
+# amplitude and period (B93_1, B93_2), depth B94_wdt, generation / beach zone
+# lengths B96_1 / B96_2, still water level F56, ramp B101 / B102
+IOWAVE_KEYS = ("b92", "amp", "period", "depth", "b96_1", "b96_2", "phimean", "b101", "b102")
+IOWAVE_DEFAULTS = dict(b92=2, amp=0.05, period=1.0, depth=0.5, b96_1=0.5, b96_2=0.5, phimean=0.5, b101=0,
+                       b102=1.0)
 
 
 def padded_shape(nx, ny, nz):
@@ -117,6 +123,23 @@ class PortOracle:
         self._body = [np.ascontiguousarray(body1, dtype=np.float64),
                       np.ascontiguousarray(body2 if body2 is not None else body1, dtype=np.float64)]
         self._lib.lso_set_direct_forcing(self.h, x45, _dp(self._body[0]), _dp(self._body[1]))
+
+    def set_io_waves(self, on=True):
+        """The inflow / outflow faces belong to iowave (no fsfinflow)."""
+        self._lib.lso_set_io_waves.argtypes = [ctypes.c_void_p, _I]
+        self._lib.lso_set_io_waves(self.h, 1 if on else 0)
+
+    def set_relaxation(self, wg, wb, phimean):
+        """iowave::phi_relax after each convection stage: weights per column
+        (nx, ny), negative outside the zone."""
+        self._rz = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (wg, wb)]
+        self._lib.lso_set_relaxation.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_double]
+        self._lib.lso_set_relaxation(self.h, *(None if a is None else _dp(a) for a in self._rz), phimean)
+
+    def set_relaxation_target(self, lsval, ramp):
+        self._rz_ls = np.ascontiguousarray(lsval, dtype=np.float64)
+        self._lib.lso_set_relaxation_target.argtypes = [ctypes.c_void_p, _D, ctypes.c_double]
+        self._lib.lso_set_relaxation_target(self.h, _dp(self._rz_ls), ramp)
 
     def io_levels(self):
         """(phimean, phiout) after the last step's fsfinflow."""
@@ -208,9 +231,11 @@ class RefOracle:
     _loaded = set()
 
     def __init__(self, nx, ny, nz, xn, yn, zn, f43=0.55, f44=3, f45=2.1, f49=1, fast=False, f46=0, f47=10,
-                 path=None, ioflow=None, x45=0, solid_forcing=None):
+                 path=None, ioflow=None, x45=0, solid_forcing=None, iowave=None):
         """ioflow: None for the closed box, else a dict of IOFLOW_DEFAULTS'
-        keys: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags."""
+        keys: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags.
+        iowave: None, else a dict of IOWAVE_KEYS (REEF3D's wave generator with
+        relaxation zones on the x faces; replaces ioflow)."""
         path = path or (REF_LIB_FAST if fast else REF_LIB)
         if path in RefOracle._loaded:
             raise RuntimeError("the reference oracle holds one grid per process")
@@ -224,6 +249,10 @@ class RefOracle:
             cells = np.ascontiguousarray(solid_forcing, dtype=np.int32).reshape(-1)
             lib.refls_set_solid_forcing.argtypes = [_I, ctypes.POINTER(ctypes.c_int)]
             lib.refls_set_solid_forcing(cells.size // 4, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        if iowave is not None:
+            lib.refls_set_iowave.argtypes = [_I] + [ctypes.c_double] * 6 + [_I, ctypes.c_double]
+            w = dict(IOWAVE_DEFAULTS, **iowave)
+            lib.refls_set_iowave(*(w[k] for k in IOWAVE_KEYS))
         if ioflow is not None:
             io = dict(IOFLOW_DEFAULTS, **ioflow)
             lib.refls_set_ioflow.argtypes = [_I, _I, _I, _I] + [ctypes.c_double] * 4 + [_I] + [ctypes.c_double] * 2
@@ -330,6 +359,66 @@ class RefOracle:
         fp = ctypes.POINTER(ctypes.c_float)
         self._lib.refls_vtu_point_data(*(a.ctypes.data_as(fp) for a in out))
         return out
+
+    def set_time(self, t):
+        """lexer::simtime (the wave generator's clock)."""
+        self._lib.refls_set_time.argtypes = [ctypes.c_double]
+        self._lib.refls_set_time(t)
+
+    def wavegen_precalc(self):
+        """iowave::wavegen_precalc: the generation zone's targets at the clock."""
+        if self._lib.refls_wavegen_precalc() != 0:
+            raise RuntimeError("no wave generator")
+
+    def iowave_weights(self):
+        """(relax4_wg, relax4_nb) per interior column as (nx, ny) arrays, -1
+        outside the zones."""
+        wg, wb = np.zeros(self.nx * self.ny), np.zeros(self.nx * self.ny)
+        self._lib.refls_iowave_weights.argtypes = [_D, _D]
+        if self._lib.refls_iowave_weights(_dp(wg), _dp(wb)) != 0:
+            raise RuntimeError("no wave generator")
+        return wg.reshape(self.nx, self.ny), wb.reshape(self.nx, self.ny)
+
+    def iowave_targets(self):
+        """(lsval, ramp) of the generation zone at the last wavegen_precalc."""
+        n = self.nx * self.ny * self.nz
+        ls, ramp = np.zeros(n), np.zeros(1)
+        self._lib.refls_iowave_targets.argtypes = [_D, ctypes.c_long, _D]
+        self._lib.refls_iowave_targets.restype = ctypes.c_long
+        m = self._lib.refls_iowave_targets(_dp(ls), n, _dp(ramp))
+        if m < 0:
+            raise RuntimeError("no wave generator")
+        return ls[:m].copy(), float(ramp[0])
+
+    def set_time(self, t):
+        """lexer::simtime (the wave generator's clock)."""
+        self._lib.refls_set_time.argtypes = [ctypes.c_double]
+        self._lib.refls_set_time(t)
+
+    def wavegen_precalc(self):
+        """iowave::wavegen_precalc: the generation zone's targets at the clock."""
+        if self._lib.refls_wavegen_precalc() != 0:
+            raise RuntimeError("no wave generator")
+
+    def iowave_weights(self):
+        """(relax4_wg, relax4_nb) per interior column as (nx, ny) arrays, -1
+        outside the zones."""
+        wg, wb = np.zeros(self.nx * self.ny), np.zeros(self.nx * self.ny)
+        self._lib.refls_iowave_weights.argtypes = [_D, _D]
+        if self._lib.refls_iowave_weights(_dp(wg), _dp(wb)) != 0:
+            raise RuntimeError("no wave generator")
+        return wg.reshape(self.nx, self.ny), wb.reshape(self.nx, self.ny)
+
+    def iowave_targets(self):
+        """(lsval, ramp) of the generation zone at the last wavegen_precalc."""
+        n = self.nx * self.ny * self.nz
+        ls, ramp = np.zeros(n), np.zeros(1)
+        self._lib.refls_iowave_targets.argtypes = [_D, ctypes.c_long, _D]
+        self._lib.refls_iowave_targets.restype = ctypes.c_long
+        m = self._lib.refls_iowave_targets(_dp(ls), n, _dp(ramp))
+        if m < 0:
+            raise RuntimeError("no wave generator")
+        return ls[:m].copy(), float(ramp[0])
 
     def io_levels(self):
         """(phimean, phiout) after the last step's fsfinflow."""

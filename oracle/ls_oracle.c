@@ -524,6 +524,54 @@ static void io_fsfrk(const lso_grid* g, const double* phi, double* f) {
             }
 }
 
+/* iowave::fsfrkin / fsfrkout (src/iowave_waterlevel.cpp:37-63): the RK
+ * buffer's inflow and outflow ghosts copy phi's. */
+static void io_fsfrk_waves(const lso_grid* g, const double* phi, double* f) {
+    for (int j = 0; j < g->ny; ++j)
+        for (int k = 0; k < g->nz; ++k)
+            for (int q = 1; q <= 3; ++q) {
+                if (g->io_in) f[lso_index(g, -q, j, k)] = phi[lso_index(g, -q, j, k)];
+                if (g->io_out) {
+                    const long c = lso_index(g, g->nx - 1 + q, j, k);
+                    f[c] = phi[c];
+                }
+            }
+}
+
+/* iowave::phi_relax (src/iowave_relax.cpp:346-378) over LOOP (i, j, k): the
+ * generation zone (distgen < 1e20) blends towards ramp * lsval[count] with
+ * count running over the zone's cells in LOOP order, then the beach
+ * (distbeach < 1e20) towards phimean - z. */
+static void phi_relax(const lso_grid* g, double* f) {
+    if (!g->rz_wg && !g->rz_wb) return;
+    long count = 0;
+    for (int i = 0; i < g->nx; ++i)
+        for (int j = 0; j < g->ny; ++j)
+            for (int k = 0; k < g->nz; ++k) {
+                const long c = lso_index(g, i, j, k);
+                const double wg = g->rz_wg ? g->rz_wg[(long)i * g->ny + j] : -1.0;
+                const double wb = g->rz_wb ? g->rz_wb[(long)i * g->ny + j] : -1.0;
+                if (wg >= 0.0) {
+                    f[c] = (1.0 - wg) * g->rz_ramp * g->rz_lsval[count] + wg * f[c];
+                    ++count;
+                }
+                if (wb >= 0.0) f[c] = (1.0 - wb) * (g->rz_phimean - g->zp[k + LSO_MARGE]) + wb * f[c];
+            }
+}
+
+void lso_set_io_waves(lso_grid* g, int on) { g->io_waves = on; }
+
+void lso_set_relaxation(lso_grid* g, const double* wg, const double* wb, double phimean) {
+    g->rz_wg = wg;
+    g->rz_wb = wb;
+    g->rz_phimean = phimean;
+}
+
+void lso_set_relaxation_target(lso_grid* g, const double* lsval, double ramp) {
+    g->rz_lsval = lsval;
+    g->rz_ramp = ramp;
+}
+
 void lso_set_ioflow(lso_grid* g, int inflow, int outflow, int f50, int b77, double f56, double f60, double f61,
                     double f62, int f64, double qi, double qo) {
     g->io_on = 1;
@@ -596,8 +644,13 @@ void lso_set_picard(lso_grid* g, int f46, int f47) {
 /* src/reini_RK3.cpp:113-138 (with picard_f when F46=1, :92 and :140) */
 void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, int iters) {
     const double vol1 = g->f46 == 1 ? picard_volume(g, f) : 0.0;
-    io_fsfrk(g, f, a1);
-    io_fsfrk(g, f, a2);
+    if (g->io_on && g->io_waves) {
+        io_fsfrk_waves(g, f, a1);
+        io_fsfrk_waves(g, f, a2);
+    } else {
+        io_fsfrk(g, f, a1);
+        io_fsfrk(g, f, a2);
+    }
     for (int q = 0; q < iters; ++q) {
         lso_reinidisc_L(g, f, L);
         for (int i = 0; i < g->nx; ++i)
@@ -636,7 +689,10 @@ void lso_reini(const lso_grid* g, double* f, double* a1, double* a2, double* L, 
 void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, const double* w,
                  double dt, double* a1, double* a2, double* L) {
     g->count += 1;
-    if (g->io_on) {
+    if (g->io_on && g->io_waves) {
+        io_fsfrk_waves(g, phi, a1);
+        io_fsfrk_waves(g, phi, a2);
+    } else if (g->io_on) {
         io_fsfinflow(g, phi);
         io_fsfrk(g, phi, a1);
         io_fsfrk(g, phi, a2);
@@ -653,6 +709,7 @@ void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, con
                 const long c = lso_index(g, i, j, k);
                 a1[c] = phi[c] + dt * L[c];
             }
+    phi_relax(g, a1);
     lso_ghost_fill(g, a1);
     solid_forcing(g, a1);
     lso_weno_L(g, a1, u, v, w, L);
@@ -662,6 +719,7 @@ void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, con
                 const long c = lso_index(g, i, j, k);
                 a2[c] = 0.75 * phi[c] + 0.25 * a1[c] + 0.25 * dt * L[c];
             }
+    phi_relax(g, a2);
     lso_ghost_fill(g, a2);
     solid_forcing(g, a2);
     lso_weno_L(g, a2, u, v, w, L);
@@ -671,6 +729,7 @@ void lso_ls_step(lso_grid* g, double* phi, const double* u, const double* v, con
                 const long c = lso_index(g, i, j, k);
                 phi[c] = (1.0 / 3.0) * phi[c] + (2.0 / 3.0) * a2[c] + (2.0 / 3.0) * dt * L[c];
             }
+    phi_relax(g, phi);
     lso_ghost_fill(g, phi);
     solid_forcing(g, phi);
     lso_reini(g, phi, a1, a2, L, g->f44);

@@ -61,6 +61,15 @@ typedef struct {
      * (i, j, k, side), caller-owned */
     int nsf;
     const int* sf;
+    /* the inflow / outflow faces belong to iowave (B90 = 1): fsfinflow
+     * imposes nothing, fsfrkin / fsfrkout copy phi's ghosts */
+    int io_waves;
+    /* relaxation zones (iowave::phi_relax): per interior column i*ny + j
+     * the generation / beach weight, < 0 outside; the generation targets
+     * (LOOP order over the zone), the ramp, the still water level;
+     * caller-owned */
+    const double *rz_wg, *rz_wb, *rz_lsval;
+    double rz_ramp, rz_phimean;
 } lso_grid;
 
 /* xn/yn/zn: node coordinates for indices -5..n+5 (n+11 values). */
@@ -115,6 +124,14 @@ void lso_set_direct_forcing(lso_grid* g, int x45, const double* body1, const dou
 
 /* solid_forcing_lsm entries (src/gc_solid_forcing_lsm.cpp:27-78), kept by pointer */
 void lso_set_solid_forcing(lso_grid* g, int n, const int* cells);
+
+/* The faces of lso_set_ioflow owned by iowave instead of ioflow_f. */
+void lso_set_io_waves(lso_grid* g, int on);
+/* iowave::phi_relax after every convection stage (src/iowave_relax.cpp:346-378):
+ * weights per column (kept by pointer; NULL: no zone), still water level. */
+void lso_set_relaxation(lso_grid* g, const double* wg, const double* wb, double phimean);
+/* the generation targets of the next step (kept by pointer) and its ramp */
+void lso_set_relaxation_target(lso_grid* g, const double* lsval, double ramp);
 
 /* opaque handle helpers (used through ctypes) */
 lso_grid* lso_new(int nx, int ny, int nz, const double* xn, const double* yn, const double* zn,

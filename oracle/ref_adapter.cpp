@@ -6,6 +6,21 @@
 // on the CPU with what the adapters compute through libreef3d_b200.so.
 // Built into oracle/_ref/libreef3d_adapter.so by oracle/Makefile.ref.
 
+// iowave's relaxation weights and targets are private; the adapter reads
+// them as the friend a REEF3D maintainer declares in src/iowave.h.  This
+// test build, which leaves the reference untouched, opens them instead.
+#include "ioflow.h"
+#include "wave_interface.h"
+#include "field1.h"
+#include "field2.h"
+#include "slice1.h"
+#include "slice2.h"
+#include "slice4.h"
+#include "sliceint4.h"
+#include "flowfile_in.h"
+#define private public
+#include "iowave.h"
+#undef private
 #include "reef3d_b200_adapters.h"
 
 #include <cstring>

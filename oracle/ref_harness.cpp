@@ -38,8 +38,26 @@
 #include "kepsilon_void.h"
 #include "mgcslice2.h"
 #include "mgcslice4.h"
+// iowave (the wave generator's relaxation zones): its own headers first, then
+// the class with its private members readable by this harness (test
+// infrastructure reading relax4_wg / relax4_nb / lsval, which the reference
+// keeps private; nothing of the reference is modified)
+#include "ioflow.h"
+#include "wave_interface.h"
+#include "field1.h"
+#include "field2.h"
+#include "slice1.h"
+#include "slice2.h"
+#include "slice4.h"
+#include "sliceint4.h"
+#include "flowfile_in.h"
+#define private public
+#include "iowave.h"
+#undef private
 
+#include <cstdlib>
 #include <cstring>
+#include <new>
 #include <vector>
 
 namespace {
@@ -65,6 +83,13 @@ struct IoFlags {
     int on = 0, inflow = 0, outflow = 0, f50 = 2, b77 = 1, f64 = 0;
     double f56 = 1.0e20, f60 = -1.0e20, f61 = -1.0e20, f62 = -1.0e20, qi = 0.0, qo = 0.0;
 } G_IO;
+// iowave (B90 = 1) with relaxation-zone wave generation (B98 = 2) and beach
+// (B99 = 2) for the next refls_init; on == 0: no wave generator
+struct WaveFlags {
+    int on = 0, b92 = 2, b101 = 0;
+    double amp = 0.0, period = 0.0, depth = 0.0, b96_1 = 0.0, b96_2 = 0.0, phimean = 0.0, b102 = 1.0;
+} G_IOW;
+iowave* WAVE = nullptr;
 ietimestep* TSTEP = nullptr;
 turbulence* TURB = nullptr;
 
@@ -138,6 +163,23 @@ void refls_set_ioflow(int inflow, int outflow, int f50, int b77, double f56, dou
     G_IO.qi = qi; G_IO.qo = qo;
 }
 
+// Wave generator of the next refls_init: REEF3D's iowave (B90 = 1) with the
+// x-min face as inflow and the x-max face as outflow, wave theory b92 (2:
+// linear waves, src/wave_interface.cpp:60-80) of amplitude amp and period
+// (B93 = 1), water depth (B94 = 1), relaxation-zone generation (B98 = 2)
+// over b96_1 from the x-min face and a relaxation beach (B99 = 2) over b96_2
+// before the x-max face (the default zone lines of src/iowave.cpp:130-170),
+// still water level phimean (F56), ramp B101/B102.
+void refls_set_iowave(int b92, double amp, double period, double depth, double b96_1, double b96_2,
+                      double phimean, int b101, double b102) {
+    G_IOW.on = 1;
+    G_IOW.b92 = b92; G_IOW.amp = amp; G_IOW.period = period; G_IOW.depth = depth;
+    G_IOW.b96_1 = b96_1; G_IOW.b96_2 = b96_2; G_IOW.phimean = phimean; G_IOW.b101 = b101; G_IOW.b102 = b102;
+    G_IO.on = 1;
+    G_IO.inflow = 1;
+    G_IO.outflow = 1;
+}
+
 // xn/yn/zn: node coordinates for index -5 .. n+5 (n+11 values), the same
 // arrays DIVEMesh writes (src/read_grid.cpp:417-433, marge=5).
 // f49 selects reinidisc_f (1) or reinidisc_fsf (0); f44 the reinit
@@ -148,7 +190,11 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     if (P) return -1;
     int argc = 0;
     char** argv = nullptr;
-    P = new lexer;
+    // members the reference never assigns are read as zero, as the fresh
+    // heap of a REEF3D process gives them (e.g. gcsldfbed4_count, read by
+    // ghostcell::solid_forcing_bed from iowave's set-up): the lexer is
+    // constructed in zeroed memory
+    P = new (std::calloc(1, sizeof(lexer))) lexer;
     PGC = new ghostcell(argc, argv, P);
     lexer* p = P;
 
@@ -160,6 +206,19 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
         p->F56 = G_IO.f56; p->F60 = G_IO.f60; p->F61 = G_IO.f61; p->F62 = G_IO.f62; p->F64 = G_IO.f64;
     }
     p->X45 = G_X45; p->X48 = 0; p->M10 = 1; p->P12 = 1000000000;
+    if (G_IOW.on) {  // control letters of the wave generator (src/ini.cpp:224-240)
+        p->B60 = 0;
+        p->B90 = 1; p->B92 = G_IOW.b92;
+        p->B93 = 1; p->B93_1 = G_IOW.amp; p->B93_2 = G_IOW.period;
+        p->B94 = 1; p->B94_wdt = G_IOW.depth;
+        p->B96_1 = G_IOW.b96_1; p->B96_2 = G_IOW.b96_2;
+        p->B98 = 2; p->B99 = 2; p->B101 = G_IOW.b101; p->B102 = G_IOW.b102;
+        p->F56 = G_IOW.phimean; p->phimean = G_IOW.phimean; p->phiout = G_IOW.phimean;
+        p->A10 = 6;
+        p->xcoormin = xn[5]; p->xcoormax = xn[5 + nx];
+        p->ycoormin = yn[5]; p->ycoormax = yn[5 + ny];
+        p->simtime = 0.0;
+    }
 
     // --- what read_grid() assigns (src/read_grid.cpp:78-300)
     p->knox = nx; p->knoy = ny; p->knoz = nz;
@@ -268,6 +327,12 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j)
             for (int k = 0; k < nz; ++k) p->flag4[ijk(i, j, k)] = WATER_FLAG;
+    // the wave generator works on the water-surface slices (SLICELOOP4 over
+    // flagslice4 > 0, src/looping2D.h:51), which a DIVEMesh grid marks for
+    // every interior column (src/read_grid.cpp:753-758)
+    if (G_IOW.on)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) p->flagslice4[(i - p->imin) * p->jmax + (j - p->jmin)] = 1;
     for (int n = 0; n < nx + 1 + 2 * p->marge; ++n) p->XN[n] = xn[n];
     for (int n = 0; n < ny + 1 + 2 * p->marge; ++n) p->YN[n] = yn[n];
     for (int n = 0; n < nz + 1 + 2 * p->marge; ++n) p->ZN[n] = zn[n];
@@ -343,7 +408,11 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     CONV = new weno_hj_df_nug(p);
     // no patch boundaries: driver::patchBC_logic picks patchBC_void
     // (src/driver_logic_cfd.cpp:661-672)
-    if (G_IO.on) FLOW = new ioflow_f(p, PGC, new patchBC_void(p));
+    if (G_IOW.on) {
+        p->phimean = p->phiout = p->phiin = G_IOW.phimean;  // src/ini_phi.cpp:33
+        FLOW = WAVE = new iowave(p, PGC, new patchBC_void(p));
+    }
+    else if (G_IO.on) FLOW = new ioflow_f(p, PGC, new patchBC_void(p));
     else FLOW = new ioflow_v(p, PGC, new patchBC_void(p));
     PART = new particle_pls_void();
     REINI = new reini_RK3(p, 0);
@@ -366,10 +435,67 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     p->Qi = p->Qo = 0.0;  // closed box: no discharge (read by picard_lsm, src/picard_lsm.cpp:95)
     if (G_IO.on) {
         p->Qi = G_IO.qi; p->Qo = G_IO.qo;
-        // inflow / outflow cell lists gcin, gcout (src/ioflow_util.cpp:30-81)
+        // inflow / outflow cell lists gcin, gcout (src/ioflow_util.cpp:30-81);
+        // iowave also fills the gcb4a lists gcin4a / gcout4a without
+        // resizing them (src/iowave_util.cpp:101-128): room for every entry
+        if (WAVE) {
+            p->Iarray(p->gcin4a, p->gcb4a_count, 6);
+            p->Iarray(p->gcout4a, p->gcb4a_count, 6);
+        }
         FLOW->gcio_update(p, A, PGC);
     }
+    if (WAVE) FLOW->ini(p, A, PGC);  // relaxation functions and the first targets (src/iowave_ini.cpp:29-50)
     return 0;
+}
+
+// The clock (lexer::simtime) the wave generator's targets and ramp read.
+void refls_set_time(double t) { P->simtime = t; }
+
+// The wave generator's per-step targets (iowave::wavegen_precalc,
+// src/driver_loop_cfd.cpp:78), as the driver computes them before each
+// free-surface step.
+int refls_wavegen_precalc() {
+    if (!WAVE) return -1;
+    FLOW->wavegen_precalc(P, PGC);
+    return 0;
+}
+
+// Relaxation weights per interior column (i * ny + j): relax4_wg(i,j) where
+// distgen < 1e20 (the generation zone), relax4_nb(i,j) where distbeach <
+// 1e20 (the beach), -1 elsewhere (src/iowave_relax.cpp:346-378).
+int refls_iowave_weights(double* wg, double* wb) {
+    if (!WAVE) return -1;
+    lexer* p = P;
+    for (int i = 0; i < p->knox; ++i)
+        for (int j = 0; j < p->knoy; ++j) {
+            increment::i = i;
+            increment::j = j;
+            increment::k = 0;
+            const double dg = WAVE->distgen(p), db = WAVE->distbeach(p);
+            wg[i * p->knoy + j] = dg < 1.0e20 ? WAVE->relax4_wg(i, j) : -1.0;
+            wb[i * p->knoy + j] = db < 1.0e20 ? WAVE->relax4_nb(i, j) : -1.0;
+        }
+    return 0;
+}
+
+// The generation zone's current targets (iowave::lsval, LOOP order over the
+// zone, src/iowave_precalc_relax.cpp) and iowave::ramp; returns their count
+// (n = capacity of lsval; -1 when larger).
+long refls_iowave_targets(double* lsval, long n, double* ramp) {
+    if (!WAVE) return -1;
+    lexer* p = P;
+    long count = 0;
+    for (int i = 0; i < p->knox; ++i)
+        for (int j = 0; j < p->knoy; ++j) {
+            increment::i = i;
+            increment::j = j;
+            increment::k = 0;
+            if (WAVE->distgen(p) < 1.0e20) count += p->knoz;
+        }
+    if (count > n) return -1;
+    for (long q = 0; q < count; ++q) lsval[q] = WAVE->lsval[q];
+    *ramp = WAVE->ramp(p);
+    return count;
 }
 
 long refls_padded_size() { return P ? ncells_padded() : -1; }

@@ -104,6 +104,7 @@ EXPORTS = {
     "r3d_set_fluid": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "r3d_fluid_update": ([_H, _D, _D], ctypes.c_int),
     "r3d_set_ioflow": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
+    "r3d_set_ioflow_waves": ([_H, ctypes.POINTER(IoflowDesc)], ctypes.c_int),
     "r3d_set_direct_forcing": ([_H, ctypes.c_int], ctypes.c_int),
     "r3d_set_relaxation": ([_H, _D, _D, ctypes.c_double], ctypes.c_int),
     "r3d_set_relaxation_target": ([_H, _D, ctypes.c_longlong, ctypes.c_double], ctypes.c_int),
@@ -449,15 +450,19 @@ class LevelSet:
     def set_ioflow(self, **flags):
         """Inflow / outflow faces with ioflow_f's hooks (r3d_set_ioflow):
         keys of IOFLOW_DEFAULTS, unspecified ones at the reference's
-        defaults.  set_ioflow(off=True) restores the closed box."""
+        defaults.  set_ioflow(off=True) restores the closed box;
+        waves=True hands the faces to the wave generator's hooks instead
+        (r3d_set_ioflow_waves)."""
         if flags.pop("off", False):
             _check(_lib.r3d_set_ioflow(self.h, None), self.h)
             return
+        waves = flags.pop("waves", False)
         unknown = set(flags) - set(IOFLOW_DEFAULTS)
         if unknown:
             raise TypeError(f"unknown ioflow flags {sorted(unknown)}")
         d = IoflowDesc(**dict(IOFLOW_DEFAULTS, **flags))
-        _check(_lib.r3d_set_ioflow(self.h, ctypes.byref(d)), self.h)
+        fn = _lib.r3d_set_ioflow_waves if waves else _lib.r3d_set_ioflow
+        _check(fn(self.h, ctypes.byref(d)), self.h)
 
     def io_levels(self):
         """(phimean, phiout) measured by the last step's fsfinflow."""

@@ -31,6 +31,12 @@
 #include "reef3d_b200.h"
 #include "reini.h"
 #include "reinidisc.h"
+// the wave generator: its relaxation weights and targets are private to
+// iowave; the adapter reads them as a friend -- a maintainer adds
+//   namespace r3d_adapter { struct WaveState; }   (before class iowave)
+//   friend struct r3d_adapter::WaveState;          (inside it)
+// to src/iowave.h
+#include "iowave.h"
 
 namespace r3d_adapter {
 
@@ -126,12 +132,22 @@ inline int gcval_iniphi(const lexer* p) {
 // (r3d_set_ioflow).  false: closed box (ioflow_v, or gcv 50, whose ghost
 // label is 4 on every face).  iowave and the gravity flow (B90, B180) have
 // relaxation zones and hooks of their own, not on the device.
-inline bool ioflow_desc(const lexer* p, int gcv, r3d_ioflow_desc* d) {
-    if (p->B90 >= 1 || p->B180 == 1 || p->B191 == 1 || p->B192 == 1) {
-        std::cout << "reef3d_b200: iowave / ioflow_gravity level-set hooks are not on the device" << std::endl;
+inline bool ioflow_desc(const lexer* p, int gcv, r3d_ioflow_desc* d, bool* waves) {
+    *waves = p->B90 >= 1;
+    if (p->B180 == 1 || p->B191 == 1 || p->B192 == 1) {
+        std::cout << "reef3d_b200: ioflow_gravity level-set hooks are not on the device" << std::endl;
         std::exit(1);
     }
-    if (p->B60 < 1 || gcv == 50) return false;
+    // the wave generator's level-set hooks on the device: relaxation-zone
+    // generation (B98 = 2) and beach (B99 = 2), faces without flow-file
+    // input (I230 = 0); Dirichlet and active wave makers set the level set
+    // in ways the device does not model
+    if (*waves && ((p->B98 != 0 && p->B98 != 2) || p->B99 > 2 || p->I230 > 0)) {
+        std::cout << "reef3d_b200: of iowave's level-set hooks the device has the relaxation zones (B98 = 2, "
+                     "B99 = 2) only" << std::endl;
+        std::exit(1);
+    }
+    if ((p->B60 < 1 && !*waves) || gcv == 50) return false;
     const int face = p->knoy * p->knoz;
     for (int n = 0; n < p->gcin_count; ++n)
         if (p->gcin[n][3] != 1 || p->gcin_count != face) {
@@ -213,9 +229,11 @@ struct IoflowState {
     r3d_ioflow_desc last{};
     void sync(r3d_handle* h, const lexer* p, int gcv) {
         r3d_ioflow_desc d{};
-        const bool now = ioflow_desc(p, gcv, &d);
+        bool waves = false;
+        const bool now = ioflow_desc(p, gcv, &d, &waves);
         if (now != on || (now && !same_ioflow(d, last))) {
-            check(h, r3d_set_ioflow(h, now ? &d : nullptr));
+            if (now && waves) check(h, r3d_set_ioflow_waves(h, &d));
+            else check(h, r3d_set_ioflow(h, now ? &d : nullptr));
             on = now;
             last = d;
         }
@@ -225,7 +243,12 @@ struct IoflowState {
     // on every slab (the grid's levels are taken from slab 0's)
     void sync(r3d_domain* dm, const lexer* p, int gcv) {
         r3d_ioflow_desc d{};
-        const bool now = ioflow_desc(p, gcv, &d);
+        bool waves = false;
+        const bool now = ioflow_desc(p, gcv, &d, &waves);
+        if (waves) {
+            std::cout << "reef3d_b200: the slab domain runs without the wave generator" << std::endl;
+            std::exit(1);
+        }
         if (now != on || (now && !same_ioflow(d, last))) {
             check_domain(dm, r3d_domain_set_ioflow(dm, now ? &d : nullptr));
             on = now;
@@ -234,6 +257,50 @@ struct IoflowState {
         r3d_handle* h = nullptr;
         for (int s = 0; r3d_domain_slab(dm, s, &h, nullptr, nullptr) == R3D_OK; ++s)
             check(h, r3d_set_step_count(h, p->count));
+    }
+};
+
+// The wave generator's relaxation zones on the level set (iowave::phi_relax,
+// src/iowave_relax.cpp:346-378, after every convection stage): the zones'
+// weights relax4_wg / relax4_nb of every column inside them (distgen /
+// distbeach < 1e20) go to the device once, and each step the targets lsval
+// that the driver's wavegen_precalc computed for it (src/driver_loop_cfd.cpp:78)
+// with the step's ramp.  Generation applies with B98 = 2 (and iowave's
+// h_switch), the beach with B99 = 2.
+struct WaveState {
+    bool set = false;
+    double phimean = 0.0;
+    bool gen = false, beach = false;
+    std::vector<double> wg, wb;
+    void sync(r3d_handle* h, lexer* p, ioflow* pflow) {
+        if (p->B90 < 1) return;
+        iowave* w = dynamic_cast<iowave*>(pflow);
+        if (!w) {
+            std::cout << "reef3d_b200: B90 >= 1 without the iowave flow object" << std::endl;
+            std::exit(1);
+        }
+        if (!set || phimean != p->phimean) {
+            gen = p->B98 == 2 && w->h_switch == 1;
+            beach = p->B99 == 2;
+            const int nx = p->knox, ny = p->knoy;
+            wg.assign((size_t)nx * ny, -1.0);
+            wb.assign((size_t)nx * ny, -1.0);
+            for (int i = 0; i < nx; ++i)
+                for (int j = 0; j < ny; ++j) {
+                    increment::i = i;
+                    increment::j = j;
+                    increment::k = 0;
+                    if (gen && w->distgen(p) < 1.0e20) wg[(size_t)i * ny + j] = w->relax4_wg(i, j);
+                    if (beach && w->distbeach(p) < 1.0e20) wb[(size_t)i * ny + j] = w->relax4_nb(i, j);
+                }
+            check(h, r3d_set_relaxation(h, gen ? wg.data() : nullptr, beach ? wb.data() : nullptr, p->phimean));
+            phimean = p->phimean;
+            set = true;
+        }
+        long long n = 0;
+        if (gen)
+            for (double x : wg) n += x >= 0.0 ? p->knoz : 0;
+        if (gen || beach) check(h, r3d_set_relaxation_target(h, w->lsval, n, w->ramp(p)));
     }
 };
 
@@ -266,10 +333,11 @@ public:
     }
     ~levelset_RK3_gpu() { r3d_destroy(h); }
 
-    void start(fdm* a, lexer* p, convection*, solver*, ghostcell* pgc, ioflow*, reini*, particle_corr*,
+    void start(fdm* a, lexer* p, convection*, solver*, ghostcell* pgc, ioflow* pflow, reini*, particle_corr*,
                field& ls) override {
         using r3d_adapter::check;
         io.sync(h, p, r3d_adapter::gcval_phi(p));
+        wave.sync(h, p, pflow);
         sf.sync(h, p);
         if (!resident || first) check(h, r3d_upload(h, R3D_PHI, ls.V, R3D_LAYOUT_REEF3D));
         first = false;
@@ -309,6 +377,7 @@ private:
     bool resident;
     bool first = true;
     r3d_adapter::IoflowState io;
+    r3d_adapter::WaveState wave;
     r3d_adapter::SolidForcingState sf;
     std::vector<double> buf;
 };

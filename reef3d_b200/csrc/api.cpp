@@ -1034,6 +1034,12 @@ int r3d_set_ioflow(r3d_handle* h, const r3d_ioflow_desc* io) {
     return R3D_OK;
 }
 
+int r3d_set_ioflow_waves(r3d_handle* h, const r3d_ioflow_desc* io) {
+    if (int rc = r3d_set_ioflow(h, io)) return rc;
+    if (io) h->iop.waves = 1;
+    return R3D_OK;
+}
+
 // ------------------------------------------------ grid spacing constants
 int r3d_grid_spacing(const r3d_grid_desc* desc, double* out) {
     std::string why;

@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(256) io_ghost_kernel(Layout L, T* __restrict__
     const double zc = p.zp[k + 5];
     const long long row = (long long)(k + L.gz) * L.sz + (long long)(j + L.gy) * L.sy + L.gx;
     if (p.inflow) {
-        if (step && p.state[kIoFound] != 0.0 && (p.f50 == 2 || p.f50 == 4)) {
+        if (step && !p.waves && p.state[kIoFound] != 0.0 && (p.f50 == 2 || p.f50 == 4)) {
             const T v = static_cast<T>(p.state[kIoPhimean] - zc);
             for (int q = 1; q <= 3; ++q) phi[row - q] = v;
         }
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(256) io_ghost_kernel(Layout L, T* __restrict__
     }
     if (p.outflow) {
         const long long c = row + L.nx - 1;
-        const bool fixed = p.f62 > -1.0e20 && p.b77 == 2;
+        const bool fixed = !p.waves && p.f62 > -1.0e20 && p.b77 == 2;
         if (step && fixed) {
             const T v = static_cast<T>(p.state[kIoWsfout] - zc);
             for (int q = 1; q <= 3; ++q) phi[c + q] = v;
@@ -759,7 +759,7 @@ int launch_io_hooks(const Layout& L, void* phi, void* a1, void* a2, bool fp32, c
     const int rows = L.ny * L.nz;
     const int blocks = (rows + 255) / 256;
     int n = 0;
-    if (step) {
+    if (step && !p.waves) {
         if (fp32) io_level_kernel<float><<<1, kIoThreads, 0, st>>>(L, static_cast<const float*>(phi), p);
         else io_level_kernel<double><<<1, kIoThreads, 0, st>>>(L, static_cast<const double*>(phi), p);
         ++n;

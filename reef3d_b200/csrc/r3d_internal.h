@@ -211,6 +211,11 @@ struct IoParams {
     const double* dzp;    // centre spacing (DZP), index k + 5
     const double* ramp;   // outflow level ramp for count = 0 .. f64-1
     double* state;        // kIo* slots below
+    // the faces belong to REEF3D's wave generator (iowave): its fsfinflow
+    // imposes nothing (src/iowave_waterlevel.cpp:29-35 without flow files or
+    // patch boundaries) and its fsfrkin / fsfrkout copy the level set's
+    // ghost layers into the stage buffers (:37-63)
+    int waves;
 };
 constexpr int kIoPhimean = 0, kIoPhiout = 1, kIoCount = 2, kIoWsfout = 3, kIoFound = 4, kIoStateLen = 8;
 // fsfinflow: advances the step count, measures the water levels, imposes

@@ -30,7 +30,10 @@ def golden_flags(g):
 
 
 def golden_ioflow(g):
-    """Inflow / outflow flags of an io golden case (None for a closed box)."""
+    """Inflow / outflow flags of an io golden case (None for a closed box;
+    the wave cases' faces, owned by iowave, at the reference's defaults)."""
+    if "wave_wgen" in g:
+        return dict(inflow=1, outflow=1)
     if "io_f50" not in g:
         return None
     ints = ("inflow", "outflow", "f50", "b77", "f64")
@@ -42,6 +45,15 @@ def golden_df(g):
     if "x45" not in g:
         return None
     return int(g["x45"]), g["body1"], g["body2"]
+
+
+def golden_wave(g):
+    """(generation weights, beach weights, still water level, per-step
+    targets, per-step ramps) of a wave-generator golden case, else None."""
+    if "wave_wgen" not in g:
+        return None
+    return (g["wave_wgen"], g["wave_wbeach"], float(g["wave_phimean"]), g["step_wave_targets"],
+            g["step_wave_ramp"])
 
 
 def golden_sf(g):

@@ -20,7 +20,10 @@ boundary with the reference's ioflow_f (B60 = 1) and record the water
 levels its fsfinflow measured at every step.  The df cases turn on the
 direct-forcing convection stencils (X45 1..6) over random body fields; the
 sf cases the solid forcing of the level set after each convection stage
-(X48 = 1) over a random direct-forcing boundary list.
+(X48 = 1) over a random direct-forcing boundary list; the wave cases run
+REEF3D's wave generator iowave (B90 = 1) with relaxation-zone generation and
+beach (B98 = B99 = 2) and record its relaxation weights and each step's
+targets and ramp.
 """
 import math
 import multiprocessing as mp
@@ -127,6 +130,30 @@ def sf_case(name, nx, ny, nz, f49, stretch, seed, nsf, steps=2):
     return c
 
 
+def wave_case(name, nx, ny, nz, f49, steps, wave, seed):
+    """A wave tank on the unit box (still water at 0.5) with REEF3D's wave
+    generator: linear waves relaxed in over the x-min zone, a relaxation
+    beach before the x-max face (iowave, B98 = B99 = 2), and a level set
+    slightly off the still water with a random flow."""
+    rng = np.random.default_rng(seed)
+    xn, yn, zn = stretched(nx, 0.0), stretched(ny, 0.0), stretched(nz, 0.0)
+    shape = (nx + 6, ny + 6, nz + 6)
+    ii = 0.5 * (xn[2:-3] + xn[3:-2])
+    jj = 0.5 * (yn[2:-3] + yn[3:-2])
+    kk = 0.5 * (zn[2:-3] + zn[3:-2])
+    X, Y, Z = np.meshgrid(ii, jj, kk, indexing="ij")
+    phi = wave["phimean"] + 0.02 * np.sin(2 * np.pi * X) - Z + 0.002 * rng.standard_normal(shape)
+    if ny == 1:
+        phi[:, :3, :] = 0.0
+        phi[:, 4:, :] = 0.0
+    u = 0.2 * np.cos(2 * np.pi * X) + 0.05 * rng.standard_normal(shape)
+    v = 0.05 * rng.standard_normal(shape)
+    w = 0.1 * np.sin(2 * np.pi * X) + 0.02 * rng.standard_normal(shape)
+    return dict(name=name, nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w,
+                f43=0.5, f44=2, f45=2.1, f49=f49, n47=0.25, steps=steps, vel_scale=None, f46=0, f47=10,
+                wave=wave)
+
+
 def setup_case(name, which, n, steps, f46=0, f47=10):
     from reef3d_b200 import setups
     c = setups.slotted_disk(n) if which == "disk" else setups.vortex3d(n)
@@ -165,6 +192,12 @@ CASES = [
     lambda: df_case("df6_box3d_uniform", 9, 7, 8, 0.0, 26, 6),
     lambda: sf_case("sf_box3d_stretched_f49_1", 9, 7, 8, 1, 0.3, 31, 60),
     lambda: sf_case("sf_box2d_uniform_f49_0", 12, 1, 10, 0, 0.0, 32, 40),
+    lambda: wave_case("wave_tank2d_relax", 32, 1, 16, 1, 4,
+                      dict(b92=2, amp=0.03, period=0.8, depth=0.5, b96_1=0.25, b96_2=0.25, phimean=0.5,
+                           b101=0, b102=1.0), 41),
+    lambda: wave_case("wave_tank3d_relax_ramp", 24, 5, 14, 0, 3,
+                      dict(b92=2, amp=0.04, period=0.7, depth=0.5, b96_1=0.3, b96_2=0.2, phimean=0.5,
+                           b101=1, b102=2.0), 42),
 ]
 
 
@@ -174,8 +207,10 @@ def run_case(idx):
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     io = c.get("io")
     x45 = c.get("x45", 0)
+    wave = c.get("wave")
     ref = RefOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
-                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io, x45=x45, solid_forcing=c.get("sf"))
+                    f49=c["f49"], f46=c["f46"], f47=c["f47"], ioflow=io, x45=x45, solid_forcing=c.get("sf"),
+                    iowave=wave)
     out = {k: c[k] for k in ("nx", "ny", "nz", "xn", "yn", "zn", "phi", "u", "v", "w", "f43", "f44", "f45",
                               "f49", "n47", "steps", "f46", "f47")}
     for a, n in enumerate((nx, ny, nz)):
@@ -189,6 +224,10 @@ def run_case(idx):
             out["io_" + k] = val
     if c.get("sf") is not None:
         out["sf"] = c["sf"]
+    if wave is not None:
+        for k, val in wave.items():
+            out["wave_" + k] = val
+        out["wave_wgen"], out["wave_wbeach"] = ref.iowave_weights()
     out["psi"] = ref.psi
     out["vel_scale"] = np.array(c["vel_scale"] or "none")
     phi, u, v, w = c["phi"], c["u"], c["v"], c["w"]
@@ -204,7 +243,7 @@ def run_case(idx):
     out["ghost"] = ref.ghost_fill(phi)
     T = 3.0
     t = 0.0
-    traj, dts, vols, ros, viscs, levels = [], [], [], [], [], []
+    traj, dts, vols, ros, viscs, levels, targets, ramps = [], [], [], [], [], [], [], []
     for s in range(c["steps"]):
         if c["vel_scale"] == "vortex":
             f = math.cos(math.pi * t / T)
@@ -213,6 +252,14 @@ def run_case(idx):
             ref.set_field(3, w * f)
         dt = ref.cfl_dt(c["n47"])
         ref.set_count(s + 1)  # lexer::count of the driver loop (read by picard_lsm)
+        if wave is not None:
+            # the driver's order: the wave generator's targets at the step's
+            # clock (src/driver_loop_cfd.cpp:78), then the free surface
+            ref.set_time(t)
+            ref.wavegen_precalc()
+            lsval, ramp = ref.iowave_targets()
+            targets.append(lsval)
+            ramps.append(ramp)
         ph = ref.step(dt)
         ros.append(ref.get_field(6))   # fluid_update_fsf inside the step (W1..W4 defaults)
         viscs.append(ref.get_field(7))
@@ -228,6 +275,9 @@ def run_case(idx):
     out["step_visc"] = np.array(viscs)
     if io is not None:
         out["step_io_levels"] = np.array(levels)
+    if wave is not None:
+        out["step_wave_targets"] = np.array(targets)
+        out["step_wave_ramp"] = np.array(ramps)
     np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), **out)
     return c["name"]
 

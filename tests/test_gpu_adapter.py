@@ -5,7 +5,9 @@ process, each reference object (levelset_RK3, weno_hj_df_nug, reinidisc_f /
 reinidisc_fsf, reini_RK3, fluid_update_fsf) and the adapter that replaces it
 start from the same REEF3D fields, and the fields they leave behind are
 compared (the tank_io cases with the reference's ioflow_f inflow / outflow
-boundaries, which the adapters hand to r3d_set_ioflow; the stretched_df
+boundaries, which the adapters hand to r3d_set_ioflow; the tank_wave cases
+with the reference's wave generator iowave, whose relaxation zones and
+per-step targets the adapter hands to r3d_set_relaxation; the stretched_df
 cases with the direct-forcing convection stencils X45 4 and 5 over the
 fdm's body fields).  FP64: the level
 set and the operators bit-identical on every cell
@@ -60,6 +62,25 @@ def _case(name):
         io = dict(f50=2, b77=2, f60=0.5, f62=0.52, f64=2) if ny > 1 else dict(f50=3, b77=1)
         return dict(nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w, f43=0.5, f44=2, f45=2.1,
                     f49=1, n47=0.25, f46=0, io=io)
+    if name.startswith("tank_wave"):
+        # REEF3D's wave generator (iowave) with relaxation-zone generation
+        # and beach on the x faces, still water at 0.5
+        rng = np.random.default_rng(7)
+        nx, ny, nz = (28, 1, 16) if name == "tank_wave2d" else (20, 5, 14)
+        xn, yn, zn = _stretched(nx, 0.0), _stretched(ny, 0.0), _stretched(nz, 0.0)
+        c = lambda a: 0.5 * (a[2:-3] + a[3:-2])
+        X, Y, Z = np.meshgrid(c(xn), c(yn), c(zn), indexing="ij")
+        phi = np.ascontiguousarray(0.5 + 0.02 * np.sin(2 * np.pi * X) - Z + 0.002 * rng.standard_normal(X.shape))
+        if ny == 1:
+            phi[:, :3, :] = 0.0
+            phi[:, 4:, :] = 0.0
+        u = np.ascontiguousarray(0.2 * np.cos(2 * np.pi * X) + 0.05 * rng.standard_normal(phi.shape))
+        v, w = (np.ascontiguousarray(0.05 * rng.standard_normal(phi.shape)) for _ in range(2))
+        wave = dict(b92=2, amp=0.03, period=0.8, depth=0.5, b96_1=0.25, b96_2=0.25, phimean=0.5)
+        if name == "tank_wave3d_ramp":
+            wave.update(b101=1, b102=2.0)
+        return dict(nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w, f43=0.5, f44=2, f45=2.1,
+                    f49=1, n47=0.25, f46=0, wave=wave)
     # random 3D case on a stretched grid, F49 = 0 (reinidisc_fsf) or picard
     rng = np.random.default_rng(4)
     nx, ny, nz = 11, 9, 10
@@ -109,7 +130,7 @@ def _run(name, precision=0):
     nx, ny, nz = c["nx"], c["ny"], c["nz"]
     ao = AdapterOracle(nx, ny, nz, c["xn"], c["yn"], c["zn"], f43=c["f43"], f44=c["f44"], f45=c["f45"],
                        f49=c["f49"], f46=c["f46"], f47=6, precision=precision, ioflow=c.get("io"),
-                       x45=c.get("x45", 0), solid_forcing=c.get("sf"))
+                       x45=c.get("x45", 0), solid_forcing=c.get("sf"), iowave=c.get("wave"))
     out = {}
     ao.set_state(c["phi"], c["u"], c["v"], c["w"])
     for fid, arr in c.get("bodies", {}).items():
@@ -120,10 +141,16 @@ def _run(name, precision=0):
                                              _interior(ao.gpu_reinidisc_L(c["phi"]), nx, ny, nz)))
     phi = c["phi"]
     out["phi"], out["rel"] = [], []
+    t = 0.0
     for s in range(3):
         ao.set_count(s + 1)
         ao.set_field(0, phi)
         dt = ao.cfl_dt(c["n47"])
+        if c.get("wave"):
+            # the driver's order: the wave generator's targets of the step,
+            # then the free surface (both adapters read the same targets)
+            ao.set_time(t)
+            ao.wavegen_precalc()
         ref = ao.step(dt)
         ref_ro, ref_visc, ref_vol = ao.get_field(6), ao.get_field(7), ao.volume()
         ao.set_field(0, phi)
@@ -143,6 +170,7 @@ def _run(name, precision=0):
                               abs(got_vol[0] - ref_vol[0]) / abs(ref_vol[0]),
                               abs(got_vol[1] - ref_vol[1]) / abs(ref_vol[1])))
         phi = ref
+        t += dt
     ao.set_count(1)
     ao.set_field(0, 1.5 * c["phi"])
     ref = ao.reini()
@@ -154,7 +182,8 @@ def _run(name, precision=0):
 
 
 @pytest.mark.parametrize("name", ["vortex3d", "disk2d", "stretched_f49_0", "stretched_picard", "tank_io3d",
-                                  "tank_io2d", "stretched_df4", "stretched_df5", "stretched_sf"])
+                                  "tank_io2d", "stretched_df4", "stretched_df5", "stretched_sf", "tank_wave2d",
+                                  "tank_wave3d_ramp"])
 def test_adapters_match_reference_objects(name):
     from oracle.bindings import AdapterOracle
     if not AdapterOracle.available():

@@ -12,8 +12,8 @@ import numpy as np
 import pytest
 
 import reef3d_b200 as r3d
-from conftest import (GOLDEN_CASES, body_field, golden_df, golden_flags, golden_ioflow, golden_sf, load_golden,
-                      velocity_at)
+from conftest import (GOLDEN_CASES, body_field, golden_df, golden_flags, golden_ioflow, golden_sf, golden_wave,
+                      load_golden, velocity_at)
 from test_oracle_golden import interior, visible_mask
 
 pytestmark = pytest.mark.gpu
@@ -29,7 +29,11 @@ def make_gpu(g, precision=r3d.FP64):
     ls = r3d.LevelSet(int(g["nx"]), int(g["ny"]), int(g["nz"]), g["xn"], g["yn"], g["zn"], precision=precision,
                       **golden_flags(g))
     io = golden_ioflow(g)
-    if io is not None:  # inflow / outflow faces with ioflow_f's hooks
+    wave = golden_wave(g)
+    if wave is not None:  # inflow / outflow faces of iowave with its relaxation zones
+        ls.set_ioflow(waves=True, **io)
+        ls.set_relaxation(wave[0], wave[1], wave[2])
+    elif io is not None:  # inflow / outflow faces with ioflow_f's hooks
         ls.set_ioflow(**io)
     df = golden_df(g)
     if df is not None:  # direct-forcing convection stencils (X45)
@@ -38,6 +42,13 @@ def make_gpu(g, precision=r3d.FP64):
     if golden_sf(g) is not None:  # solid forcing after each convection stage (X48)
         ls.set_solid_forcing(golden_sf(g))
     return ls
+
+
+def wave_targets(ls, g, s):
+    """The wave generator's targets of step s (wave golden cases)."""
+    wave = golden_wave(g)
+    if wave is not None:
+        ls.set_relaxation_target(wave[3][s], float(wave[4][s]))
 
 
 def levels_close(got, ref):
@@ -78,6 +89,7 @@ def test_steps_vs_reference(name):
             ls.upload(r3d.W, w)
             dt = ls.cfl_dt()
             assert dt == float(g["step_dt"][s])  # exact max reduction and dt expression
+            wave_targets(ls, g, s)
             ls.step()
             phi = ls.download(r3d.PHI)
             ref = g["step_phi"][s]
@@ -106,6 +118,7 @@ def test_fluid_update_vs_reference(name):
             for f, a in ((r3d.U, u), (r3d.V, v), (r3d.W, w)):
                 ls.upload(f, a)
             t += ls.cfl_dt()
+            wave_targets(ls, g, s)
             ls.step()
             for fid, key in ((r3d.RO, "step_ro"), (r3d.VISC, "step_visc")):
                 got, ref = ls.download(fid), g[key][s]

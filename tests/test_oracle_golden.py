@@ -5,7 +5,8 @@ layers; edge and corner ghosts are outside every stencil of the path)."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, golden_df, golden_flags, golden_ioflow, golden_sf, load_golden, velocity_at
+from conftest import (GOLDEN_CASES, golden_df, golden_flags, golden_ioflow, golden_sf, golden_wave, load_golden,
+                      velocity_at)
 
 
 def visible_mask(nx, ny, nz):
@@ -30,6 +31,10 @@ def case(request, port_lib):
         o.set_direct_forcing(*df)
     if golden_sf(g) is not None:  # solid forcing after each convection stage (X48)
         o.set_solid_forcing(golden_sf(g))
+    wave = golden_wave(g)
+    if wave is not None:  # iowave's faces and relaxation zones
+        o.set_io_waves()
+        o.set_relaxation(wave[0], wave[1], wave[2])
     return g, o
 
 
@@ -66,6 +71,9 @@ def test_steps_dt_volume(case):
         u, v, w = velocity_at(g, t)
         dt = o.cfl_dt(u, v, w)
         assert dt == g["step_dt"][s]
+        wave = golden_wave(g)
+        if wave is not None:  # the wave generator's targets of the step
+            o.set_relaxation_target(wave[3][s], float(wave[4][s]))
         phi = o.step(phi, u, v, w, dt)
         assert np.array_equal(phi[m], g["step_phi"][s][m])
         assert o.volume(phi) == tuple(g["step_volume"][s])
