@@ -59,6 +59,7 @@
 #include <cstring>
 #include <new>
 #include <vector>
+#include <unistd.h>
 
 namespace {
 
@@ -410,7 +411,14 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
     // (src/driver_logic_cfd.cpp:661-672)
     if (G_IOW.on) {
         p->phimean = p->phiout = p->phiin = G_IOW.phimean;  // src/ini_phi.cpp:33
+        // iowave's constructor writes the wave time series into
+        // ./REEF3D_Log-Wave (src/iowave_timeseries.cpp:38-58): construct it
+        // from a scratch directory so the caller's working directory stays clean
+        char cwd[4096];
+        char scratch[] = "/tmp/refls_wave_XXXXXX";
+        bool moved = getcwd(cwd, sizeof cwd) != nullptr && mkdtemp(scratch) != nullptr && chdir(scratch) == 0;
         FLOW = WAVE = new iowave(p, PGC, new patchBC_void(p));
+        if (moved && chdir(cwd) != 0) return -2;
     }
     else if (G_IO.on) FLOW = new ioflow_f(p, PGC, new patchBC_void(p));
     else FLOW = new ioflow_v(p, PGC, new patchBC_void(p));
