@@ -29,10 +29,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_CELLS_EDGE = 256
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# the dominant FP32 kernel, the tiled reinitialisation stage 2, measured by ncu
-# on the 256^3 vortex (profiles/tile_stage_kernels_vortex.txt)
-NCU_TRAFFIC = {(256, "reinit_stage"): 145.90e6 + 45.69e6}
+# ncu summary of the tiled FP32 stage kernels on the vortex: its "traffic:"
+# lines carry the DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
+# one launch per (stage kind, grid edge, tile configuration, z chunk), from
+# the capture whose command the file gives
+TRAFFIC_PROFILE = os.path.join("profiles", "tile_stage_kernels_vortex.txt")
 METRIC = "level-set cell-updates/s (RK3+reinit), FP64 plain vs FP32 batched; p50/p99 latency"
 WORKLOAD = "3D single-vortex deformation 256^3, CFL 0.25, F44=2 reinit pseudo-steps, T=3"
 
@@ -46,6 +47,9 @@ def parse():
     ap.add_argument("--edge", type=int, default=N_CELLS_EDGE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile-cache", default=None,
+                    help="autotune cache file: a run reuses the tile configuration an earlier run stored there "
+                         "(so that a profiled run launches the same kernels as the timed one)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other workloads (slotted disc, vortex accuracy, wave tank, ensemble, serving)")
     return ap.parse_args()
@@ -214,7 +218,7 @@ def reference_cpu(edge, steps, warmup, procs):
         return None, {"unavailable": "reference process failed: " + errs[0]}
     per = [t for r, _ in res for t in r]
     cells = edge ** 3 * steps
-    return cells / wall, {"cores": procs, "kind": "reference", "host": host_cpu(),
+    return cells / wall, {"cores": procs, "kind": "reference", "host": host_cpu(), "timed_s": wall,
                           "build": "-O3 -mavx2 -mfma" if fast else "-O2 -ffp-contract=off",
                           "steps": steps, "warmup": warmup,
                           "s_per_step_one_core": statistics.mean(per),
@@ -282,7 +286,7 @@ def run_reference_arm(args, rank):
         print(json.dumps({"impl": "reference", "unavailable": info["unavailable"]}))
         return
     base = {"metric": METRIC, "impl": "reference", "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.edge ** 3 / rate,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * info["timed_s"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "edge": args.edge, "cells_per_step": args.edge ** 3,
                        "form": "the reference's FP64 code on the host cores"},
@@ -361,6 +365,28 @@ def stage_roofline(ls, cells, elem, peak_gbs, reps=20):
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
             "frac": achieved / peak_gbs, "bytes_per_launch": alg, "ms_per_launch": t,
             "conv_stage_ms": t_conv, "reinit_stage_ms": t_rein}
+
+
+def profiled_traffic(kind, edge, cfg, chunk):
+    """DRAM bytes of one launch of the dominant stage kernel from the ncu
+    summary committed under profiles/ (None when that file holds no capture
+    of this stage kind, grid, tile configuration and chunk).  A line reads
+    `traffic: <kind> edge=<n> cfg=<id> chunk=<kc> read=<bytes> write=<bytes>`."""
+    try:
+        lines = open(os.path.join(ROOT, TRAFFIC_PROFILE)).read().splitlines()
+    except OSError:
+        return None
+    for ln in lines:
+        if not ln.startswith("traffic: "):
+            continue
+        f = ln.split()
+        kv = dict(x.split("=", 1) for x in f[2:] if "=" in x)
+        if f[1] == kind and int(kv["edge"]) == edge and int(kv["cfg"]) == cfg and int(kv["chunk"]) == chunk:
+            rd, wr = float(kv["read"]), float(kv["write"])
+            return {"bytes": rd + wr, "read": rd, "write": wr, "source": TRAFFIC_PROFILE,
+                    "note": "one ncu capture of a launch; output lines still in L2 when the kernel ends are "
+                            "written back after it and are not in its write figure"}
+    return None
 
 
 def tile_variants(ls, reps=10):
@@ -460,7 +486,7 @@ def run_ours(args):
     ls32 = make_instance(case, r3d.FP32)
     # tile configuration and z chunk per stage kind, picked by timing
     # (r3d_autotune; untimed, before the warm-up)
-    cfg, kc = ls32.autotune()
+    cfg, kc = ls32.autotune(args.tile_cache)
     tile_cfg = {"convection": {"cfg": cfg, "chunk": kc, "tile": r3d.tile_configs()[cfg]},
                 "reinit": {"cfg": ls32.get_option(r3d.OPT_TILE_CFG_REINIT),
                            "chunk": ls32.get_option(r3d.OPT_CHUNK_REINIT),
@@ -501,6 +527,8 @@ def run_ours(args):
     configs = None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_configs:
         configs = run_configs(ctx)
+    kind = "reinit" if roof32["kernel"] == "reinit_stage" else "convection"
+    traffic = profiled_traffic(kind, args.edge, tile_cfg[kind]["cfg"], tile_cfg[kind]["chunk"])
     value32 = cells * args.steps * ctx.world / (total32 * 1e-3)
     value64 = cells * args.steps * ctx.world / (total64 * 1e-3)
     out = {
@@ -518,7 +546,7 @@ def run_ours(args):
                        "p99_ms": float(np.percentile(per64, 99)), "roofline": roof64,
                        "gpu_launches": launches64},
         "fp32_over_fp64": value32 / value64,
-        "roofline": dict(roof32, traffic=NCU_TRAFFIC.get((args.edge, roof32["kernel"])), peak_source=peak_src),
+        "roofline": dict(roof32, traffic=(traffic or {}).get("bytes"), traffic_detail=traffic, peak_source=peak_src),
         "tile_variants": variants,
         "tile_config": tile_cfg,
         "gpu_launches": launches32,

@@ -167,6 +167,31 @@ int r3d_write_vtu(r3d_handle* h, const char* path);
 int r3d_save_state(r3d_handle* h, const char* path);
 int r3d_load_state(r3d_handle* h, const char* path);
 
+/* The reference's restart state file, so that a REEF3D run restarts from a
+ * state this library wrote and the reverse: replaces cfd_state::write
+ * (src/cfd_state.cpp:201-220 -> write_result, src/cfd_state_write.cpp:34-146)
+ * and cfd_state::read (src/cfd_state_read.cpp:44-195) for a single rank.
+ * The file holds the header below and single-precision blocks in the
+ * reference's loop order: topo, u, v, w, press, phi, kin, eps, eddyv, the
+ * bed-load slice qbe, conc (u, v, w without the far wall face, ulast =
+ * vlast = wlast = 1; no v block on a 2D grid; every cell fluid).  The level
+ * set and the velocities come from / go to the instance; the other fields
+ * from / to `extra` (7 pointers in the order topo, press, kin, eps, eddyv,
+ * qbe, conc: dense x-contiguous arrays, qbe nx*ny; a NULL array, or a NULL
+ * `extra`, writes zeros / skips the field).  The reference names the file
+ * REEF3D_CFD_STATE/REEF3D-CFD-State-<num %08d>-<rank+1 %06d>.r3d.  Reading
+ * keeps the instance's values where the file has none (ghost cells, the far
+ * wall faces), then refills the level set's ghost cells (ghostcell::start4,
+ * as the reference does).  Synchronous. */
+typedef struct r3d_state_info {
+    int count;       /* p->count, the step number */
+    int printcount;  /* p->printcount */
+    double simtime, printtime, sedprinttime, fsfprinttime, probeprinttime, stateprinttime;
+} r3d_state_info;
+int r3d_write_reef3d_state(r3d_handle* h, const char* path, const r3d_state_info* info,
+                           const double* const* extra);
+int r3d_read_reef3d_state(r3d_handle* h, const char* path, r3d_state_info* info, double* const* extra);
+
 /* Volume sums of the smoothed Heaviside (fluid_update_fsf::start,
  * src/fluid_update_fsf.cpp:39-74), FP64.  Synchronous. */
 int r3d_volume(r3d_handle* h, double* volume1, double* volume2);
@@ -269,10 +294,12 @@ int r3d_cfl_dt_from_max(r3d_handle* h, const double* vmax, double* dt);
  * x45 != 0 and uploaded like any field (REEF3D layout: its ghost cells are
  * read too); it is held in FP64 in both arithmetic forms, so the mask
  * decisions are the reference's.  The reinitialisation is unchanged (the
- * reference applies X45 to the convection only).  FP32 instances take X45
- * 1..5 (the 1e20 of X45 6 squares past the FP32 range) and run the
- * one-cell-per-thread kernels.  0 turns it off.  Synchronous.  Not for
- * batch members. */
+ * reference applies X45 to the convection only).  FP32 instances run the
+ * one-cell-per-thread kernels; with X45 6 (masked differences 1e20, whose
+ * squares pass the FP32 range) a stencil holding a masked difference gets
+ * weight 0 (~1e-80 relative in the reference's FP64), and a cell whose
+ * three stencils all hold one is evaluated in FP64.  0 turns it off.
+ * Synchronous.  Not for batch members. */
 int r3d_set_direct_forcing(r3d_handle* h, int x45);
 
 /* Relaxation zones of REEF3D's wave generator and numerical beach on the

@@ -294,6 +294,25 @@ class RefOracle:
         self._lib.refls_get_field(fid, _dp(a))
         return a
 
+    def write_state(self, directory, count, printcount, simtime):
+        """The reference's restart state file (cfd_state::write) of the
+        current fields under directory/REEF3D_CFD_STATE/; returns its path."""
+        lib = self._lib
+        lib.refls_write_state.argtypes = [ctypes.c_char_p, _I, _I, ctypes.c_double]
+        if lib.refls_write_state(os.fsencode(directory), count, printcount, simtime) != 0:
+            raise RuntimeError("refls_write_state failed")
+        return os.path.join(directory, "REEF3D_CFD_STATE", "REEF3D-CFD-State-%08i-%06i.r3d" % (0, 1))
+
+    def read_state(self, directory, num=0):
+        """cfd_state::read of state `num` from directory/REEF3D_CFD_STATE/;
+        returns (count, simtime)."""
+        lib = self._lib
+        lib.refls_read_state.argtypes = [ctypes.c_char_p, _I, ctypes.POINTER(ctypes.c_int), _D]
+        c, t = ctypes.c_int(), ctypes.c_double()
+        if lib.refls_read_state(os.fsencode(directory), num, ctypes.byref(c), ctypes.byref(t)) != 0:
+            raise RuntimeError("refls_read_state failed")
+        return c.value, t.value
+
     def set_state(self, phi, u, v, w):
         for fid, arr in ((0, phi), (1, u), (2, v), (3, w)):
             self.set_field(fid, arr)

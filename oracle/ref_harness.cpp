@@ -53,8 +53,11 @@
 #include "flowfile_in.h"
 #define private public
 #include "iowave.h"
+#include "cfd_state.h"
+#include "sediment_void.h"
 #undef private
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -113,6 +116,10 @@ field* field_by_id(int id) {
         case 10: return &A->fbh5;
         case 11: return &A->solid;
         case 12: return &A->topo;
+        // further fields of the restart state file (src/cfd_state_write.cpp)
+        case 13: return &A->press;
+        case 14: return &A->eddyv;
+        case 15: return &A->conc;
         default: return nullptr;
     }
 }
@@ -645,6 +652,62 @@ double refls_cfl_dt(double n47) {
 int refls_update() {
     LS->update(P, A, PGC, A->phi);
     return 0;
+}
+
+// The reference's restart state file of the current fields: cfd_state::write
+// (src/cfd_state.cpp:201-220, i.e. write_result, src/cfd_state_write.cpp:34-146)
+// with the step count, print count and time given, from the working
+// directory `dir` (the file lands in dir/REEF3D_CFD_STATE/, named
+// REEF3D-CFD-State-00000000-000001.r3d: the first file of a single rank,
+// P15 = 1).  Turbulence and sediment are the void models (k, epsilon and the
+// bed-load slice written as their zeros).  P45 = 1: no continuous file.
+// The water-surface slices of every interior column, as a DIVEMesh grid
+// marks them (src/read_grid.cpp:753-758), while a state file is written or
+// read (its bed-load block is a SLICELOOP4); the harness's marks otherwise.
+struct SliceMarks {
+    std::vector<int> saved;
+    SliceMarks() {
+        const long n = (long)P->imax * P->jmax;
+        saved.assign(P->flagslice4, P->flagslice4 + n);
+        for (int i = 0; i < P->knox; ++i)
+            for (int j = 0; j < P->knoy; ++j) P->flagslice4[(i - P->imin) * P->jmax + (j - P->jmin)] = 1;
+    }
+    ~SliceMarks() { std::copy(saved.begin(), saved.end(), P->flagslice4); }
+};
+
+int refls_write_state(const char* dir, int count, int printcount, double simtime) {
+    char cwd[4096];
+    if (!P || !getcwd(cwd, sizeof cwd) || chdir(dir) != 0) return -1;
+    SliceMarks marks;
+    P->count = count;
+    P->printcount = printcount;
+    P->simtime = simtime;
+    P->P15 = 1; P->P40 = 0; P->P43 = 0; P->P45 = 1;
+    {
+        sediment_void sed;
+        cfd_state st(P, A, PGC, 0);
+        st.write(P, A, PGC, TURB, &sed);
+    }
+    return chdir(cwd) == 0 ? 0 : -2;
+}
+
+// cfd_state::read (src/cfd_state_read.cpp) of state number num from
+// dir/REEF3D_CFD_STATE/, with the control file's defaults for the topo
+// ghost condition (S50 = 4, src/ini.cpp:783); the fields and p->count /
+// p->simtime are then the file's.
+int refls_read_state(const char* dir, int num, int* count, double* simtime) {
+    char cwd[4096];
+    if (!P || !getcwd(cwd, sizeof cwd) || chdir(dir) != 0) return -1;
+    P->I41 = num; P->P43 = 0; P->P45 = 1; P->S50 = 4;
+    SliceMarks marks;
+    {
+        sediment_void sed;
+        cfd_state st(P, A, PGC, 1);
+        st.read(P, A, PGC, TURB, &sed);
+    }
+    *count = P->count;
+    *simtime = P->simtime;
+    return chdir(cwd) == 0 ? 0 : -2;
 }
 
 }  // extern "C"

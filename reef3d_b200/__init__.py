@@ -46,6 +46,23 @@ class GridDesc(ctypes.Structure):
     ]
 
 
+class StateInfo(ctypes.Structure):
+    """r3d_state_info: the header of the reference's restart state file."""
+    _fields_ = [("count", ctypes.c_int), ("printcount", ctypes.c_int)] + [
+        (n, ctypes.c_double) for n in ("simtime", "printtime", "sedprinttime", "fsfprinttime", "probeprinttime",
+                                       "stateprinttime")]
+
+
+# the fields of the reference's state file the library does not hold, in the
+# order of r3d_write_reef3d_state's `extra`
+STATE_EXTRA = ("topo", "press", "kin", "eps", "eddyv", "qbe", "conc")
+
+
+def reef3d_state_name(num, rank=0):
+    """The reference's state file name (src/cfd_state_filename.cpp:27)."""
+    return "REEF3D-CFD-State-%08i-%06i.r3d" % (num, rank + 1)
+
+
 class IoflowDesc(ctypes.Structure):
     """r3d_ioflow_desc: inflow (x-min) / outflow (x-max) faces and ioflow_f's flags."""
     _fields_ = [
@@ -113,6 +130,8 @@ EXPORTS = {
     "r3d_write_vtu": ([_H, ctypes.c_char_p], ctypes.c_int),
     "r3d_save_state": ([_H, ctypes.c_char_p], ctypes.c_int),
     "r3d_load_state": ([_H, ctypes.c_char_p], ctypes.c_int),
+    "r3d_write_reef3d_state": ([_H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "r3d_read_reef3d_state": ([_H, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "r3d_grid_spacing": ([ctypes.POINTER(GridDesc), _D], ctypes.c_int),
     "r3d_set_grid_spacing": ([_H, ctypes.c_double, ctypes.c_double, ctypes.c_double], ctypes.c_int),
     "r3d_halo_bytes": ([_H, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
@@ -215,6 +234,25 @@ def _check(rc, h=None):
     if rc != R3D_OK:
         msg = _lib.r3d_last_error(h)
         raise R3DError(rc, msg.decode() if msg else "")
+
+
+def _extra_arrays(extra, dims, fill):
+    """The 7 `extra` pointers of the state-file calls: dense arrays (shape
+    (nz, ny, nx), qbe (ny, nx)) given (fill) or allocated to receive."""
+    if extra is None:
+        return None, None
+    nx, ny, nz = dims
+    keep, ptrs = [], (_D * len(STATE_EXTRA))()
+    for q, name in enumerate(STATE_EXTRA):
+        shape = (ny, nx) if name == "qbe" else (nz, ny, nx)
+        a = extra.get(name)
+        if a is None and fill:
+            keep.append(None)
+            continue
+        a = np.zeros(shape) if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(shape)
+        keep.append(a)
+        ptrs[q] = _dp(a)
+    return keep, ptrs
 
 
 def _dp(a):
@@ -414,6 +452,29 @@ class LevelSet:
     def load_state(self, path):
         """Resume from a checkpoint of the same grid and configuration."""
         _check(_lib.r3d_load_state(self.h, os.fsencode(path)), self.h)
+
+    def write_reef3d_state(self, path, count=0, printcount=0, simtime=0.0, times=None, extra=None):
+        """The reference's restart state file of this instance
+        (r3d_write_reef3d_state): level set and velocities from the device;
+        `extra` maps names of STATE_EXTRA to dense arrays (x contiguous,
+        `qbe` nx*ny), the others are written as zeros; `times` maps the
+        header's other times (printtime, ...) to values."""
+        info = StateInfo(count=count, printcount=printcount, simtime=simtime, **(times or {}))
+        keep, ptrs = _extra_arrays(extra, (self.nx, self.ny, self.nz), fill=True)
+        _check(_lib.r3d_write_reef3d_state(self.h, os.fsencode(path), ctypes.byref(info), ptrs), self.h)
+        del keep
+
+    def read_reef3d_state(self, path, extra=False):
+        """Load the level set and velocities of a reference state file
+        (r3d_read_reef3d_state); returns the header as a dict, with the
+        file's other fields under "extra" (dense arrays) when `extra`."""
+        info = StateInfo()
+        keep, ptrs = _extra_arrays({n: None for n in STATE_EXTRA} if extra else None, (self.nx, self.ny, self.nz), fill=False)
+        _check(_lib.r3d_read_reef3d_state(self.h, os.fsencode(path), ctypes.byref(info), ptrs), self.h)
+        out = {n: getattr(info, n) for n, _ in StateInfo._fields_}
+        if extra:
+            out["extra"] = dict(zip(STATE_EXTRA, keep))
+        return out
 
     def set_halo(self, zlo, zhi):
         """Mark the z-min / z-max faces as subdomain boundaries (r3d_set_halo)."""

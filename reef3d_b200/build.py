@@ -35,6 +35,7 @@ UNITS = [
     ("api.cpp", []),
     ("batch.cpp", []),
     ("serve.cpp", []),
+    ("state.cpp", []),
 ]
 HEADERS = ["r3d_internal.h", "stencil_f64.cuh", "stencil_f32.cuh", "tile_host.h", "cell_f32.cuh", "handle.h", "batch_internal.h"]
 

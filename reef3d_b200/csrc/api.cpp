@@ -66,7 +66,7 @@ size_t footprint(const r3d_grid_desc* d, const Layout& L) {
     size_t b = 7 * (size_t)L.ncell * e;
     size_t tab = 0;
     const int n[3] = {d->nx, d->ny, d->nz};
-    for (int a = 0; a < 3; ++a) tab += 2 * (size_t)(n[a] + 21) + (size_t)(n[a] + 8) * 36;
+    for (int a = 0; a < 3; ++a) tab += 3 * (size_t)(n[a] + 21) + (size_t)(n[a] + 8) * 36;
     b += tab * (8 + 4);
     const long long blocks = (long long)((d->nx + 31) / 32) * ((d->ny + 3) / 4 + 4) * (d->nz + 4);
     b += (size_t)(blocks + (long long)d->ny * d->nz + 64) * 16 + 256;
@@ -82,6 +82,9 @@ void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
         const size_t o_dxp = off;
         for (double v : h->M.dxp[a]) host.push_back((T)v);
         off = host.size();
+        const size_t o_rdxp = off;
+        for (double v : h->M.dxp[a]) host.push_back((T)(1.0 / v));
+        off = host.size();
         const size_t o_dxn = off;
         for (double v : h->M.dxn[a]) host.push_back((T)v);
         off = host.size();
@@ -95,6 +98,7 @@ void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
         for (double v : h->M.isf[a]) host.push_back((T)v);
         off = host.size();
         g.dxp[a] = base + o_dxp;
+        g.rdxp[a] = base + o_rdxp;
         g.dxn[a] = base + o_dxn;
         g.qf[a] = base + o_qf;
         g.cf[a] = base + o_cf;
@@ -113,7 +117,7 @@ void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
 size_t metric_count(const r3d_handle* h) {
     size_t c = 0;
     for (int a = 0; a < 3; ++a)
-        c += h->M.dxp[a].size() + h->M.dxn[a].size() + h->M.qf[a].size() + h->M.cf[a].size() + h->M.isf[a].size();
+        c += 2 * h->M.dxp[a].size() + h->M.dxn[a].size() + h->M.qf[a].size() + h->M.cf[a].size() + h->M.isf[a].size();
     return c;
 }
 
@@ -1281,8 +1285,6 @@ int r3d_set_direct_forcing(r3d_handle* h, int x45) {
     if (!h) return fail(nullptr, R3D_EINVAL, "null handle");
     if (h->batch_stream) return fail(h, R3D_ESTATE, "the instance is a batch member");
     if (x45 < 0 || x45 > 6) return fail(h, R3D_EINVAL, "x45 must be 0..6");
-    if (x45 == 6 && fp32(h))
-        return fail(h, R3D_EINVAL, "X45 6 (1e20 in masked differences, whose squares overflow FP32) runs in FP64");
     DeviceGuard dg(h->device, h->batch_stream);
     if (x45 != 0 && !h->field[R3D_BODY]) {
         const size_t bytes = (size_t)h->L.ncell * sizeof(double);

@@ -15,8 +15,8 @@ __device__ __forceinline__ void load7(const float* __restrict__ f, long long c, 
 
 // Direct-forcing divided difference of the X45 stencils
 // (src/weno_hj_df_nug.cpp:398-987) in the FP32 form: the mask decisions on
-// the FP64 body field (the reference's), the difference in FP32.  X45 1..5
-// (6 writes 1e20 into masked differences, whose squares overflow FP32).
+// the FP64 body field (the reference's), the difference in FP32.  X45 6
+// (masked differences 1e20) is handled by deriv_tables_df6.
 __device__ __forceinline__ float df_q32(int x45, double thr, float fa, float fb, double ha, double hb, double hw,
                                         float d) {
     switch (x45) {
@@ -26,6 +26,67 @@ __device__ __forceinline__ float df_q32(int x45, double thr, float fa, float fb,
         case 4: return __fdividef((float)hw * (fb - fa), d);
         default: return (hb > 0.0 && ha > 0.0) ? __fdividef(fb - fa, d) : 0.0f;
     }
+}
+
+// X45 = 6 (src/weno_hj_df_nug.cpp:868-987): a difference whose pair of
+// cells is not all fluid (fbh4 >= 0.5 at either) is 1e20 in the reference,
+// and 1e20 squared overflows FP32.  In the reference's FP64 a stencil that
+// holds such a difference has a smoothness indicator ~1e40, hence a weight
+// ~1e-80 relative to any stencil without one: here that weight is exactly 0.
+// When all three stencils hold one (the upwind face of the cell is masked,
+// or one face on each side), or the FP32 weights leave the FP32 range (the
+// 1e20-scale values such cells feed into the next stages), the reference's
+// arithmetic runs in FP64 on the FP32 values and tables and is rounded to
+// FP32.
+__device__ __forceinline__ float deriv_tables_df6(const float* fv, const double* hv, bool plus,
+                                                  const float* __restrict__ dp, const float* __restrict__ qf,
+                                                  const float* __restrict__ cf, const float* __restrict__ isf, int t) {
+    const int off = plus ? 1 : 0;
+    float q[5];
+    bool masked[5];
+#pragma unroll
+    for (int m = 1; m <= 5; ++m) {
+        const int a = m - 1 + off, b = m + off;
+        masked[m - 1] = !(hv[b] < 0.5 && hv[a] < 0.5);
+        q[m - 1] = masked[m - 1] ? 0.0f : __fdividef(fv[b] - fv[a], __ldg(dp + t - 4 + m + off));
+    }
+    const int side = plus ? 1 : 0;
+    const float* Q = qf + t * 12 + side * 6;
+    const float* C = cf + t * 6 + side * 3;
+    const float* S = isf + t * 18 + side * 9;
+    const bool z1 = masked[2] || masked[3] || masked[4];  // stencil (q3, q4, q5)
+    const bool z2 = masked[1] || masked[2] || masked[3];  // (q2, q3, q4)
+    const bool z3 = masked[0] || masked[1] || masked[2];  // (q1, q2, q3)
+    if (!(z1 && z2 && z3)) {
+        const float r = f32::weno5_tables(Q, C, S, plus, q[0], q[1], q[2], q[3], q[4], z1, z2, z3);
+        if (isfinite(r)) return r;
+    }
+    // the reference's weighting (src/weno_nug_func.h:48-73, 133-153) in FP64
+    double d[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+        d[m] = masked[m] ? 1.0e20 : (double)(fv[m + 1 + off] - fv[m + off]) / (double)__ldg(dp + t - 3 + m + off);
+    const double dq12 = d[0] - d[1], dq23 = d[1] - d[2], dq32 = d[2] - d[1];
+    const double dq34 = d[2] - d[3], dq43 = d[3] - d[2], dq54 = d[4] - d[3];
+    const double is1 = (double)__ldg(S + 0) * dq54 * dq54 + (double)__ldg(S + 1) * dq54 * dq34 +
+                       (double)__ldg(S + 2) * dq34 * dq34 + 1.0e-6;
+    const double is2 = (double)__ldg(S + 3) * dq23 * dq23 + (double)__ldg(S + 4) * dq43 * dq23 +
+                       (double)__ldg(S + 5) * dq43 * dq43 + 1.0e-6;
+    const double is3 = (double)__ldg(S + 6) * dq12 * dq12 + (double)__ldg(S + 7) * dq32 * dq12 +
+                       (double)__ldg(S + 8) * dq32 * dq32 + 1.0e-6;
+    const double al1 = (double)__ldg(C + 0) / (is1 * is1), al2 = (double)__ldg(C + 1) / (is2 * is2),
+                 al3 = (double)__ldg(C + 2) / (is3 * is3);
+    double p1, p2, p3;
+    if (!plus) {
+        p1 = d[3] + (double)__ldg(Q + 0) * (d[2] - d[3]) - (double)__ldg(Q + 1) * (d[4] - d[3]);
+        p2 = d[2] + (double)__ldg(Q + 2) * (d[3] - d[2]) - (double)__ldg(Q + 3) * (d[1] - d[2]);
+        p3 = d[1] + (double)__ldg(Q + 4) * (d[0] - d[1]) + (double)__ldg(Q + 5) * (d[2] - d[1]);
+    } else {
+        p1 = d[3] + (double)__ldg(Q + 0) * (d[2] - d[3]) + (double)__ldg(Q + 1) * (d[4] - d[3]);
+        p2 = d[2] + (double)__ldg(Q + 2) * (d[1] - d[2]) - (double)__ldg(Q + 3) * (d[3] - d[2]);
+        p3 = d[1] + (double)__ldg(Q + 4) * (d[2] - d[1]) - (double)__ldg(Q + 5) * (d[0] - d[1]);
+    }
+    return (float)((al1 * p1 + al2 * p2 + al3 * p3) / (al1 + al2 + al3));
 }
 
 // deriv_tables with the X45 differences: fv, hv the 7-point windows of the
@@ -66,6 +127,7 @@ __device__ __forceinline__ float conv_L(const KGrid<float>& g, const float* __re
     auto axis = [&](long long s, int a, int t, bool plus) {
         if (DF) {
             load7d(g.body, c, s, hv);
+            if (g.x45 == 6) return deriv_tables_df6(fv, hv, plus, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t);
             return deriv_tables_df(fv, hv, plus, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, g.x45, g.df_thr);
         }
         return UNIFORM ? f32::deriv_uniform<float>(fv, plus, g.rh[a], g.eps_u * g.h[a] * g.h[a])

@@ -72,6 +72,7 @@ template <typename T>
 struct KGrid {
     Layout L;
     const T* dxp[3];
+    const T* rdxp[3];  // 1 / DXP, the IEEE quotient (the FP64 face divisions, div_rn)
     const T* dxn[3];
     const T* qf[3];
     const T* cf[3];

@@ -61,16 +61,22 @@ __device__ __forceinline__ R weno5_uniform(bool plus, R d1, R d2, R d3, R d4, R 
 }
 
 // The reference's non-uniform form (tables, divided differences) in FP32.
+// zero1..zero3: the weight of stencil (q3,q4,q5) / (q2,q3,q4) / (q1,q2,q3)
+// is set to 0 (the X45 = 6 masked differences; at least one stays on).
 __device__ __forceinline__ float weno5_tables(const float* __restrict__ Q, const float* __restrict__ C,
                                               const float* __restrict__ S, bool plus, float q1, float q2,
-                                              float q3, float q4, float q5) {
+                                              float q3, float q4, float q5, bool zero1 = false,
+                                              bool zero2 = false, bool zero3 = false) {
     const float dq12 = q1 - q2, dq23 = q2 - q3, dq32 = q3 - q2;
     const float dq34 = q3 - q4, dq43 = q4 - q3, dq54 = q5 - q4;
     const float is1 = __ldg(S + 0) * dq54 * dq54 + __ldg(S + 1) * dq54 * dq34 + __ldg(S + 2) * dq34 * dq34;
     const float is2 = __ldg(S + 3) * dq23 * dq23 + __ldg(S + 4) * dq43 * dq23 + __ldg(S + 5) * dq43 * dq43;
     const float is3 = __ldg(S + 6) * dq12 * dq12 + __ldg(S + 7) * dq32 * dq12 + __ldg(S + 8) * dq32 * dq32;
     const float r1 = __frcp_rn(is1 + 1.0e-6f), r2 = __frcp_rn(is2 + 1.0e-6f), r3 = __frcp_rn(is3 + 1.0e-6f);
-    const float al1 = __ldg(C + 0) * r1 * r1, al2 = __ldg(C + 1) * r2 * r2, al3 = __ldg(C + 2) * r3 * r3;
+    float al1 = __ldg(C + 0) * r1 * r1, al2 = __ldg(C + 1) * r2 * r2, al3 = __ldg(C + 2) * r3 * r3;
+    if (zero1) al1 = 0.0f;
+    if (zero2) al2 = 0.0f;
+    if (zero3) al3 = 0.0f;
     const float inv = __frcp_rn(al1 + al2 + al3);
     float p1, p2, p3;
     if (!plus) {

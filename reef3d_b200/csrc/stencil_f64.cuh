@@ -2,13 +2,31 @@
 // operation order.  Included only by translation units compiled with
 // -fmad=false, so every product and sum rounds separately as in the
 // reference built without FMA contraction; double division and sqrt are
-// IEEE round-to-nearest on the device as on the host.
+// IEEE round-to-nearest on the device as on the host (the divisions by grid
+// spacings through div_rn, which forms the same quotient).
 #pragma once
 
 #include "r3d_internal.h"
 
+
 namespace r3d {
 namespace f64 {
+
+// a / b rounded to nearest from r = 1/b rounded to nearest (the IEEE
+// reciprocal, tabulated per grid spacing): q0 = a r, then two residual
+// corrections with fused multiply-adds (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990).  The first correction makes the quotient faithful; a
+// faithful quotient corrected once more with the correctly rounded
+// reciprocal is the correctly rounded quotient (Markstein's theorem), i.e.
+// the IEEE a / b.  Valid when the residual neither overflows nor underflows,
+// which holds for level-set differences over grid spacings.  A zero
+// numerator gives +0 where the IEEE quotient of -0 is -0.
+__device__ __forceinline__ double div_rn(double a, double b, double r) {
+    const double q0 = a * r;
+    const double q1 = fma(fma(-b, q0, a), r, q0);
+    return fma(fma(-b, q1, a), r, q1);
+}
 
 // WENO5 derivative from the divided differences q1..q5 of the upwind set,
 // node tables of index t.  Minus side: IS src/weno_nug_func.h:48-60,
@@ -51,22 +69,24 @@ __device__ __forceinline__ double weno5(const double* __restrict__ Q, const doub
 // cell index t = idx+5.  Minus stencil src/weno_hj_df_nug.cpp:344-351, plus
 // stencil :371-378 (shared with src/ddweno_nug_sf.cpp:225-277): the six
 // points f[c+(o+m)s], m = 0..5, with o = -3 (minus) or -2 (plus), and
-// q_m = (f_m - f_{m-1}) / DXP[t+o+m-1].  The side is a runtime value, so a
+// q_m = (f_m - f_{m-1}) / DXP[t+o+m-1], the IEEE quotient formed by div_rn
+// from the reciprocal table rp of dp.  The side is a runtime value, so a
 // warp whose cells take different sides runs one evaluation, not both.
 __device__ __forceinline__ double deriv(const double* __restrict__ f, long long c, long long s,
-                                        const double* __restrict__ dp, const double* __restrict__ qf,
-                                        const double* __restrict__ cf, const double* __restrict__ isf, int t,
-                                        bool plus) {
+                                        const double* __restrict__ dp, const double* __restrict__ rp,
+                                        const double* __restrict__ qf, const double* __restrict__ cf,
+                                        const double* __restrict__ isf, int t, bool plus) {
     const int o = plus ? -2 : -3;
     const double* p = f + c + o * s;
     const double* d = dp + t + o;
+    const double* rd = rp + t + o;
     const double f0 = __ldg(p), f1 = __ldg(p + s), f2 = __ldg(p + 2 * s);
     const double f3 = __ldg(p + 3 * s), f4 = __ldg(p + 4 * s), f5 = __ldg(p + 5 * s);
-    const double q1 = (f1 - f0) / __ldg(d);
-    const double q2 = (f2 - f1) / __ldg(d + 1);
-    const double q3 = (f3 - f2) / __ldg(d + 2);
-    const double q4 = (f4 - f3) / __ldg(d + 3);
-    const double q5 = (f5 - f4) / __ldg(d + 4);
+    const double q1 = div_rn(f1 - f0, __ldg(d), __ldg(rd));
+    const double q2 = div_rn(f2 - f1, __ldg(d + 1), __ldg(rd + 1));
+    const double q3 = div_rn(f3 - f2, __ldg(d + 2), __ldg(rd + 2));
+    const double q4 = div_rn(f4 - f3, __ldg(d + 3), __ldg(rd + 3));
+    const double q5 = div_rn(f5 - f4, __ldg(d + 4), __ldg(rd + 4));
     const int side = plus ? 1 : 0;
     return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
                  isf + (long long)t * 18 + side * 9, plus, q1, q2, q3, q4, q5);
@@ -149,7 +169,7 @@ __device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* _
     const double kadvec = 0.5 * (vs * __ldg(w + c) + vs * __ldg(w + c - sz));
     auto axis = [&](long long s, int a, int t, bool plus) {
         if (DF) return deriv_df(f, g.body, c, s, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus, g.x45, g.df_thr);
-        return deriv(f, c, s, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus);
+        return deriv(f, c, s, g.dxp[a], g.rdxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus);
     };
     // advec > 0: minus side, < 0: plus side, == 0: no contribution (grad 0)
     double grad = axis(1, 0, i + 5, iadvec < 0.0);
@@ -183,16 +203,18 @@ __device__ __forceinline__ bool same_sign(const double* __restrict__ f, long lon
 
 // The six face divided differences around the cell along one axis (stride
 // s, cell index t = idx + 5): Q[m] = (f[c+(m-2)s] - f[c+(m-3)s]) /
-// DXP[t+m-3], the layout deriv_q reads.  Each is the division deriv forms
-// for that face, and faces 2 and 3 are the backward and forward differences
-// of the reinitialisation's Godunov test.
+// DXP[t+m-3] (div_rn with the reciprocal table rp of dp), the layout deriv_q
+// reads.  Each is the quotient deriv forms for that face, and faces 2 and 3
+// are the backward and forward differences of the reinitialisation's
+// Godunov test.
 __device__ __forceinline__ void faces6(const double* __restrict__ f, long long c, long long s,
-                                       const double* __restrict__ dp, int t, double* Q) {
+                                       const double* __restrict__ dp, const double* __restrict__ rp, int t,
+                                       double* Q) {
     double fv[7];
 #pragma unroll
     for (int m = 0; m < 7; ++m) fv[m] = __ldg(f + c + (m - 3) * s);
 #pragma unroll
-    for (int m = 0; m < 6; ++m) Q[m] = (fv[m + 1] - fv[m]) / __ldg(dp + t + m - 3);
+    for (int m = 0; m < 6; ++m) Q[m] = div_rn(fv[m + 1] - fv[m], __ldg(dp + t + m - 3), __ldg(rp + t + m - 3));
 }
 
 // One axis of the reinitialisation right-hand side: the Godunov selection
@@ -223,16 +245,21 @@ __device__ __forceinline__ double reini_L(const KGrid<double>& g, const double* 
     const int ti = i + 5, tj = j + 5, tk = k + 5;
     double dx = 0.0, dy = 0.0, dz = 0.0;
     const double lsv = __ldg(f + c);
-    double lsSig = lsv / sqrt(lsv * lsv);
+    // lsv / sqrt(lsv * lsv): the square root of a correctly rounded square
+    // is |lsv| exactly (binary arithmetic, round to nearest, no overflow), so
+    // the quotient is the sign; the formula itself where the square overflows
+    // (or lsv is NaN)
+    double lsSig = lsv > 0.0 ? 1.0 : -1.0;
+    if (!(fabs(lsv) < 1.0e150)) lsSig = lsv / sqrt(lsv * lsv);
     if (fabs(lsv) < 1.0e-8) lsSig = 1.0;
     double Q[6];
-    faces6(f, c, 1, g.dxp[0], ti, Q);
+    faces6(f, c, 1, g.dxp[0], g.rdxp[0], ti, Q);
     dx = reini_axis(Q, lsSig, g.qf[0], g.cf[0], g.isf[0], ti);
     if (!TWO_D) {
-        faces6(f, c, sy, g.dxp[1], tj, Q);
+        faces6(f, c, sy, g.dxp[1], g.rdxp[1], tj, Q);
         dy = reini_axis(Q, lsSig, g.qf[1], g.cf[1], g.isf[1], tj);
     }
-    faces6(f, c, sz, g.dxp[2], tk, Q);
+    faces6(f, c, sz, g.dxp[2], g.rdxp[2], tk, Q);
     dz = reini_axis(Q, lsSig, g.qf[2], g.cf[2], g.isf[2], tk);
 
     const double dnorm = sqrt(dx * dx + dy * dy + dz * dz);

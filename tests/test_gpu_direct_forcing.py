@@ -5,7 +5,8 @@ golden df* cases against the reference itself run in test_gpu_parity.py;
 here larger cases against the C restatement (pinned bit-exact to the
 reference by test_oracle_golden.py): the operator bit-identical, phi within
 the FP64 tolerance of 1e-12 relative max-norm per step; the FP32 form
-(X45 1..5) within the FP32 tolerance of the FP64 path."""
+within the FP32 tolerance of the FP64 path (X45 6 on its own terms: its
+masked differences are 1e20)."""
 import numpy as np
 import pytest
 
@@ -135,10 +136,42 @@ def test_direct_forcing_fp32_within_tolerance_of_fp64(x45, dims):
         assert relmax(a[m], b[m]) <= 2e-5
 
 
+@pytest.mark.parametrize("dims", [(40, 33, 27), (64, 1, 48)])
+def test_direct_forcing_6_fp32_against_fp64(dims):
+    """X45 6 in the FP32 form, one step from the same state as the FP64 path
+    (src/weno_hj_df_nug.cpp:868-987: a difference whose pair of cells is not
+    all fluid is 1e20).  A stencil holding a masked difference has a weight
+    ~1e-80 relative in FP64 and exactly 0 in FP32: cells with at least one
+    stencil free of them agree within the FP32 tolerance of 2e-5 (relative
+    to their largest value); cells whose three stencils all hold one get the
+    reference's 1e20-scale derivative, computed in FP64 from FP32 operands:
+    the same value to 1 % cell by cell (the later stages difference
+    1e18-scale neighbours stored in FP32, where single-precision rounding of
+    nearly equal values cancels).  One step: the reference's own 1e20-scale
+    values are the masked-difference sentinel, not a level set."""
+    nx, ny, nz = dims
+    xn, yn, zn, phi, (u, v, w) = random_state(nx, ny, nz, seed=nx + 6)
+    b1, b2 = bodies(6, phi.shape, 1.0 / nx, seed=6)
+    m = visible_mask(nx, ny, nz)
+    out = {}
+    for prec in (r3d.FP64, r3d.FP32):
+        with r3d.LevelSet(nx, ny, nz, xn, yn, zn, precision=prec, f43=0.5, f44=0, f45=2.1, n47=0.125) as ls:
+            ls.set_direct_forcing(6)
+            ls.upload(r3d.BODY, body_field(6, b1, b2))
+            for f, a in ((r3d.PHI, phi), (r3d.U, u), (r3d.V, v), (r3d.W, w)):
+                ls.upload(f, a)
+            ls.set_dt(0.25 / nx)
+            ls.step()
+            out[prec] = ls.download(r3d.PHI)[m]
+    a, b = out[r3d.FP32], out[r3d.FP64]
+    assert np.all(np.isfinite(a))
+    huge = np.abs(b) > 1e10
+    assert huge.any() and (~huge).any()
+    assert relmax(a[~huge], b[~huge]) <= 2e-5
+    assert np.max(np.abs(a[huge] - b[huge]) / np.abs(b[huge])) <= 1e-2
+
+
 def test_direct_forcing_refusals():
-    with r3d.LevelSet(16, 16, 16, precision=r3d.FP32) as ls:
-        with pytest.raises(r3d.R3DError):
-            ls.set_direct_forcing(6)  # 1e20 differences overflow FP32: FP64 only
     with r3d.LevelSet(16, 16, 16, precision=r3d.FP64) as ls:
         with pytest.raises(r3d.R3DError):
             ls.download(r3d.BODY)  # not enabled yet
