@@ -66,7 +66,7 @@ size_t footprint(const r3d_grid_desc* d, const Layout& L) {
     size_t b = 7 * (size_t)L.ncell * e;
     size_t tab = 0;
     const int n[3] = {d->nx, d->ny, d->nz};
-    for (int a = 0; a < 3; ++a) tab += 3 * (size_t)(n[a] + 21) + (size_t)(n[a] + 8) * 36;
+    for (int a = 0; a < 3; ++a) tab += 4 * (size_t)(n[a] + 21) + 2 * (size_t)(n[a] + 8) * 36 + 8;
     b += tab * (8 + 4);
     const long long blocks = (long long)((d->nx + 31) / 32) * ((d->ny + 3) / 4 + 4) * (d->nz + 4);
     b += (size_t)(blocks + (long long)d->ny * d->nz + 64) * 16 + 256;
@@ -82,9 +82,6 @@ void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
         const size_t o_dxp = off;
         for (double v : h->M.dxp[a]) host.push_back((T)v);
         off = host.size();
-        const size_t o_rdxp = off;
-        for (double v : h->M.dxp[a]) host.push_back((T)(1.0 / v));
-        off = host.size();
         const size_t o_dxn = off;
         for (double v : h->M.dxn[a]) host.push_back((T)v);
         off = host.size();
@@ -98,11 +95,28 @@ void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
         for (double v : h->M.isf[a]) host.push_back((T)v);
         off = host.size();
         g.dxp[a] = base + o_dxp;
-        g.rdxp[a] = base + o_rdxp;
         g.dxn[a] = base + o_dxn;
         g.qf[a] = base + o_qf;
         g.cf[a] = base + o_cf;
         g.isf[a] = base + o_isf;
+    }
+    // packed forms read by the FP64 stencils, each 16-byte aligned
+    for (int a = 0; a < 3; ++a) {
+        while (host.size() % 4) host.push_back((T)0);
+        g.dpr[a] = base + host.size();
+        for (double v : h->M.dxp[a]) {
+            host.push_back((T)v);
+            host.push_back((T)(1.0 / v));
+        }
+        while (host.size() % 4) host.push_back((T)0);
+        g.wt[a] = base + host.size();
+        const size_t nt = h->M.cf[a].size() / 6;
+        for (size_t t = 0; t < nt; ++t)
+            for (int side = 0; side < 2; ++side) {
+                for (int m = 0; m < 6; ++m) host.push_back((T)h->M.qf[a][t * 12 + side * 6 + m]);
+                for (int m = 0; m < 3; ++m) host.push_back((T)h->M.cf[a][t * 6 + side * 3 + m]);
+                for (int m = 0; m < 9; ++m) host.push_back((T)h->M.isf[a][t * 18 + side * 9 + m]);
+            }
     }
     g.f43 = h->desc.f43;
     g.f49 = h->desc.f49;
@@ -117,7 +131,8 @@ void fill_kgrid(r3d_handle* h, KGrid<T>& g, T* base, std::vector<T>& host) {
 size_t metric_count(const r3d_handle* h) {
     size_t c = 0;
     for (int a = 0; a < 3; ++a)
-        c += 2 * h->M.dxp[a].size() + h->M.dxn[a].size() + h->M.qf[a].size() + h->M.cf[a].size() + h->M.isf[a].size();
+        c += h->M.dxp[a].size() + h->M.dxn[a].size() + h->M.qf[a].size() + h->M.cf[a].size() + h->M.isf[a].size()
+             + 2 * h->M.dxp[a].size() + 6 * h->M.cf[a].size() + 8;  // packed pairs and records, padding
     return c;
 }
 

@@ -12,6 +12,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "batch_internal.h"
@@ -338,7 +339,7 @@ void save_cache(const char* path) {
 std::vector<std::pair<int, int>> tile_candidates() {
     std::vector<std::pair<int, int>> out;
     for (int c = 0; c < tile_cfg_count(); ++c)
-        for (int kc : {8, 16, 32}) out.push_back({c, kc});
+        for (int kc : {6, 7, 8, 10, 12, 16, 32}) out.push_back({c, kc});
     return out;
 }
 
@@ -614,28 +615,53 @@ int r3d_autotune(r3d_handle* h, const char* cache_path, int* cfg_out, int* kc_ou
     const int c0 = h->tile_cfg, k0 = h->kc, cr0 = h->tile_cfg_r, kr0 = h->kc_r;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return R3D_EDEVICE;
-    float best[2] = {1e30f, 1e30f};
-    int bc[2] = {c0, cr0}, bk[2] = {k0, kr0};
     int rc = R3D_OK;
+    // ms per launch of stage 2 of one kind under (cfg, kc); < 0: not tiled
+    auto time_stage = [&](int cfg, int kc, int kind, int reps) -> float {
+        if ((rc = r3d_set_option(h, R3D_OPT_TILE_CFG, cfg)) || (rc = r3d_set_option(h, R3D_OPT_CHUNK, kc)))
+            return -1.f;
+        if ((rc = r3d_get_option(h, R3D_OPT_TILED, &on)) || !on) return -1.f;  // e.g. more items than scratch
+        const int st = kind ? R3D_STAGE_REINIT : R3D_STAGE_CONVECTION;
+        if ((rc = r3d_stage(h, st, 2))) return -1.f;  // warm
+        cudaEventRecord(e0, h->stream);
+        for (int rep = 0; rep < reps && !rc; ++rep) rc = r3d_stage(h, st, 2);
+        cudaEventRecord(e1, h->stream);
+        if (rc || cudaEventSynchronize(e1) != cudaSuccess) {
+            if (!rc) rc = R3D_EDEVICE;
+            return -1.f;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms / reps;
+    };
+    // a sweep of every candidate, then the three fastest of each kind timed
+    // again, longer and interleaved, so that run-to-run noise of a few per
+    // cent does not pick a slower configuration
+    std::vector<std::tuple<float, int, int>> seen[2];
     for (auto [cfg, kc] : tile_candidates()) {
-        if ((rc = r3d_set_option(h, R3D_OPT_TILE_CFG, cfg)) || (rc = r3d_set_option(h, R3D_OPT_CHUNK, kc))) break;
-        if ((rc = r3d_get_option(h, R3D_OPT_TILED, &on))) break;
-        if (!on) continue;  // e.g. more items than the volume scratch holds
         for (int kind = 0; kind < 2 && !rc; ++kind) {
-            const int st = kind ? R3D_STAGE_REINIT : R3D_STAGE_CONVECTION;
-            if ((rc = r3d_stage(h, st, 2))) break;  // warm
-            cudaEventRecord(e0, h->stream);
-            for (int rep = 0; rep < 5 && !rc; ++rep) rc = r3d_stage(h, st, 2);
-            cudaEventRecord(e1, h->stream);
-            if (rc || cudaEventSynchronize(e1) != cudaSuccess) {
-                if (!rc) rc = R3D_EDEVICE;
-                break;
-            }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best[kind]) { best[kind] = ms; bc[kind] = cfg; bk[kind] = kc; }
+            const float ms = time_stage(cfg, kc, kind, 5);
+            if (ms >= 0.f) seen[kind].emplace_back(ms, cfg, kc);
         }
         if (rc) break;
+    }
+    float best[2] = {1e30f, 1e30f};
+    int bc[2] = {c0, cr0}, bk[2] = {k0, kr0};
+    for (int kind = 0; kind < 2 && !rc; ++kind) {
+        std::sort(seen[kind].begin(), seen[kind].end());
+        const size_t top = std::min<size_t>(3, seen[kind].size());
+        std::vector<float> t(top, 1e30f);
+        for (int round = 0; round < 3 && !rc; ++round)
+            for (size_t q = 0; q < top && !rc; ++q) {
+                const float ms = time_stage(std::get<1>(seen[kind][q]), std::get<2>(seen[kind][q]), kind, 10);
+                if (ms >= 0.f) t[q] = std::min(t[q], ms);
+            }
+        for (size_t q = 0; q < top; ++q)
+            if (t[q] < best[kind]) {
+                best[kind] = t[q];
+                bc[kind] = std::get<1>(seen[kind][q]);
+                bk[kind] = std::get<2>(seen[kind][q]);
+            }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

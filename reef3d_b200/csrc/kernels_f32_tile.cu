@@ -26,6 +26,8 @@
 #include "stencil_f32.cuh"
 #include "tile_host.h"
 
+
+
 namespace r3d {
 
 namespace {
@@ -99,29 +101,32 @@ __device__ __forceinline__ float2 sel2(bool cx, bool cy, float2 a, float2 b) {
 // The smoothness indicators are formed at the scale of divided differences
 // (IS coefficients times 1/h^2, so s = IS + psi with the reference's
 // psi = 1e-6 exactly as in src/weno_nug_func.h:133-143), and the nonlinear
-// weights w_r = (c_r/s_r^2) / sum_q (c_q/s_q^2) are evaluated as
-// c_r prod_{q!=r} s_q^2 / sum_q c_q prod_{p!=q} s_p^2 with one reciprocal.
+// weights w_r = (c_r/s_r^2) / sum_q (c_q/s_q^2) are evaluated with one
+// reciprocal as n_r / sum_q n_q, n_r = prod_{q!=r} t_q^2, where
+// t_q = s_q / sqrt(c_q) (the 1/sqrt(c_q) folded into the coefficients of s_q).
 // ih2 = 1/h^2 of the axis.
 __device__ __forceinline__ float2 weno5_2(float2 d1, float2 d2, float2 d3, float2 d4, float2 d5, float ih2) {
     const float2 a1 = sub2(d3, d4), b1 = sub2(d5, d4);
     const float2 b2 = sub2(d2, d3), b3 = sub2(d1, d2);
-    const float2 k43 = f2(ih2 * (4.0f / 3.0f)), k103 = f2(ih2 * (10.0f / 3.0f));
-    const float2 k113 = f2(ih2 * (11.0f / 3.0f)), k53 = f2(ih2 * (5.0f / 3.0f));
-    const float2 psi = f2(1.0e-6f);
-    // s1 = IS1 + psi = (10/3 a1 + 11/3 b1) a1 + 4/3 b1^2 + psi, etc.
-    // (IS2 = (4/3 a1 - 5/3 b2) a1 + 4/3 b2^2, IS3 = (10/3 b2 - 11/3 b3) b2 + 4/3 b3^2)
-    const float2 s1 = fma2(fma2(k103, a1, mul2(k113, b1)), a1, fma2(mul2(k43, b1), b1, psi));
-    const float2 s2 = fma2(fma2(k43, a1, mul2(make_float2(-k53.x, -k53.y), b2)), a1, fma2(mul2(k43, b2), b2, psi));
-    const float2 s3 = fma2(fma2(k103, b2, mul2(make_float2(-k113.x, -k113.y), b3)), b2, fma2(mul2(k43, b3), b3, psi));
-    // s lies in [1e-6, 1e6] (clamped above for fields far from a distance
-    // function): the products below stay inside the FP32 range
-    const float2 c1 = make_float2(fminf(s1.x, 1.0e6f), fminf(s1.y, 1.0e6f));
-    const float2 c2 = make_float2(fminf(s2.x, 1.0e6f), fminf(s2.y, 1.0e6f));
-    const float2 c3 = make_float2(fminf(s3.x, 1.0e6f), fminf(s3.y, 1.0e6f));
+    // s_r scaled by 1/sqrt(c_r) (c = 0.3, 0.6, 0.1): n_r = prod_{q!=r} s_q^2;
+    // s1 = IS1 + psi = (10/3 a1 + 11/3 b1) a1 + 4/3 b1^2 + psi,
+    // IS2 = (4/3 a1 - 5/3 b2) a1 + 4/3 b2^2, IS3 = (10/3 b2 - 11/3 b3) b2 + 4/3 b3^2
+    constexpr float G1 = 1.8257418583505538f, G2 = 1.2909944487358056f, G3 = 3.1622776601683795f;
+    const float2 s1 = fma2(fma2(f2(ih2 * (10.0f / 3.0f * G1)), a1, mul2(f2(ih2 * (11.0f / 3.0f * G1)), b1)), a1,
+                           fma2(mul2(f2(ih2 * (4.0f / 3.0f * G1)), b1), b1, f2(1.0e-6f * G1)));
+    const float2 s2 = fma2(fma2(f2(ih2 * (4.0f / 3.0f * G2)), a1, mul2(f2(ih2 * (-5.0f / 3.0f * G2)), b2)), a1,
+                           fma2(mul2(f2(ih2 * (4.0f / 3.0f * G2)), b2), b2, f2(1.0e-6f * G2)));
+    const float2 s3 = fma2(fma2(f2(ih2 * (10.0f / 3.0f * G3)), b2, mul2(f2(ih2 * (-11.0f / 3.0f * G3)), b3)), b2,
+                           fma2(mul2(f2(ih2 * (4.0f / 3.0f * G3)), b3), b3, f2(1.0e-6f * G3)));
+    // IS + psi clamped at 1e6 (fields far from a distance function): the
+    // products below stay inside the FP32 range
+    const float2 c1 = make_float2(fminf(s1.x, 1.0e6f * G1), fminf(s1.y, 1.0e6f * G1));
+    const float2 c2 = make_float2(fminf(s2.x, 1.0e6f * G2), fminf(s2.y, 1.0e6f * G2));
+    const float2 c3 = make_float2(fminf(s3.x, 1.0e6f * G3), fminf(s3.y, 1.0e6f * G3));
     const float2 q1 = mul2(c1, c1), q2 = mul2(c2, c2), q3 = mul2(c3, c3);
-    const float2 n1 = mul2(mul2(f2(0.3f), q2), q3);
-    const float2 n2 = mul2(mul2(f2(0.6f), q1), q3);
-    const float2 n3 = mul2(mul2(f2(0.1f), q1), q2);
+    const float2 n1 = mul2(q2, q3);
+    const float2 n2 = mul2(q1, q3);
+    const float2 n3 = mul2(q1, q2);
     const float2 inv = rcp2(add2(add2(n1, n2), n3));
     // p1 = d4 + a1/3 - b1/6, p2 = d3 - a1/3 - b2/6, p3 = d2 + b3/3 - 11/6 b2
     const float2 p1 = fma2(f2(-1.0f / 6.0f), b1, fma2(f2(1.0f / 3.0f), a1, d4));

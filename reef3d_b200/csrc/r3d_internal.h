@@ -72,7 +72,12 @@ template <typename T>
 struct KGrid {
     Layout L;
     const T* dxp[3];
-    const T* rdxp[3];  // 1 / DXP, the IEEE quotient (the FP64 face divisions, div_rn)
+    // (DXP, 1/DXP) pairs per index, 1/DXP the IEEE quotient (the FP64 face
+    // divisions, div_rn), 16-byte aligned
+    const T* dpr[3];
+    // the WENO node tables of one (index, side) in one record of 18 values:
+    // Q0..Q5, C0..C2, S0..S8 (record 2t + side), 16-byte aligned
+    const T* wt[3];
     const T* dxn[3];
     const T* qf[3];
     const T* cf[3];

@@ -29,27 +29,32 @@ __device__ __forceinline__ double div_rn(double a, double b, double r) {
 }
 
 // WENO5 derivative from the divided differences q1..q5 of the upwind set,
-// node tables of index t.  Minus side: IS src/weno_nug_func.h:48-60,
-// weights :133-143, reconstruction src/weno_hj_df_nug.cpp:155-159.  Plus
-// side: :61-73, :144-153, :186-190.  epsilon = 0, psi = 1e-6
-// (src/weno_nug_func.cpp:26).
-__device__ __forceinline__ double weno5(const double* __restrict__ Q, const double* __restrict__ C,
-                                        const double* __restrict__ S, bool plus, double q1, double q2,
-                                        double q3, double q4, double q5) {
+// node tables of index t and the side: the record W = wt + 18 (2t + side)
+// holds Q0..Q5, C0..C2, S0..S8 (16-byte aligned: nine 16-byte loads).
+// Minus side: IS src/weno_nug_func.h:48-60, weights :133-143,
+// reconstruction src/weno_hj_df_nug.cpp:155-159.  Plus side: :61-73,
+// :144-153, :186-190.  epsilon = 0, psi = 1e-6 (src/weno_nug_func.cpp:26).
+__device__ __forceinline__ double2 ldg2(const double* p) { return __ldg(reinterpret_cast<const double2*>(p)); }
+
+__device__ __forceinline__ double weno5(const double* __restrict__ W, bool plus, double q1, double q2, double q3,
+                                        double q4, double q5) {
+    const double2 w01 = ldg2(W + 0), w23 = ldg2(W + 2), w45 = ldg2(W + 4), w67 = ldg2(W + 6);
+    const double2 w89 = ldg2(W + 8), wab = ldg2(W + 10), wcd = ldg2(W + 12), wef = ldg2(W + 14);
+    const double2 wgh = ldg2(W + 16);
+    const double S[9] = {w89.y, wab.x, wab.y, wcd.x, wcd.y, wef.x, wef.y, wgh.x, wgh.y};
     const double psi = 1.0e-6, eps = 0.0;
     const double dq12 = q1 - q2, dq23 = q2 - q3, dq32 = q3 - q2;
     const double dq34 = q3 - q4, dq43 = q4 - q3, dq54 = q5 - q4;
-    const double is1 = __ldg(S + 0) * dq54 * dq54 + __ldg(S + 1) * (dq54) * (dq34) + __ldg(S + 2) * dq34 * dq34;
-    const double is2 = __ldg(S + 3) * dq23 * dq23 + __ldg(S + 4) * (dq43) * (dq23) + __ldg(S + 5) * dq43 * dq43;
-    const double is3 = __ldg(S + 6) * dq12 * dq12 + __ldg(S + 7) * (dq32) * (dq12) + __ldg(S + 8) * dq32 * dq32;
+    const double is1 = S[0] * dq54 * dq54 + S[1] * (dq54) * (dq34) + S[2] * dq34 * dq34;
+    const double is2 = S[3] * dq23 * dq23 + S[4] * (dq43) * (dq23) + S[5] * dq43 * dq43;
+    const double is3 = S[6] * dq12 * dq12 + S[7] * (dq32) * (dq12) + S[8] * dq32 * dq32;
     const double a = is1 + psi, b = is2 + psi, c = is3 + psi;
-    const double c0 = __ldg(C + 0), c1 = __ldg(C + 1), c2 = __ldg(C + 2);
+    const double c0 = w67.x, c1 = w67.y, c2 = w89.x;
     const double sum = c0 / (a * a) + c1 / (b * b) + c2 / (c * c);
     const double w1 = c0 / (eps + (a * a) * sum);
     const double w2 = c1 / (eps + (b * b) * sum);
     const double w3 = c2 / (eps + (c * c) * sum);
-    const double Q0 = __ldg(Q + 0), Q1 = __ldg(Q + 1), Q2 = __ldg(Q + 2);
-    const double Q3 = __ldg(Q + 3), Q4 = __ldg(Q + 4), Q5 = __ldg(Q + 5);
+    const double Q0 = w01.x, Q1 = w01.y, Q2 = w23.x, Q3 = w23.y, Q4 = w45.x, Q5 = w45.y;
     // The two sides' reconstructions differ only in which differences enter
     // and in two signs (minus side :155-159, plus side :186-190); selecting
     // those operands keeps every rounding of either side:
@@ -73,23 +78,20 @@ __device__ __forceinline__ double weno5(const double* __restrict__ Q, const doub
 // from the reciprocal table rp of dp.  The side is a runtime value, so a
 // warp whose cells take different sides runs one evaluation, not both.
 __device__ __forceinline__ double deriv(const double* __restrict__ f, long long c, long long s,
-                                        const double* __restrict__ dp, const double* __restrict__ rp,
-                                        const double* __restrict__ qf, const double* __restrict__ cf,
-                                        const double* __restrict__ isf, int t, bool plus) {
+                                        const double* __restrict__ dpr, const double* __restrict__ wt, int t,
+                                        bool plus) {
     const int o = plus ? -2 : -3;
     const double* p = f + c + o * s;
-    const double* d = dp + t + o;
-    const double* rd = rp + t + o;
+    const double* d = dpr + 2 * (t + o);
     const double f0 = __ldg(p), f1 = __ldg(p + s), f2 = __ldg(p + 2 * s);
     const double f3 = __ldg(p + 3 * s), f4 = __ldg(p + 4 * s), f5 = __ldg(p + 5 * s);
-    const double q1 = div_rn(f1 - f0, __ldg(d), __ldg(rd));
-    const double q2 = div_rn(f2 - f1, __ldg(d + 1), __ldg(rd + 1));
-    const double q3 = div_rn(f3 - f2, __ldg(d + 2), __ldg(rd + 2));
-    const double q4 = div_rn(f4 - f3, __ldg(d + 3), __ldg(rd + 3));
-    const double q5 = div_rn(f5 - f4, __ldg(d + 4), __ldg(rd + 4));
-    const int side = plus ? 1 : 0;
-    return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
-                 isf + (long long)t * 18 + side * 9, plus, q1, q2, q3, q4, q5);
+    const double2 e1 = ldg2(d), e2 = ldg2(d + 2), e3 = ldg2(d + 4), e4 = ldg2(d + 6), e5 = ldg2(d + 8);
+    const double q1 = div_rn(f1 - f0, e1.x, e1.y);
+    const double q2 = div_rn(f2 - f1, e2.x, e2.y);
+    const double q3 = div_rn(f3 - f2, e3.x, e3.y);
+    const double q4 = div_rn(f4 - f3, e4.x, e4.y);
+    const double q5 = div_rn(f5 - f4, e5.x, e5.y);
+    return weno5(wt + 18 * (2 * (long long)t + (plus ? 1 : 0)), plus, q1, q2, q3, q4, q5);
 }
 
 // deriv from precomputed face differences: Q[m] = (f_{c+m-2} - f_{c+m-3}) /
@@ -98,12 +100,8 @@ __device__ __forceinline__ double deriv(const double* __restrict__ f, long long 
 // stencil reads faces 0..4, the plus stencil faces 1..5, in the order deriv
 // forms them; each face value is the same IEEE operation whichever cell
 // computes it, so the result is deriv's bit for bit.
-__device__ __forceinline__ double deriv_q(const double* Q, const double* __restrict__ qf,
-                                          const double* __restrict__ cf, const double* __restrict__ isf, int t,
-                                          bool plus) {
-    const int side = plus ? 1 : 0;
-    return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
-                 isf + (long long)t * 18 + side * 9, plus, plus ? Q[1] : Q[0], plus ? Q[2] : Q[1],
+__device__ __forceinline__ double deriv_q(const double* Q, const double* __restrict__ wt, int t, bool plus) {
+    return weno5(wt + 18 * (2 * (long long)t + (plus ? 1 : 0)), plus, plus ? Q[1] : Q[0], plus ? Q[2] : Q[1],
                  plus ? Q[3] : Q[2], plus ? Q[4] : Q[3], plus ? Q[5] : Q[4]);
 }
 
@@ -133,8 +131,7 @@ __device__ __forceinline__ double df_q(int x45, double thr, double fa, double fb
 // deriv with the direct-forcing differences of df_q.
 __device__ __forceinline__ double deriv_df(const double* __restrict__ f, const double* __restrict__ h, long long c,
                                            long long s, const double* __restrict__ dp,
-                                           const double* __restrict__ qf, const double* __restrict__ cf,
-                                           const double* __restrict__ isf, int t, bool plus, int x45, double thr) {
+                                           const double* __restrict__ wt, int t, bool plus, int x45, double thr) {
     const int o = plus ? -2 : -3;
     const long long b0 = c + o * s;
     const double* d = dp + t + o;
@@ -148,9 +145,7 @@ __device__ __forceinline__ double deriv_df(const double* __restrict__ f, const d
 #pragma unroll
     for (int m = 1; m <= 5; ++m)
         q[m - 1] = df_q(x45, thr, fv[m - 1], fv[m], hv[m - 1], hv[m], plus ? hv[m] : hv[m - 1], __ldg(d + m - 1));
-    const int side = plus ? 1 : 0;
-    return weno5(qf + (long long)t * 12 + side * 6, cf + (long long)t * 6 + side * 3,
-                 isf + (long long)t * 18 + side * 9, plus, q[0], q[1], q[2], q[3], q[4]);
+    return weno5(wt + 18 * (2 * (long long)t + (plus ? 1 : 0)), plus, q[0], q[1], q[2], q[3], q[4]);
 }
 
 // -u.grad(f) at interior cell (i,j,k): src/weno_hj_df_nug.cpp:93-111 with the
@@ -168,8 +163,8 @@ __device__ __forceinline__ double conv_L(const KGrid<double>& g, const double* _
     const double iadvec = 0.5 * (vs * __ldg(u + c) + vs * __ldg(u + c - 1));
     const double kadvec = 0.5 * (vs * __ldg(w + c) + vs * __ldg(w + c - sz));
     auto axis = [&](long long s, int a, int t, bool plus) {
-        if (DF) return deriv_df(f, g.body, c, s, g.dxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus, g.x45, g.df_thr);
-        return deriv(f, c, s, g.dxp[a], g.rdxp[a], g.qf[a], g.cf[a], g.isf[a], t, plus);
+        if (DF) return deriv_df(f, g.body, c, s, g.dxp[a], g.wt[a], t, plus, g.x45, g.df_thr);
+        return deriv(f, c, s, g.dpr[a], g.wt[a], t, plus);
     };
     // advec > 0: minus side, < 0: plus side, == 0: no contribution (grad 0)
     double grad = axis(1, 0, i + 5, iadvec < 0.0);
@@ -203,31 +198,32 @@ __device__ __forceinline__ bool same_sign(const double* __restrict__ f, long lon
 
 // The six face divided differences around the cell along one axis (stride
 // s, cell index t = idx + 5): Q[m] = (f[c+(m-2)s] - f[c+(m-3)s]) /
-// DXP[t+m-3] (div_rn with the reciprocal table rp of dp), the layout deriv_q
+// DXP[t+m-3] (div_rn with the (DXP, 1/DXP) pairs dpr), the layout deriv_q
 // reads.  Each is the quotient deriv forms for that face, and faces 2 and 3
 // are the backward and forward differences of the reinitialisation's
 // Godunov test.
 __device__ __forceinline__ void faces6(const double* __restrict__ f, long long c, long long s,
-                                       const double* __restrict__ dp, const double* __restrict__ rp, int t,
-                                       double* Q) {
+                                       const double* __restrict__ dpr, int t, double* Q) {
     double fv[7];
 #pragma unroll
     for (int m = 0; m < 7; ++m) fv[m] = __ldg(f + c + (m - 3) * s);
 #pragma unroll
-    for (int m = 0; m < 6; ++m) Q[m] = div_rn(fv[m + 1] - fv[m], __ldg(dp + t + m - 3), __ldg(rp + t + m - 3));
+    for (int m = 0; m < 6; ++m) {
+        const double2 e = ldg2(dpr + 2 * (t + m - 3));
+        Q[m] = div_rn(fv[m + 1] - fv[m], e.x, e.y);
+    }
 }
 
 // One axis of the reinitialisation right-hand side: the Godunov selection
 // of src/reinidisc_f.cpp:70-109 on the backward / forward differences (faces
 // 2, 3), then the one-sided WENO derivative of the selected side from the
 // same faces (src/ddweno_nug_sf.cpp), or 0.
-__device__ __forceinline__ double reini_axis(const double* Q, double lsSig, const double* __restrict__ qf,
-                                             const double* __restrict__ cf, const double* __restrict__ isf, int t) {
+__device__ __forceinline__ double reini_axis(const double* Q, double lsSig, const double* __restrict__ wt, int t) {
     const double xmin = Q[2], xplus = Q[3];
     // minus side if c1, plus side if c2 (the later test wins, as there), else 0
     const bool c1 = xmin * lsSig > 0.0 && xplus * lsSig > -xmin * lsSig;
     const bool c2 = xplus * lsSig < 0.0 && xmin * lsSig < -xplus * lsSig;
-    double d = deriv_q(Q, qf, cf, isf, t, c2);
+    double d = deriv_q(Q, wt, t, c2);
     if (!(c1 || c2)) d = 0.0;
     if (xplus * lsSig > 0.0 && xmin * lsSig < 0.0) d = 0.0;
     return d;
@@ -253,14 +249,14 @@ __device__ __forceinline__ double reini_L(const KGrid<double>& g, const double* 
     if (!(fabs(lsv) < 1.0e150)) lsSig = lsv / sqrt(lsv * lsv);
     if (fabs(lsv) < 1.0e-8) lsSig = 1.0;
     double Q[6];
-    faces6(f, c, 1, g.dxp[0], g.rdxp[0], ti, Q);
-    dx = reini_axis(Q, lsSig, g.qf[0], g.cf[0], g.isf[0], ti);
+    faces6(f, c, 1, g.dpr[0], ti, Q);
+    dx = reini_axis(Q, lsSig, g.wt[0], ti);
     if (!TWO_D) {
-        faces6(f, c, sy, g.dxp[1], g.rdxp[1], tj, Q);
-        dy = reini_axis(Q, lsSig, g.qf[1], g.cf[1], g.isf[1], tj);
+        faces6(f, c, sy, g.dpr[1], tj, Q);
+        dy = reini_axis(Q, lsSig, g.wt[1], tj);
     }
-    faces6(f, c, sz, g.dxp[2], g.rdxp[2], tk, Q);
-    dz = reini_axis(Q, lsSig, g.qf[2], g.cf[2], g.isf[2], tk);
+    faces6(f, c, sz, g.dpr[2], tk, Q);
+    dz = reini_axis(Q, lsSig, g.wt[2], tk);
 
     const double dnorm = sqrt(dx * dx + dy * dy + dz * dz);
     double deltax;
