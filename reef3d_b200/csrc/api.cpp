@@ -486,7 +486,8 @@ int r3d_create(const r3d_grid_desc* desc, r3d_handle** out) {
     launch_set_scalar(h->S.vscale, 1.0, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return bail(R3D_EDEVICE, std::string("initialisation: ") + cudaGetErrorString(e));
-    if (fp32(h) && !h->L.two_d && h->M.uniform) {
+    // the tiled kernels index a field with 32-bit offsets
+    if (fp32(h) && !h->L.two_d && h->M.uniform && h->L.ncell < (1ll << 31)) {
         std::string why;
         const int ids[3] = {R3D_PHI, R3D_WORK1, R3D_WORK2};
         bool ok = true;

@@ -271,6 +271,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     int* s_issued = rel + RING + 1;  // last plane issued
 
     const Layout& L = a.L;
+    const int sy = (int)L.sy, sz = (int)L.sz;
     const int tid = threadIdx.x, lane = tid & 31;
     const int tx = tid % C::TPR, tg = tid / C::TPR;
     const int i0 = bx * C::TX + 2 * tx;
@@ -283,14 +284,14 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     const int plast = k1 + 2;   // last plane staged
     const int rowb = tg * RY;   // box row of the first y-stencil point of the thread's first row
     bool act0[RY], act1[RY], gside[RY], gxlo[RY], gxhi1[RY], gxhi2[RY], gylo[RY], gyhi[RY];
-    long long col[RY];
+    int col[RY];  // 32-bit offsets: the host enables tiles only for fields of < 2^31 cells
     int own[RY];  // the thread's two cells of row r in a box
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
         const int j = jb + r;
         act0[r] = i0 < L.nx && j < L.ny;
         act1[r] = i0 + 1 < L.nx && j < L.ny;
-        col[r] = (long long)(j + L.gy) * L.sy + (i0 + L.gx);
+        col[r] = (j + L.gy) * sy + (i0 + L.gx);
         own[r] = (rowb + r + 3) * BX + 2 * tx + 4;
         // wall ghost layers this thread writes on every plane (x, y faces)
         gxlo[r] = act0[r] && i0 == 0;
@@ -330,13 +331,13 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
 
     const float vs = (float)*a.vscale;
     const float dtc = REINI ? a.dtr : (float)*a.dt;
-    const long long c0 = (long long)(k0 + L.gz) * L.sz;
+    const int c0 = (k0 + L.gz) * sz;
     float2 wprev[RY];
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
         wprev[r] = make_float2(0.f, 0.f);
         if (!REINI && act0[r]) {
-            const float* wp = a.w + c0 + col[r] - L.sz;
+            const float* wp = a.w + c0 + col[r] - sz;
             wprev[r] = act1[r] ? __ldg(reinterpret_cast<const float2*>(wp)) : make_float2(__ldg(wp), 0.f);
         }
     }
@@ -353,22 +354,22 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
         num[r] = 0.f;
     }
     nvm0 = make_float2(0.f, 0.f);
-    auto fetch = [&](long long cz) {
+    auto fetch = [&](int cz) {
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             if (!act0[r]) continue;
-            const long long cc = cz + col[r];
+            const int cc = cz + col[r];
             if (!REINI) {
                 if (act1[r]) {
                     nu[r] = __ldg(reinterpret_cast<const float2*>(a.u + cc));
                     nv[r] = __ldg(reinterpret_cast<const float2*>(a.v + cc));
                     nw[r] = __ldg(reinterpret_cast<const float2*>(a.w + cc));
-                    if (r == 0) nvm0 = __ldg(reinterpret_cast<const float2*>(a.v + cc - L.sy));
+                    if (r == 0) nvm0 = __ldg(reinterpret_cast<const float2*>(a.v + cc - sy));
                 } else {
                     nu[r].x = __ldg(a.u + cc);
                     nv[r].x = __ldg(a.v + cc);
                     nw[r].x = __ldg(a.w + cc);
-                    if (r == 0) nvm0.x = __ldg(a.v + cc - L.sy);
+                    if (r == 0) nvm0.x = __ldg(a.v + cc - sy);
                 }
                 num[r] = __ldg(a.u + cc - 1);
             }
@@ -380,8 +381,8 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
 
     int sb = 0;          // ring slot of position n = k - k0 (plane k-3)
     int ws = 6, wp = 0;  // ring slot and phase parity of position n + 6 (plane k+3)
-    long long cz = c0;
-    for (int k = k0; k < k1; ++k, cz += L.sz) {
+    int cz = c0;
+    for (int k = k0; k < k1; ++k, cz += sz) {
         ok = __all_sync(0xffffffffu, mbar_wait_bounded(bar + ws, (uint32_t)wp, spin));
         if (!ok) *s_abort = 1;
         if (__any_sync(0xffffffffu, *s_abort != 0)) break;
@@ -414,7 +415,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
 #pragma unroll
         for (int r = 0; r < RY; ++r) { fnr[r] = nfn[r]; ucr[r] = nu[r]; vcr[r] = nv[r]; wcr[r] = nw[r]; umr[r] = num[r]; }
         vm0 = nvm0;
-        if (k + 1 < k1) fetch(cz + L.sz);
+        if (k + 1 < k1) fetch(cz + sz);
 
         float2 f0[RY], Lc[RY];
         bool bandx[RY], bandy[RY];
@@ -575,7 +576,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                 if (STAGE == 2) val = fma2(f2(0.75f), fnr[r], mul2(f2(0.25f), sdl));
                 else val = fma2(f2(1.0f / 3.0f), fnr[r], mul2(f2(2.0f / 3.0f), sdl));
             }
-            const long long c = cz + col[r];
+            const int c = cz + col[r];
             if (act1[r]) *reinterpret_cast<float2*>(a.out + c) = val;
             else a.out[c] = val.x;
             // wall ghost copies (src/gc_neumann.cpp:29-54)
@@ -586,16 +587,16 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                 const int nw = act1[r] ? 2 : 1;
                 if (gylo[r])
                     for (int q = 1; q <= 3; ++q)
-                        for (int e = 0; e < nw; ++e) a.out[c - q * L.sy + e] = e ? val.y : val.x;
+                        for (int e = 0; e < nw; ++e) a.out[c - q * sy + e] = e ? val.y : val.x;
                 if (gyhi[r])
                     for (int q = 1; q <= 3; ++q)
-                        for (int e = 0; e < nw; ++e) a.out[c + q * L.sy + e] = e ? val.y : val.x;
+                        for (int e = 0; e < nw; ++e) a.out[c + q * sy + e] = e ? val.y : val.x;
                 if (k == 0 && !(L.io & kHaloZLo))  // a slab face's ghosts come from the neighbour
                     for (int q = 1; q <= 3; ++q)
-                        for (int e = 0; e < nw; ++e) a.out[c - q * L.sz + e] = e ? val.y : val.x;
+                        for (int e = 0; e < nw; ++e) a.out[c - q * sz + e] = e ? val.y : val.x;
                 if (k == L.nz - 1 && !(L.io & kHaloZHi))
                     for (int q = 1; q <= 3; ++q)
-                        for (int e = 0; e < nw; ++e) a.out[c + q * L.sz + e] = e ? val.y : val.x;
+                        for (int e = 0; e < nw; ++e) a.out[c + q * sz + e] = e ? val.y : val.x;
             }
             if (volume) {
                 // smoothed Heaviside in FP64 (src/fluid_update_fsf.cpp:50-71)
