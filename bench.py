@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--tile-cache", default=None,
                     help="autotune cache file: a run reuses the tile configuration an earlier run stored there "
                          "(so that a profiled run launches the same kernels as the timed one)")
+    ap.add_argument("--tile-sweep", action="store_true",
+                    help="launch stage 2 of both kinds once under every tile configuration and z chunk the "
+                         "autotuner tries, then exit (the DRAM traffic of each, for the ncu summary the "
+                         "roofline's traffic is read from)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other workloads (slotted disc, vortex accuracy, wave tank, ensemble, serving)")
     return ap.parse_args()
@@ -464,6 +468,32 @@ def e2e_steps(case, precision, steps, warmup):
     return n ** 3 * steps / el, 3 * nbytes, nbytes, copy_ms, el * 1e3 / steps
 
 
+TILE_CHUNKS = (6, 7, 8, 10, 12, 16, 32)  # the autotuner's z chunks
+
+
+def tile_sweep(args):
+    """One launch of convection and reinitialisation stage 2 per (tile
+    configuration, z chunk), in that order, on the benchmark grid."""
+    import reef3d_b200 as r3d
+    from reef3d_b200 import setups
+    case = setups.vortex3d(args.edge)
+    ls = make_instance(case, r3d.FP32)
+    ls.set_dt(ls.cfl_dt())
+    done = []
+    for cfg in range(len(r3d.tile_configs())):
+        for kc in TILE_CHUNKS:
+            ls.set_option(r3d.OPT_TILE_CFG, cfg)
+            ls.set_option(r3d.OPT_CHUNK, kc)
+            if not ls.get_option(r3d.OPT_TILED):
+                continue
+            ls.stage(r3d.STAGE_CONVECTION, 2)
+            ls.stage(r3d.STAGE_REINIT, 2)
+            done.append([cfg, kc])
+    ls.sync()
+    ls.close()
+    print(json.dumps({"tile_sweep": done, "edge": args.edge}))
+
+
 def run_ours(args):
     import torch
 
@@ -564,6 +594,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args, int(os.environ.get("RANK", "0")))
+        return
+    if args.tile_sweep:
+        tile_sweep(args)
         return
     run_ours(args)
 

@@ -40,10 +40,12 @@ IOFLOW_DEFAULTS = dict(inflow=1, outflow=1, f50=2, b77=1, f56=1.0e20, f60=-1.0e2
                        f64=0, qi=0.0, qo=0.0)
 # iowave flags in refls_set_iowave's argument order: wave theory B92, wave
 # amplitude and period (B93_1, B93_2), depth B94_wdt, generation / beach zone
-# lengths B96_1 / B96_2, still water level F56, ramp B101 / B102
-IOWAVE_KEYS = ("b92", "amp", "period", "depth", "b96_1", "b96_2", "phimean", "b101", "b102")
+# lengths B96_1 / B96_2, still water level F56, ramp B101 / B102, wave maker
+# B98 (2 relaxation zone, 3 Dirichlet, 4 active) and beach B99 (2 relaxation
+# zone, 3-5 active)
+IOWAVE_KEYS = ("b92", "amp", "period", "depth", "b96_1", "b96_2", "phimean", "b101", "b102", "b98", "b99")
 IOWAVE_DEFAULTS = dict(b92=2, amp=0.05, period=1.0, depth=0.5, b96_1=0.5, b96_2=0.5, phimean=0.5, b101=0,
-                       b102=1.0)
+                       b102=1.0, b98=2, b99=2)
 
 
 def padded_shape(nx, ny, nz):
@@ -250,7 +252,7 @@ class RefOracle:
             lib.refls_set_solid_forcing.argtypes = [_I, ctypes.POINTER(ctypes.c_int)]
             lib.refls_set_solid_forcing(cells.size // 4, cells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
         if iowave is not None:
-            lib.refls_set_iowave.argtypes = [_I] + [ctypes.c_double] * 6 + [_I, ctypes.c_double]
+            lib.refls_set_iowave.argtypes = [_I] + [ctypes.c_double] * 6 + [_I, ctypes.c_double, _I, _I]
             w = dict(IOWAVE_DEFAULTS, **iowave)
             lib.refls_set_iowave(*(w[k] for k in IOWAVE_KEYS))
         if ioflow is not None:

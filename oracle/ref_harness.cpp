@@ -87,10 +87,11 @@ struct IoFlags {
     int on = 0, inflow = 0, outflow = 0, f50 = 2, b77 = 1, f64 = 0;
     double f56 = 1.0e20, f60 = -1.0e20, f61 = -1.0e20, f62 = -1.0e20, qi = 0.0, qo = 0.0;
 } G_IO;
-// iowave (B90 = 1) with relaxation-zone wave generation (B98 = 2) and beach
-// (B99 = 2) for the next refls_init; on == 0: no wave generator
+// iowave (B90 = 1) for the next refls_init, wave maker B98 (2: relaxation
+// zone, 3: Dirichlet, 4: active) and beach B99 (2: relaxation zone, 3-5:
+// active); on == 0: no wave generator
 struct WaveFlags {
-    int on = 0, b92 = 2, b101 = 0;
+    int on = 0, b92 = 2, b101 = 0, b98 = 2, b99 = 2;
     double amp = 0.0, period = 0.0, depth = 0.0, b96_1 = 0.0, b96_2 = 0.0, phimean = 0.0, b102 = 1.0;
 } G_IOW;
 iowave* WAVE = nullptr;
@@ -174,13 +175,15 @@ void refls_set_ioflow(int inflow, int outflow, int f50, int b77, double f56, dou
 // Wave generator of the next refls_init: REEF3D's iowave (B90 = 1) with the
 // x-min face as inflow and the x-max face as outflow, wave theory b92 (2:
 // linear waves, src/wave_interface.cpp:60-80) of amplitude amp and period
-// (B93 = 1), water depth (B94 = 1), relaxation-zone generation (B98 = 2)
-// over b96_1 from the x-min face and a relaxation beach (B99 = 2) over b96_2
-// before the x-max face (the default zone lines of src/iowave.cpp:130-170),
-// still water level phimean (F56), ramp B101/B102.
+// (B93 = 1), water depth (B94 = 1), the wave maker b98 (2: relaxation-zone
+// generation over b96_1 from the x-min face; 3 Dirichlet, 4 active) and the
+// beach b99 (2: relaxation zone over b96_2 before the x-max face, the default
+// zone lines of src/iowave.cpp:130-170; 3-5 active absorption), still water
+// level phimean (F56), ramp B101/B102.
 void refls_set_iowave(int b92, double amp, double period, double depth, double b96_1, double b96_2,
-                      double phimean, int b101, double b102) {
+                      double phimean, int b101, double b102, int b98, int b99) {
     G_IOW.on = 1;
+    G_IOW.b98 = b98; G_IOW.b99 = b99;
     G_IOW.b92 = b92; G_IOW.amp = amp; G_IOW.period = period; G_IOW.depth = depth;
     G_IOW.b96_1 = b96_1; G_IOW.b96_2 = b96_2; G_IOW.phimean = phimean; G_IOW.b101 = b101; G_IOW.b102 = b102;
     G_IO.on = 1;
@@ -220,7 +223,7 @@ int refls_init(int nx, int ny, int nz, const double* xn, const double* yn, const
         p->B93 = 1; p->B93_1 = G_IOW.amp; p->B93_2 = G_IOW.period;
         p->B94 = 1; p->B94_wdt = G_IOW.depth;
         p->B96_1 = G_IOW.b96_1; p->B96_2 = G_IOW.b96_2;
-        p->B98 = 2; p->B99 = 2; p->B101 = G_IOW.b101; p->B102 = G_IOW.b102;
+        p->B98 = G_IOW.b98; p->B99 = G_IOW.b99; p->B101 = G_IOW.b101; p->B102 = G_IOW.b102;
         p->F56 = G_IOW.phimean; p->phimean = G_IOW.phimean; p->phiout = G_IOW.phimean;
         p->A10 = 6;
         p->xcoormin = xn[5]; p->xcoormax = xn[5 + nx];

@@ -139,12 +139,16 @@ inline bool ioflow_desc(const lexer* p, int gcv, r3d_ioflow_desc* d, bool* waves
         std::exit(1);
     }
     // the wave generator's level-set hooks on the device: relaxation-zone
-    // generation (B98 = 2) and beach (B99 = 2), faces without flow-file
-    // input (I230 = 0); Dirichlet and active wave makers set the level set
-    // in ways the device does not model
-    if (*waves && ((p->B98 != 0 && p->B98 != 2) || p->B99 > 2 || p->I230 > 0)) {
-        std::cout << "reef3d_b200: of iowave's level-set hooks the device has the relaxation zones (B98 = 2, "
-                     "B99 = 2) only" << std::endl;
+    // generation (B98 = 2) and beach (B99 = 2) in phi_relax, the face copies
+    // of fsfrkin / fsfrkout; faces without flow-file input (I230 = 0).  The
+    // Dirichlet and active wave makers (B98 = 3, 4) and active beaches (B99 =
+    // 3..5) set the velocities at the faces (iowave::inflow,
+    // src/iowave_inflow.cpp:30-52), which reach the device with the host's
+    // u, v, w; of the level set they only read phi, and phi_relax leaves it
+    // alone for them (src/iowave_relax.cpp:346-378)
+    if (*waves && (p->B98 < 0 || p->B98 > 4 || p->B99 < 0 || p->B99 > 5 || p->I230 > 0)) {
+        std::cout << "reef3d_b200: iowave's level-set hooks run on the device for B98 = 0..4, B99 = 0..5 "
+                     "without flow-file input" << std::endl;
         std::exit(1);
     }
     if ((p->B60 < 1 && !*waves) || gcv == 50) return false;

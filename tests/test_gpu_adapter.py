@@ -79,6 +79,10 @@ def _case(name):
         wave = dict(b92=2, amp=0.03, period=0.8, depth=0.5, b96_1=0.25, b96_2=0.25, phimean=0.5)
         if name == "tank_wave3d_ramp":
             wave.update(b101=1, b102=2.0)
+        if name == "tank_wave3d_active":
+            # Dirichlet wave maker and active absorbing beach: iowave sets
+            # the face velocities (host side), the level set has no zones
+            wave.update(b98=3, b99=3)
         return dict(nx=nx, ny=ny, nz=nz, xn=xn, yn=yn, zn=zn, phi=phi, u=u, v=v, w=w, f43=0.5, f44=2, f45=2.1,
                     f49=1, n47=0.25, f46=0, wave=wave)
     # random 3D case on a stretched grid, F49 = 0 (reinidisc_fsf) or picard
@@ -183,7 +187,7 @@ def _run(name, precision=0):
 
 @pytest.mark.parametrize("name", ["vortex3d", "disk2d", "stretched_f49_0", "stretched_picard", "tank_io3d",
                                   "tank_io2d", "stretched_df4", "stretched_df5", "stretched_sf", "tank_wave2d",
-                                  "tank_wave3d_ramp"])
+                                  "tank_wave3d_ramp", "tank_wave3d_active"])
 def test_adapters_match_reference_objects(name):
     from oracle.bindings import AdapterOracle
     if not AdapterOracle.available():
