@@ -5,6 +5,8 @@
 // launch per RK stage over every member, the step replayed from a CUDA
 // graph), FP64 jobs each on its own instance.  Jobs join and leave between
 // steps; a job's result does not depend on which others shared its steps.
+#include <cuda_runtime.h>
+
 #include "reef3d_b200.h"
 
 #include <algorithm>
@@ -41,6 +43,14 @@ struct r3d_server {
     std::vector<long long> active;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     std::string err;
+    // the batch stream's progress at the end of each of the last two polls:
+    // a poll returns once the work of the poll before it is done, so the
+    // host runs at most one poll ahead of the device and jobs that arrive
+    // meanwhile are admitted at the next step, not after a long queue of
+    // steps already issued for the jobs before them
+    cudaEvent_t done_ev[2] = {nullptr, nullptr};
+    int ev_next = 0;
+    bool ev_pending[2] = {false, false};
 
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -157,6 +167,8 @@ int r3d_serve_destroy(r3d_server* s) {
             r3d_destroy(kv.second.h);
         }
     if (s->batch) r3d_batch_destroy(s->batch);
+    for (cudaEvent_t ev : s->done_ev)
+        if (ev) cudaEventDestroy(ev);
     delete s;
     return R3D_OK;
 }
@@ -204,9 +216,27 @@ int r3d_serve_poll(r3d_server* s, int max_steps, int* nfinished) {
     for (long long id : s->active) n = std::min(n, s->jobs[id].steps - s->jobs[id].done_steps);
     if (s->batch) {
         if (int rc = r3d_batch_step(s->batch, n)) return sfail(s, rc, r3d_batch_last_error(s->batch));
+        void* st = nullptr;
+        r3d_batch_stream(s->batch, &st);
+        cudaEvent_t& ev = s->done_ev[s->ev_next];
+        if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            return sfail(s, R3D_EDEVICE, "event creation failed");
+        if (cudaEventRecord(ev, (cudaStream_t)st) != cudaSuccess) return sfail(s, R3D_EDEVICE, "event record failed");
+        s->ev_pending[s->ev_next] = true;
+        s->ev_next ^= 1;
+        // the previous poll's work
+        if (s->ev_pending[s->ev_next]) {
+            if (cudaEventSynchronize(s->done_ev[s->ev_next]) != cudaSuccess)
+                return sfail(s, R3D_EDEVICE, "batch step failed on the device");
+            s->ev_pending[s->ev_next] = false;
+        }
     } else {
         for (long long id : s->active)
             if (int rc = r3d_ls_run(s->jobs[id].h, n, 1)) return sfail(s, rc, r3d_last_error(s->jobs[id].h));
+        // FP64 steps take milliseconds each: wait for this poll's (the
+        // instances run on their own streams)
+        for (long long id : s->active)
+            if (int rc = r3d_sync(s->jobs[id].h)) return sfail(s, rc, r3d_last_error(s->jobs[id].h));
     }
     std::vector<long long> still;
     int fin = 0;

@@ -150,9 +150,11 @@ class TransportServer:
     def serve(self, jobs, realtime=True):
         """Runs the stream to completion.  With realtime, a job is submitted
         at its arrival time on the wall clock (measured from the start of
-        serve) and the runtime advances one step per poll; otherwise all
-        jobs are submitted at once and each poll runs up to the next job
-        completion.  Returns the finished jobs."""
+        serve) and the runtime advances one step per poll (it returns once
+        the previous poll's step is done, so an arrival joins at the next
+        step); without realtime, all jobs are submitted at once and each
+        poll runs up to the next job completion.  Returns the finished
+        jobs."""
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
         out = {}  # server job id -> (job, offset of the server clock)
         t0 = self.clock()
