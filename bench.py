@@ -479,9 +479,6 @@ def e2e_steps(case, precision, steps, warmup):
     return n ** 3 * steps / el, 3 * nbytes, nbytes, copy_ms, el * 1e3 / steps
 
 
-TILE_CHUNKS = (6, 7, 8, 10, 12, 16, 32)  # the autotuner's z chunks
-
-
 def tile_sweep(args):
     """One launch of convection and reinitialisation stage 2 per (tile
     configuration, z chunk), in that order, on the benchmark grid."""
@@ -492,7 +489,7 @@ def tile_sweep(args):
     ls.set_dt(ls.cfl_dt())
     done = []
     for cfg in range(len(r3d.tile_configs())):
-        for kc in TILE_CHUNKS:
+        for kc in r3d.tile_chunks():
             ls.set_option(r3d.OPT_TILE_CFG, cfg)
             ls.set_option(r3d.OPT_CHUNK, kc)
             if not ls.get_option(r3d.OPT_TILED):

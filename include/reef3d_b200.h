@@ -449,6 +449,9 @@ int r3d_get_option(r3d_handle* h, int option, int* value);
  * the shared-memory ring and threads per CTA (R3D_EINVAL for a bad id). */
 int r3d_tile_config_count(void);
 int r3d_tile_config_describe(int cfg, int* tx, int* ty, int* rows_per_thread, int* ring, int* threads);
+/* The z chunks (planes per CTA work item) the autotuners try: writes up to
+ * max of them to out and returns how many there are. */
+int r3d_tile_chunk_candidates(int* out, int max);
 /* Picks the instance's tile configuration and z chunk, for the convection
  * and the reinitialisation stages separately, by timing a stage of each
  * kind under every candidate (the level set is untouched: the timed stages

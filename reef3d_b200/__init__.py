@@ -149,6 +149,7 @@ EXPORTS = {
     "r3d_set_option": ([_H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "r3d_get_option": ([_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_tile_config_count": ([], ctypes.c_int),
+    "r3d_tile_chunk_candidates": ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
     "r3d_tile_config_describe": ([ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 5, ctypes.c_int),
     "r3d_autotune": ([_H, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "r3d_sync": ([_H], ctypes.c_int),
@@ -199,6 +200,15 @@ EXPORTS = {
     "r3d_serve_release": ([_H, ctypes.c_longlong], ctypes.c_int),
     "r3d_serve_batch": ([_H, ctypes.POINTER(_H)], ctypes.c_int),
 }
+
+
+def tile_chunks():
+    """The z chunks the autotuners try (r3d_tile_chunk_candidates)."""
+    lib = load_library()
+    n = lib.r3d_tile_chunk_candidates(None, 0)
+    buf = (ctypes.c_int * n)()
+    lib.r3d_tile_chunk_candidates(buf, n)
+    return list(buf)
 
 
 def tile_configs():

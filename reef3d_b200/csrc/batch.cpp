@@ -335,17 +335,26 @@ void save_cache(const char* path) {
     }
 }
 
-// The (tile configuration, z chunk) candidates of the autotuners.
+// The z chunks and the (tile configuration, z chunk) candidates of the
+// autotuners.
+constexpr int kChunks[] = {6, 7, 8, 10, 12, 16, 32};
+
 std::vector<std::pair<int, int>> tile_candidates() {
     std::vector<std::pair<int, int>> out;
     for (int c = 0; c < tile_cfg_count(); ++c)
-        for (int kc : {6, 7, 8, 10, 12, 16, 32}) out.push_back({c, kc});
+        for (int kc : kChunks) out.push_back({c, kc});
     return out;
 }
 
 }  // namespace
 
 extern "C" {
+
+int r3d_tile_chunk_candidates(int* out, int max) {
+    const int n = (int)(sizeof(kChunks) / sizeof(kChunks[0]));
+    for (int q = 0; q < n && q < max && out; ++q) out[q] = kChunks[q];
+    return n;
+}
 
 const char* r3d_batch_last_error(const r3d_batch* b) { return b ? b->err.c_str() : g_batch_err.c_str(); }
 
