@@ -503,7 +503,13 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                 }
             }
         }
+        bool band_here = false;
         if (REINI && a.f49 != 0 && a.band64) {
+#pragma unroll
+            for (int r = 0; r < RY; ++r) band_here = band_here || (act0[r] && bandx[r]) || (act1[r] && bandy[r]);
+        }
+        // one vote for the plane: most warps hold no band cell in it
+        if (REINI && a.f49 != 0 && a.band64 && __any_sync(0xffffffffu, band_here)) {
             // The warp's band cells of row r (at most 64) are dealt out to
             // its lanes, one FP64 evaluation each, stencils from shared
             // memory; results go back to the owning lanes by shuffles.
