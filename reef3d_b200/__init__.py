@@ -479,7 +479,8 @@ class LevelSet:
         (r3d_read_reef3d_state); returns the header as a dict, with the
         file's other fields under "extra" (dense arrays) when `extra`."""
         info = StateInfo()
-        keep, ptrs = _extra_arrays({n: None for n in STATE_EXTRA} if extra else None, (self.nx, self.ny, self.nz), fill=False)
+        want = {n: None for n in STATE_EXTRA} if extra else None
+        keep, ptrs = _extra_arrays(want, (self.nx, self.ny, self.nz), fill=False)
         _check(_lib.r3d_read_reef3d_state(self.h, os.fsencode(path), ctypes.byref(info), ptrs), self.h)
         out = {n: getattr(info, n) for n, _ in StateInfo._fields_}
         if extra:
