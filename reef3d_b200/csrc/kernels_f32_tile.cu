@@ -238,7 +238,8 @@ struct TileCfg {
     X(2, 64, 16, 2, 10, 2)      \
     X(3, 32, 16, 2, 12, 4)      \
     X(4, 128, 8, 2, 8, 2)       \
-    X(5, 64, 8, 1, 10, 4)
+    X(5, 64, 8, 1, 10, 4)       \
+    X(6, 32, 16, 2, 12, 5)
 
 #define R3D_CFG_TYPE(id, tx, ty, ry, ring, minb) using Cfg##id = TileCfg<tx, ty, ry, ring, minb>;
 R3D_TILE_CFGS(R3D_CFG_TYPE)
