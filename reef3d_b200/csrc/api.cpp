@@ -236,6 +236,8 @@ TileArgs make_tile_args(r3d_handle* h, int stage) {
     for (int d = 0; d < 3; ++d) {
         a.rh[d] = (float)(1.0 / h->M.h[d]);
         a.eps[d] = (float)(1.0 / (h->M.h[d] * h->M.h[d]));
+        const double hb = 1.0 / (double)a.rh[d];
+        a.beps[d] = 1.0e-6 * hb * hb;
         hmin = std::fmin(hmin, h->M.h[d]);
     }
     a.dtr = (float)(h->desc.f43 * hmin);

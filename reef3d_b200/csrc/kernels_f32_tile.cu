@@ -169,10 +169,12 @@ __device__ __forceinline__ double weno5_d(double d1, double d2, double d3, doubl
 // Reinitialisation right-hand side of one cell in FP64 from its FP32
 // stencils (the interface band): Godunov selection, one-sided WENO5 per
 // axis and the smoothed sign of src/reinidisc_f.cpp:58-127 on a uniform
-// grid.  X, Y, Z: the 7-point stencils along x, y, z (centre at [3]).
+// grid.  X, Y, Z: the 7-point stencils along x, y, z (centre at [3]); rh*:
+// the FP32 1/h per axis, eps* = 1e-6 h^2 with h = 1/(double)rh (host-made).
 __device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, const float* Z, float rhx, float rhy,
-                                              float rhz, float deltax) {
+                                              float rhz, double epsx, double epsy, double epsz, float deltax) {
     const float rh[3] = {rhx, rhy, rhz};
+    const double epsd[3] = {epsx, epsy, epsz};
     const double f0 = X[3];
     const double sg = fabs(f0) < 1.0e-8 ? 1.0 : (f0 > 0.0 ? 1.0 : -1.0);
     const float* ax[3] = {X, Y, Z};
@@ -186,8 +188,7 @@ __device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, co
         const double ms = D[2] * sg, ps = D[3] * sg, sum = ms + ps;
         const bool c1 = ms > 0.0 && sum > 0.0, c2 = ps < 0.0 && sum < 0.0;
         if (c1 || c2) {
-            const double h = 1.0 / (double)rh[d];
-            const double eps = 1.0e-6 * h * h;
+            const double eps = epsd[d];
             const double w = c2 ? weno5_d(D[5], D[4], D[3], D[2], D[1], eps)
                                 : weno5_d(D[0], D[1], D[2], D[3], D[4], eps);
             const double gd = w * (double)rh[d];
@@ -199,6 +200,25 @@ __device__ __noinline__ float reini_cell_fp64(const float* X, const float* Y, co
     double S = f0 / sqrt(f0 * f0 + dn * dn * dl * dl);
     if (S != S) S = 1.0;
     return (float)(S - S * dn);  // -(S |grad| - S)
+}
+
+// Position of the n-th (from 0) set bit of m, for n < popc(m): a binary
+// search on the set-bit counts of halves, quarters, ... (always 0..31).
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) {
+        const unsigned low = m & ((1u << w) - 1u);
+        const int c = __popc(low);
+        if (n >= c) {
+            n -= c;
+            m >>= w;
+            pos += w;
+        } else {
+            m = low;
+        }
+    }
+    return pos;
 }
 
 // 3-input minimum / maximum (one instruction on sm_100)
@@ -528,9 +548,7 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                         if (b < total) {
                             const bool isy = b >= cx;
                             // the lane holding the (b or b-cx)-th set bit of the mask
-                            unsigned msk = isy ? my : mx;
-                            for (int q = isy ? b - cx : b; q > 0; --q) msk &= msk - 1u;
-                            const int src = __ffs(msk) - 1;
+                            const int src = nth_set_bit(isy ? my : mx, isy ? b - cx : b);
                             const int st = (tid & ~31) + src;  // the source lane's thread
                             const int sx = 2 * (st % C::TPR) + (isy ? 1 : 0);
                             const int srow = (st / C::TPR) * RY + r;  // its y-stencil base row
@@ -541,7 +559,8 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                                 Y[m] = sl[(srow + m) * BX + sx + 4];
                                 Z[m] = slot[m][(srow + 3) * BX + sx + 4];
                             }
-                            res = reini_cell_fp64(X, Y, Z, a.rh[0], a.rh[1], a.rh[2], a.deltax);
+                            res = reini_cell_fp64(X, Y, Z, a.rh[0], a.rh[1], a.rh[2], a.beps[0], a.beps[1],
+                                                  a.beps[2], a.deltax);
                         }
                         const float rx = __shfl_sync(0xffffffffu, res, (bxi - base) & 31);
                         const float ry = __shfl_sync(0xffffffffu, res, (byi - base) & 31);

@@ -19,7 +19,8 @@ struct TileArgs {
     double* partial;
     int* err;
     float rh[3];
-    float eps[3];  // 1/h^2 per axis
+    float eps[3];    // 1/h^2 per axis
+    double beps[3];  // FP64 interface band: 1e-6 h^2 per axis, h = 1/(double)rh
     float dtr;
     float deltax;
     int f49;
