@@ -48,6 +48,7 @@ struct r3d_batch {
     // tile configuration and z chunk of the tiled members' launches (the
     // batch encodes its own tensor maps of their fields for it)
     int tile_cfg = 0;
+    bool tile_iso = false;  // every tiled member has cubic cells (tile_args_iso)
     int tile_kc = 16;
     bool tuned = false;  // rows/ctas set explicitly or by the autotuner
     bool dirty = true;
@@ -116,6 +117,7 @@ int rebuild(r3d_batch* b) {
     std::vector<TiledMember> tiled(b->n_tiled);
     std::vector<CUtensorMap> maps(3 * (size_t)b->n_tiled);
     b->max_f44 = 0;
+    bool iso = true;
     for (size_t q = 0; q < nm; ++q) {
         r3d_handle* h = order[q];
         desc[q] = describe(h);
@@ -126,6 +128,7 @@ int rebuild(r3d_batch* b) {
             TiledMember& m = tiled[q];
             m.args = make_tile_args(h, 1);
             m.args.kc = b->tile_kc;
+            iso = iso && tile_args_iso(m.args);
             m.phi = static_cast<float*>(h->field[R3D_PHI]);
             m.a1 = static_cast<float*>(h->field[R3D_WORK1]);
             m.a2 = static_cast<float*>(h->field[R3D_WORK2]);
@@ -138,6 +141,7 @@ int rebuild(r3d_batch* b) {
         }
     }
     b->t_tiled = tile0[b->n_tiled];
+    b->tile_iso = iso;
     b->ntiles = tile0[nm];
     if ((size_t)b->n_tiled > b->cap_tiled) {
         if (b->d_tiled) cudaFree(b->d_tiled);
@@ -249,7 +253,7 @@ long long enqueue_stage(r3d_batch* b, bool reini, int s, int q) {
         b,
         [&](cudaStream_t st) {
             return (long long)launch_batch_tile_stage(b->d_tiled, b->d_maps, b->d_tile0, b->n_tiled, b->tile_cfg,
-                                                      reini, s, q, b->d_vol, b->d_work, tiled_grid(b), st);
+                                                      b->tile_iso, reini, s, q, b->d_vol, b->d_work, tiled_grid(b), st);
         },
         [&](cudaStream_t st) { return (long long)launch_batch_stage(cell_launch_of(b), reini ? 0 : 1, s, q, st); });
 }

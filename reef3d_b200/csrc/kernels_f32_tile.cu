@@ -271,6 +271,8 @@ R3D_TILE_CFGS(R3D_CFG_TYPE)
 // item's volume partials (when `volume`) go to partial_out[0..1].  The
 // mbarriers are initialised at the start of the item and invalidated at its
 // end, so a persistent CTA can run items back to back.
+// ISO: the three axes have bitwise-equal spacing constants (cubic cells), so
+// axis 0's are used for all three and held once.
 //
 // Shared memory is a ring of RING plane boxes: the x and y stencils of
 // plane k come from its box, the z stencil from the thread's own column in
@@ -280,7 +282,7 @@ R3D_TILE_CFGS(R3D_CFG_TYPE)
 // release counter), so that warps drift apart where their work differs
 // (interface-band cells in FP64, wall ghosts) instead of meeting at a CTA
 // barrier every plane.
-template <class C, bool REINI, int STAGE>
+template <class C, bool REINI, int STAGE, bool ISO>
 __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArgs& a, int bx, int by, int bz,
                                           bool volume, unsigned char* smem_raw, double* red_a, double* red_b,
                                           double* partial_out) {
@@ -476,8 +478,9 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                 const float2 ka = mul2(h2, add2(wcr[r], wprev[r]));
                 wprev[r] = wcr[r];
                 const float2 gx = mul2(f2(a.rh[0]), deriv2(Dx, ia.x < 0.f, ia.y < 0.f, a.eps[0]));
-                const float2 gy = mul2(f2(a.rh[1]), deriv2(Dy, ja.x < 0.f, ja.y < 0.f, a.eps[1]));
-                const float2 gz = mul2(f2(a.rh[2]), deriv2(Dz, ka.x < 0.f, ka.y < 0.f, a.eps[2]));
+                constexpr int AY = ISO ? 0 : 1, AZ = ISO ? 0 : 2;
+                const float2 gy = mul2(f2(a.rh[AY]), deriv2(Dy, ja.x < 0.f, ja.y < 0.f, a.eps[AY]));
+                const float2 gz = mul2(f2(a.rh[AZ]), deriv2(Dz, ka.x < 0.f, ka.y < 0.f, a.eps[AZ]));
                 Lc[r] = mul2(f2(-1.f), fma2(ka, gz, fma2(ja, gy, mul2(ia, gx))));
             } else {
                 // Godunov selection per axis (src/reinidisc_f.cpp:70-109) on the
@@ -498,7 +501,8 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
                     const float2 sum = add2(ms, ps);
                     const bool c1x = ms.x > 0.f && sum.x > 0.f, c2x = ps.x < 0.f && sum.x < 0.f;
                     const bool c1y = ms.y > 0.f && sum.y > 0.f, c2y = ps.y < 0.f && sum.y < 0.f;
-                    float2 g = mul2(f2(a.rh[d]), deriv2(D, c2x, c2y, a.eps[d]));
+                    const int ad = ISO ? 0 : d;
+                    float2 g = mul2(f2(a.rh[ad]), deriv2(D, c2x, c2y, a.eps[ad]));
                     g.x = (c1x || c2x) ? g.x : 0.f;
                     g.y = (c1y || c2y) ? g.y : 0.f;
                     g2 = fma2(g, g, g2);
@@ -682,12 +686,12 @@ __device__ __forceinline__ bool tile_item(const CUtensorMap* tmap, const TileArg
     return true;
 }
 
-template <class C, bool REINI, int STAGE, bool VOLUME>
+template <class C, bool REINI, int STAGE, bool VOLUME, bool ISO>
 __global__ void __launch_bounds__(C::NT, C::MINB) tile_kernel(const __grid_constant__ CUtensorMap tmap, TileArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_a[C::NW], red_b[C::NW];
     const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    tile_item<C, REINI, STAGE>(&tmap, a, blockIdx.x, blockIdx.y, blockIdx.z, VOLUME, smem_raw, red_a, red_b,
+    tile_item<C, REINI, STAGE, ISO>(&tmap, a, blockIdx.x, blockIdx.y, blockIdx.z, VOLUME, smem_raw, red_a, red_b,
                                a.partial + 2 * b);
 }
 
@@ -698,7 +702,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) tile_kernel(const __grid_const
 // last CTA to leave resets the counter pair work[0..1] for the next launch
 // on the stream.  Reinitialisation pseudo-step q is skipped by members with
 // f44 <= q; the last stage of a member's step adds its volume partials.
-template <class C, bool REINI, int STAGE>
+template <class C, bool REINI, int STAGE, bool ISO>
 __global__ void __launch_bounds__(C::NT, C::MINB) batch_tile_kernel(const TiledMember* __restrict__ members,
                                                                     const CUtensorMap* __restrict__ maps,
                                                                     const long long* __restrict__ tile0, int nm,
@@ -744,7 +748,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) batch_tile_kernel(const TiledM
         // the item's arguments in a thread-local copy: the plane loop reads
         // them across CTA barriers, after which shared memory would be reread
         const TileArgs a = sa;
-        if (!tile_item<C, REINI, STAGE>(maps + 3 * m + (STAGE - 1), a, bx, by, bz, volume, smem_raw, red_a, red_b,
+        if (!tile_item<C, REINI, STAGE, ISO>(maps + 3 * m + (STAGE - 1), a, bx, by, bz, volume, smem_raw, red_a, red_b,
                                         vol_part + 2 * t))
             break;
     }
@@ -830,27 +834,31 @@ bool tile_attr(K kernel, size_t bytes) {
            cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
 }
 
-template <class C>
-bool cfg_prepare() {
-    const size_t b = C::smem();
-    return tile_attr(tile_kernel<C, false, 1, false>, b) && tile_attr(tile_kernel<C, false, 2, false>, b) &&
-           tile_attr(tile_kernel<C, false, 3, false>, b) && tile_attr(tile_kernel<C, false, 1, true>, b) &&
-           tile_attr(tile_kernel<C, false, 2, true>, b) && tile_attr(tile_kernel<C, false, 3, true>, b) &&
-           tile_attr(tile_kernel<C, true, 1, false>, b) && tile_attr(tile_kernel<C, true, 2, false>, b) &&
-           tile_attr(tile_kernel<C, true, 3, false>, b) && tile_attr(tile_kernel<C, true, 1, true>, b) &&
-           tile_attr(tile_kernel<C, true, 2, true>, b) && tile_attr(tile_kernel<C, true, 3, true>, b) &&
-           tile_attr(batch_tile_kernel<C, false, 1>, b) && tile_attr(batch_tile_kernel<C, false, 2>, b) &&
-           tile_attr(batch_tile_kernel<C, false, 3>, b) && tile_attr(batch_tile_kernel<C, true, 1>, b) &&
-           tile_attr(batch_tile_kernel<C, true, 2>, b) && tile_attr(batch_tile_kernel<C, true, 3>, b);
+template <class C, bool ISO>
+bool cfg_prepare_iso(size_t b) {
+    return tile_attr(tile_kernel<C, false, 1, false, ISO>, b) && tile_attr(tile_kernel<C, false, 2, false, ISO>, b) &&
+           tile_attr(tile_kernel<C, false, 3, false, ISO>, b) && tile_attr(tile_kernel<C, false, 1, true, ISO>, b) &&
+           tile_attr(tile_kernel<C, false, 2, true, ISO>, b) && tile_attr(tile_kernel<C, false, 3, true, ISO>, b) &&
+           tile_attr(tile_kernel<C, true, 1, false, ISO>, b) && tile_attr(tile_kernel<C, true, 2, false, ISO>, b) &&
+           tile_attr(tile_kernel<C, true, 3, false, ISO>, b) && tile_attr(tile_kernel<C, true, 1, true, ISO>, b) &&
+           tile_attr(tile_kernel<C, true, 2, true, ISO>, b) && tile_attr(tile_kernel<C, true, 3, true, ISO>, b) &&
+           tile_attr(batch_tile_kernel<C, false, 1, ISO>, b) && tile_attr(batch_tile_kernel<C, false, 2, ISO>, b) &&
+           tile_attr(batch_tile_kernel<C, false, 3, ISO>, b) && tile_attr(batch_tile_kernel<C, true, 1, ISO>, b) &&
+           tile_attr(batch_tile_kernel<C, true, 2, ISO>, b) && tile_attr(batch_tile_kernel<C, true, 3, ISO>, b);
 }
 
 template <class C>
+bool cfg_prepare() {
+    return cfg_prepare_iso<C, false>(C::smem()) && cfg_prepare_iso<C, true>(C::smem());
+}
+
+template <class C, bool ISO>
 void launch_stage_cfg(const CUtensorMap& map, const TileArgs& a, bool reini, int stage, bool volume,
                       cudaStream_t st) {
     const dim3 grid((a.L.nx + C::TX - 1) / C::TX, (a.L.ny + C::TY - 1) / C::TY, (a.L.nz + a.kc - 1) / a.kc);
     const dim3 block(C::NT);
     const size_t sm = C::smem();
-#define R3D_TL(R, S, V) tile_kernel<C, R, S, V><<<grid, block, sm, st>>>(map, a)
+#define R3D_TL(R, S, V) tile_kernel<C, R, S, V, ISO><<<grid, block, sm, st>>>(map, a)
     if (reini) {
         if (stage == 1) { if (volume) R3D_TL(true, 1, true); else R3D_TL(true, 1, false); }
         else if (stage == 2) { if (volume) R3D_TL(true, 2, true); else R3D_TL(true, 2, false); }
@@ -863,13 +871,13 @@ void launch_stage_cfg(const CUtensorMap& map, const TileArgs& a, bool reini, int
 #undef R3D_TL
 }
 
-template <class C>
+template <class C, bool ISO>
 void launch_batch_cfg(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
                       bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
                       cudaStream_t st) {
     const size_t sm = C::smem();
     const dim3 g(grid), block(C::NT);
-#define R3D_BT(R, S) batch_tile_kernel<C, R, S><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part, work)
+#define R3D_BT(R, S) batch_tile_kernel<C, R, S, ISO><<<g, block, sm, st>>>(members, maps, tile0, nm, q, vol_part, work)
     if (reini) {
         if (stage == 1) R3D_BT(true, 1);
         else if (stage == 2) R3D_BT(true, 2);
@@ -937,16 +945,18 @@ long long tile_items_of(const Layout& L, int kc, int cfg) {
 }
 
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
-                            int cfg, bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
-                            cudaStream_t st) {
+                            int cfg, bool iso, bool reini, int stage, int q, double* vol_part, unsigned* work,
+                            unsigned grid, cudaStream_t st) {
     tile_prepare();  // a failure here makes the launch below fail, which the caller reports
+#define R3D_BATCH(C, I) launch_batch_cfg<C, I>(members, maps, tile0, nm, reini, stage, q, vol_part, work, grid, st)
     switch (cfg) {
 #define R3D_CFG_CASE(id, tx, ty, ry, ring, minb) \
-    case id: launch_batch_cfg<Cfg##id>(members, maps, tile0, nm, reini, stage, q, vol_part, work, grid, st); break;
+    case id: if (iso) R3D_BATCH(Cfg##id, true); else R3D_BATCH(Cfg##id, false); break;
         R3D_TILE_CFGS(R3D_CFG_CASE)
 #undef R3D_CFG_CASE
-        default: launch_batch_cfg<Cfg0>(members, maps, tile0, nm, reini, stage, q, vol_part, work, grid, st);
+        default: if (iso) R3D_BATCH(Cfg0, true); else R3D_BATCH(Cfg0, false);
     }
+#undef R3D_BATCH
     return 1;
 }
 
@@ -1008,13 +1018,16 @@ dim3 tile_grid(const Layout& L, int kc, int cfg) {
 int launch_tile_stage(const CUtensorMap& map, const TileArgs& a, int cfg, bool reini, int stage, bool volume,
                       cudaStream_t st) {
     tile_prepare();  // a failure here makes the launch below fail, which the caller reports
+    const bool iso = tile_args_iso(a);
+#define R3D_STAGE(C, I) launch_stage_cfg<C, I>(map, a, reini, stage, volume, st)
     switch (cfg) {
 #define R3D_CFG_CASE(id, tx, ty, ry, ring, minb) \
-    case id: launch_stage_cfg<Cfg##id>(map, a, reini, stage, volume, st); break;
+    case id: if (iso) R3D_STAGE(Cfg##id, true); else R3D_STAGE(Cfg##id, false); break;
         R3D_TILE_CFGS(R3D_CFG_CASE)
 #undef R3D_CFG_CASE
-        default: launch_stage_cfg<Cfg0>(map, a, reini, stage, volume, st);
+        default: if (iso) R3D_STAGE(Cfg0, true); else R3D_STAGE(Cfg0, false);
     }
+#undef R3D_STAGE
     return 1;
 }
 

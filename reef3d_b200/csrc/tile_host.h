@@ -32,6 +32,12 @@ struct TileArgs {
     int kc;
 };
 
+// True when the three axes' spacing constants are bitwise equal (cubic
+// cells): the kernels then hold one set for all axes, with the same results.
+inline bool tile_args_iso(const TileArgs& a) {
+    return a.rh[0] == a.rh[1] && a.rh[1] == a.rh[2] && a.eps[0] == a.eps[1] && a.eps[1] == a.eps[2];
+}
+
 // A member of a batch that runs on the tiled kernels (3D, uniform, FP32).
 struct TiledMember {
     TileArgs args;  // fn, u, v, w, dt, vscale, err, metrics, kc; out set per stage
@@ -60,9 +66,10 @@ long long tile_items_of(const Layout& L, int kc, int cfg);
 // maps were encoded for configuration `cfg`.
 // work: two zero-initialised counters the launch takes items from (it leaves
 // them at zero for the next launch on the same stream).
+// iso: every member's spacing constants satisfy tile_args_iso.
 int launch_batch_tile_stage(const TiledMember* members, const CUtensorMap* maps, const long long* tile0, int nm,
-                            int cfg, bool reini, int stage, int q, double* vol_part, unsigned* work, unsigned grid,
-                            cudaStream_t st);
+                            int cfg, bool iso, bool reini, int stage, int q, double* vol_part, unsigned* work,
+                            unsigned grid, cudaStream_t st);
 // Per-item face maxima of the tiled members (3 doubles per item).
 int launch_batch_tile_vmax(const TiledMember* members, const long long* tile0, int nm, int cfg, double* vmax_part,
                            unsigned grid, cudaStream_t st);
