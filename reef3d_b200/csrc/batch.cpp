@@ -629,15 +629,19 @@ int r3d_autotune(r3d_handle* h, const char* cache_path, int* cfg_out, int* kc_ou
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return R3D_EDEVICE;
     int rc = R3D_OK;
-    // ms per launch of stage 2 of one kind under (cfg, kc); < 0: not tiled
+    // ms per launch of one kind under (cfg, kc), timed over pairs of stage 1
+    // and stage 2 as a step runs them (stage 2 reading the output stage 1
+    // just wrote; the level set itself, which stage 3 writes, is left as it
+    // is); < 0: not tiled
     auto time_stage = [&](int cfg, int kc, int kind, int reps) -> float {
         if ((rc = r3d_set_option(h, R3D_OPT_TILE_CFG, cfg)) || (rc = r3d_set_option(h, R3D_OPT_CHUNK, kc)))
             return -1.f;
         if ((rc = r3d_get_option(h, R3D_OPT_TILED, &on)) || !on) return -1.f;  // e.g. more items than scratch
         const int st = kind ? R3D_STAGE_REINIT : R3D_STAGE_CONVECTION;
-        if ((rc = r3d_stage(h, st, 2))) return -1.f;  // warm
+        if ((rc = r3d_stage(h, st, 1)) || (rc = r3d_stage(h, st, 2))) return -1.f;  // warm
         cudaEventRecord(e0, h->stream);
-        for (int rep = 0; rep < reps && !rc; ++rep) rc = r3d_stage(h, st, 2);
+        for (int rep = 0; rep < reps && !rc; ++rep)
+            if (!(rc = r3d_stage(h, st, 1))) rc = r3d_stage(h, st, 2);
         cudaEventRecord(e1, h->stream);
         if (rc || cudaEventSynchronize(e1) != cudaSuccess) {
             if (!rc) rc = R3D_EDEVICE;
@@ -645,7 +649,7 @@ int r3d_autotune(r3d_handle* h, const char* cache_path, int* cfg_out, int* kc_ou
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        return ms / reps;
+        return ms / (2 * reps);
     };
     // a sweep of every candidate, then the three fastest of each kind timed
     // again, longer and interleaved, so that run-to-run noise of a few per
