@@ -453,9 +453,9 @@ int r3d_tile_config_describe(int cfg, int* tx, int* ty, int* rows_per_thread, in
  * max of them to out and returns how many there are. */
 int r3d_tile_chunk_candidates(int* out, int max);
 /* Picks the instance's tile configuration and z chunk, for the convection
- * and the reinitialisation stages separately, by timing a stage of each
- * kind under every candidate (the level set is untouched: the timed stages
- * write only a stage buffer), and caches the choice per grid size, in
+ * and the reinitialisation stages separately, by timing stages 1 and 2 of
+ * each kind under every candidate (the level set is untouched: those stages
+ * write only the stage buffers), and caches the choice per grid size, in
  * memory and in cache_path (may be NULL; the file r3d_batch_autotune
  * uses).  cfg/chunk receive the convection stages' choice (the
  * reinitialisation stages': R3D_OPT_TILE_CFG_REINIT, R3D_OPT_CHUNK_REINIT).
